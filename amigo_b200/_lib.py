@@ -1,0 +1,117 @@
+"""ctypes binding of libamigo_b200.so (the C ABI in include/amigo_b200.h).
+
+The library is built in-tree by ``python -m amigo_b200.build``.  Importing
+this module never falls back to another implementation: a missing library
+raises immediately.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libamigo_b200.so")
+
+AB_OK = 0
+AB_ERR = {
+    -1: "bad argument",
+    -2: "CUDA runtime error",
+    -3: "not factored",
+    -4: "unsupported option",
+    -5: "non-finite pivot in the factorization",
+    -6: "workspace capacity",
+}
+
+_i = ctypes.c_int
+_d = ctypes.c_double
+_vp = ctypes.c_void_p
+_ip = ctypes.POINTER(ctypes.c_int)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class IpmProblem(ctypes.Structure):
+    _fields_ = [("n", _i), ("np", _i), ("nc", _i), ("pidx", _vp),
+                ("cidx", _vp), ("lbx", _vp), ("ubx", _vp), ("lbh", _vp)]
+
+
+class IpmState(ctypes.Structure):
+    _fields_ = [("xlam", _vp), ("zl", _vp), ("zu", _vp), ("sl", _vp),
+                ("su", _vp)]
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "ab_ldl_create": (_i, [_i, _ip, _ip, _i, _i, _d, _d, _d, ctypes.POINTER(_vp)]),
+    "ab_ldl_analyze": (_i, [_i, _ip, _ip, _i, ctypes.POINTER(_vp)]),
+    "ab_ldl_destroy": (_i, [_vp]),
+    "ab_ldl_symbolic_sizes": (_i, [_vp, _ip, _ip]),
+    "ab_ldl_symbolic_arrays": (_i, [_vp, _ip, _ip, _ip, _ip, _ip, _ip, _ip]),
+    "ab_ldl_factor": (_i, [_vp, _vp, _vp]),
+    "ab_ldl_inertia": (_i, [_vp, _vp, _ip, _ip]),
+    "ab_ldl_solve": (_i, [_vp, _vp, _i, _i, _vp]),
+    "ab_ldl_stats": (_i, [_vp, _vp, _dp, _dp, _ip, _ip, _ip]),
+    "ab_ldl_node_pivots": (_i, [_vp, _vp, _ip, _ip]),
+    "ab_ipm_residual": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
+                             _d, _vp, _vp, _vp, _vp]),
+    "ab_ipm_diagonal": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
+                             _vp, _vp]),
+    "ab_ipm_bound_dual_step": (_i, [ctypes.POINTER(IpmProblem),
+                                    ctypes.POINTER(IpmState), _d, _vp, _vp,
+                                    _vp, _vp]),
+    "ab_ipm_max_step": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
+                             _d, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ab_ipm_apply_step": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
+                               _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                               _vp]),
+    "ab_ipm_reductions": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
+                               _d, _vp, _vp, _vp]),
+    "ab_ipm_barrier_dphi": (_i, [ctypes.POINTER(IpmProblem),
+                                 ctypes.POINTER(IpmState), _d, _vp, _vp, _vp,
+                                 _vp]),
+    "ab_ipm_reset_bound_multipliers": (_i, [ctypes.POINTER(IpmProblem),
+                                            ctypes.POINTER(IpmState), _d, _d,
+                                            _vp, _vp, _vp]),
+    "ab_ipm_affine_start_point": (_i, [ctypes.POINTER(IpmProblem),
+                                       ctypes.POINTER(IpmState), _d, _vp, _vp,
+                                       _vp, _vp, _vp]),
+    "ab_csr_add_diagonal": (_i, [_i, _vp, _vp, _vp, _vp]),
+    "ab_csr_matvec": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
+}
+
+_lib = None
+
+
+def exported_symbols():
+    """Names of every entry point the binding declares."""
+    return sorted(_SIGS)
+
+
+def lib():
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "libamigo_b200.so is not built (run python -m amigo_b200.build); "
+                "there is no fallback implementation")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class AmigoB200Error(RuntimeError):
+    def __init__(self, name, code):
+        super().__init__("%s failed: %s (%d)" % (name, AB_ERR.get(code, "error"), code))
+        self.code = code
+
+
+def check(name, code):
+    if code < 0:
+        raise AmigoB200Error(name, code)
+    return code
+
+
+def call(name, *args):
+    return check(name, getattr(lib(), name)(*args))

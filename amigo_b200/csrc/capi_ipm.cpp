@@ -1,0 +1,143 @@
+// extern "C" entry points for the IPM vector kernels and CSR utilities
+// (include/amigo_b200.h).  The deterministic reductions need a small
+// per-device scratch array for block partials; it is allocated once per
+// device on first use and kept until process exit.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "../../include/amigo_b200.h"
+#include "ipm_internal.h"
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double* g_scratch[kMaxDevices] = {nullptr};
+
+double* device_scratch() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    return nullptr;
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch[dev]) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, (size_t)ab::ipm_scratch_doubles() * sizeof(double)) !=
+        cudaSuccess)
+      return nullptr;
+    g_scratch[dev] = static_cast<double*>(p);
+  }
+  return g_scratch[dev];
+}
+
+bool bad(const ab_ipm_problem* p, const ab_ipm_state* s) {
+  if (!p || !s) return true;
+  if (p->n < 0 || p->np < 0 || p->nc < 0) return true;
+  if (p->np > 0 && (!p->pidx || !p->lbx || !p->ubx || !s->zl || !s->zu ||
+                    !s->sl || !s->su))
+    return true;
+  if (p->nc > 0 && (!p->cidx || !p->lbh)) return true;
+  return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ab_ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
+                    const double* grad, double* res, double* out2,
+                    void* stream) {
+  if (bad(p, s) || !grad || !res) return AB_ERR_ARG;
+  double* scratch = nullptr;
+  if (out2 && !(scratch = device_scratch())) return AB_ERR_CUDA;
+  return ab::ipm_residual(p, s, mu, grad, res, out2, (cudaStream_t)stream,
+                          scratch);
+}
+
+int ab_ipm_diagonal(const ab_ipm_problem* p, const ab_ipm_state* s,
+                    double* diag, void* stream) {
+  if (bad(p, s) || !diag) return AB_ERR_ARG;
+  return ab::ipm_diagonal(p, s, diag, (cudaStream_t)stream);
+}
+
+int ab_ipm_bound_dual_step(const ab_ipm_problem* p, const ab_ipm_state* s,
+                           double mu, const double* px, double* dzl,
+                           double* dzu, void* stream) {
+  if (bad(p, s) || !px || !dzl || !dzu) return AB_ERR_ARG;
+  return ab::ipm_bound_dual_step(p, s, mu, px, dzl, dzu, (cudaStream_t)stream);
+}
+
+int ab_ipm_max_step(const ab_ipm_problem* p, const ab_ipm_state* s,
+                    double tau, const double* px, const double* dzl,
+                    const double* dzu, double* out, int* iout, void* stream) {
+  if (bad(p, s) || !px || !dzl || !dzu || !out || !iout) return AB_ERR_ARG;
+  double* scratch = device_scratch();
+  if (!scratch) return AB_ERR_CUDA;
+  return ab::ipm_max_step(p, s, tau, px, dzl, dzu, out, iout,
+                          (cudaStream_t)stream, scratch);
+}
+
+int ab_ipm_apply_step(const ab_ipm_problem* p, const ab_ipm_state* s,
+                      double ax, double az, const double* dxlam,
+                      const double* dzl, const double* dzu, double* xlam_new,
+                      double* zl_new, double* zu_new, double* sl_new,
+                      double* su_new, void* stream) {
+  if (bad(p, s) || !s->xlam || !dxlam || !dzl || !dzu || !xlam_new ||
+      !zl_new || !zu_new || !sl_new || !su_new)
+    return AB_ERR_ARG;
+  return ab::ipm_apply_step(p, s, ax, az, dxlam, dzl, dzu, xlam_new, zl_new,
+                            zu_new, sl_new, su_new, (cudaStream_t)stream);
+}
+
+int ab_ipm_reductions(const ab_ipm_problem* p, const ab_ipm_state* s,
+                      double mu, const double* grad, double* out,
+                      void* stream) {
+  if (bad(p, s) || !out) return AB_ERR_ARG;
+  double* scratch = device_scratch();
+  if (!scratch) return AB_ERR_CUDA;
+  return ab::ipm_reductions(p, s, mu, grad, out, (cudaStream_t)stream,
+                            scratch);
+}
+
+int ab_ipm_barrier_dphi(const ab_ipm_problem* p, const ab_ipm_state* s,
+                        double mu, const double* grad, const double* px,
+                        double* out, void* stream) {
+  if (bad(p, s) || !grad || !px || !out) return AB_ERR_ARG;
+  double* scratch = device_scratch();
+  if (!scratch) return AB_ERR_CUDA;
+  return ab::ipm_barrier_dphi(p, s, mu, grad, px, out, (cudaStream_t)stream,
+                              scratch);
+}
+
+int ab_ipm_reset_bound_multipliers(const ab_ipm_problem* p,
+                                   const ab_ipm_state* s, double mu,
+                                   double kappa, double* zl_out,
+                                   double* zu_out, void* stream) {
+  if (bad(p, s) || !zl_out || !zu_out) return AB_ERR_ARG;
+  return ab::ipm_reset_bound_multipliers(p, s, mu, kappa, zl_out, zu_out,
+                                         (cudaStream_t)stream);
+}
+
+int ab_ipm_affine_start_point(const ab_ipm_problem* p, const ab_ipm_state* s,
+                              double beta_min, const double* dzl,
+                              const double* dzu, double* zl_out,
+                              double* zu_out, void* stream) {
+  if (bad(p, s) || !dzl || !dzu || !zl_out || !zu_out) return AB_ERR_ARG;
+  return ab::ipm_affine_start_point(p, s, beta_min, dzl, dzu, zl_out, zu_out,
+                                    (cudaStream_t)stream);
+}
+
+int ab_csr_add_diagonal(int n, const int* diag_pos, const double* d,
+                        double* vals, void* stream) {
+  if (n < 0 || (n > 0 && (!diag_pos || !d || !vals))) return AB_ERR_ARG;
+  return ab::csr_add_diagonal(n, diag_pos, d, vals, (cudaStream_t)stream);
+}
+
+int ab_csr_matvec(int n, const int* rowp, const int* cols, const double* vals,
+                  const double* x, double* y, void* stream) {
+  if (n < 0 || (n > 0 && (!rowp || !cols || !vals || !x || !y)))
+    return AB_ERR_ARG;
+  return ab::csr_matvec(n, rowp, cols, vals, x, y, (cudaStream_t)stream);
+}
+
+}  // extern "C"

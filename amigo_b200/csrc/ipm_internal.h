@@ -1,0 +1,50 @@
+// Host launchers of the IPM vector kernels (ipm_kernels.cu).  `scratch` is
+// device memory of at least ipm_scratch_doubles() doubles that holds the
+// per-block partial results of the deterministic reductions.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/amigo_b200.h"
+
+namespace ab {
+
+__device__ void block_sum2(double a, double b, double* partial);
+
+long long ipm_scratch_doubles();
+int ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
+                 const double* grad, double* res, double* out2,
+                 cudaStream_t st, double* scratch);
+int ipm_diagonal(const ab_ipm_problem* p, const ab_ipm_state* s, double* diag,
+                 cudaStream_t st);
+int ipm_bound_dual_step(const ab_ipm_problem* p, const ab_ipm_state* s,
+                        double mu, const double* px, double* dzl, double* dzu,
+                        cudaStream_t st);
+int ipm_max_step(const ab_ipm_problem* p, const ab_ipm_state* s, double tau,
+                 const double* px, const double* dzl, const double* dzu,
+                 double* out, int* iout, cudaStream_t st, double* scratch);
+int ipm_apply_step(const ab_ipm_problem* p, const ab_ipm_state* s, double ax,
+                   double az, const double* dxlam, const double* dzl,
+                   const double* dzu, double* xlam_new, double* zl_new,
+                   double* zu_new, double* sl_new, double* su_new,
+                   cudaStream_t st);
+int ipm_reductions(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
+                   const double* grad, double* out, cudaStream_t st,
+                   double* scratch);
+int ipm_barrier_dphi(const ab_ipm_problem* p, const ab_ipm_state* s,
+                     double mu, const double* grad, const double* px,
+                     double* out, cudaStream_t st, double* scratch);
+int ipm_reset_bound_multipliers(const ab_ipm_problem* p,
+                                const ab_ipm_state* s, double mu,
+                                double kappa, double* zl_out, double* zu_out,
+                                cudaStream_t st);
+int ipm_affine_start_point(const ab_ipm_problem* p, const ab_ipm_state* s,
+                           double beta_min, const double* dzl,
+                           const double* dzu, double* zl_out, double* zu_out,
+                           cudaStream_t st);
+
+int csr_add_diagonal(int n, const int* diag_pos, const double* d,
+                     double* vals, cudaStream_t st);
+int csr_matvec(int n, const int* rowp, const int* cols, const double* vals,
+               const double* x, double* y, cudaStream_t st);
+
+}  // namespace ab

@@ -1,0 +1,499 @@
+// IPM vector kernels (include/interior_point_backend.h on the device).
+//
+// Elementwise kernels evaluate exactly the reference's expressions in the
+// same order; this file is compiled with --fmad=false so no multiply-add is
+// contracted and the results equal the reference's CPU results bit for bit.
+// Reductions are deterministic: a fixed grid writes per-block partials in a
+// fixed order to a scratch array and one block combines them in order.
+// Argmin reductions keep the first index among equal minima, which is what
+// the reference's sequential strict-less-than loop returns.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+
+#include "../../include/amigo_b200.h"
+#include "ipm_internal.h"
+
+namespace ab {
+namespace {
+
+constexpr int RT = 256;          // threads per block
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs: fixed grid for reductions
+
+__device__ __forceinline__ bool finite_bound(double b) { return !isinf(b); }
+
+struct P {
+  int n, np, nc;
+  const int* pidx;
+  const int* cidx;
+  const double* lbx;
+  const double* ubx;
+  const double* lbh;
+};
+struct S {
+  const double* xlam;
+  const double* zl;
+  const double* zu;
+  const double* sl;
+  const double* su;
+};
+P mkP(const ab_ipm_problem* p) {
+  return P{p->n, p->np, p->nc, p->pidx, p->cidx, p->lbx, p->ubx, p->lbh};
+}
+S mkS(const ab_ipm_state* s) { return S{s->xlam, s->zl, s->zu, s->sl, s->su}; }
+
+int grid_for(long long m) {
+  long long g = (m + RT - 1) / RT;
+  if (g < 1) g = 1;
+  if (g > 148 * 16) g = 148 * 16;
+  return (int)g;
+}
+
+// ---------------------------------------------------------------- residual
+// interior_point_backend.h:203-266
+__global__ void k_residual(P p, S s, double mu, const double* grad,
+                           double* res, double* partial) {
+  double dsq = 0.0, psq = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    const int idx = p.pidx[i];
+    const double rhs_stat = grad[idx] - s.zl[i] + s.zu[i];
+    dsq += rhs_stat * rhs_stat;
+    double aug = rhs_stat;
+    if (finite_bound(p.lbx[i])) {
+      const double gap = s.sl[i];
+      aug += (gap * s.zl[i] - mu) / gap;
+    }
+    if (finite_bound(p.ubx[i])) {
+      const double gap = s.su[i];
+      aug -= (gap * s.zu[i] - mu) / gap;
+    }
+    res[idx] = -aug;
+  }
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p.nc; j += stride) {
+    const int idx = p.cidx[j];
+    const double rp = grad[idx] - p.lbh[j];
+    psq += rp * rp;
+    res[idx] = -rp;
+  }
+  if (partial) block_sum2(dsq, psq, partial);
+}
+
+// ---------------------------------------------------------------- diagonal
+// interior_point_backend.h:277-288
+__global__ void k_diagonal(P p, S s, double* diag) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    double sigma = 0.0;
+    if (finite_bound(p.lbx[i])) sigma += s.zl[i] / s.sl[i];
+    if (finite_bound(p.ubx[i])) sigma += s.zu[i] / s.su[i];
+    diag[p.pidx[i]] = sigma;
+  }
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p.nc; j += stride)
+    diag[p.cidx[j]] = 0.0;
+}
+
+// ------------------------------------------------------- bound dual step
+// interior_point_backend.h:303-321
+__global__ void k_bound_dual_step(P p, S s, double mu, const double* px,
+                                  double* dzl, double* dzu) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    const double dx = px[p.pidx[i]];
+    double a = 0.0, b = 0.0;
+    if (finite_bound(p.lbx[i])) {
+      const double gap = s.sl[i];
+      const double rc = gap * s.zl[i] - mu;
+      a = -(rc + s.zl[i] * dx) / gap;
+    }
+    if (finite_bound(p.ubx[i])) {
+      const double gap = s.su[i];
+      const double rc = gap * s.zu[i] - mu;
+      b = -(rc - s.zu[i] * dx) / gap;
+    }
+    dzl[i] = a;
+    dzu[i] = b;
+  }
+}
+
+// ------------------------------------------------------------- max step
+// interior_point_backend.h:329-369.  Candidates are only considered when
+// strictly below the running minimum, starting from 1.0 (the binding's
+// seed), so the result is (min over candidates < 1, first index) or
+// (1, -1).
+__device__ __forceinline__ void amin(double& v, int& i, double v2, int i2) {
+  if (v2 < v || (v2 == v && i2 < i)) {
+    v = v2;
+    i = i2;
+  }
+}
+
+__global__ void k_max_step(P p, S s, double tau, const double* px,
+                           const double* dzl, const double* dzu,
+                           double* pv, int* pi) {
+  double ax = 1.0, az = 1.0;
+  int xo = 0x7fffffff, zo = 0x7fffffff;  // order key: primal position
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    const double dx = px[p.pidx[i]];
+    if (finite_bound(p.lbx[i])) {
+      if (dx < 0.0) {
+        double a = -tau * s.sl[i] / dx;
+        if (a < ax) { ax = a; xo = i; }
+      }
+      if (dzl[i] < 0.0) {
+        double a = -tau * s.zl[i] / dzl[i];
+        if (a < az) { az = a; zo = i; }
+      }
+    }
+    if (finite_bound(p.ubx[i])) {
+      if (dx > 0.0) {
+        double a = tau * s.su[i] / dx;
+        if (a < ax) { ax = a; xo = i; }
+      }
+      if (dzu[i] < 0.0) {
+        double a = -tau * s.zu[i] / dzu[i];
+        if (a < az) { az = a; zo = i; }
+      }
+    }
+  }
+  // Within a thread the loop visits increasing i, so (value, first i) is
+  // kept; across threads merge lexicographically.
+  __shared__ double sv[2][RT / 32];
+  __shared__ int si[2][RT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    double v2 = __shfl_down_sync(0xffffffffu, ax, o);
+    int i2 = __shfl_down_sync(0xffffffffu, xo, o);
+    amin(ax, xo, v2, i2);
+    v2 = __shfl_down_sync(0xffffffffu, az, o);
+    i2 = __shfl_down_sync(0xffffffffu, zo, o);
+    amin(az, zo, v2, i2);
+  }
+  if (lane == 0) {
+    sv[0][warp] = ax; si[0][warp] = xo;
+    sv[1][warp] = az; si[1][warp] = zo;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < RT / 32; w++) {
+      amin(sv[0][0], si[0][0], sv[0][w], si[0][w]);
+      amin(sv[1][0], si[1][0], sv[1][w], si[1][w]);
+    }
+    pv[2 * blockIdx.x] = sv[0][0];
+    pv[2 * blockIdx.x + 1] = sv[1][0];
+    pi[2 * blockIdx.x] = si[0][0];
+    pi[2 * blockIdx.x + 1] = si[1][0];
+  }
+}
+
+__global__ void k_max_step_final(int nblocks, const int* pidx,
+                                 const double* pv, const int* pi,
+                                 double* out, int* iout) {
+  if (threadIdx.x != 0) return;
+  double ax = 1.0, az = 1.0;
+  int xo = 0x7fffffff, zo = 0x7fffffff;
+  for (int b = 0; b < nblocks; b++) {
+    amin(ax, xo, pv[2 * b], pi[2 * b]);
+    amin(az, zo, pv[2 * b + 1], pi[2 * b + 1]);
+  }
+  out[0] = ax;
+  out[1] = az;
+  iout[0] = xo == 0x7fffffff ? -1 : pidx[xo];
+  iout[1] = zo == 0x7fffffff ? -1 : pidx[zo];
+}
+
+// ------------------------------------------------------------ apply step
+// interior_point_backend.h:376-392
+__global__ void k_apply_step(P p, S s, double ax, double az,
+                             const double* dxlam, const double* dzl,
+                             const double* dzu, double* xlam_new,
+                             double* zl_new, double* zu_new, double* sl_new,
+                             double* su_new) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride)
+    xlam_new[i] = s.xlam[i] + ax * dxlam[i];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    const bool hl = finite_bound(p.lbx[i]), hu = finite_bound(p.ubx[i]);
+    if (hl) zl_new[i] = s.zl[i] + az * dzl[i];
+    if (hu) zu_new[i] = s.zu[i] + az * dzu[i];
+    const double dx = ax * dxlam[p.pidx[i]];
+    if (hl) sl_new[i] = s.sl[i] + dx;
+    if (hu) su_new[i] = s.su[i] - dx;
+  }
+}
+
+// ------------------------------------------------------------ reductions
+// Ten quantities per block (see ab_ipm_reductions in amigo_b200.h).
+constexpr int NQ = 10;
+__global__ void k_reductions(P p, S s, double mu, const double* grad,
+                             double* partial) {
+  double q[NQ];
+  q[0] = 0.0;                 // sum of complementarity products
+  q[1] = 0.0;                 // count
+  q[2] = INFINITY;            // min product
+  q[3] = 0.0;                 // dual inf-norm
+  q[4] = 0.0;                 // primal inf-norm
+  q[5] = 0.0;                 // comp inf-norm (|gap z - mu|)
+  q[6] = 0.0;                 // barrier log-sum
+  q[7] = 0.0;                 // constraint violation 1-norm
+  q[8] = 0.0;                 // max comp deviation
+  q[9] = 0.0;                 // sum of squared (gap z - mu)
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    if (grad) {
+      const int idx = p.pidx[i];
+      q[3] = fmax(q[3], fabs(grad[idx] - s.zl[i] + s.zu[i]));
+    }
+    if (finite_bound(p.lbx[i])) {
+      const double c = s.sl[i] * s.zl[i];
+      q[0] += c;
+      q[1] += 1.0;
+      q[2] = fmin(q[2], c);
+      const double dev = fabs(c - mu);
+      q[5] = fmax(q[5], dev);
+      q[8] = fmax(q[8], dev);
+      q[9] += (c - mu) * (c - mu);
+      const double g = s.sl[i];
+      if (g > 0) q[6] -= mu * log(g);
+    }
+    if (finite_bound(p.ubx[i])) {
+      const double c = s.su[i] * s.zu[i];
+      q[0] += c;
+      q[1] += 1.0;
+      q[2] = fmin(q[2], c);
+      const double dev = fabs(c - mu);
+      q[5] = fmax(q[5], dev);
+      q[8] = fmax(q[8], dev);
+      q[9] += (c - mu) * (c - mu);
+      const double g = s.su[i];
+      if (g > 0) q[6] -= mu * log(g);
+    }
+  }
+  if (grad) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p.nc; j += stride) {
+      const double r = fabs(grad[p.cidx[j]] - p.lbh[j]);
+      q[4] = fmax(q[4], r);
+      q[7] += r;
+    }
+  }
+  __shared__ double sh[NQ][RT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t < NQ; t++) {
+    double v = q[t];
+    for (int o = 16; o > 0; o >>= 1) {
+      double w = __shfl_down_sync(0xffffffffu, v, o);
+      if (t == 2) v = fmin(v, w);
+      else if (t == 3 || t == 4 || t == 5 || t == 8) v = fmax(v, w);
+      else v += w;
+    }
+    if (lane == 0) sh[t][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NQ) {
+    const int t = threadIdx.x;
+    double v = sh[t][0];
+    for (int w = 1; w < RT / 32; w++) {
+      double x = sh[t][w];
+      if (t == 2) v = fmin(v, x);
+      else if (t == 3 || t == 4 || t == 5 || t == 8) v = fmax(v, x);
+      else v += x;
+    }
+    partial[blockIdx.x * NQ + t] = v;
+  }
+}
+
+__global__ void k_reductions_final(int nblocks, const double* partial,
+                                   double* out) {
+  const int t = threadIdx.x;
+  if (t >= NQ) return;
+  double v = partial[t];
+  for (int b = 1; b < nblocks; b++) {
+    double x = partial[b * NQ + t];
+    if (t == 2) v = fmin(v, x);
+    else if (t == 3 || t == 4 || t == 5 || t == 8) v = fmax(v, x);
+    else v += x;
+  }
+  out[t] = v;
+}
+
+// ------------------------------------------------------------ barrier dphi
+// interior_point_backend.h:491-502
+__global__ void k_barrier_dphi(P p, S s, double mu, const double* grad,
+                               const double* px, double* partial) {
+  double acc = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    const int idx = p.pidx[i];
+    const double dx = px[idx];
+    acc += grad[idx] * dx;
+    if (finite_bound(p.lbx[i])) acc -= mu * dx / s.sl[i];
+    if (finite_bound(p.ubx[i])) acc += mu * dx / s.su[i];
+  }
+  block_sum2(acc, 0.0, partial);
+}
+
+// ----------------------------------------------- multiplier reset / start
+// interior_point_backend.h:508-535
+__global__ void k_reset_bound_multipliers(P p, S s, double mu, double kappa,
+                                          double* zl_out, double* zu_out) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    if (finite_bound(p.lbx[i])) {
+      const double g = s.sl[i];
+      zl_out[i] = fmax(fmin(s.zl[i], kappa * mu / g), mu / (kappa * g));
+    }
+    if (finite_bound(p.ubx[i])) {
+      const double g = s.su[i];
+      zu_out[i] = fmax(fmin(s.zu[i], kappa * mu / g), mu / (kappa * g));
+    }
+  }
+}
+
+__global__ void k_affine_start_point(P p, S s, double beta_min,
+                                     const double* dzl, const double* dzu,
+                                     double* zl_out, double* zu_out) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    if (finite_bound(p.lbx[i])) zl_out[i] = fmax(s.zl[i] + dzl[i], beta_min);
+    if (finite_bound(p.ubx[i])) zu_out[i] = fmax(s.zu[i] + dzu[i], beta_min);
+  }
+}
+
+__global__ void k_sum2_final(int nblocks, const double* partial, double* out) {
+  if (threadIdx.x != 0) return;
+  double a = 0.0, b = 0.0;
+  for (int k = 0; k < nblocks; k++) {
+    a += partial[2 * k];
+    b += partial[2 * k + 1];
+  }
+  out[0] = a;
+  out[1] = b;
+}
+
+__global__ void k_sum1_final(int nblocks, const double* partial, double* out) {
+  if (threadIdx.x != 0) return;
+  double a = 0.0;
+  for (int k = 0; k < nblocks; k++) a += partial[2 * k];
+  out[0] = a;
+}
+
+}  // namespace
+
+// Two-value block sum written to partial[2 * blockIdx.x + {0, 1}].
+__device__ void block_sum2(double a, double b, double* partial) {
+  __shared__ double sa[RT / 32], sb[RT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  if (lane == 0) {
+    sa[warp] = a;
+    sb[warp] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double x = 0.0, y = 0.0;
+    for (int w = 0; w < RT / 32; w++) {
+      x += sa[w];
+      y += sb[w];
+    }
+    partial[2 * blockIdx.x] = x;
+    partial[2 * blockIdx.x + 1] = y;
+  }
+}
+
+int ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
+                 const double* grad, double* res, double* out2,
+                 cudaStream_t st, double* scratch) {
+  P pp = mkP(p);
+  S ss = mkS(s);
+  if (out2) {
+    k_residual<<<kRedBlocks, RT, 0, st>>>(pp, ss, mu, grad, res, scratch);
+    k_sum2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out2);
+  } else {
+    long long m = p->np > p->nc ? p->np : p->nc;
+    k_residual<<<grid_for(m), RT, 0, st>>>(pp, ss, mu, grad, res, nullptr);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_diagonal(const ab_ipm_problem* p, const ab_ipm_state* s, double* diag,
+                 cudaStream_t st) {
+  long long m = p->np > p->nc ? p->np : p->nc;
+  k_diagonal<<<grid_for(m), RT, 0, st>>>(mkP(p), mkS(s), diag);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_bound_dual_step(const ab_ipm_problem* p, const ab_ipm_state* s,
+                        double mu, const double* px, double* dzl, double* dzu,
+                        cudaStream_t st) {
+  k_bound_dual_step<<<grid_for(p->np), RT, 0, st>>>(mkP(p), mkS(s), mu, px,
+                                                     dzl, dzu);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_max_step(const ab_ipm_problem* p, const ab_ipm_state* s, double tau,
+                 const double* px, const double* dzl, const double* dzu,
+                 double* out, int* iout, cudaStream_t st, double* scratch) {
+  double* pv = scratch;
+  int* pi = reinterpret_cast<int*>(scratch + 2 * kRedBlocks);
+  k_max_step<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), tau, px, dzl, dzu, pv,
+                                        pi);
+  k_max_step_final<<<1, 32, 0, st>>>(kRedBlocks, p->pidx, pv, pi, out, iout);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_apply_step(const ab_ipm_problem* p, const ab_ipm_state* s, double ax,
+                   double az, const double* dxlam, const double* dzl,
+                   const double* dzu, double* xlam_new, double* zl_new,
+                   double* zu_new, double* sl_new, double* su_new,
+                   cudaStream_t st) {
+  long long m = p->n > p->np ? p->n : p->np;
+  k_apply_step<<<grid_for(m), RT, 0, st>>>(mkP(p), mkS(s), ax, az, dxlam, dzl,
+                                           dzu, xlam_new, zl_new, zu_new,
+                                           sl_new, su_new);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_reductions(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
+                   const double* grad, double* out, cudaStream_t st,
+                   double* scratch) {
+  k_reductions<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, scratch);
+  k_reductions_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_barrier_dphi(const ab_ipm_problem* p, const ab_ipm_state* s,
+                     double mu, const double* grad, const double* px,
+                     double* out, cudaStream_t st, double* scratch) {
+  k_barrier_dphi<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, px,
+                                            scratch);
+  k_sum1_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_reset_bound_multipliers(const ab_ipm_problem* p,
+                                const ab_ipm_state* s, double mu,
+                                double kappa, double* zl_out, double* zu_out,
+                                cudaStream_t st) {
+  k_reset_bound_multipliers<<<grid_for(p->np), RT, 0, st>>>(
+      mkP(p), mkS(s), mu, kappa, zl_out, zu_out);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_affine_start_point(const ab_ipm_problem* p, const ab_ipm_state* s,
+                           double beta_min, const double* dzl,
+                           const double* dzu, double* zl_out, double* zu_out,
+                           cudaStream_t st) {
+  k_affine_start_point<<<grid_for(p->np), RT, 0, st>>>(
+      mkP(p), mkS(s), beta_min, dzl, dzu, zl_out, zu_out);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+long long ipm_scratch_doubles() { return (long long)kRedBlocks * 10 + 64; }
+
+}  // namespace ab

@@ -1,0 +1,101 @@
+// Internal structures of the multifrontal LDL^T handle.
+//
+// Layout in HBM (device):
+//   * static plan (uploaded once per pattern): per-node sizes, the level
+//     schedule, the CSR-entry -> front-position map for assembling A, and the
+//     child-contribution-row -> parent-front-position map for extend-add;
+//   * per-factorization pools: every front F (f x f, column-major, ld = f)
+//     plus its panel workspace W (f x NB) is carved from one FP64 pool with
+//     an atomic bump pointer, so fronts whose size grows with delayed pivots
+//     need no host round trip; after factorization the first npiv columns of
+//     F hold L (unit lower, D on the diagonal / 2x2 blocks) and the trailing
+//     block F[npiv:, npiv:] holds the contribution passed to the parent;
+//   * an int pool with each front's variable list (pivots first, 2x2 pivots
+//     encoded as -(var+1), then delayed, then contribution rows) followed by
+//     the fully-summed permutation used by the forward solve.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "symbolic.h"
+
+namespace ab {
+
+// Panel width of the blocked in-front factorization.  The panel loop takes
+// columns while kw < kPanel - 1 so that a 2x2 pivot still fits.
+constexpr int kPanel = 32;
+constexpr int kThreads = 256;
+
+// Status bits written by device code.
+enum : int {
+  ST_POOL_F = 1,     // FP64 front pool exhausted
+  ST_POOL_I = 2,     // int pool exhausted
+  ST_NAN = 4,        // non-finite pivot met
+};
+
+struct DevicePlan {
+  int n = 0, nn = 0, nnz = 0, num_levels = 0;
+  // per node
+  int* ns = nullptr;           // node width (static fully-summed count)
+  int* nc = nullptr;           // static contribution rows
+  int* var_ptr = nullptr;      // node_ptr
+  int* vars = nullptr;         // node_to_var
+  int* cptr = nullptr;         // contrib_ptr
+  int* crows = nullptr;        // contrib_rows (original numbering)
+  int* cmap = nullptr;         // contrib row -> parent static index
+  int* kid_ptr = nullptr;      // children_ptr (first nn+1 entries)
+  int* kids = nullptr;         // children
+  int* amap_ptr = nullptr;     // per node range into amap
+  int* amap_pos = nullptr;     // CSR position
+  int* amap_row = nullptr;     // static front row
+  int* amap_col = nullptr;     // front column (< ns)
+  int* level_nodes = nullptr;  // nodes sorted by level
+  // dynamic, per factorization
+  int* f = nullptr;            // front size
+  int* npiv = nullptr;         // pivots eliminated
+  int* ndel = nullptr;         // delayed pivots passed to parent
+  int* ndin = nullptr;         // delayed pivots received from children
+  long long* foff = nullptr;   // offset of F in the FP64 pool
+  long long* ioff = nullptr;   // offset of the var list in the int pool
+  int* inertia = nullptr;      // [npos, nneg]
+  int* status = nullptr;       // ST_* bits
+  unsigned long long* counters = nullptr;  // [F pool top, int pool top]
+  double* fpool = nullptr;
+  int* ipool = nullptr;
+  long long fcap = 0, icap = 0;
+};
+
+struct LdlHandle {
+  int device = 0;
+  double ustab = 0.01, pivot_tol = 1e-14, delay_growth = 2.0;
+  int order = ORDER_AMD;
+  SymbolicTree sym;
+  std::vector<int> level_ptr;     // host copy: level boundaries
+  std::vector<int> level_nodes;   // host copy
+  std::vector<int> h_ns, h_nc;    // host copies of static sizes
+  std::vector<int> level_max_f;   // static max front per level
+  long long f_static_total = 0;   // sum of static (f^2 + f*kPanel)
+  long long i_static_total = 0;
+  DevicePlan d;
+  bool has_plan = false;   // false for analysis-only handles
+  bool factored = false;
+  int last_status = 0;
+  // per-factorization host copies (filled at the end of factor)
+  std::vector<int> h_f, h_npiv, h_ndel;
+  // solve scratch
+  double* ubuf = nullptr;         // update vectors passed up the tree
+  long long ubuf_cap = 0;
+  long long* uoff = nullptr;      // per node offset into ubuf (device)
+  std::vector<long long> h_uoff;
+  int uoff_nrhs = 0;
+};
+
+int build_plan(LdlHandle& h, const int* rowp, const int* cols);
+void free_plan(LdlHandle& h);
+int factor_numeric(LdlHandle& h, const double* d_vals, cudaStream_t s);
+int solve_numeric(LdlHandle& h, double* d_x, int nrhs, int ldx,
+                  cudaStream_t s);
+
+}  // namespace ab

@@ -1,0 +1,311 @@
+"""Device-resident CSRMat / Vector / SparseLDL with amigo's interfaces.
+
+These classes mirror the Python-visible API that amigo's pybind module
+exposes for the same objects (amigo/amigo.cpp:323-402 for CSRMat and
+Vector, 616-694 for SparseLDL), but their numeric data live in HBM as torch
+tensors and every numeric operation runs in libamigo_b200.so.  Host copies
+exist only where amigo's API hands out numpy arrays.
+"""
+import ctypes
+import enum
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+class OrderingType(enum.IntEnum):
+    """Same values as amigo.OrderingType (include/ordering_utils.h:21)."""
+    NESTED_DISSECTION = 0
+    AMD = 1
+    MULTI_COLOR = 2
+    NATURAL = 3
+    # amigo.OrderingType.DEFAULT is AMD when METIS is not available
+    # (amigo/amigo.cpp:301-311).
+    DEFAULT = 1
+
+
+class SolverType(enum.IntEnum):
+    """Same values as amigo.SolverType (amigo/amigo.cpp:611-614)."""
+    LDL = 0
+    CHOLESKY = 1
+
+
+def _device(device=None):
+    if device is None:
+        if not torch.cuda.is_available():
+            raise RuntimeError("amigo_b200 needs a CUDA device")
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device(device)
+
+
+def _stream_ptr(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _iptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class Vector:
+    """amigo.Vector with a host array and a device mirror (HOST_AND_DEVICE).
+
+    ``get_array()`` returns the host numpy array (a view, as amigo's does);
+    ``copy_host_to_device`` / ``copy_device_to_host`` synchronise the two.
+    Kernels read and write ``self.dev``.
+    """
+
+    def __init__(self, size, device=None, dev=None):
+        self.device = _device(device) if dev is None else dev.device
+        self.size = int(size)
+        self.host = np.zeros(self.size)
+        self.dev = (torch.zeros(self.size, dtype=torch.float64, device=self.device)
+                    if dev is None else dev)
+
+    def get_size(self):
+        return self.size
+
+    def get_array(self):
+        return self.host
+
+    def __len__(self):
+        return self.size
+
+    def __getitem__(self, k):
+        return self.host[k]
+
+    def __setitem__(self, k, v):
+        self.host[k] = v
+
+    def copy_host_to_device(self):
+        self.dev.copy_(torch.from_numpy(self.host))
+
+    def copy_device_to_host(self):
+        self.host[:] = self.dev.cpu().numpy()
+
+    def zero(self):
+        self.host[:] = 0.0
+        self.dev.zero_()
+
+
+class CSRMat:
+    """Square symmetric CSR matrix (both triangles stored) with device values.
+
+    Mirrors amigo.CSRMat(nrows, ncols, rowp, cols, vals) and its
+    ``get_nonzero_structure``, ``get_data``, ``copy_data_device_to_host``
+    (amigo/amigo.cpp:323-402).  The device array ``self.vals`` is the
+    authoritative copy; ``get_data()`` returns the host mirror.
+    """
+
+    def __init__(self, nrows, ncols, rowp, cols, vals=None, device=None):
+        self.device = _device(device)
+        self.nrows = int(nrows)
+        self.ncols = int(ncols)
+        self.rowp = np.ascontiguousarray(rowp, dtype=np.int32)
+        self.cols = np.ascontiguousarray(cols, dtype=np.int32)
+        self.nnz = int(self.rowp[-1])
+        self.host_data = np.zeros(self.nnz)
+        if vals is not None:
+            self.host_data[:] = np.asarray(vals, dtype=np.float64)
+        self.vals = torch.from_numpy(self.host_data.copy()).to(self.device)
+        self.d_rowp = torch.from_numpy(self.rowp).to(self.device)
+        self.d_cols = torch.from_numpy(self.cols).to(self.device)
+        diag = np.full(self.nrows, -1, dtype=np.int32)
+        for i in range(self.nrows):
+            row = self.cols[self.rowp[i]:self.rowp[i + 1]]
+            hit = np.nonzero(row == i)[0]
+            if len(hit):
+                diag[i] = self.rowp[i] + hit[0]
+        self.diag = diag
+        self.d_diag = torch.from_numpy(np.maximum(diag, 0)).to(self.device)
+
+    def get_nonzero_structure(self):
+        return self.nrows, self.ncols, self.nnz, self.rowp, self.cols
+
+    def get_data(self):
+        return self.host_data
+
+    def copy_data_device_to_host(self):
+        self.host_data[:] = self.vals.cpu().numpy()
+
+    def copy_data_host_to_device(self):
+        self.vals.copy_(torch.from_numpy(self.host_data))
+
+    def zero(self):
+        self.vals.zero_()
+
+    def add_diagonal(self, diag):
+        """vals[diag_pos[i]] += diag[i] on the device (CSRMat::add_diagonal,
+        include/csr_matrix.h:508-528).  ``diag`` is a device tensor, a Vector
+        or a host array."""
+        if np.any(self.diag < 0):
+            raise ValueError("matrix pattern lacks a diagonal entry")
+        d = diag.dev if isinstance(diag, Vector) else diag
+        if not torch.is_tensor(d):
+            d = torch.as_tensor(np.asarray(d, dtype=np.float64), device=self.device)
+        d = d.to(self.device, torch.float64).contiguous()
+        _lib.call("ab_csr_add_diagonal", self.nrows, self.d_diag.data_ptr(),
+                  d.data_ptr(), self.vals.data_ptr(), _stream_ptr(self.device))
+
+    def mult(self, x, y):
+        """y = K x on the device; x, y are device tensors or Vectors."""
+        xd = x.dev if isinstance(x, Vector) else x
+        yd = y.dev if isinstance(y, Vector) else y
+        _lib.call("ab_csr_matvec", self.nrows, self.d_rowp.data_ptr(),
+                  self.d_cols.data_ptr(), self.vals.data_ptr(), xd.data_ptr(),
+                  yd.data_ptr(), _stream_ptr(self.device))
+
+
+class SparseLDL:
+    """amigo.SparseLDL on the GPU (include/sparse_ldl.h:20).
+
+    ``SparseLDL(mat, solver_type=LDL, ustab=0.01, pivot_tol=1e-14,
+    delay_growth=2.0, order=NATURAL)`` performs the symbolic analysis (host,
+    bit-identical to the reference's) and uploads the device plan;
+    ``factor()`` factors ``mat``'s current device values and returns 0;
+    ``solve(x)`` overwrites x (a Vector, a device tensor, or a float64 numpy
+    array of shape (n,) or (n, nrhs)); ``get_inertia()`` returns
+    (npos, nneg).
+    """
+
+    def __init__(self, mat, solver_type=SolverType.LDL, ustab=0.01,
+                 pivot_tol=1e-14, delay_growth=2.0,
+                 order=OrderingType.NATURAL):
+        if int(solver_type) != int(SolverType.LDL):
+            raise NotImplementedError(
+                "SolverType.CHOLESKY is not provided by amigo_b200")
+        self.mat = mat
+        self.n = mat.nrows
+        self.device = mat.device
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.call("ab_ldl_create", self.n, _iptr(mat.rowp), _iptr(mat.cols),
+                      int(order), int(solver_type), float(ustab),
+                      float(pivot_tol), float(delay_growth), ctypes.byref(h))
+        self._h = h
+        self._factored = False
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().ab_ldl_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def symbolic(self):
+        return symbolic_arrays(self._h)
+
+    def factor(self):
+        with torch.cuda.device(self.device):
+            _lib.call("ab_ldl_factor", self._h, self.mat.vals.data_ptr(),
+                      _stream_ptr(self.device))
+        self._factored = True
+        return 0
+
+    def get_inertia(self):
+        p, q = ctypes.c_int(), ctypes.c_int()
+        _lib.call("ab_ldl_inertia", self._h, _stream_ptr(self.device),
+                  ctypes.byref(p), ctypes.byref(q))
+        return p.value, q.value
+
+    def stats(self):
+        fl, fe = ctypes.c_double(), ctypes.c_double()
+        mf, nd, lv = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.call("ab_ldl_stats", self._h, _stream_ptr(self.device),
+                  ctypes.byref(fl), ctypes.byref(fe), ctypes.byref(mf),
+                  ctypes.byref(nd), ctypes.byref(lv))
+        return dict(flops=fl.value, factor_entries=fe.value, max_front=mf.value,
+                    num_delayed=nd.value, levels=lv.value)
+
+    def node_pivots(self):
+        nn = self.symbolic()["num_nodes"]
+        a = np.zeros(nn, np.int32)
+        b = np.zeros(nn, np.int32)
+        _lib.call("ab_ldl_node_pivots", self._h, _stream_ptr(self.device),
+                  _iptr(a), _iptr(b))
+        return a, b
+
+    def solve_device(self, xd):
+        """Solve in place on a device tensor of shape (n,) or (nrhs, n)
+        (rows contiguous: each right-hand side is one contiguous column of
+        the column-major n x nrhs array)."""
+        if xd.dtype != torch.float64 or not xd.is_cuda or not xd.is_contiguous():
+            raise TypeError("expected a contiguous float64 CUDA tensor")
+        nrhs = 1 if xd.dim() == 1 else xd.shape[0]
+        with torch.cuda.device(self.device):
+            _lib.call("ab_ldl_solve", self._h, xd.data_ptr(), nrhs, self.n,
+                      _stream_ptr(self.device))
+
+    def solve(self, x):
+        if isinstance(x, Vector):
+            self.solve_device(x.dev)
+            return
+        if torch.is_tensor(x):
+            self.solve_device(x)
+            return
+        if isinstance(x, np.ndarray):
+            if x.dtype != np.float64:
+                raise TypeError("NumPy array must have dtype=float64")
+            if x.ndim not in (1, 2):
+                raise TypeError("NumPy array must be 1D or 2D")
+            if not x.flags.writeable:
+                raise TypeError("NumPy array must be writeable")
+            cols = x.reshape(self.n, -1).T if x.ndim == 2 else x[None, :]
+            xd = torch.from_numpy(np.ascontiguousarray(cols)).to(self.device)
+            self.solve_device(xd if x.ndim == 2 else xd[0])
+            out = xd.cpu().numpy()
+            if x.ndim == 1:
+                x[:] = out[0]
+            else:
+                x[:, :] = out.T
+            return
+        raise RuntimeError("Expected either a NumPy array or amigo_b200.Vector")
+
+
+def symbolic_arrays(h):
+    nn, nc = ctypes.c_int(), ctypes.c_int()
+    _lib.call("ab_ldl_symbolic_sizes", h, ctypes.byref(nn), ctypes.byref(nc))
+    nn, nc = nn.value, nc.value
+    cp = ctypes.c_int()
+    out = {}
+    # n is recovered from the node partition
+    arrs = dict(node_ptr=np.zeros(nn + 1, np.int32))
+    _lib.call("ab_ldl_symbolic_arrays", h, _iptr(arrs["node_ptr"]), None, None,
+              None, None, None, None)
+    n = int(arrs["node_ptr"][-1]) if nn > 0 else 0
+    out = dict(
+        node_ptr=arrs["node_ptr"],
+        node_to_var=np.zeros(max(n, 1), np.int32),
+        children_ptr=np.zeros(nn + 2, np.int32),
+        children=np.zeros(max(nn, 1), np.int32),
+        contrib_ptr=np.zeros(nn + 1, np.int32),
+        contrib_rows=np.zeros(max(nc, 1), np.int32),
+        invperm=np.zeros(max(n, 1), np.int32),
+    )
+    _lib.call("ab_ldl_symbolic_arrays", h, *[_iptr(out[k]) for k in (
+        "node_ptr", "node_to_var", "children_ptr", "children", "contrib_ptr",
+        "contrib_rows", "invperm")])
+    out["node_to_var"] = out["node_to_var"][:n]
+    out["invperm"] = out["invperm"][:n]
+    out["children"] = out["children"][:nn]
+    out["contrib_rows"] = out["contrib_rows"][:nc]
+    out["num_nodes"] = nn
+    del cp
+    return out
+
+
+def analyze(n, rowp, cols, order=OrderingType.AMD):
+    """Host-only symbolic analysis (no GPU needed); returns the arrays of
+    ``SparseLDL.symbolic()``."""
+    rowp = np.ascontiguousarray(rowp, dtype=np.int32)
+    cols = np.ascontiguousarray(cols, dtype=np.int32)
+    h = ctypes.c_void_p()
+    _lib.call("ab_ldl_analyze", int(n), _iptr(rowp), _iptr(cols), int(order),
+              ctypes.byref(h))
+    try:
+        return symbolic_arrays(h)
+    finally:
+        _lib.lib().ab_ldl_destroy(h)

@@ -1,0 +1,193 @@
+/*
+ * amigo_b200.h -- C ABI of the B200-native numeric core of amigo's
+ * interior-point iteration.
+ *
+ * Plain C types only: host arrays are passed as pointers + sizes, device
+ * buffers as raw device pointers (for example torch.Tensor.data_ptr()),
+ * CUDA streams as `void*` (a cudaStream_t; NULL = the legacy default stream).
+ * No call frees a caller buffer; handles own their device workspaces.
+ * Every entry point returns an int status: 0 = OK, < 0 = error (see
+ * AB_ERR_*), > 0 = warning.  No C++ exception crosses this boundary.
+ *
+ * Each entry point names the reference interface it replaces (file:line in
+ * smdogroup/amigo).
+ */
+#ifndef AMIGO_B200_H
+#define AMIGO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AB_OK 0
+#define AB_ERR_ARG -1         /* bad argument (null pointer, size, order) */
+#define AB_ERR_CUDA -2        /* a CUDA runtime call failed */
+#define AB_ERR_NOT_FACTORED -3 /* solve/inertia before a successful factor */
+#define AB_ERR_UNSUPPORTED -4 /* option not provided by this library */
+#define AB_ERR_NUMERIC -5     /* NaN/Inf met in the factorization */
+#define AB_ERR_CAPACITY -6    /* workspace could not be grown */
+
+typedef struct ab_ldl* ab_ldl_t;
+
+/* ----------------------------------------------------------------------
+ * Sparse LDL^T (multifrontal, threshold 1x1/2x2 pivoting, exact inertia)
+ * -------------------------------------------------------------------- */
+
+/* Symbolic analysis + device plan.  Replaces the SparseLDL constructor
+ * (include/sparse_ldl.h:65-118; binding amigo/amigo.cpp:616-625).
+ * rowp[n+1], cols[nnz]: host CSR pattern of the full symmetric matrix.
+ * order: 0 NESTED_DISSECTION, 1 AMD, 3 NATURAL (include/ordering_utils.h:21).
+ * solver_type: 0 LDL (1 CHOLESKY is rejected with AB_ERR_UNSUPPORTED).
+ * ustab is clamped to [0, 0.5] and delay_growth to [1, 10] as in the
+ * reference.  The CUDA device current at this call is used for the handle. */
+int ab_ldl_create(int n, const int* rowp, const int* cols, int order,
+                  int solver_type, double ustab, double pivot_tol,
+                  double delay_growth, ab_ldl_t* out);
+int ab_ldl_destroy(ab_ldl_t h);
+
+/* Symbolic analysis only (host; makes no CUDA call).  The handle answers
+ * ab_ldl_symbolic_sizes / ab_ldl_symbolic_arrays and must be released with
+ * ab_ldl_destroy; ab_ldl_factor on it returns AB_ERR_UNSUPPORTED.  Mirrors
+ * SparseLDL::symbolic_analysis (include/sparse_ldl.h:2204-2358). */
+int ab_ldl_analyze(int n, const int* rowp, const int* cols, int order,
+                   ab_ldl_t* out);
+
+/* Sizes and copies of the symbolic arrays, for bit-exact comparison with
+ * the reference's private members node_ptr, node_to_var,
+ * node_children_ptr, node_children, contrib_ptr, contrib_rows, invperm
+ * (include/sparse_ldl.h:3240-3262). */
+int ab_ldl_symbolic_sizes(ab_ldl_t h, int* num_nodes, int* contrib_total);
+int ab_ldl_symbolic_arrays(ab_ldl_t h, int* node_ptr, int* node_to_var,
+                           int* children_ptr, int* children, int* contrib_ptr,
+                           int* contrib_rows, int* invperm);
+
+/* Numeric factorization of device CSR values d_vals[nnz] (FP64) on the
+ * pattern given at create time.  Replaces SparseLDL::factor
+ * (include/sparse_ldl.h:136-151).  Asynchronous on `stream` except when a
+ * workspace must grow, which needs one synchronisation. */
+int ab_ldl_factor(ab_ldl_t h, const double* d_vals, void* stream);
+
+/* Inertia (npos, nneg) of the last factorization; synchronises `stream`.
+ * Replaces SparseLDL::get_inertia (include/sparse_ldl.h:198-206). */
+int ab_ldl_inertia(ab_ldl_t h, void* stream, int* npos, int* nneg);
+
+/* In-place solve L D L^T x = b for nrhs right-hand sides stored column-major
+ * with leading dimension ldx >= n in device memory.  Replaces
+ * SparseLDL::solve (include/sparse_ldl.h:162-190). */
+int ab_ldl_solve(ab_ldl_t h, double* d_x, int nrhs, int ldx, void* stream);
+
+/* Statistics of the last factorization (host values; synchronises).
+ * flops: sum over fronts of p^3/3 + p^2 c + p c^2 with p = pivots, c =
+ * contribution size; factor_entries: sum f*p; max_front; num_delayed:
+ * total delayed pivots; levels: elimination-tree levels. */
+int ab_ldl_stats(ab_ldl_t h, void* stream, double* flops,
+                 double* factor_entries, int* max_front, int* num_delayed,
+                 int* levels);
+
+/* Per-node pivot and delayed-pivot counts of the last factorization
+ * (host arrays of num_nodes ints; synchronises).  Mirrors the
+ * reference's MatrixFactor::get_factor counts (include/sparse_ldl.h:418-445). */
+int ab_ldl_node_pivots(ab_ldl_t h, void* stream, int* num_pivots,
+                       int* num_delayed);
+
+/* ----------------------------------------------------------------------
+ * IPM vector kernels (include/interior_point_backend.h).  All array
+ * arguments are device pointers; index arrays are int32.  The problem
+ * description (ProblemInfo, interior_point_backend.h:55-63):
+ *   np, nc: number of primal / constraint entries
+ *   pidx[np], cidx[nc]: their positions in the n-vector xlam
+ *   lbx[np], ubx[np]: bounds (+-inf allowed), lbh[nc]: constraint targets
+ * The state (State, interior_point_backend.h:67-77):
+ *   xlam[n], zl[np], zu[np], sl[np], su[np]
+ * Scalar results are written to a device array `out` and are ready when
+ * `stream` reaches the end of the call.
+ * -------------------------------------------------------------------- */
+typedef struct ab_ipm_problem {
+  int n, np, nc;
+  const int* pidx;
+  const int* cidx;
+  const double* lbx;
+  const double* ubx;
+  const double* lbh;
+} ab_ipm_problem;
+
+typedef struct ab_ipm_state {
+  const double* xlam;
+  const double* zl;
+  const double* zu;
+  const double* sl;
+  const double* su;
+} ab_ipm_state;
+
+/* compute_residual (interior_point_backend.h:203-229); when out2 != NULL
+ * also the squared dual/primal infeasibilities of
+ * compute_residual_and_infeasibility (:234-266) -> out2[0..1]. */
+int ab_ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
+                    const double* grad, double* res, double* out2,
+                    void* stream);
+/* compute_diagonal (:277-288) */
+int ab_ipm_diagonal(const ab_ipm_problem* p, const ab_ipm_state* s,
+                    double* diag, void* stream);
+/* compute_bound_dual_step (:303-321) */
+int ab_ipm_bound_dual_step(const ab_ipm_problem* p, const ab_ipm_state* s,
+                           double mu, const double* px, double* dzl,
+                           double* dzu, void* stream);
+/* compute_max_step (:329-369), seeded ax = az = 1, xi = zi = -1 as the
+ * binding does (amigo/amigo.cpp:768-775).  out[0] = ax, out[1] = az,
+ * iout[0] = xi, iout[1] = zi.  Ties resolve to the first index in primal
+ * order, which is what the sequential reference loop returns. */
+int ab_ipm_max_step(const ab_ipm_problem* p, const ab_ipm_state* s,
+                    double tau, const double* px, const double* dzl,
+                    const double* dzu, double* out, int* iout, void* stream);
+/* apply_step (:376-392) into new-state arrays */
+int ab_ipm_apply_step(const ab_ipm_problem* p, const ab_ipm_state* s,
+                      double ax, double az, const double* dxlam,
+                      const double* dzl, const double* dzu, double* xlam_new,
+                      double* zl_new, double* zu_new, double* sl_new,
+                      double* su_new, void* stream);
+/* Reductions, written to out[]:
+ *  compute_complementarity (:397-413): out[0] = sum, out[1] = count,
+ *    out[2] = min;
+ *  compute_kkt_error (:450-466): out[3] = dual, out[4] = primal,
+ *    out[5] = comp;
+ *  compute_barrier_log_sum (:471-484): out[6];
+ *  compute_constraint_violation_1norm (:565-573): out[7];
+ *  compute_max_comp_deviation (:417-426): out[8];
+ *  compute_complementarity_sq (:430-443): out[9].
+ * grad may be NULL (then out[3..5] and out[7] are not computed). */
+int ab_ipm_reductions(const ab_ipm_problem* p, const ab_ipm_state* s,
+                      double mu, const double* grad, double* out,
+                      void* stream);
+/* compute_barrier_dphi (:491-502) -> out[0] */
+int ab_ipm_barrier_dphi(const ab_ipm_problem* p, const ab_ipm_state* s,
+                        double mu, const double* grad, const double* px,
+                        double* out, void* stream);
+/* reset_bound_multipliers (:508-522) */
+int ab_ipm_reset_bound_multipliers(const ab_ipm_problem* p,
+                                   const ab_ipm_state* s, double mu,
+                                   double kappa, double* zl_out,
+                                   double* zu_out, void* stream);
+/* compute_affine_start_point (:526-535) */
+int ab_ipm_affine_start_point(const ab_ipm_problem* p, const ab_ipm_state* s,
+                              double beta_min, const double* dzl,
+                              const double* dzu, double* zl_out,
+                              double* zu_out, void* stream);
+
+/* ----------------------------------------------------------------------
+ * KKT matrix utilities (CSR values on the device)
+ * -------------------------------------------------------------------- */
+
+/* vals[diag_pos[i]] += d[i] for i < n.  Replaces CSRMat::add_diagonal
+ * (include/csr_matrix.h:508-528). */
+int ab_csr_add_diagonal(int n, const int* diag_pos, const double* d,
+                        double* vals, void* stream);
+/* y = K x for the symmetric CSR matrix (both triangles stored), nrhs
+ * columns with leading dimension ld.  Used by iterative refinement
+ * (amigo/algorithm/solvers/linear_solver.py:196-200). */
+int ab_csr_matvec(int n, const int* rowp, const int* cols, const double* vals,
+                  const double* x, double* y, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMIGO_B200_H */
