@@ -72,6 +72,12 @@ _SIGS = {
     "ab_ipm_affine_start_point": (_i, [ctypes.POINTER(IpmProblem),
                                        ctypes.POINTER(IpmState), _d, _vp, _vp,
                                        _vp, _vp, _vp]),
+    "ab_ipm_barrier_dphi_kkt": (_i, [ctypes.POINTER(IpmProblem),
+                                     ctypes.POINTER(IpmState), _vp, _vp, _vp,
+                                     _vp, _vp]),
+    "ab_ipm_relax_bounds": (_i, [_i, _vp, _vp, _vp, _vp, _d, _d, _vp]),
+    "ab_ipm_initialize": (_i, [ctypes.POINTER(IpmProblem), _vp, _vp, _vp, _vp,
+                               _vp, _d, _d, _vp]),
     "ab_csr_add_diagonal": (_i, [_i, _vp, _vp, _vp, _vp]),
     "ab_csr_matvec": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
 }

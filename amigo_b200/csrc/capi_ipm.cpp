@@ -127,6 +127,38 @@ int ab_ipm_affine_start_point(const ab_ipm_problem* p, const ab_ipm_state* s,
                                     (cudaStream_t)stream);
 }
 
+int ab_ipm_barrier_dphi_kkt(const ab_ipm_problem* p, const ab_ipm_state* s,
+                            const double* res, const double* px,
+                            const double* diag, double* out, void* stream) {
+  if (bad(p, s) || !res || !px || !diag || !out ||
+      (p->nc > 0 && !s->xlam))
+    return AB_ERR_ARG;
+  double* scratch = device_scratch();
+  if (!scratch) return AB_ERR_CUDA;
+  return ab::ipm_barrier_dphi_kkt(p, s, res, px, diag, out,
+                                  (cudaStream_t)stream, scratch);
+}
+
+int ab_ipm_relax_bounds(int np, const double* lbx, const double* ubx,
+                        double* lbx_out, double* ubx_out, double factor,
+                        double constr_viol_tol, void* stream) {
+  if (np < 0 || (np > 0 && (!lbx || !ubx || !lbx_out || !ubx_out)))
+    return AB_ERR_ARG;
+  return ab::ipm_relax_bounds(np, lbx, ubx, lbx_out, ubx_out, factor,
+                              constr_viol_tol, (cudaStream_t)stream);
+}
+
+int ab_ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
+                      double* zu, double* sl, double* su, double kappa1,
+                      double kappa2, void* stream) {
+  if (!p || p->np < 0 ||
+      (p->np > 0 && (!p->pidx || !p->lbx || !p->ubx || !xlam || !zl || !zu ||
+                     !sl || !su)))
+    return AB_ERR_ARG;
+  return ab::ipm_initialize(p, xlam, zl, zu, sl, su, kappa1, kappa2,
+                            (cudaStream_t)stream);
+}
+
 int ab_csr_add_diagonal(int n, const int* diag_pos, const double* d,
                         double* vals, void* stream) {
   if (n < 0 || (n > 0 && (!diag_pos || !d || !vals))) return AB_ERR_ARG;

@@ -42,6 +42,17 @@ int ipm_affine_start_point(const ab_ipm_problem* p, const ab_ipm_state* s,
                            const double* dzu, double* zl_out, double* zu_out,
                            cudaStream_t st);
 
+int ipm_barrier_dphi_kkt(const ab_ipm_problem* p, const ab_ipm_state* s,
+                         const double* res, const double* px,
+                         const double* diag, double* out, cudaStream_t st,
+                         double* scratch);
+int ipm_relax_bounds(int np, const double* lbx, const double* ubx,
+                     double* lo, double* hi, double factor, double tol,
+                     cudaStream_t st);
+int ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
+                   double* zu, double* sl, double* su, double kappa1,
+                   double kappa2, cudaStream_t st);
+
 int csr_add_diagonal(int n, const int* diag_pos, const double* d,
                      double* vals, cudaStream_t st);
 int csr_matvec(int n, const int* rowp, const int* cols, const double* vals,

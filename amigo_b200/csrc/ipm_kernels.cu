@@ -226,7 +226,7 @@ __global__ void k_apply_step(P p, S s, double ax, double az,
 
 // ------------------------------------------------------------ reductions
 // Ten quantities per block (see ab_ipm_reductions in amigo_b200.h).
-constexpr int NQ = 10;
+constexpr int NQ = 13;
 __global__ void k_reductions(P p, S s, double mu, const double* grad,
                              double* partial) {
   double q[NQ];
@@ -240,11 +240,16 @@ __global__ void k_reductions(P p, S s, double mu, const double* grad,
   q[7] = 0.0;                 // constraint violation 1-norm
   q[8] = 0.0;                 // max comp deviation
   q[9] = 0.0;                 // sum of squared (gap z - mu)
+  q[10] = 0.0;                // dual residual sum of squares
+  q[11] = 0.0;                // primal residual sum of squares
+  q[12] = 0.0;                // sum of squared products gap z
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
     if (grad) {
       const int idx = p.pidx[i];
-      q[3] = fmax(q[3], fabs(grad[idx] - s.zl[i] + s.zu[i]));
+      const double rd = grad[idx] - s.zl[i] + s.zu[i];
+      q[3] = fmax(q[3], fabs(rd));
+      q[10] += rd * rd;
     }
     if (finite_bound(p.lbx[i])) {
       const double c = s.sl[i] * s.zl[i];
@@ -255,6 +260,7 @@ __global__ void k_reductions(P p, S s, double mu, const double* grad,
       q[5] = fmax(q[5], dev);
       q[8] = fmax(q[8], dev);
       q[9] += (c - mu) * (c - mu);
+      q[12] += c * c;
       const double g = s.sl[i];
       if (g > 0) q[6] -= mu * log(g);
     }
@@ -267,15 +273,18 @@ __global__ void k_reductions(P p, S s, double mu, const double* grad,
       q[5] = fmax(q[5], dev);
       q[8] = fmax(q[8], dev);
       q[9] += (c - mu) * (c - mu);
+      q[12] += c * c;
       const double g = s.su[i];
       if (g > 0) q[6] -= mu * log(g);
     }
   }
   if (grad) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p.nc; j += stride) {
-      const double r = fabs(grad[p.cidx[j]] - p.lbh[j]);
+      const double rp = grad[p.cidx[j]] - p.lbh[j];
+      const double r = fabs(rp);
       q[4] = fmax(q[4], r);
       q[7] += r;
+      q[11] += rp * rp;
     }
   }
   __shared__ double sh[NQ][RT / 32];
@@ -359,6 +368,66 @@ __global__ void k_affine_start_point(P p, S s, double beta_min,
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
     if (finite_bound(p.lbx[i])) zl_out[i] = fmax(s.zl[i] + dzl[i], beta_min);
     if (finite_bound(p.ubx[i])) zu_out[i] = fmax(s.zu[i] + dzu[i], beta_min);
+  }
+}
+
+// compute_barrier_dphi_from_kkt (interior_point_backend.h:597-611)
+__global__ void k_barrier_dphi_kkt(P p, S s, const double* res,
+                                   const double* px, const double* diag,
+                                   double* partial) {
+  double acc = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    const int idx = p.pidx[i];
+    acc -= res[idx] * px[idx];
+  }
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p.nc; j += stride) {
+    const int idx = p.cidx[j];
+    const double lam = s.xlam[idx];
+    const double jdx = res[idx] - diag[idx] * px[idx];
+    acc -= lam * jdx;
+  }
+  block_sum2(acc, 0.0, partial);
+}
+
+// relax_bounds (interior_point_backend.h:126-146)
+__global__ void k_relax_bounds(int np, const double* lbx, const double* ubx,
+                               double* lo, double* hi, double factor,
+                               double tol) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += gridDim.x * blockDim.x) {
+    const double l = lbx[i], u = ubx[i];
+    lo[i] = isinf(l) ? l : l - fmin(tol, factor * fmax(1.0, fabs(l)));
+    hi[i] = isinf(u) ? u : u + fmin(tol, factor * fmax(1.0, fabs(u)));
+  }
+}
+
+// project_primals_into_interior + initialize_bound_duals +
+// initialize_slacks (interior_point_backend.h:82-88, 156-188)
+__global__ void k_initialize(P p, double* xlam, double* zl, double* zu,
+                             double* sl, double* su, double kappa1,
+                             double kappa2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np;
+       i += gridDim.x * blockDim.x) {
+    const int idx = p.pidx[i];
+    double x = xlam[idx];
+    const double lb = p.lbx[i], ub = p.ubx[i];
+    const bool hl = !isinf(lb), hu = !isinf(ub);
+    if (hl && hu) {
+      const double range = ub - lb;
+      const double pl = fmin(kappa1 * fmax(1.0, fabs(lb)), kappa2 * range);
+      const double pu = fmin(kappa1 * fmax(1.0, fabs(ub)), kappa2 * range);
+      x = fmax(fmin(x, ub - pu), lb + pl);
+    } else if (hl) {
+      x = fmax(x, lb + kappa1 * fmax(1.0, fabs(lb)));
+    } else if (hu) {
+      x = fmin(x, ub - kappa1 * fmax(1.0, fabs(ub)));
+    }
+    xlam[idx] = x;
+    zl[i] = hl ? 1.0 : 0.0;
+    zu[i] = hu ? 1.0 : 0.0;
+    sl[i] = hl ? (x - lb) : 1.0;
+    su[i] = hu ? (ub - x) : 1.0;
   }
 }
 
@@ -494,6 +563,34 @@ int ipm_affine_start_point(const ab_ipm_problem* p, const ab_ipm_state* s,
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
-long long ipm_scratch_doubles() { return (long long)kRedBlocks * 10 + 64; }
+int ipm_barrier_dphi_kkt(const ab_ipm_problem* p, const ab_ipm_state* s,
+                         const double* res, const double* px,
+                         const double* diag, double* out, cudaStream_t st,
+                         double* scratch) {
+  k_barrier_dphi_kkt<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), res, px, diag,
+                                                scratch);
+  k_sum1_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_relax_bounds(int np, const double* lbx, const double* ubx,
+                     double* lo, double* hi, double factor, double tol,
+                     cudaStream_t st) {
+  if (np <= 0) return 0;
+  k_relax_bounds<<<grid_for(np), RT, 0, st>>>(np, lbx, ubx, lo, hi, factor,
+                                               tol);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
+                   double* zu, double* sl, double* su, double kappa1,
+                   double kappa2, cudaStream_t st) {
+  if (p->np <= 0) return 0;
+  k_initialize<<<grid_for(p->np), RT, 0, st>>>(mkP(p), xlam, zl, zu, sl, su,
+                                                kappa1, kappa2);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+long long ipm_scratch_doubles() { return (long long)kRedBlocks * 16 + 64; }
 
 }  // namespace ab

@@ -153,8 +153,11 @@ int ab_ipm_apply_step(const ab_ipm_problem* p, const ab_ipm_state* s,
  *  compute_barrier_log_sum (:471-484): out[6];
  *  compute_constraint_violation_1norm (:565-573): out[7];
  *  compute_max_comp_deviation (:417-426): out[8];
- *  compute_complementarity_sq (:430-443): out[9].
- * grad may be NULL (then out[3..5] and out[7] are not computed). */
+ *  compute_complementarity_sq (:430-443): out[9];
+ *  compute_kkt_error_sq (:539-561): out[10] = dual_sq, out[11] = primal_sq,
+ *    out[12] = comp_sq.
+ * out must hold 13 doubles.  grad may be NULL (then out[3], out[4],
+ * out[7], out[10], out[11] are 0). */
 int ab_ipm_reductions(const ab_ipm_problem* p, const ab_ipm_state* s,
                       double mu, const double* grad, double* out,
                       void* stream);
@@ -162,6 +165,22 @@ int ab_ipm_reductions(const ab_ipm_problem* p, const ab_ipm_state* s,
 int ab_ipm_barrier_dphi(const ab_ipm_problem* p, const ab_ipm_state* s,
                         double mu, const double* grad, const double* px,
                         double* out, void* stream);
+/* compute_barrier_dphi_from_kkt (:597-611) -> out[0]; res, px, diag are
+ * n-vectors. */
+int ab_ipm_barrier_dphi_kkt(const ab_ipm_problem* p, const ab_ipm_state* s,
+                            const double* res, const double* px,
+                            const double* diag, double* out, void* stream);
+/* relax_bounds (:126-146): lbx_out/ubx_out may alias lbx/ubx. */
+int ab_ipm_relax_bounds(int np, const double* lbx, const double* ubx,
+                        double* lbx_out, double* ubx_out, double factor,
+                        double constr_viol_tol, void* stream);
+/* project_primals_into_interior (:156-177), initialize_bound_duals
+ * (:182-188) and initialize_slacks (:82-88) in one pass, as
+ * InteriorPointOptimizer::initialize_multipliers_and_slacks does
+ * (include/interior_point_optimizer.h:202-212).  Uses p->lbx/ubx. */
+int ab_ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
+                      double* zu, double* sl, double* su, double kappa1,
+                      double kappa2, void* stream);
 /* reset_bound_multipliers (:508-522) */
 int ab_ipm_reset_bound_multipliers(const ab_ipm_problem* p,
                                    const ab_ipm_state* s, double mu,

@@ -50,12 +50,19 @@ def lib():
         L.ref_ldl_solve.argtypes = [_vp, _i, _dp, _i]
         L.ref_ldl_node_pivots.argtypes = [_vp, _ip, _ip]
         L.ref_order.argtypes = [_i, _ip, _ip, _i, _ip, _ip]
+        L.ref_set_blas_threads.argtypes = [_i]
+        L.ref_set_blas_threads(1)
         for name in ("ref_ipm_compute_barrier_log_sum",
                      "ref_ipm_compute_barrier_dphi",
                      "ref_ipm_compute_constraint_violation_1norm"):
             getattr(L, name).restype = _d
         _lib = L
     return _lib
+
+
+def set_blas_threads(n):
+    """OpenBLAS threads used inside the reference's BLAS/LAPACK calls."""
+    lib().ref_set_blas_threads(int(n))
 
 
 def _ptr(a, kind):

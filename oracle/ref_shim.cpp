@@ -60,6 +60,12 @@ OrderingType to_order(int order) {
 
 extern "C" {
 
+// Thread count of the bundled OpenBLAS (its pthread pool must not be nested
+// inside the reference's OpenMP task region, so the checker runs BLAS
+// single-threaded unless asked otherwise).
+void scipy_openblas_set_num_threads(int);
+void ref_set_blas_threads(int n) { scipy_openblas_set_num_threads(n); }
+
 // order: 0 = NESTED_DISSECTION (identity without METIS), 1 = AMD,
 // 2 = MULTI_COLOR, 3 = NATURAL.  solver: 0 = LDL, 1 = CHOLESKY.
 void* ref_ldl_create(int n, const int* rowp, const int* cols, int order,

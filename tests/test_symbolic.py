@@ -1,0 +1,87 @@
+"""Bit-exact parity of the host symbolic analysis (CPU only).
+
+The product's ordering + supernode partition must equal the reference
+SparseLDL's private arrays (include/sparse_ldl.h:2204-2358) exactly: against
+the committed golden fixtures (generated from the reference by
+tests/golden/make_golden.py) and, when oracle/_ref is built, against the
+reference itself on further patterns.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from amigo_b200 import linalg
+from matrices import csr_arrays, kkt_matrix, ldl_unit_matrix, poisson_2d
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "ldl_golden.npz")
+KEYS = ("node_ptr", "node_to_var", "children_ptr", "children", "contrib_ptr",
+        "contrib_rows", "invperm")
+
+
+def golden_cases():
+    z = np.load(GOLD)
+    names = sorted({k.split("/")[0] for k in z.files})
+    return z, names
+
+
+def test_golden_symbolic_bit_exact():
+    z, names = golden_cases()
+    assert len(names) == 22
+    for name in names:
+        rp, ci = z[name + "/rowp"], z[name + "/cols"]
+        n = len(rp) - 1
+        got = linalg.analyze(n, rp, ci, int(z[name + "/order"]))
+        for k in KEYS:
+            np.testing.assert_array_equal(got[k], z[name + "/" + k],
+                                          err_msg="%s %s" % (name, k))
+
+
+def _patterns():
+    mats = []
+    for i in range(7):
+        mats.append(ldl_unit_matrix(i)[0])
+    for n in (10, 20, 50):
+        mats.append(poisson_2d(n)[0])
+    for s, (a, b) in enumerate([(50, 30), (500, 300), (2000, 1500)]):
+        mats.append(kkt_matrix(a, b, 100 + s))
+    # unsorted column indices inside rows
+    M = kkt_matrix(300, 200, 7, sort=False)
+    mats.append(M)
+    return mats
+
+
+@pytest.mark.parametrize("order", ["NATURAL", "AMD", "NESTED_DISSECTION"])
+def test_symbolic_matches_reference(oracle_ref, order):
+    for M in _patterns():
+        n, rp, ci, _ = csr_arrays(M)
+        want = oracle_ref.RefSparseLDL(n, rp, ci, order=order).symbolic()
+        got = linalg.analyze(n, rp, ci, linalg.OrderingType[order])
+        assert got["num_nodes"] == want["num_nodes"]
+        for k in KEYS:
+            np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+
+
+def test_amd_permutation_matches_reference(oracle_ref):
+    for M in _patterns():
+        n, rp, ci, _ = csr_arrays(M)
+        perm, iperm = oracle_ref.order(n, rp, ci, "AMD")
+        got = linalg.analyze(n, rp, ci, linalg.OrderingType.AMD)
+        np.testing.assert_array_equal(got["invperm"], iperm)
+
+
+def test_empty_and_tiny():
+    got = linalg.analyze(1, np.array([0, 1]), np.array([0]))
+    assert got["num_nodes"] == 1
+    np.testing.assert_array_equal(got["node_ptr"], [0, 1])
+    got = linalg.analyze(2, np.array([0, 1, 2]), np.array([0, 1]))  # two roots
+    assert got["num_nodes"] >= 1
+    assert got["children_ptr"][-1] == got["num_nodes"]
+
+
+def test_bad_arguments():
+    with pytest.raises(Exception):
+        linalg.analyze(2, np.array([0, 1, 2]), np.array([0, 5]))
+    with pytest.raises(Exception):
+        linalg.analyze(2, np.array([0, 1, 2]), np.array([0, 1]),
+                       linalg.OrderingType.MULTI_COLOR)
