@@ -37,6 +37,20 @@ class IpmState(ctypes.Structure):
                 ("su", _vp)]
 
 
+class Simp2DStruct(ctypes.Structure):
+    """Mirror of ab_simp2d (include/amigo_b200.h)."""
+    _fields_ = ([(k, _i) for k in ("n", "nnz", "nelems", "nnodes", "u0", "rt0",
+                                   "re0", "s_index", "lam0", "mu0", "nu_index")]
+                + [("color_ptr", _i * 5)]
+                + [(k, _vp) for k in ("color_elems", "ev", "fv", "epos", "fpos",
+                                      "vpos", "spos", "fixed", "fixed_zero_pos",
+                                      "fixed_diag_pos", "load_idx", "load_val",
+                                      "K0", "A")]
+                + [(k, _i) for k in ("nfixed", "nfixed_zero", "nload")]
+                + [(k, _d) for k in ("Bq", "vcoef", "volfrac", "E0", "Emin",
+                                     "penalty")])
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "ab_ldl_create": (_i, [_i, _ip, _ip, _i, _i, _d, _d, _d, ctypes.POINTER(_vp)]),
@@ -78,8 +92,18 @@ _SIGS = {
     "ab_ipm_relax_bounds": (_i, [_i, _vp, _vp, _vp, _vp, _d, _d, _vp]),
     "ab_ipm_initialize": (_i, [ctypes.POINTER(IpmProblem), _vp, _vp, _vp, _vp,
                                _vp, _d, _d, _vp]),
+    "ab_ipm_refine_init": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
+                                _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ab_ipm_refine_residual": (_i, [ctypes.POINTER(IpmProblem),
+                                    ctypes.POINTER(IpmState), _d, _vp, _vp, _vp,
+                                    _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ab_ipm_refine_update": (_i, [ctypes.POINTER(IpmProblem),
+                                  ctypes.POINTER(IpmState), _vp, _vp, _vp, _vp,
+                                  _vp, _vp, _vp]),
     "ab_csr_add_diagonal": (_i, [_i, _vp, _vp, _vp, _vp]),
     "ab_csr_matvec": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ab_simp2d_gradient": (_i, [ctypes.POINTER(Simp2DStruct), _vp, _d, _vp, _vp]),
+    "ab_simp2d_hessian": (_i, [ctypes.POINTER(Simp2DStruct), _vp, _d, _vp, _vp]),
 }
 
 _lib = None

@@ -31,7 +31,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 EXTRA = {"ipm_kernels.cu": ["--fmad=false"]}
 
 SOURCES = ["symbolic.cpp", "ldl_plan.cpp", "ldl_factor.cu", "ldl_solve.cu",
-           "capi.cpp", "ipm_kernels.cu", "capi_ipm.cpp", "csr_kernels.cu"]
+           "capi.cpp", "ipm_kernels.cu", "capi_ipm.cpp", "csr_kernels.cu",
+           "fem2d.cu"]
 
 
 def nvcc():

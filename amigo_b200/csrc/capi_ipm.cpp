@@ -47,7 +47,7 @@ extern "C" {
 int ab_ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
                     const double* grad, double* res, double* out2,
                     void* stream) {
-  if (bad(p, s) || !grad || !res) return AB_ERR_ARG;
+  if (bad(p, s) || (p->n > 0 && (!grad || !res))) return AB_ERR_ARG;
   double* scratch = nullptr;
   if (out2 && !(scratch = device_scratch())) return AB_ERR_CUDA;
   return ab::ipm_residual(p, s, mu, grad, res, out2, (cudaStream_t)stream,
@@ -56,21 +56,22 @@ int ab_ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
 
 int ab_ipm_diagonal(const ab_ipm_problem* p, const ab_ipm_state* s,
                     double* diag, void* stream) {
-  if (bad(p, s) || !diag) return AB_ERR_ARG;
+  if (bad(p, s) || (p->n > 0 && !diag)) return AB_ERR_ARG;
   return ab::ipm_diagonal(p, s, diag, (cudaStream_t)stream);
 }
 
 int ab_ipm_bound_dual_step(const ab_ipm_problem* p, const ab_ipm_state* s,
                            double mu, const double* px, double* dzl,
                            double* dzu, void* stream) {
-  if (bad(p, s) || !px || !dzl || !dzu) return AB_ERR_ARG;
+  if (bad(p, s) || (p->np > 0 && (!px || !dzl || !dzu))) return AB_ERR_ARG;
   return ab::ipm_bound_dual_step(p, s, mu, px, dzl, dzu, (cudaStream_t)stream);
 }
 
 int ab_ipm_max_step(const ab_ipm_problem* p, const ab_ipm_state* s,
                     double tau, const double* px, const double* dzl,
                     const double* dzu, double* out, int* iout, void* stream) {
-  if (bad(p, s) || !px || !dzl || !dzu || !out || !iout) return AB_ERR_ARG;
+  if (bad(p, s) || !out || !iout || (p->np > 0 && (!px || !dzl || !dzu)))
+    return AB_ERR_ARG;
   double* scratch = device_scratch();
   if (!scratch) return AB_ERR_CUDA;
   return ab::ipm_max_step(p, s, tau, px, dzl, dzu, out, iout,
@@ -82,8 +83,8 @@ int ab_ipm_apply_step(const ab_ipm_problem* p, const ab_ipm_state* s,
                       const double* dzl, const double* dzu, double* xlam_new,
                       double* zl_new, double* zu_new, double* sl_new,
                       double* su_new, void* stream) {
-  if (bad(p, s) || !s->xlam || !dxlam || !dzl || !dzu || !xlam_new ||
-      !zl_new || !zu_new || !sl_new || !su_new)
+  if (bad(p, s) || (p->n > 0 && (!s->xlam || !dxlam || !xlam_new)) ||
+      (p->np > 0 && (!dzl || !dzu || !zl_new || !zu_new || !sl_new || !su_new)))
     return AB_ERR_ARG;
   return ab::ipm_apply_step(p, s, ax, az, dxlam, dzl, dzu, xlam_new, zl_new,
                             zu_new, sl_new, su_new, (cudaStream_t)stream);
@@ -102,7 +103,7 @@ int ab_ipm_reductions(const ab_ipm_problem* p, const ab_ipm_state* s,
 int ab_ipm_barrier_dphi(const ab_ipm_problem* p, const ab_ipm_state* s,
                         double mu, const double* grad, const double* px,
                         double* out, void* stream) {
-  if (bad(p, s) || !grad || !px || !out) return AB_ERR_ARG;
+  if (bad(p, s) || !out || (p->np > 0 && (!grad || !px))) return AB_ERR_ARG;
   double* scratch = device_scratch();
   if (!scratch) return AB_ERR_CUDA;
   return ab::ipm_barrier_dphi(p, s, mu, grad, px, out, (cudaStream_t)stream,
@@ -113,7 +114,7 @@ int ab_ipm_reset_bound_multipliers(const ab_ipm_problem* p,
                                    const ab_ipm_state* s, double mu,
                                    double kappa, double* zl_out,
                                    double* zu_out, void* stream) {
-  if (bad(p, s) || !zl_out || !zu_out) return AB_ERR_ARG;
+  if (bad(p, s) || (p->np > 0 && (!zl_out || !zu_out))) return AB_ERR_ARG;
   return ab::ipm_reset_bound_multipliers(p, s, mu, kappa, zl_out, zu_out,
                                          (cudaStream_t)stream);
 }
@@ -122,7 +123,8 @@ int ab_ipm_affine_start_point(const ab_ipm_problem* p, const ab_ipm_state* s,
                               double beta_min, const double* dzl,
                               const double* dzu, double* zl_out,
                               double* zu_out, void* stream) {
-  if (bad(p, s) || !dzl || !dzu || !zl_out || !zu_out) return AB_ERR_ARG;
+  if (bad(p, s) || (p->np > 0 && (!dzl || !dzu || !zl_out || !zu_out)))
+    return AB_ERR_ARG;
   return ab::ipm_affine_start_point(p, s, beta_min, dzl, dzu, zl_out, zu_out,
                                     (cudaStream_t)stream);
 }
@@ -157,6 +159,47 @@ int ab_ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
     return AB_ERR_ARG;
   return ab::ipm_initialize(p, xlam, zl, zu, sl, su, kappa1, kappa2,
                             (cudaStream_t)stream);
+}
+
+int ab_ipm_refine_init(const ab_ipm_problem* p, const ab_ipm_state* s,
+                       double mu, const double* grad, const double* rhs_saved,
+                       const double* px, double* dzl, double* dzu, double* out,
+                       void* stream) {
+  if (bad(p, s) || !out || (p->n > 0 && (!grad || !rhs_saved || !px)) ||
+      (p->np > 0 && (!dzl || !dzu)))
+    return AB_ERR_ARG;
+  double* scratch = device_scratch();
+  if (!scratch) return AB_ERR_CUDA;
+  return ab::ipm_refine_init(p, s, mu, grad, rhs_saved, px, dzl, dzu, out,
+                             (cudaStream_t)stream, scratch);
+}
+
+int ab_ipm_refine_residual(const ab_ipm_problem* p, const ab_ipm_state* s,
+                           double mu, const double* grad,
+                           const double* rhs_saved, const double* kpx,
+                           const double* px, const double* dzl,
+                           const double* dzu, double* e_cond, double* e_zl,
+                           double* e_zu, double* out, void* stream) {
+  if (bad(p, s) || !out ||
+      (p->n > 0 && (!grad || !rhs_saved || !kpx || !px || !e_cond)) ||
+      (p->np > 0 && (!dzl || !dzu || !e_zl || !e_zu)))
+    return AB_ERR_ARG;
+  double* scratch = device_scratch();
+  if (!scratch) return AB_ERR_CUDA;
+  return ab::ipm_refine_residual(p, s, mu, grad, rhs_saved, kpx, px, dzl, dzu,
+                                 e_cond, e_zl, e_zu, out, (cudaStream_t)stream,
+                                 scratch);
+}
+
+int ab_ipm_refine_update(const ab_ipm_problem* p, const ab_ipm_state* s,
+                         const double* corr, const double* e_zl,
+                         const double* e_zu, double* px, double* dzl,
+                         double* dzu, void* stream) {
+  if (bad(p, s) || (p->n > 0 && (!corr || !px)) ||
+      (p->np > 0 && (!e_zl || !e_zu || !dzl || !dzu)))
+    return AB_ERR_ARG;
+  return ab::ipm_refine_update(p, s, corr, e_zl, e_zu, px, dzl, dzu,
+                               (cudaStream_t)stream);
 }
 
 int ab_csr_add_diagonal(int n, const int* diag_pos, const double* d,

@@ -9,6 +9,7 @@
 namespace ab {
 
 __device__ void block_sum2(double a, double b, double* partial);
+__device__ void block_max2(double a, double b, double* partial);
 
 long long ipm_scratch_doubles();
 int ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
@@ -52,6 +53,21 @@ int ipm_relax_bounds(int np, const double* lbx, const double* ubx,
 int ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
                    double* zu, double* sl, double* su, double kappa1,
                    double kappa2, cudaStream_t st);
+
+int ipm_refine_init(const ab_ipm_problem* p, const ab_ipm_state* s,
+                    double mu, const double* grad, const double* rhs_saved,
+                    const double* px, double* dzl, double* dzu, double* out,
+                    cudaStream_t st, double* scratch);
+int ipm_refine_residual(const ab_ipm_problem* p, const ab_ipm_state* s,
+                        double mu, const double* grad, const double* rhs_saved,
+                        const double* kpx, const double* px, const double* dzl,
+                        const double* dzu, double* e_cond, double* e_zl,
+                        double* e_zu, double* out, cudaStream_t st,
+                        double* scratch);
+int ipm_refine_update(const ab_ipm_problem* p, const ab_ipm_state* s,
+                      const double* corr, const double* e_zl,
+                      const double* e_zu, double* px, double* dzl,
+                      double* dzu, cudaStream_t st);
 
 int csr_add_diagonal(int n, const int* diag_pos, const double* d,
                      double* vals, cudaStream_t st);

@@ -431,6 +431,111 @@ __global__ void k_initialize(P p, double* xlam, double* zl, double* zu,
   }
 }
 
+// ---------------------------------------------------- iterative refinement
+// Refinement on the unreduced 8-block Newton system, restating
+// DirectSparseSolver.iterative_refinement
+// (amigo/algorithm/solvers/linear_solver.py:109-264) on the device.
+// gl = sl where the lower bound is finite, else 1 (gu likewise).
+__device__ __forceinline__ void ir_bounds(const P& p, const S& s, int i,
+                                          bool& fl, bool& fu, double& gl,
+                                          double& gu) {
+  fl = finite_bound(p.lbx[i]);
+  fu = finite_bound(p.ubx[i]);
+  gl = fl ? s.sl[i] : 1.0;
+  gu = fu ? s.su[i] : 1.0;
+}
+
+// Initial bound-dual steps from back-substitution and ||rhs||_inf over the
+// four blocks (linear_solver.py:168-191).
+__global__ void k_ir_init(P p, S s, double mu, const double* grad,
+                          const double* rhs_saved, const double* px,
+                          double* dzl, double* dzu, double* partial) {
+  double nrm = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    bool fl, fu;
+    double gl, gu;
+    ir_bounds(p, s, i, fl, fu, gl, gu);
+    const int idx = p.pidx[i];
+    const double zl = s.zl[i], zu = s.zu[i], dx = px[idx];
+    dzl[i] = fl ? (mu - gl * zl - zl * dx) / gl : 0.0;
+    dzu[i] = fu ? (mu - gu * zu + zu * dx) / gu : 0.0;
+    const double rx = -(grad[idx] - zl + zu);
+    nrm = fmax(nrm, fabs(rx));
+    if (fl) nrm = fmax(nrm, fabs(mu - gl * zl));
+    if (fu) nrm = fmax(nrm, fabs(mu - gu * zu));
+  }
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p.nc; j += stride)
+    nrm = fmax(nrm, fabs(rhs_saved[p.cidx[j]]));
+  block_max2(nrm, 0.0, partial);
+}
+
+// Residuals of the 8-block system at (px, dzl, dzu), the condensed
+// correction right-hand side, and the two norms of the stopping test
+// (linear_solver.py:202-244).
+__global__ void k_ir_residual(P p, S s, double mu, const double* grad,
+                              const double* rhs_saved, const double* kpx,
+                              const double* px, const double* dzl,
+                              const double* dzu, double* e_cond,
+                              double* e_zl, double* e_zu, double* partial) {
+  double nres = 0.0, nsol = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    bool fl, fu;
+    double gl, gu;
+    ir_bounds(p, s, i, fl, fu, gl, gu);
+    const int idx = p.pidx[i];
+    const double zl = s.zl[i], zu = s.zu[i], dx = px[idx];
+    const double sigma = (fl ? zl / gl : 0.0) + (fu ? zu / gu : 0.0);
+    const double rx = -(grad[idx] - zl + zu);
+    const double ex = rx - kpx[idx] + sigma * dx + dzl[i] - dzu[i];
+    const double ezl = fl ? (mu - gl * zl) - zl * dx - gl * dzl[i] : 0.0;
+    const double ezu = fu ? (mu - gu * zu) + zu * dx - gu * dzu[i] : 0.0;
+    e_zl[i] = ezl;
+    e_zu[i] = ezu;
+    e_cond[idx] = ex + (fl ? ezl / gl : 0.0) - (fu ? ezu / gu : 0.0);
+    nres = fmax(nres, fmax(fabs(ex), fmax(fabs(ezl), fabs(ezu))));
+    nsol = fmax(nsol, fmax(fabs(dx), fmax(fabs(dzl[i]), fabs(dzu[i]))));
+  }
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p.nc; j += stride) {
+    const int idx = p.cidx[j];
+    const double ec = rhs_saved[idx] - kpx[idx];
+    e_cond[idx] = ec;
+    nres = fmax(nres, fabs(ec));
+    nsol = fmax(nsol, fabs(px[idx]));
+  }
+  block_max2(nres, nsol, partial);
+}
+
+// Back-substitute the bound-dual corrections and accumulate the solution
+// (linear_solver.py:255-262).
+__global__ void k_ir_update(P p, S s, const double* corr, const double* e_zl,
+                            const double* e_zu, double* px, double* dzl,
+                            double* dzu) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    bool fl, fu;
+    double gl, gu;
+    ir_bounds(p, s, i, fl, fu, gl, gu);
+    const double dc = corr[p.pidx[i]];
+    if (fl) dzl[i] += (e_zl[i] - s.zl[i] * dc) / gl;
+    if (fu) dzu[i] += (e_zu[i] + s.zu[i] * dc) / gu;
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride)
+    px[i] += corr[i];
+}
+
+__global__ void k_max2_final(int nblocks, const double* partial, double* out) {
+  if (threadIdx.x != 0) return;
+  double a = 0.0, b = 0.0;
+  for (int k = 0; k < nblocks; k++) {
+    a = fmax(a, partial[2 * k]);
+    b = fmax(b, partial[2 * k + 1]);
+  }
+  out[0] = a;
+  out[1] = b;
+}
+
 __global__ void k_sum2_final(int nblocks, const double* partial, double* out) {
   if (threadIdx.x != 0) return;
   double a = 0.0, b = 0.0;
@@ -450,6 +555,30 @@ __global__ void k_sum1_final(int nblocks, const double* partial, double* out) {
 }
 
 }  // namespace
+
+// Two-value block maximum written to partial[2 * blockIdx.x + {0, 1}].
+__device__ void block_max2(double a, double b, double* partial) {
+  __shared__ double sa[RT / 32], sb[RT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
+    b = fmax(b, __shfl_down_sync(0xffffffffu, b, o));
+  }
+  if (lane == 0) {
+    sa[warp] = a;
+    sb[warp] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double x = 0.0, y = 0.0;
+    for (int w = 0; w < RT / 32; w++) {
+      x = fmax(x, sa[w]);
+      y = fmax(y, sb[w]);
+    }
+    partial[2 * blockIdx.x] = x;
+    partial[2 * blockIdx.x + 1] = y;
+  }
+}
 
 // Two-value block sum written to partial[2 * blockIdx.x + {0, 1}].
 __device__ void block_sum2(double a, double b, double* partial) {
@@ -588,6 +717,39 @@ int ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
   if (p->np <= 0) return 0;
   k_initialize<<<grid_for(p->np), RT, 0, st>>>(mkP(p), xlam, zl, zu, sl, su,
                                                 kappa1, kappa2);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_refine_init(const ab_ipm_problem* p, const ab_ipm_state* s,
+                    double mu, const double* grad, const double* rhs_saved,
+                    const double* px, double* dzl, double* dzu, double* out,
+                    cudaStream_t st, double* scratch) {
+  k_ir_init<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, rhs_saved,
+                                       px, dzl, dzu, scratch);
+  k_max2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_refine_residual(const ab_ipm_problem* p, const ab_ipm_state* s,
+                        double mu, const double* grad, const double* rhs_saved,
+                        const double* kpx, const double* px, const double* dzl,
+                        const double* dzu, double* e_cond, double* e_zl,
+                        double* e_zu, double* out, cudaStream_t st,
+                        double* scratch) {
+  k_ir_residual<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, rhs_saved,
+                                           kpx, px, dzl, dzu, e_cond, e_zl,
+                                           e_zu, scratch);
+  k_max2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_refine_update(const ab_ipm_problem* p, const ab_ipm_state* s,
+                      const double* corr, const double* e_zl,
+                      const double* e_zu, double* px, double* dzl,
+                      double* dzu, cudaStream_t st) {
+  long long m = p->n > p->np ? p->n : p->np;
+  k_ir_update<<<grid_for(m), RT, 0, st>>>(mkP(p), mkS(s), corr, e_zl, e_zu,
+                                          px, dzl, dzu);
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 

@@ -20,7 +20,10 @@
 
 #include <cfloat>
 #include <cmath>
+#include <algorithm>
 #include <cstdio>
+#include <cstdlib>
+#include <vector>
 
 #include "ldl_internal.h"
 
@@ -30,7 +33,6 @@ namespace {
 constexpr int NT = kThreads;
 constexpr int NB = kPanel;
 constexpr int NWARP = NT / 32;
-constexpr int kMaxDynSmem = 190 * 1024;
 constexpr int kTile = 64;
 
 struct Ctl {
@@ -138,10 +140,67 @@ __device__ void swap_wrows(double* W, int ldw, int ncol, int a, int b) {
   }
 }
 
-// Trailing update C -= A * B^T on the lower triangle of the (n-k) x (n-k)
-// block starting at (k, k):  A = F[k:, kstart:kstart+kw], B = W[k:, 0:kw].
-// `tiles` (>= 2 * kTile * NB doubles of shared memory) enables the tiled
-// form used for fronts kept in HBM.
+// Row stride of the staged A/B tiles: one double of padding makes the
+// 16 rows a warp reads in one step fall on distinct shared-memory banks.
+constexpr int TP = NB + 1;
+constexpr int kTileSmem = 2 * kTile * TP;  // doubles
+
+// C tile (ti, tj) of the trailing block F[k:, k:] -= A * B^T with
+// A = F[k:, kstart:kstart+kw] (L columns of the panel) and
+// B = W[k:, 0:kw] (their L*D columns); only the lower triangle is written.
+__device__ void update_tile(double* F, int ld, const double* W, int ldw,
+                            int n, int k, int kstart, int kw, int ti, int tj,
+                            double* As, double* Bs) {
+  const int tid = threadIdx.x;
+  const int r0 = k + ti * kTile, c0 = k + tj * kTile;
+  for (int idx = tid; idx < kTile * kw; idx += NT) {
+    const int rr = idx % kTile, jj = idx / kTile;
+    As[rr * TP + jj] = (r0 + rr < n) ? F[r0 + rr + (size_t)(kstart + jj) * ld] : 0.0;
+    Bs[rr * TP + jj] = (c0 + rr < n) ? W[c0 + rr + (size_t)jj * ldw] : 0.0;
+  }
+  __syncthreads();
+  const int tr = tid % 16, tc = tid / 16;  // 16 x 16 threads, 4 x 4 outputs each
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+  for (int jj = 0; jj < kw; jj++) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) av[a] = As[(tr + 16 * a) * TP + jj];
+#pragma unroll
+    for (int b = 0; b < 4; b++) bv[b] = Bs[(tc + 16 * b) * TP + jj];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    const int r = r0 + tr + 16 * a;
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int c = c0 + tc + 16 * b;
+      if (r < n && c < n && r >= c) F[r + (size_t)c * ld] -= acc[a][b];
+    }
+  }
+  __syncthreads();
+}
+
+// Lower-triangle tile index t -> (ti, tj), ti >= tj.
+__device__ __forceinline__ void tile_coords(int t, int& ti, int& tj) {
+  int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((i + 1) * (i + 2) / 2 <= t) i++;
+  while (i * (i + 1) / 2 > t) i--;
+  ti = i;
+  tj = t - i * (i + 1) / 2;
+}
+
+// Trailing update of the whole block by one CTA.  `tiles` (kTileSmem
+// doubles of shared memory) selects the tiled form used for fronts kept in
+// HBM; without it the entries are updated directly (fronts in shared
+// memory).
 __device__ void trailing_update(double* F, int ld, const double* W, int ldw,
                                 int n, int k, int kstart, int kw,
                                 double* tiles) {
@@ -161,49 +220,11 @@ __device__ void trailing_update(double* F, int ld, const double* W, int ldw,
     __syncthreads();
     return;
   }
-  // Tiled: kTile x kTile output tiles over the lower triangle; A and B tiles
-  // are staged in shared memory (kw <= NB).
-  double* As = tiles;                 // kTile x NB, row-major by tile row
-  double* Bs = tiles + kTile * NB;    // kTile x NB
   const int nt = (m + kTile - 1) / kTile;
-  const int tr = tid % 16, tc = tid / 16;  // 16 x 16 threads, 4x4 each
-  for (int tj = 0; tj < nt; tj++) {
-    for (int ti = tj; ti < nt; ti++) {
-      const int r0 = k + ti * kTile, c0 = k + tj * kTile;
-      for (int idx = tid; idx < kTile * kw; idx += NT) {
-        int rr = idx % kTile, jj = idx / kTile;
-        As[rr * NB + jj] = (r0 + rr < n) ? F[r0 + rr + (size_t)(kstart + jj) * ld] : 0.0;
-        Bs[rr * NB + jj] = (c0 + rr < n) ? W[c0 + rr + (size_t)jj * ldw] : 0.0;
-      }
-      __syncthreads();
-      double acc[4][4];
-#pragma unroll
-      for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
-      for (int jj = 0; jj < kw; jj++) {
-        double av[4], bv[4];
-#pragma unroll
-        for (int a = 0; a < 4; a++) av[a] = As[(tr + 16 * a) * NB + jj];
-#pragma unroll
-        for (int b = 0; b < 4; b++) bv[b] = Bs[(tc + 16 * b) * NB + jj];
-#pragma unroll
-        for (int a = 0; a < 4; a++)
-#pragma unroll
-          for (int b = 0; b < 4; b++) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
-      }
-#pragma unroll
-      for (int a = 0; a < 4; a++) {
-        int r = r0 + tr + 16 * a;
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          int c = c0 + tc + 16 * b;
-          if (r < n && c < n && r >= c) F[r + (size_t)c * ld] -= acc[a][b];
-        }
-      }
-      __syncthreads();
-    }
-  }
+  for (int tj = 0; tj < nt; tj++)
+    for (int ti = tj; ti < nt; ti++)
+      update_tile(F, ld, W, ldw, n, k, kstart, kw, ti, tj, tiles,
+                  tiles + kTile * TP);
 }
 
 // W[r, col] = src(r) - F[r, kstart:kstart+kw] . ctl.wrow  for r in [k, n),
@@ -215,7 +236,7 @@ __device__ void trailing_update(double* F, int ld, const double* W, int ldw,
 //           reduces max over [k, n) \ {imax} -> ctl.rowmax.
 __device__ void build_column(double* F, int ld, double* W, int ldw, int n,
                              int k, int kstart, int kw, int col, int mode,
-                             int imax, int nc, Ctl& ctl) {
+                             int imax, int nc, Ctl& ctl, int* status) {
   const int tid = threadIdx.x;
   double bestv = -1.0, tailv = 0.0;
   int besti = 0x7fffffff;
@@ -240,7 +261,14 @@ __device__ void build_column(double* F, int ld, double* W, int ldw, int n,
   block_argmax(ctl, bestv, besti, tailv);
   if (tid == 0) {
     if (mode == 0) {
-      ctl.imax = ctl.red_i[0];
+      int im = ctl.red_i[0];
+      if (im >= nc || im <= k) {
+        // No finite candidate entry (all NaN, or no candidates): keep the
+        // index in range; NaN is reported through the status word.
+        if (k + 1 < nc) atomicOr(status, ST_NAN);
+        im = (k + 1 < n) ? k + 1 : k;
+      }
+      ctl.imax = im;
       ctl.abswik = ctl.red_v[0] < 0.0 ? 0.0 : ctl.red_v[0];
       ctl.ctail = ctl.red_v2[0];
     } else {
@@ -256,154 +284,167 @@ __device__ void load_wrow(const double* W, int ldw, int row, int kw, Ctl& ctl) {
   __syncthreads();
 }
 
-// Factor the fully-summed columns [0, fs) of the n x n front F (lower
-// triangle valid).  Returns the number of pivots (== fs for a root front).
+// One panel of the blocked factorization of the fully-summed columns of the
+// n x n front F (lower triangle valid): candidates are taken from column k
+// on while kw < NB - 1, each either eliminated (1x1 or 2x2, its L column(s)
+// written to F and its L*D column(s) kept in W) or delayed to the end of the
+// candidate set.  The trailing update of F[k:, k:] is left to the caller.
+__device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
+                             bool root, int* vars, int* fsperm, double ustab,
+                             double pivot_tol, int* status, Ctl& ctl, int& k_,
+                             int& nc_, int& kw_) {
+  const int tid = threadIdx.x;
+  const double bk_alpha = (1.0 + sqrt(17.0)) / 8.0;
+  int k = k_, nc = nc_, kw = 0;
+  const int kstart = k;
+  while (kw < NB - 1 && k < nc) {
+    load_wrow(W, ldw, k, kw, ctl);
+    build_column(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status);
+    const double wkk = W[k + (size_t)kw * ldw];
+    const double abswkk = fabs(wkk);
+    const int imax = ctl.imax;
+    const double abswik = ctl.abswik;
+    int step = 0, kpiv = -1;
+    bool zero_pivot = false;
+    if (!root) {
+      const double colmax = fmax(abswik, ctl.ctail);
+      if (abswkk >= pivot_tol && abswkk >= ustab * colmax) {
+        step = 1;
+        kpiv = k;
+      } else if (k + 1 < nc) {
+        load_wrow(W, ldw, imax, kw, ctl);
+        build_column(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
+        const double rowmax = ctl.rowmax;
+        const double wii = W[imax + (size_t)(kw + 1) * ldw];
+        const double abswii = fabs(wii);
+        if (abswii >= pivot_tol && abswii >= ustab * rowmax) {
+          for (int r = k + tid; r < n; r += NT)
+            W[r + (size_t)kw * ldw] = W[r + (size_t)(kw + 1) * ldw];
+          __syncthreads();
+          step = 1;
+          kpiv = imax;
+        } else {
+          const double wik = W[imax + (size_t)kw * ldw];
+          const double det = fabs(wkk * wii - wik * wik);
+          if (det >= pivot_tol) {
+            const double delta = det / fmax(abswii + abswik, abswkk + abswik);
+            if (delta >= ustab * colmax && delta >= ustab * rowmax) {
+              step = 2;
+              kpiv = imax;
+            }
+          }
+        }
+      }
+    } else {
+      // Bunch-Kaufman (LAPACK dsytf2/dlasyf, lower): every column is
+      // eliminated, by a 1x1 or a 2x2 pivot.
+      const double colmax = abswik;  // nc == n: all rows are candidates
+      if (!(fmax(abswkk, colmax) > 0.0)) {
+        step = 1;
+        kpiv = k;
+        zero_pivot = true;
+      } else if (abswkk >= bk_alpha * colmax) {
+        step = 1;
+        kpiv = k;
+      } else {
+        load_wrow(W, ldw, imax, kw, ctl);
+        build_column(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
+        const double rowmax = ctl.rowmax;
+        const double abswii = fabs(W[imax + (size_t)(kw + 1) * ldw]);
+        if (abswkk >= bk_alpha * colmax * (colmax / rowmax)) {
+          step = 1;
+          kpiv = k;
+        } else if (abswii >= bk_alpha * rowmax) {
+          for (int r = k + tid; r < n; r += NT)
+            W[r + (size_t)kw * ldw] = W[r + (size_t)(kw + 1) * ldw];
+          __syncthreads();
+          step = 1;
+          kpiv = imax;
+        } else {
+          step = 2;
+          kpiv = imax;
+        }
+      }
+    }
+
+    if (step == 0) {
+      // Delay candidate k: move it to the end of the candidate set.
+      if (k < nc - 1) {
+        symm_swap(F, ld, n, vars, fsperm, k, nc - 1);
+        swap_wrows(W, ldw, kw, k, nc - 1);
+        __syncthreads();
+      }
+      nc -= 1;
+      continue;
+    }
+    const int ksrc = k + step - 1;
+    if (kpiv != ksrc) {
+      symm_swap(F, ld, n, vars, fsperm, ksrc, kpiv);
+      swap_wrows(W, ldw, kw + step, ksrc, kpiv);
+      __syncthreads();
+    }
+    if (step == 1) {
+      const double d = W[k + (size_t)kw * ldw];
+      if (!isfinite(d) && tid == 0) atomicOr(status, ST_NAN);
+      const double dinv = zero_pivot ? 0.0 : 1.0 / d;
+      for (int r = k + tid; r < n; r += NT) {
+        double w = W[r + (size_t)kw * ldw];
+        F[r + (size_t)k * ld] = (r == k) ? w : w * dinv;
+      }
+    } else {
+      const double d11 = W[k + (size_t)kw * ldw];
+      const double d21 = W[k + 1 + (size_t)kw * ldw];
+      const double d22 = W[k + 1 + (size_t)(kw + 1) * ldw];
+      const double detinv = 1.0 / (d11 * d22 - d21 * d21);
+      if (!isfinite(detinv) && tid == 0) atomicOr(status, ST_NAN);
+      const double i00 = d22 * detinv, i10 = -d21 * detinv,
+                   i01 = -d21 * detinv, i11 = d11 * detinv;
+      for (int r = k + 2 + tid; r < n; r += NT) {
+        double w0 = W[r + (size_t)kw * ldw], w1 = W[r + (size_t)(kw + 1) * ldw];
+        F[r + (size_t)k * ld] = w0 * i00 + w1 * i10;
+        F[r + (size_t)(k + 1) * ld] = w0 * i01 + w1 * i11;
+      }
+      if (tid == 0) {
+        F[k + (size_t)k * ld] = d11;
+        F[k + 1 + (size_t)k * ld] = d21;
+        F[k + 1 + (size_t)(k + 1) * ld] = d22;
+        vars[k] = -(vars[k] + 1);
+        vars[k + 1] = -(vars[k + 1] + 1);
+      }
+    }
+    __syncthreads();
+    k += step;
+    kw += step;
+  }
+  k_ = k;
+  nc_ = nc;
+  kw_ = kw;
+}
+
+// Factor the fully-summed columns [0, fs) of the n x n front F in one CTA.
+// Returns the number of pivots (== fs for a root front).
 __device__ int factor_front(double* F, int ld, double* W, int ldw, int n,
                             int fs, bool root, int* vars, int* fsperm,
                             double ustab, double pivot_tol, double* tiles,
                             int* status, Ctl& ctl) {
-  const int tid = threadIdx.x;
-  const double bk_alpha = (1.0 + sqrt(17.0)) / 8.0;
   int nc = fs;
   int k = 0;
   while (k < nc) {
     const int kstart = k;
     int kw = 0;
-    while (kw < NB - 1 && k < nc) {
-      load_wrow(W, ldw, k, kw, ctl);
-      build_column(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl);
-      const double wkk = W[k + (size_t)kw * ldw];
-      const double abswkk = fabs(wkk);
-      const int imax = ctl.imax;
-      const double abswik = ctl.abswik;
-      int step = 0, kpiv = -1;
-      bool zero_pivot = false;
-      if (!root) {
-        const double colmax = fmax(abswik, ctl.ctail);
-        if (abswkk >= pivot_tol && abswkk >= ustab * colmax) {
-          step = 1;
-          kpiv = k;
-        } else if (k + 1 < nc) {
-          load_wrow(W, ldw, imax, kw, ctl);
-          build_column(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl);
-          const double rowmax = ctl.rowmax;
-          const double wii = W[imax + (size_t)(kw + 1) * ldw];
-          const double abswii = fabs(wii);
-          if (abswii >= pivot_tol && abswii >= ustab * rowmax) {
-            for (int r = k + tid; r < n; r += NT)
-              W[r + (size_t)kw * ldw] = W[r + (size_t)(kw + 1) * ldw];
-            __syncthreads();
-            step = 1;
-            kpiv = imax;
-          } else {
-            const double wik = W[imax + (size_t)kw * ldw];
-            const double det = fabs(wkk * wii - wik * wik);
-            if (det >= pivot_tol) {
-              const double delta = det / fmax(abswii + abswik, abswkk + abswik);
-              if (delta >= ustab * colmax && delta >= ustab * rowmax) {
-                step = 2;
-                kpiv = imax;
-              }
-            }
-          }
-        }
-      } else {
-        // Bunch-Kaufman (LAPACK dsytf2/dlasyf, lower): every column is
-        // eliminated, by a 1x1 or a 2x2 pivot.
-        const double colmax = abswik;  // nc == n: all rows are candidates
-        if (!(fmax(abswkk, colmax) > 0.0)) {
-          step = 1;
-          kpiv = k;
-          zero_pivot = true;
-        } else if (abswkk >= bk_alpha * colmax) {
-          step = 1;
-          kpiv = k;
-        } else {
-          load_wrow(W, ldw, imax, kw, ctl);
-          build_column(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl);
-          const double rowmax = ctl.rowmax;
-          const double abswii = fabs(W[imax + (size_t)(kw + 1) * ldw]);
-          if (abswkk >= bk_alpha * colmax * (colmax / rowmax)) {
-            step = 1;
-            kpiv = k;
-          } else if (abswii >= bk_alpha * rowmax) {
-            for (int r = k + tid; r < n; r += NT)
-              W[r + (size_t)kw * ldw] = W[r + (size_t)(kw + 1) * ldw];
-            __syncthreads();
-            step = 1;
-            kpiv = imax;
-          } else {
-            step = 2;
-            kpiv = imax;
-          }
-        }
-      }
-
-      if (step == 0) {
-        // Delay candidate k: move it to the end of the candidate set.
-        if (k < nc - 1) {
-          symm_swap(F, ld, n, vars, fsperm, k, nc - 1);
-          swap_wrows(W, ldw, kw, k, nc - 1);
-          __syncthreads();
-        }
-        nc -= 1;
-        continue;
-      }
-      const int ksrc = k + step - 1;
-      if (kpiv != ksrc) {
-        symm_swap(F, ld, n, vars, fsperm, ksrc, kpiv);
-        swap_wrows(W, ldw, kw + step, ksrc, kpiv);
-        __syncthreads();
-      }
-      if (step == 1) {
-        const double d = W[k + (size_t)kw * ldw];
-        if (!isfinite(d) && tid == 0) atomicOr(status, ST_NAN);
-        const double dinv = zero_pivot ? 0.0 : 1.0 / d;
-        for (int r = k + tid; r < n; r += NT) {
-          double w = W[r + (size_t)kw * ldw];
-          F[r + (size_t)k * ld] = (r == k) ? w : w * dinv;
-        }
-      } else {
-        const double d11 = W[k + (size_t)kw * ldw];
-        const double d21 = W[k + 1 + (size_t)kw * ldw];
-        const double d22 = W[k + 1 + (size_t)(kw + 1) * ldw];
-        const double detinv = 1.0 / (d11 * d22 - d21 * d21);
-        if (!isfinite(detinv) && tid == 0) atomicOr(status, ST_NAN);
-        const double i00 = d22 * detinv, i10 = -d21 * detinv,
-                     i01 = -d21 * detinv, i11 = d11 * detinv;
-        for (int r = k + 2 + tid; r < n; r += NT) {
-          double w0 = W[r + (size_t)kw * ldw], w1 = W[r + (size_t)(kw + 1) * ldw];
-          F[r + (size_t)k * ld] = w0 * i00 + w1 * i10;
-          F[r + (size_t)(k + 1) * ld] = w0 * i01 + w1 * i11;
-        }
-        if (tid == 0) {
-          F[k + (size_t)k * ld] = d11;
-          F[k + 1 + (size_t)k * ld] = d21;
-          F[k + 1 + (size_t)(k + 1) * ld] = d22;
-          vars[k] = -(vars[k] + 1);
-          vars[k + 1] = -(vars[k + 1] + 1);
-        }
-      }
-      __syncthreads();
-      k += step;
-      kw += step;
-    }
+    panel_factor(F, ld, W, ldw, n, root, vars, fsperm, ustab, pivot_tol,
+                 status, ctl, k, nc, kw);
     trailing_update(F, ld, W, ldw, n, k, kstart, kw, tiles);
     __syncthreads();
   }
   return nc;
 }
 
-// Per-level kernel: set up, assemble and factor one front per CTA.
-__global__ void __launch_bounds__(NT)
-k_factor_level(DevicePlan d, const int* __restrict__ nodes, int count,
-               const double* __restrict__ vals, double ustab,
-               double pivot_tol, int smem_doubles) {
-  extern __shared__ double smem[];
-  __shared__ Ctl ctl;
+// Front set-up shared by both paths (thread 0 sizes and allocates; all
+// threads fill the variable list and the fully-summed permutation record).
+// Returns false when the front must be skipped (a pool ran out earlier).
+__device__ bool setup_front(const DevicePlan& d, int node, Ctl& ctl) {
   const int tid = threadIdx.x;
-  const int node = nodes[blockIdx.x];
-
   if (tid == 0) {
     ctl.skip = (*((volatile int*)d.status) & (ST_POOL_F | ST_POOL_I)) ? 1 : 0;
     const int ns = d.ns[node], nc = d.nc[node];
@@ -419,13 +460,14 @@ k_factor_level(DevicePlan d, const int* __restrict__ nodes, int count,
       // F followed by W, rounded to 8 doubles (64-byte alignment)
       const unsigned long long need =
           (((unsigned long long)f * f + (unsigned long long)f * NB) + 15) & ~7ull;
+      const unsigned long long ineed = (4ull * f + 15) & ~7ull;
       unsigned long long off = atomicAdd(&d.counters[0], need);
-      unsigned long long ioff = atomicAdd(&d.counters[1], (4ull * f + 15) & ~7ull);
+      unsigned long long ioff = atomicAdd(&d.counters[1], ineed);
       if (off + need > (unsigned long long)d.fcap) {
         atomicOr(d.status, ST_POOL_F);
         ctl.skip = 1;
       }
-      if (ioff + ((4ull * f + 15) & ~7ull) > (unsigned long long)d.icap) {
+      if (ioff + ineed > (unsigned long long)d.icap) {
         atomicOr(d.status, ST_POOL_I);
         ctl.skip = 1;
       }
@@ -436,99 +478,57 @@ k_factor_level(DevicePlan d, const int* __restrict__ nodes, int count,
     d.ndin[node] = ndin;
     d.foff[node] = ctl.skip ? 0 : ctl.foff;
     d.ioff[node] = ctl.skip ? 0 : ctl.ioff;
+    d.pstate[4 * node + 0] = 0;          // k
+    d.pstate[4 * node + 1] = ns + ndin;  // candidates left
+    d.pstate[4 * node + 2] = 0;          // kstart of the last panel
+    d.pstate[4 * node + 3] = 0;          // kw of the last panel
     if (ctl.skip) {
       d.npiv[node] = 0;
       d.ndel[node] = 0;
+      d.pstate[4 * node + 1] = 0;
     }
   }
   __syncthreads();
-  if (ctl.skip) return;
-
-  const int f = ctl.f, fs = ctl.fs, ns = ctl.ns, ndin = ctl.ndin;
+  if (ctl.skip) return false;
+  const int f = ctl.f, fs = ctl.fs, ns = ctl.ns;
   int* fvars = d.ipool + ctl.ioff;
   int* fsperm = fvars + f;
-  double* Fg = d.fpool + ctl.foff;
-  const bool in_smem = (long long)f * f + (long long)f * NB <= smem_doubles;
-  double* F = in_smem ? smem : Fg;
-  double* W = in_smem ? smem + (size_t)f * f : Fg + (size_t)f * f;
-  double* tiles = nullptr;
-  if (!in_smem && smem_doubles >= 2 * kTile * NB) tiles = smem;
-
   // Variable list: node vars, delayed pivots of the children, contribution
   // rows (include/sparse_ldl.h:957-987, 596-616).
-  {
-    const int vbase = d.var_ptr[node];
-    for (int r = tid; r < ns; r += NT) fvars[r] = d.vars[vbase + r];
-    int choff = ns;
-    for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
-      const int c = d.kids[q];
-      const int ndc = d.ndel[c];
-      const int* cv = d.ipool + d.ioff[c] + d.npiv[c];
-      for (int t = tid; t < ndc; t += NT) fvars[choff + t] = cv[t];
-      choff += ndc;
-    }
-    const int cb = d.cptr[node];
-    for (int t = tid; t < d.nc[node]; t += NT) fvars[fs + t] = d.crows[cb + t];
-    for (int r = tid; r < fs; r += NT) fsperm[r] = r;
+  const int vbase = d.var_ptr[node];
+  for (int r = tid; r < ns; r += NT) fvars[r] = d.vars[vbase + r];
+  int choff = ns;
+  for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
+    const int c = d.kids[q];
+    const int ndc = d.ndel[c];
+    const int* cv = d.ipool + d.ioff[c] + d.npiv[c];
+    for (int t = tid; t < ndc; t += NT) fvars[choff + t] = cv[t];
+    choff += ndc;
   }
-
-  // Assemble: zero, add A, extend-add the children.
-  for (size_t idx = tid; idx < (size_t)f * f; idx += NT) F[idx] = 0.0;
+  const int cb = d.cptr[node];
+  for (int t = tid; t < d.nc[node]; t += NT) fvars[fs + t] = d.crows[cb + t];
+  for (int r = tid; r < fs; r += NT) fsperm[r] = r;
   __syncthreads();
-  for (int t = d.amap_ptr[node] + tid; t < d.amap_ptr[node + 1]; t += NT) {
-    const int r0 = d.amap_row[t];
-    const int r = r0 < ns ? r0 : r0 + ndin;
-    F[r + (size_t)d.amap_col[t] * f] += vals[d.amap_pos[t]];
-  }
-  __syncthreads();
-  {
-    int* rmap = reinterpret_cast<int*>(W);  // W is free until factoring
-    int choff = ns;
-    for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
-      const int c = d.kids[q];
-      const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
-      const int cc = fc - npc;
-      const double* C = d.fpool + d.foff[c];
-      const int cb = d.cptr[c];
-      for (int a = tid; a < cc; a += NT) {
-        int pos;
-        if (a < ndc) {
-          pos = choff + a;
-        } else {
-          int r0 = d.cmap[cb + a - ndc];
-          pos = r0 < ns ? r0 : r0 + ndin;
-        }
-        rmap[a] = pos;
-      }
-      __syncthreads();
-      for (int b = 0; b < cc; b++) {
-        const int pb = rmap[b];
-        const double* Cb = C + (size_t)(npc + b) * fc + npc;
-        for (int a = b + tid; a < cc; a += NT) {
-          const int pa = rmap[a];
-          const double v = Cb[a];
-          if (pa >= pb) F[pa + (size_t)pb * f] += v;
-          else F[pb + (size_t)pa * f] += v;
-        }
-      }
-      __syncthreads();
-      choff += ndc;
-    }
-  }
+  return true;
+}
 
-  const bool root = (fs == f);
-  const int npiv = factor_front(F, f, W, f, f, fs, root, fvars, fsperm, ustab,
-                                pivot_tol, tiles, d.status, ctl);
+// Static position of a child's contribution row `a` in the parent front.
+__device__ __forceinline__ int child_row_pos(const DevicePlan& d, int cb,
+                                             int ndc, int choff, int ns,
+                                             int ndin, int a) {
+  if (a < ndc) return choff + a;
+  const int r0 = d.cmap[cb + a - ndc];
+  return r0 < ns ? r0 : r0 + ndin;
+}
 
-  if (in_smem) {
-    for (size_t idx = tid; idx < (size_t)f * f; idx += NT) Fg[idx] = F[idx];
-  }
-  // Inertia of the D blocks, scanned in pivot order as the reference does
-  // (include/sparse_ldl.h:1937-1968).
-  // Also records the pivot kinds (0: 1x1, 1/2: first/second column of a
-  // 2x2 block) and the inverse of the fully-summed permutation, both used
-  // by the solves.
-  __syncthreads();
+// Inertia of the D blocks, scanned in pivot order as the reference does
+// (include/sparse_ldl.h:1937-1968); also records the pivot kinds (0: 1x1,
+// 1/2: first/second column of a 2x2 block) and the inverse of the
+// fully-summed permutation, both used by the solves.
+__device__ void finish_front(const DevicePlan& d, int node, const double* F,
+                             int f, int fs, int npiv, int* fvars) {
+  const int tid = threadIdx.x;
+  const int* fsperm = fvars + f;
   int* fsinv = fvars + 2 * f;
   int* kind = fvars + 3 * f;
   for (int r = tid; r < fs; r += NT) fsinv[fsperm[r]] = r;
@@ -562,6 +562,220 @@ k_factor_level(DevicePlan d, const int* __restrict__ nodes, int count,
   }
 }
 
+// Small/medium fronts: set up, assemble and factor one front per CTA, in
+// shared memory when it fits.
+__global__ void __launch_bounds__(NT)
+k_factor_level(DevicePlan d, const int* __restrict__ nodes, int count,
+               const double* __restrict__ vals, double ustab,
+               double pivot_tol, int smem_doubles) {
+  extern __shared__ double smem[];
+  __shared__ Ctl ctl;
+  const int tid = threadIdx.x;
+  const int node = nodes[blockIdx.x];
+  if (!setup_front(d, node, ctl)) return;
+
+  const int f = ctl.f, fs = ctl.fs, ns = ctl.ns, ndin = ctl.ndin;
+  int* fvars = d.ipool + ctl.ioff;
+  int* fsperm = fvars + f;
+  double* Fg = d.fpool + ctl.foff;
+  const bool in_smem = (long long)f * f + (long long)f * NB <= smem_doubles;
+  double* F = in_smem ? smem : Fg;
+  double* W = in_smem ? smem + (size_t)f * f : Fg + (size_t)f * f;
+  double* tiles = nullptr;
+  if (!in_smem && smem_doubles >= kTileSmem) tiles = smem;
+
+  // Assemble: zero, add A, extend-add the children.
+  for (size_t idx = tid; idx < (size_t)f * f; idx += NT) F[idx] = 0.0;
+  __syncthreads();
+  for (int t = d.amap_ptr[node] + tid; t < d.amap_ptr[node + 1]; t += NT) {
+    const int r0 = d.amap_row[t];
+    const int r = r0 < ns ? r0 : r0 + ndin;
+    F[r + (size_t)d.amap_col[t] * f] += vals[d.amap_pos[t]];
+  }
+  __syncthreads();
+  {
+    int* rmap = reinterpret_cast<int*>(W);  // W is free until factoring
+    int choff = ns;
+    for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
+      const int c = d.kids[q];
+      const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
+      const int cc = fc - npc;
+      const double* C = d.fpool + d.foff[c];
+      const int cb = d.cptr[c];
+      for (int a = tid; a < cc; a += NT)
+        rmap[a] = child_row_pos(d, cb, ndc, choff, ns, ndin, a);
+      __syncthreads();
+      for (int b = 0; b < cc; b++) {
+        const int pb = rmap[b];
+        const double* Cb = C + (size_t)(npc + b) * fc + npc;
+        for (int a = b + tid; a < cc; a += NT) {
+          const int pa = rmap[a];
+          const double v = Cb[a];
+          if (pa >= pb) F[pa + (size_t)pb * f] += v;
+          else F[pb + (size_t)pa * f] += v;
+        }
+      }
+      __syncthreads();
+      choff += ndc;
+    }
+  }
+
+  const bool root = (fs == f);
+  const int npiv = factor_front(F, f, W, f, f, fs, root, fvars, fsperm, ustab,
+                                pivot_tol, tiles, d.status, ctl);
+  if (in_smem) {
+    for (size_t idx = tid; idx < (size_t)f * f; idx += NT) Fg[idx] = F[idx];
+  }
+  __syncthreads();
+  finish_front(d, node, F, f, fs, npiv, fvars);
+}
+
+// ---------------------------------------------------------------------------
+// Large fronts: one CTA sets each front up, grids of CTAs assemble it, then
+// the factorization alternates a one-CTA panel kernel with a multi-CTA
+// trailing-update kernel over 64 x 64 tiles.
+
+__global__ void __launch_bounds__(NT)
+k_big_setup(DevicePlan d, const int* __restrict__ nodes) {
+  __shared__ Ctl ctl;
+  setup_front(d, nodes[blockIdx.x], ctl);
+}
+
+__device__ __forceinline__ bool big_skip(const DevicePlan& d) {
+  return (*((volatile int*)d.status) & (ST_POOL_F | ST_POOL_I)) != 0;
+}
+
+__global__ void __launch_bounds__(NT)
+k_big_zero(DevicePlan d, const int* __restrict__ nodes) {
+  if (big_skip(d)) return;
+  const int node = nodes[blockIdx.x];
+  const size_t f = d.f[node];
+  double* F = d.fpool + d.foff[node];
+  for (size_t idx = (size_t)blockIdx.y * NT + threadIdx.x; idx < f * f;
+       idx += (size_t)gridDim.y * NT)
+    F[idx] = 0.0;
+}
+
+__global__ void __launch_bounds__(NT)
+k_big_add_A(DevicePlan d, const int* __restrict__ nodes,
+            const double* __restrict__ vals) {
+  if (big_skip(d)) return;
+  const int node = nodes[blockIdx.x];
+  const int f = d.f[node], ns = d.ns[node], ndin = d.ndin[node];
+  double* F = d.fpool + d.foff[node];
+  for (int t = d.amap_ptr[node] + blockIdx.y * NT + threadIdx.x;
+       t < d.amap_ptr[node + 1]; t += gridDim.y * NT) {
+    const int r0 = d.amap_row[t];
+    const int r = r0 < ns ? r0 : r0 + ndin;
+    F[r + (size_t)d.amap_col[t] * f] += vals[d.amap_pos[t]];
+  }
+}
+
+// Extend-add of the q-th child of every front (one launch per child rank,
+// so that no two writers of a launch touch the same parent entry).
+__global__ void __launch_bounds__(NT)
+k_big_extend(DevicePlan d, const int* __restrict__ nodes, int q) {
+  if (big_skip(d)) return;
+  const int node = nodes[blockIdx.x];
+  const int q0 = d.kid_ptr[node];
+  if (q0 + q >= d.kid_ptr[node + 1]) return;
+  const int f = d.f[node], ns = d.ns[node], ndin = d.ndin[node];
+  int choff = ns;
+  for (int t = 0; t < q; t++) choff += d.ndel[d.kids[q0 + t]];
+  const int c = d.kids[q0 + q];
+  const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
+  const int cc = fc - npc, cb = d.cptr[c];
+  const double* C = d.fpool + d.foff[c];
+  double* F = d.fpool + d.foff[node];
+  for (int b = blockIdx.y; b < cc; b += gridDim.y) {
+    const int pb = child_row_pos(d, cb, ndc, choff, ns, ndin, b);
+    const double* Cb = C + (size_t)(npc + b) * fc + npc;
+    for (int a = b + threadIdx.x; a < cc; a += NT) {
+      const int pa = child_row_pos(d, cb, ndc, choff, ns, ndin, a);
+      const double v = Cb[a];
+      if (pa >= pb) F[pa + (size_t)pb * f] += v;
+      else F[pb + (size_t)pa * f] += v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(NT)
+k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
+            double pivot_tol) {
+  __shared__ Ctl ctl;
+  if (big_skip(d)) return;
+  const int node = nodes[blockIdx.x];
+  int* st = d.pstate + 4 * node;
+  int k = st[0], nc = st[1];
+  if (k >= nc) {
+    if (threadIdx.x == 0) st[3] = 0;
+    return;
+  }
+  const int f = d.f[node];
+  const int fs = d.ns[node] + d.ndin[node];
+  double* F = d.fpool + d.foff[node];
+  double* W = F + (size_t)f * f;
+  int* fvars = d.ipool + d.ioff[node];
+  const int kstart = k;
+  int kw = 0;
+  panel_factor(F, f, W, f, f, fs == f, fvars, fvars + f, ustab, pivot_tol,
+               d.status, ctl, k, nc, kw);
+  if (threadIdx.x == 0) {
+    st[0] = k;
+    st[1] = nc;
+    st[2] = kstart;
+    st[3] = kw;
+  }
+}
+
+__global__ void __launch_bounds__(NT)
+k_big_update(DevicePlan d, const int* __restrict__ nodes) {
+  extern __shared__ double tiles[];
+  if (big_skip(d)) return;
+  const int node = nodes[blockIdx.x];
+  const int* st = d.pstate + 4 * node;
+  const int k = st[0], kstart = st[2], kw = st[3];
+  if (kw == 0) return;
+  const int f = d.f[node];
+  const int m = f - k;
+  if (m <= 0) return;
+  double* F = d.fpool + d.foff[node];
+  const double* W = F + (size_t)f * f;
+  const int nt = (m + kTile - 1) / kTile;
+  const int ntiles = nt * (nt + 1) / 2;
+  for (int t = blockIdx.y; t < ntiles; t += gridDim.y) {
+    int ti, tj;
+    tile_coords(t, ti, tj);
+    update_tile(F, f, W, f, f, k, kstart, kw, ti, tj, tiles,
+                tiles + kTile * TP);
+  }
+}
+
+__global__ void __launch_bounds__(NT)
+k_big_finalize(DevicePlan d, const int* __restrict__ nodes) {
+  if (big_skip(d)) return;
+  const int node = nodes[blockIdx.x];
+  const int f = d.f[node];
+  const int fs = d.ns[node] + d.ndin[node];
+  const int npiv = d.pstate[4 * node + 1];
+  finish_front(d, node, d.fpool + d.foff[node], f, fs, npiv,
+               d.ipool + d.ioff[node]);
+}
+
+// Number of large fronts of the level still holding candidates; 0 when a
+// pool ran out (the fronts stopped and the host grows the pool and
+// restarts the factorization).
+__global__ void k_big_remaining(DevicePlan d, const int* __restrict__ nodes,
+                                int count, int* out) {
+  int r = 0;
+  for (int i = threadIdx.x; i < count; i += blockDim.x) {
+    const int* st = d.pstate + 4 * nodes[i];
+    r += st[0] < st[1] ? 1 : 0;
+  }
+  for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  if (threadIdx.x == 0) *out = big_skip(d) ? 0 : r;
+}
+
 }  // namespace
 
 #define FCUDA(call)                                                       \
@@ -581,22 +795,96 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     FCUDA(cudaFuncSetAttribute(k_factor_level,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kMaxDynSmem));
+    FCUDA(cudaFuncSetAttribute(k_big_update,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kTileSmem * 8));
     attr_set = true;
   }
   FCUDA(cudaMemsetAsync(d.counters, 0, 2 * sizeof(unsigned long long), s));
   FCUDA(cudaMemsetAsync(d.inertia, 0, 2 * sizeof(int), s));
   FCUDA(cudaMemsetAsync(d.status, 0, sizeof(int), s));
+  // AMIGO_B200_TRACE=1 prints the device time of every level's small- and
+  // large-front phases to stderr (diagnostics only).
+  static const bool trace = std::getenv("AMIGO_B200_TRACE") != nullptr;
+  std::vector<cudaEvent_t> ev;
+  if (trace) {
+    ev.resize(3 * d.num_levels);
+    for (auto& e : ev) cudaEventCreate(&e);
+  }
   for (int l = 0; l < d.num_levels; l++) {
-    const int b = h.level_ptr[l], cnt = h.level_ptr[l + 1] - b;
-    if (cnt == 0) continue;
-    long long fm = h.level_max_f[l] + 16;
-    long long want = (fm * fm + fm * NB) * 8;
-    long long need_tiles = 2LL * kTile * NB * 8;
-    long long bytes = want < need_tiles ? need_tiles : want;
-    if (bytes > kMaxDynSmem) bytes = kMaxDynSmem;
-    k_factor_level<<<cnt, NT, (size_t)bytes, s>>>(
-        d, d.level_nodes + b, cnt, d_vals, h.ustab, h.pivot_tol,
-        (int)(bytes / 8));
+    const LevelSchedule& L = h.sched[l];
+    if (trace) cudaEventRecord(ev[3 * l], s);
+    if (L.nsmall) {
+      long long fm = L.small_max_f + 16;
+      long long bytes = (fm * fm + fm * NB) * 8;
+      if (bytes < (long long)kTileSmem * 8) bytes = (long long)kTileSmem * 8;
+      if (bytes > kMaxDynSmem) bytes = kMaxDynSmem;
+      k_factor_level<<<L.nsmall, NT, (size_t)bytes, s>>>(
+          d, d.sched_nodes + L.small_begin, L.nsmall, d_vals, h.ustab,
+          h.pivot_tol, (int)(bytes / 8));
+    }
+    if (trace) cudaEventRecord(ev[3 * l + 1], s);
+    if (L.nbig) {
+      const int* nodes = d.sched_nodes + L.big_begin;
+      const int B = L.nbig;
+      const long long fm = L.big_max_f;
+      int gz = (int)std::min<long long>(512, (fm * fm + 4095) / 4096);
+      int ga = (int)std::min<long long>(256, (L.big_max_amap + NT - 1) / NT);
+      int ge = (int)std::min<long long>(1024, fm);
+      k_big_setup<<<B, NT, 0, s>>>(d, nodes);
+      k_big_zero<<<dim3(B, std::max(gz, 1)), NT, 0, s>>>(d, nodes);
+      k_big_add_A<<<dim3(B, std::max(ga, 1)), NT, 0, s>>>(d, nodes, d_vals);
+      for (int q = 0; q < L.big_max_kids; q++)
+        k_big_extend<<<dim3(B, std::max(ge, 1)), NT, 0, s>>>(d, nodes, q);
+      const long long ntl = (fm + kTile - 1) / kTile;
+      int gu = (int)std::min<long long>(4 * 148, ntl * (ntl + 1) / 2);
+      int panels = (int)((L.big_max_fs + NB - 2) / (NB - 1)) + 2;
+      // Every panel consumes at least one candidate of every unfinished
+      // front, so no front needs more panels than it has rows.
+      long long budget = 0;
+      const long long max_panels = (long long)d.n + 8;
+      for (;;) {
+        budget += panels;
+        for (int it = 0; it < panels; it++) {
+          k_big_panel<<<B, NT, 0, s>>>(d, nodes, h.ustab, h.pivot_tol);
+          k_big_update<<<dim3(B, std::max(gu, 1)), NT, kTileSmem * 8, s>>>(
+              d, nodes);
+        }
+        // Delayed pivots received from the children can make a front need
+        // more panels than its static size implies: check and continue.
+        k_big_remaining<<<1, 32, 0, s>>>(d, nodes, B, d.scratch_int);
+        int left = 0;
+        FCUDA(cudaMemcpyAsync(&left, d.scratch_int, sizeof(int),
+                              cudaMemcpyDeviceToHost, s));
+        FCUDA(cudaStreamSynchronize(s));
+        if (left == 0) break;
+        if (budget > max_panels) {
+          std::fprintf(stderr, "amigo_b200: large-front panels did not finish\n");
+          return -6;
+        }
+        panels = 4;
+      }
+      k_big_finalize<<<B, NT, 0, s>>>(d, nodes);
+    }
+    if (trace) cudaEventRecord(ev[3 * l + 2], s);
+  }
+  if (trace) {
+    cudaStreamSynchronize(s);
+    float tot_s = 0.f, tot_b = 0.f;
+    for (int l = 0; l < d.num_levels; l++) {
+      float a = 0.f, b = 0.f;
+      cudaEventElapsedTime(&a, ev[3 * l], ev[3 * l + 1]);
+      cudaEventElapsedTime(&b, ev[3 * l + 1], ev[3 * l + 2]);
+      tot_s += a;
+      tot_b += b;
+      std::fprintf(stderr,
+                   "level %3d: small %5d (fmax %5d) %8.3f ms | large %4d "
+                   "(fmax %5d) %8.3f ms\n",
+                   l, h.sched[l].nsmall, h.sched[l].small_max_f, a,
+                   h.sched[l].nbig, h.sched[l].big_max_f, b);
+    }
+    std::fprintf(stderr, "total: small %.3f ms, large %.3f ms\n", tot_s, tot_b);
+    for (auto& e : ev) cudaEventDestroy(e);
   }
   FCUDA(cudaGetLastError());
   return 0;

@@ -27,6 +27,10 @@ namespace ab {
 // columns while kw < kPanel - 1 so that a 2x2 pivot still fits.
 constexpr int kPanel = 32;
 constexpr int kThreads = 256;
+// Dynamic shared memory of the one-CTA-per-front kernel; a front is
+// scheduled on that kernel when (f + 16)^2 + (f + 16) * kPanel doubles fit
+// (16 rows of slack for delayed pivots), otherwise on the multi-CTA path.
+constexpr int kMaxDynSmem = 190 * 1024;
 
 // Status bits written by device code.
 enum : int {
@@ -52,6 +56,7 @@ struct DevicePlan {
   int* amap_row = nullptr;     // static front row
   int* amap_col = nullptr;     // front column (< ns)
   int* level_nodes = nullptr;  // nodes sorted by level
+  int* sched_nodes = nullptr;  // per level: small fronts, then large fronts
   // dynamic, per factorization
   int* f = nullptr;            // front size
   int* npiv = nullptr;         // pivots eliminated
@@ -61,10 +66,19 @@ struct DevicePlan {
   long long* ioff = nullptr;   // offset of the var list in the int pool
   int* inertia = nullptr;      // [npos, nneg]
   int* status = nullptr;       // ST_* bits
+  int* pstate = nullptr;       // per node: k, candidates left, kstart, kw
+  int* scratch_int = nullptr;  // small device scratch for host queries
   unsigned long long* counters = nullptr;  // [F pool top, int pool top]
   double* fpool = nullptr;
   int* ipool = nullptr;
   long long fcap = 0, icap = 0;
+};
+
+// Per-level launch schedule (host side).
+struct LevelSchedule {
+  int small_begin = 0, nsmall = 0, big_begin = 0, nbig = 0;
+  int small_max_f = 0, big_max_f = 0, big_max_fs = 0, big_max_kids = 0;
+  long long big_max_amap = 0;
 };
 
 struct LdlHandle {
@@ -76,6 +90,7 @@ struct LdlHandle {
   std::vector<int> level_nodes;   // host copy
   std::vector<int> h_ns, h_nc;    // host copies of static sizes
   std::vector<int> level_max_f;   // static max front per level
+  std::vector<LevelSchedule> sched;
   long long f_static_total = 0;   // sum of static (f^2 + f*kPanel)
   long long i_static_total = 0;
   DevicePlan d;

@@ -145,6 +145,39 @@ int build_plan(LdlHandle& h, const int* rowp, const int* cols) {
     mark_front(k, 0);
   }
 
+  // Launch schedule: per level, the fronts that fit the shared-memory kernel
+  // (by static size) first, then the large ones.
+  std::vector<int> sched_nodes;
+  sched_nodes.reserve(nn);
+  h.sched.assign(L, LevelSchedule());
+  for (int l = 0; l < L; l++) {
+    LevelSchedule& S = h.sched[l];
+    std::vector<int> small, big;
+    for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++) {
+      const int k = h.level_nodes[q];
+      const long long f = h.h_ns[k] + h.h_nc[k];
+      const long long fm = f + 16;
+      if ((fm * fm + fm * kPanel) * 8 <= kMaxDynSmem) {
+        small.push_back(k);
+        S.small_max_f = std::max<int>(S.small_max_f, (int)f);
+      } else {
+        big.push_back(k);
+        S.big_max_f = std::max<int>(S.big_max_f, (int)f);
+        S.big_max_fs = std::max<int>(S.big_max_fs, h.h_ns[k]);
+        S.big_max_kids = std::max<int>(
+            S.big_max_kids, T.children_ptr[k + 1] - T.children_ptr[k]);
+        S.big_max_amap = std::max<long long>(
+            S.big_max_amap, (long long)amap_ptr[k + 1] - amap_ptr[k]);
+      }
+    }
+    S.small_begin = (int)sched_nodes.size();
+    S.nsmall = (int)small.size();
+    sched_nodes.insert(sched_nodes.end(), small.begin(), small.end());
+    S.big_begin = (int)sched_nodes.size();
+    S.nbig = (int)big.size();
+    sched_nodes.insert(sched_nodes.end(), big.begin(), big.end());
+  }
+
   std::vector<int> ns_v(h.h_ns), nc_v(h.h_nc);
   std::vector<int> kid_ptr(T.children_ptr.begin(), T.children_ptr.begin() + nn + 1);
   int rc = 0;
@@ -162,6 +195,9 @@ int build_plan(LdlHandle& h, const int* rowp, const int* cols) {
   rc |= upload(&d.amap_row, amap_row);
   rc |= upload(&d.amap_col, amap_col);
   rc |= upload(&d.level_nodes, h.level_nodes);
+  rc |= upload(&d.sched_nodes, sched_nodes);
+  rc |= zalloc(&d.pstate, 4 * (size_t)nn);
+  rc |= zalloc(&d.scratch_int, 4);
   rc |= zalloc(&d.f, nn);
   rc |= zalloc(&d.npiv, nn);
   rc |= zalloc(&d.ndel, nn);
@@ -186,7 +222,8 @@ void free_plan(LdlHandle& h) {
   DevicePlan& d = h.d;
   void* ptrs[] = {d.ns, d.nc, d.var_ptr, d.vars, d.cptr, d.crows, d.cmap,
                   d.kid_ptr, d.kids, d.amap_ptr, d.amap_pos, d.amap_row,
-                  d.amap_col, d.level_nodes, d.f, d.npiv, d.ndel, d.ndin,
+                  d.amap_col, d.level_nodes, d.sched_nodes, d.pstate,
+                  d.scratch_int, d.f, d.npiv, d.ndel, d.ndin,
                   d.foff, d.ioff, d.inertia, d.status, d.counters, d.fpool,
                   d.ipool, h.ubuf, h.uoff};
   for (void* p : ptrs)

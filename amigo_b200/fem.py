@@ -1,0 +1,63 @@
+"""Device-side models for the component evaluation kernels (fem2d.cu)."""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import Simp2DStruct
+from .linalg import _stream_ptr
+
+
+class Simp2DDevice:
+    """Uploads a problems.simp2d.Simp2D model's index maps and constants."""
+
+    def __init__(self, model, device):
+        from .problems import simp2d as S
+        self.model = model
+        self.device = torch.device(device)
+        t = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).to(self.device)
+        colors = model.color_lists()
+        cptr = np.cumsum([0] + [len(c) for c in colors])
+        self._keep = dict(
+            color_elems=t(np.concatenate(colors), np.int32),
+            ev=t(model.ev, np.int32), fv=t(model.fv, np.int32),
+            epos=t(model.epos, np.int32), fpos=t(model.fpos, np.int32),
+            vpos=t(model.vpos, np.int32), spos=t(model.spos, np.int32),
+            fixed=t(model.fixed, np.int32),
+            fixed_zero_pos=t(model.fixed_zero_pos, np.int32),
+            fixed_diag_pos=t(model.fixed_diag_pos, np.int32),
+            load_idx=t(np.nonzero(model.f[model.u0:model.u0 + 2 * model.nnodes])[0],
+                       np.int32),
+            load_val=t(model.f[model.u0:model.u0 + 2 * model.nnodes][
+                np.nonzero(model.f[model.u0:model.u0 + 2 * model.nnodes])[0]],
+                np.float64),
+            K0=t(model.K0, np.float64), A=t(model.A, np.float64),
+        )
+        k = self._keep
+        st = Simp2DStruct()
+        st.n, st.nnz, st.nelems, st.nnodes = model.n, model.nnz, model.nelems, model.nnodes
+        st.u0, st.rt0, st.re0, st.s_index = model.u0, model.rt0, model.re0, model.s0
+        st.lam0, st.mu0, st.nu_index = model.lam0, model.mu0, model.nu0
+        for i in range(5):
+            st.color_ptr[i] = int(cptr[i])
+        for name in ("color_elems", "ev", "fv", "epos", "fpos", "vpos", "spos",
+                     "fixed", "fixed_zero_pos", "fixed_diag_pos", "load_idx",
+                     "load_val", "K0", "A"):
+            setattr(st, name, k[name].data_ptr())
+        st.nfixed = len(model.fixed)
+        st.nfixed_zero = len(model.fixed_zero_pos)
+        st.nload = int(k["load_idx"].numel())
+        st.Bq = 0.25
+        st.vcoef = 1.0 / model.nelems
+        st.volfrac = model.volfrac
+        st.E0, st.Emin, st.penalty = S.E0, S.EMIN, S.PENALTY
+        self.st = st
+
+    def gradient(self, x, alpha, grad):
+        _lib.call("ab_simp2d_gradient", ctypes.byref(self.st), x.data_ptr(),
+                  float(alpha), grad.data_ptr(), _stream_ptr(self.device))
+
+    def hessian(self, x, alpha, vals):
+        _lib.call("ab_simp2d_hessian", ctypes.byref(self.st), x.data_ptr(),
+                  float(alpha), vals.data_ptr(), _stream_ptr(self.device))

@@ -1,0 +1,474 @@
+"""Benchmark: the IPM numeric core on the 2D SIMP compliance KKT (128 x 64).
+
+One step = one interior-point iteration's numeric core on the full-space 2D
+SIMP KKT system (n = 58,504, nnz = 2.24e6), all on the GPU:
+  Hessian of the Lagrangian scattered into the CSR KKT values, barrier
+  diagonal + delta_w added, multifrontal LDL^T factorization with the
+  inertia read back, condensed residual, solve, one iterative-refinement
+  step (K p, residual, correction solve), bound-dual back-substitution,
+  fraction-to-boundary step length, step application, gradient.
+`value` is the KKT factorization throughput in TFLOP/s: the algorithmic
+factor flops of the step (sum over fronts of p^3/3 + p^2 c + p c^2) divided
+by the device time of the whole step.  `e2e` is the same metric through the
+public SparseLDL API with the KKT values and right-hand side starting in
+host memory and the solution copied back every step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun each rank runs an independent replica on its own GPU
+(the path does not shard); the device time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("IPM solves/s & KKT factor TFLOP/s, mixed vs FP64 GPU at 1e-8 err; "
+          "p50/p99 latency")
+WORKLOAD = "2D SIMP compliance 128x64 full-space KKT, one IPM iteration core"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=128)
+    ap.add_argument("--ny", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def config(args, world):
+    return {"workload": WORKLOAD, "n": None, "nnz": None,
+            "mesh": "%dx%d" % (args.nx, args.ny), "ordering": "AMD",
+            "precision": "fp64", "parallelism": "replicas%d" % world,
+            "l2": "256 MiB buffer written between timed steps"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, path, index):
+        self.path = path
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines()]
+            sm = [float(r[0]) for r in rows if r[0].strip().isdigit()]
+            mx = max(float(r[1]) for r in rows)
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                     "sw_power_cap"]
+            reasons = sorted({names[k] for r in rows for k in range(4)
+                              if r[4 + k].strip() == "Active"})
+            return {"sm_mhz": float(np.median(sm)) if sm else None,
+                    "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+
+
+# --------------------------------------------------------------- our arm
+class Core:
+    """The IPM iteration numeric core on one GPU (see module docstring)."""
+
+    def __init__(self, device, nx, ny):
+        import torch
+        from amigo_b200 import linalg
+        from amigo_b200.fem import Simp2DDevice
+        from amigo_b200.ipm import InteriorPointOptimizer
+        from amigo_b200.problems.simp2d import Simp2D
+        self.torch = torch
+        self.dev = device
+        m = Simp2D(nx, ny)
+        self.m = m
+        self.fem = Simp2DDevice(m, device)
+        self.K = linalg.CSRMat(m.n, m.n, m.rowp, m.cols, device=device)
+        self.ldl = linalg.SparseLDL(self.K, ustab=0.01, pivot_tol=1e-14,
+                                    order=linalg.OrderingType.AMD)
+        self.opt = InteriorPointOptimizer(m.mult, m.lower, m.upper, device=device)
+        self.opt.relax_bounds()
+        f64 = dict(dtype=torch.float64, device=device)
+        self.x = torch.from_numpy(m.initial_point()).to(device)
+        self.vars = self.opt.create_opt_vector(self.x)
+        self.opt.initialize_multipliers_and_slacks(0.1, None, self.vars)
+        self.grad = torch.zeros(m.n, **f64)
+        self.res = torch.zeros(m.n, **f64)
+        self.diag = torch.zeros(m.n, **f64)
+        self.px = torch.zeros(m.n, **f64)
+        self.r2 = torch.zeros(m.n, **f64)
+        self.kp = torch.zeros(m.n, **f64)
+        self.upd = self.opt.create_opt_vector()
+        self.tmp = self.opt.create_opt_vector()
+        self.primal = torch.from_numpy(~m.mult).to(device)
+        self.mu = 0.1
+        self.fem.gradient(self.x, 1.0, self.grad)
+        self.flops = None
+        self.launches = None
+
+    def step(self):
+        torch = self.torch
+        m, opt, v = self.m, self.opt, self.vars
+        self.fem.hessian(v.x, 1.0, self.K.vals)
+        opt.compute_diagonal(v, self.diag)
+        self.diag.add_(self.primal, alpha=1e-8)
+        self.K.add_diagonal(self.diag)
+        self.ldl.factor()
+        inertia = self.ldl.get_inertia()
+        opt.compute_residual(self.mu, v, self.grad, self.res)
+        self.px.copy_(self.res)
+        self.ldl.solve_device(self.px)
+        # one refinement step on the condensed system
+        self.K.mult(self.px, self.kp)
+        torch.sub(self.res, self.kp, out=self.r2)
+        self.ldl.solve_device(self.r2)
+        self.px.add_(self.r2)
+        opt.compute_update(self.mu, v, self.px, self.upd)
+        ax, xi, az, zi = opt.compute_max_step(0.99, v, self.upd)
+        opt.apply_step_update(ax, az, v, self.upd, self.tmp)
+        self.fem.gradient(self.tmp.x, 1.0, self.grad)
+        return inertia
+
+
+def count_launches(core):
+    """Kernels of ours launched per step: element kernels, IPM kernels, the
+    factor (one per level) and the solves (two per level, two solves)."""
+    st = core.ldl.stats()
+    L = st["levels"]
+    hess = 4 + 1 + 2          # colours + global + fixed rows/diagonal
+    grad = 4 + 1 + 1
+    ipm = 1 + 1 + 1 + 2 + 1   # diagonal, residual, bound-dual, max-step (2), apply
+    csr = 1 + 1               # add_diagonal, matvec
+    return hess + grad + ipm + csr + L + 2 * (2 * L)
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    core = Core(device, args.nx, args.ny)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
+    for _ in range(args.warmup):
+        core.step()
+    torch.cuda.synchronize()
+    st = core.ldl.stats()
+    flops = st["flops"]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    fev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    clk = ClockSampler(os.path.join(ROOT, "gpurun_out" if os.path.isdir(
+        os.path.join(ROOT, "gpurun_out")) else ".", "clocks_rank%d.csv" % rank), local)
+    t0 = time.time()
+    with clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+            # factor timing inside the step (same stream)
+            core.fem.hessian(core.vars.x, 1.0, core.K.vals)
+            core.opt.compute_diagonal(core.vars, core.diag)
+            core.diag.add_(core.primal, alpha=1e-8)
+            core.K.add_diagonal(core.diag)
+            fev[k][0].record(stream)
+            core.ldl.factor()
+            fev[k][1].record(stream)
+            core.ldl.get_inertia()
+            opt, v = core.opt, core.vars
+            opt.compute_residual(core.mu, v, core.grad, core.res)
+            core.px.copy_(core.res)
+            core.ldl.solve_device(core.px)
+            core.K.mult(core.px, core.kp)
+            torch.sub(core.res, core.kp, out=core.r2)
+            core.ldl.solve_device(core.r2)
+            core.px.add_(core.r2)
+            opt.compute_update(core.mu, v, core.px, core.upd)
+            ax, xi, az, zi = opt.compute_max_step(0.99, v, core.upd)
+            opt.apply_step_update(ax, az, v, core.upd, core.tmp)
+            core.fem.gradient(core.tmp.x, 1.0, core.grad)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    wall = time.time() - t0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    fac_ms = [a.elapsed_time(b) for a, b in fev]
+    dev_ms = float(np.sum(step_ms))
+    fac_tot = float(np.sum(fac_ms))
+    if world > 1:
+        t = torch.tensor([dev_ms, fac_tot], device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        dev_ms, fac_tot = float(t[0]), float(t[1])
+    value = world * flops * args.steps / (dev_ms * 1e-3) / 1e12
+
+    # e2e through the public API with host buffers
+    e2e = run_e2e(core, args, device)
+
+    out = {
+        "metric": METRIC,
+        "value": round(value, 6),
+        "unit": "TFLOP/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(dev_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: 2D SIMP KKT at the seeded initial point",
+        "config": dict(config(args, world), n=core.m.n, nnz=core.m.nnz),
+        "factor_flops_per_step": flops,
+        "factor_ms_per_step": round(fac_tot / args.steps, 4),
+        "ipm_iterations_per_s": round(world * args.steps / (dev_ms * 1e-3), 3),
+        "wall_s": round(wall, 3),
+        "e2e": e2e,
+        "gpu_launches": count_launches(core) * args.steps,
+        "clocks": clk.summary(),
+        "ldl_stats": st,
+    }
+    out["roofline"] = roofline(core, fac_tot / args.steps)
+    return out
+
+
+def roofline(core, fac_ms):
+    """Dominant kernel: the per-level front factorization.  Algorithmic
+    bytes of one factorization: 8 (c(c+1)/2 child-contribution read +
+    f p factor write + c(c+1)/2 contribution write) per front + 12 nnz(A)."""
+    ldl = core.ldl
+    h = ldl._h
+    npiv, ndel = ldl.node_pivots()
+    sym = ldl.symbolic()
+    ns = np.diff(sym["node_ptr"])
+    nc = np.diff(sym["contrib_ptr"])
+    # front sizes: pivots + delayed out + contribution rows; delayed in are
+    # the children's delayed out
+    kids_ptr, kids = sym["children_ptr"], sym["children"]
+    ndin = np.zeros(len(ns))
+    for k in range(len(ns)):
+        ndin[k] = ndel[kids[kids_ptr[k]:kids_ptr[k + 1]]].sum()
+    f = ns + ndin + nc
+    p = npiv.astype(float)
+    c = f - p
+    bytes_ = (8 * (c * (c + 1) / 2 + f * p + c * (c + 1) / 2)).sum() + 12 * core.m.nnz
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = bytes_ / (fac_ms * 1e-3) / 1e9
+    del h
+    return {"kernel": "k_factor_level (all levels of one factorization)",
+            "bound": "hbm", "achieved": round(achieved, 2),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5),
+            "traffic": None,
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "algorithmic_bytes_per_launch_set": float(bytes_)}
+
+
+def run_e2e(core, args, device):
+    import torch
+    m = core.m
+    # KKT values and rhs in pinned host memory, copied in every step
+    core.fem.hessian(core.vars.x, 1.0, core.K.vals)
+    core.K.add_diagonal(core.diag)
+    hvals = core.K.vals.cpu().pin_memory()
+    hrhs = core.res.cpu().pin_memory()
+    hx = torch.empty_like(hrhs).pin_memory()
+    flops = core.ldl.stats()["flops"]
+    steps = max(3, args.steps // 2)
+    stream = torch.cuda.current_stream()
+    for _ in range(2):
+        core.K.vals.copy_(hvals, non_blocking=True)
+        core.ldl.factor()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(steps):
+        core.K.vals.copy_(hvals, non_blocking=True)
+        core.ldl.factor()
+        core.ldl.get_inertia()
+        core.px.copy_(hrhs, non_blocking=True)
+        core.ldl.solve_device(core.px)
+        hx.copy_(core.px, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / steps
+    return {"value": round(flops / (ms * 1e-3) / 1e12, 6), "unit": "TFLOP/s",
+            "ms_per_step": round(ms, 4),
+            "h2d_bytes_per_step": int(8 * (m.nnz + m.n)),
+            "d2h_bytes_per_step": int(8 * m.n)}
+
+
+# ---------------------------------------------------------- reference arm
+def kkt_values_host(nx, ny):
+    """The same KKT matrix on the host (reference-arm input), from the
+    numpy restatement of the model at the same initial point and the same
+    barrier diagonal as the GPU step's first factorization."""
+    from amigo_b200.problems.simp2d import Simp2D
+    from oracle import simp2d_oracle as O
+    m = Simp2D(nx, ny)
+    x = m.initial_point()
+    vals = O.hessian_values(m, x)
+    lb, ub = m.lower.copy(), m.upper.copy()
+    prim = ~m.mult
+    for arr, sgn in ((lb, -1.0), (ub, 1.0)):
+        fin = np.isfinite(arr) & prim
+        arr[fin] += sgn * np.minimum(1e-4, 1e-8 * np.maximum(1.0, np.abs(arr[fin])))
+    d = np.zeros(m.n)
+    fl = np.isfinite(lb) & prim
+    fu = np.isfinite(ub) & prim
+    d[fl] += 1.0 / (x[fl] - lb[fl]).clip(1e-2)
+    d[fu] += 1.0 / (ub[fu] - x[fu]).clip(1e-2)
+    d[prim] += 1e-8
+    vals[m.diag_pos] += d
+    vals[m.fixed_diag_pos] = 1.0
+    return m, vals
+
+
+def run_reference_timed(nx, ny, max_seconds, warmup=1, steps=None):
+    """The reference's own SparseLDL (oracle/_ref: include/sparse_ldl.h built
+    from the reference sources) on this host's cores: factor + solve."""
+    from oracle import ref
+    m, vals = kkt_values_host(nx, ny)
+    cores = os.cpu_count() or 1
+    ref.set_blas_threads(1)
+    R = ref.RefSparseLDL(m.n, m.rowp, m.cols, order="AMD")
+    b = np.ones(m.n)
+    for _ in range(warmup):
+        R.factor(vals)
+        R.solve(b)
+    times = []
+    t_end = time.time() + max_seconds
+    while (steps is None and time.time() < t_end) or (steps is not None and len(times) < steps):
+        t = time.time()
+        R.factor(vals)
+        R.solve(b)
+        times.append(time.time() - t)
+        if steps is None and len(times) >= 20:
+            break
+    npiv, ndel = R.node_pivots()
+    return m, np.array(times), R, cores
+
+
+def factor_flops_from_ref(R):
+    sym = R.symbolic()
+    npiv, ndel = R.node_pivots()
+    ns = np.diff(sym["node_ptr"]).astype(float)
+    nc = np.diff(sym["contrib_ptr"]).astype(float)
+    kp, kids = sym["children_ptr"], sym["children"]
+    ndin = np.array([ndel[kids[kp[k]:kp[k + 1]]].sum() for k in range(len(ns))])
+    f = ns + ndin + nc
+    p = npiv.astype(float)
+    c = f - p
+    return float((p ** 3 / 3 + p * p * c + p * c * c).sum())
+
+
+def cpu_baseline():
+    m, times, R, cores = run_reference_timed(128, 64, max_seconds=12.0)
+    flops = factor_flops_from_ref(R)
+    med = float(np.median(times))
+    return {"value": round(flops / med / 1e12, 6), "unit": "TFLOP/s",
+            "cores": cores, "kind": "reference",
+            "sample": "%d factor+solve runs of the 2D SIMP 128x64 KKT with the "
+                      "reference SparseLDL (AMD, OpenMP tree tasks, 1 BLAS "
+                      "thread), median %.3f s" % (len(times), med)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    m, times, R, cores = run_reference_timed(args.nx, args.ny, max_seconds=120.0,
+                                             warmup=max(1, min(args.warmup, 2)),
+                                             steps=min(args.steps, 10))
+    flops = factor_flops_from_ref(R)
+    tot = float(np.sum(times))
+    value = flops * len(times) / tot / 1e12
+    return {
+        "metric": METRIC, "impl": "reference", "value": round(value, 6),
+        "unit": "TFLOP/s", "n_gpus": world, "steps": len(times),
+        "warmup": args.warmup, "ms_per_step": round(1e3 * tot / len(times), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic: 2D SIMP KKT at the seeded initial point",
+        "config": dict(config(args, 1), n=m.n, nnz=m.nnz),
+        "cpu_baseline": {"value": round(value, 6), "unit": "TFLOP/s",
+                         "cores": cores, "kind": "reference",
+                         "sample": "reference SparseLDL factor+solve of the full "
+                                   "KKT, %d steps" % len(times)},
+        "e2e": {"value": round(value, 6), "unit": "TFLOP/s",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        torch.distributed.init_process_group(
+            backend, timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            out = run_reference(args, rank, world)
+        else:
+            out = run_ours(args, rank, world, local)
+            if rank == 0 and world == 1 and not args.no_cpu_baseline:
+                from oracle import ref
+                if ref.available():
+                    out["cpu_baseline"] = cpu_baseline()
+        if rank == 0 and out is not None:
+            print(json.dumps(out))
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

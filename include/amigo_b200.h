@@ -181,6 +181,31 @@ int ab_ipm_relax_bounds(int np, const double* lbx, const double* ubx,
 int ab_ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
                       double* zu, double* sl, double* su, double kappa1,
                       double kappa2, void* stream);
+/* Iterative refinement on the unreduced 8-block Newton system, the device
+ * form of DirectSparseSolver.iterative_refinement
+ * (amigo/algorithm/solvers/linear_solver.py:109-264).  rhs_saved is the
+ * condensed right-hand side of the first solve; grad, rhs_saved, px, kpx,
+ * e_cond, corr are n-vectors; dzl, dzu, e_zl, e_zu are np-vectors.
+ *  refine_init: initial dzl/dzu by back-substitution, out[0] = ||rhs||_inf
+ *    over the four blocks;
+ *  refine_residual: given kpx = K px, the block residuals, the condensed
+ *    correction rhs e_cond, out[0] = ||residual||_inf,
+ *    out[1] = max(||px||, ||dzl||, ||dzu||)_inf;
+ *  refine_update: dzl/dzu corrections from corr = K^-1 e_cond, px += corr. */
+int ab_ipm_refine_init(const ab_ipm_problem* p, const ab_ipm_state* s,
+                       double mu, const double* grad, const double* rhs_saved,
+                       const double* px, double* dzl, double* dzu, double* out,
+                       void* stream);
+int ab_ipm_refine_residual(const ab_ipm_problem* p, const ab_ipm_state* s,
+                           double mu, const double* grad,
+                           const double* rhs_saved, const double* kpx,
+                           const double* px, const double* dzl,
+                           const double* dzu, double* e_cond, double* e_zl,
+                           double* e_zu, double* out, void* stream);
+int ab_ipm_refine_update(const ab_ipm_problem* p, const ab_ipm_state* s,
+                         const double* corr, const double* e_zl,
+                         const double* e_zu, double* px, double* dzl,
+                         double* dzu, void* stream);
 /* reset_bound_multipliers (:508-522) */
 int ab_ipm_reset_bound_multipliers(const ab_ipm_problem* p,
                                    const ab_ipm_state* s, double mu,
@@ -205,6 +230,43 @@ int ab_csr_add_diagonal(int n, const int* diag_pos, const double* d,
  * (amigo/algorithm/solvers/linear_solver.py:196-200). */
 int ab_csr_matvec(int n, const int* rowp, const int* cols, const double* vals,
                   const double* x, double* y, void* stream);
+
+/* ----------------------------------------------------------------------
+ * Component evaluation for the 2D SIMP full-space model: gradient of the
+ * Lagrangian and its Hessian scattered into the CSR KKT values.  Replaces
+ * OptimizationProblem::gradient / hessian (include/optimization_problem.h:
+ * 742-762, 801-818) for that model's components.  All pointers are device
+ * pointers except color_ptr, which is held in the struct.
+ * -------------------------------------------------------------------- */
+typedef struct ab_simp2d {
+  int n, nnz, nelems, nnodes;
+  int u0, rt0, re0, s_index, lam0, mu0, nu_index;
+  int color_ptr[5];          /* element colour boundaries in color_elems */
+  const int* color_elems;    /* elements sorted by colour */
+  const int* ev;             /* [nelems x 20] u(8) rt(4) lam(8) indices */
+  const int* fv;             /* [nelems x 9] rt(4) re mu(4) indices */
+  const int* epos;           /* [nelems x 400] CSR positions of ev x ev */
+  const int* fpos;           /* [nelems x 81] CSR positions of fv x fv */
+  const int* vpos;           /* [nelems x 2] (re,nu), (nu,re) positions */
+  const int* spos;           /* [2] (s,nu), (nu,s) positions */
+  const int* fixed;          /* fixed variable indices */
+  const int* fixed_zero_pos; /* off-diagonal positions in fixed rows/cols */
+  const int* fixed_diag_pos; /* diagonal positions of fixed variables */
+  const int* load_idx;       /* load dof (relative to u0 / lam0) */
+  const double* load_val;
+  const double* K0;          /* 8x8 unit-modulus element stiffness */
+  const double* A;           /* 4x4 filter matrix M + r^2 K_lap */
+  int nfixed, nfixed_zero, nload;
+  double Bq, vcoef, volfrac, E0, Emin, penalty;
+} ab_simp2d;
+
+/* grad = nabla_x L(x) with objective weight alpha (fixed rows zeroed). */
+int ab_simp2d_gradient(const ab_simp2d* m, const double* x, double alpha,
+                       double* grad, void* stream);
+/* vals = nabla^2 L(x) on the KKT pattern (fixed rows/columns zeroed, unit
+ * diagonal). */
+int ab_simp2d_hessian(const ab_simp2d* m, const double* x, double alpha,
+                      double* vals, void* stream);
 
 #ifdef __cplusplus
 }
