@@ -51,6 +51,13 @@ class Simp2DStruct(ctypes.Structure):
                                      "penalty")])
 
 
+class CartPoleStruct(ctypes.Structure):
+    """Mirror of ab_cartpole (include/amigo_b200.h)."""
+    _fields_ = ([(k, _i) for k in ("n", "nnz", "N")]
+                + [(k, _d) for k in ("h", "M", "m", "l", "g")]
+                + [(k, _vp) for k in ("iv", "ipos", "bv", "bpos")])
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "ab_ldl_create": (_i, [_i, _ip, _ip, _i, _i, _d, _d, _d, ctypes.POINTER(_vp)]),
@@ -102,6 +109,8 @@ _SIGS = {
                                   _vp, _vp, _vp]),
     "ab_csr_add_diagonal": (_i, [_i, _vp, _vp, _vp, _vp]),
     "ab_csr_matvec": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ab_cartpole_gradient": (_i, [ctypes.POINTER(CartPoleStruct), _vp, _d, _vp, _vp]),
+    "ab_cartpole_hessian": (_i, [ctypes.POINTER(CartPoleStruct), _vp, _d, _vp, _vp]),
     "ab_simp2d_gradient": (_i, [ctypes.POINTER(Simp2DStruct), _vp, _d, _vp, _vp]),
     "ab_simp2d_hessian": (_i, [ctypes.POINTER(Simp2DStruct), _vp, _d, _vp, _vp]),
 }

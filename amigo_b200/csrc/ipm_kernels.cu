@@ -756,3 +756,4 @@ int ipm_refine_update(const ab_ipm_problem* p, const ab_ipm_state* s,
 long long ipm_scratch_doubles() { return (long long)kRedBlocks * 16 + 64; }
 
 }  // namespace ab
+

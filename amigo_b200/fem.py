@@ -61,3 +61,30 @@ class Simp2DDevice:
     def hessian(self, x, alpha, vals):
         _lib.call("ab_simp2d_hessian", ctypes.byref(self.st), x.data_ptr(),
                   float(alpha), vals.data_ptr(), _stream_ptr(self.device))
+
+
+class CartPoleDevice:
+    """Uploads a problems.cartpole.CartPole model's index maps."""
+
+    def __init__(self, model, device):
+        from ._lib import CartPoleStruct
+        from .problems import cartpole as C
+        self.model = model
+        self.device = torch.device(device)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.int32)).to(self.device)
+        self._keep = dict(iv=t(model.iv), ipos=t(model.ipos), bv=t(model.bv),
+                          bpos=t(model.bpos))
+        st = CartPoleStruct()
+        st.n, st.nnz, st.N = model.n, model.nnz, model.N
+        st.h, st.M, st.m, st.l, st.g = model.h, C.M_CART, model.m_pole, C.L_POLE, C.GRAV
+        for k, v in self._keep.items():
+            setattr(st, k, v.data_ptr())
+        self.st = st
+
+    def gradient(self, x, alpha, grad):
+        _lib.call("ab_cartpole_gradient", ctypes.byref(self.st), x.data_ptr(),
+                  float(alpha), grad.data_ptr(), _stream_ptr(self.device))
+
+    def hessian(self, x, alpha, vals):
+        _lib.call("ab_cartpole_hessian", ctypes.byref(self.st), x.data_ptr(),
+                  float(alpha), vals.data_ptr(), _stream_ptr(self.device))

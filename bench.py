@@ -54,6 +54,27 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(values, device=None):
+    """Element-wise maximum of a list of floats over all ranks (device times
+    are reported as the slowest rank's)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64,
+                     device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def replica_items(n_items, rank, world):
+    """Independent problems are split over ranks in contiguous blocks (the
+    replicas-only decomposition): returns this rank's [begin, end)."""
+    base, extra = divmod(n_items, world)
+    begin = rank * base + min(rank, extra)
+    return begin, begin + base + (1 if rank < extra else 0)
+
+
 def config(args, world):
     return {"workload": WORKLOAD, "n": None, "nnz": None,
             "mesh": "%dx%d" % (args.nx, args.ny), "ordering": "AMD",
@@ -235,10 +256,7 @@ def run_ours(args, rank, world, local):
     fac_ms = [a.elapsed_time(b) for a, b in fev]
     dev_ms = float(np.sum(step_ms))
     fac_tot = float(np.sum(fac_ms))
-    if world > 1:
-        t = torch.tensor([dev_ms, fac_tot], device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        dev_ms, fac_tot = float(t[0]), float(t[1])
+    dev_ms, fac_tot = max_over_ranks([dev_ms, fac_tot], device)
     value = world * flops * args.steps / (dev_ms * 1e-3) / 1e12
 
     # e2e through the public API with host buffers

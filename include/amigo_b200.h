@@ -268,6 +268,26 @@ int ab_simp2d_gradient(const ab_simp2d* m, const double* x, double alpha,
 int ab_simp2d_hessian(const ab_simp2d* m, const double* x, double alpha,
                       double* vals, void* stream);
 
+/* ----------------------------------------------------------------------
+ * Component evaluation for the cart-pole trapezoidal-collocation model
+ * (gradient and Hessian of the Lagrangian; exact derivatives by hyper-dual
+ * numbers).  Replaces OptimizationProblem::gradient / hessian for that
+ * model.  Device pointers except where noted.
+ * -------------------------------------------------------------------- */
+typedef struct ab_cartpole {
+  int n, nnz, N;
+  double h, M, m, l, g;
+  const int* iv;    /* [N x 14]: z_k (5), z_k+1 (5), defect multipliers (4) */
+  const int* ipos;  /* [N x 196] CSR positions of iv x iv */
+  const int* bv;    /* [2 x 8]: boundary states (4), multipliers (4) */
+  const int* bpos;  /* [2 x 64] CSR positions of bv x bv */
+} ab_cartpole;
+
+int ab_cartpole_gradient(const ab_cartpole* m, const double* x, double alpha,
+                         double* grad, void* stream);
+int ab_cartpole_hessian(const ab_cartpole* m, const double* x, double alpha,
+                        double* vals, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
