@@ -79,6 +79,9 @@ _SIGS = {
                                     _vp, _vp]),
     "ab_ipm_max_step": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
                              _d, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ab_ipm_max_step_noalloc": (_i, [ctypes.POINTER(IpmProblem),
+                                     ctypes.POINTER(IpmState), _d, _vp, _vp,
+                                     _vp, _vp, _vp, _vp]),
     "ab_ipm_apply_step": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
                                _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                _vp]),

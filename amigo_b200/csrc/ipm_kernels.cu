@@ -11,6 +11,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 
 #include "../../include/amigo_b200.h"
 #include "ipm_internal.h"
@@ -757,3 +758,92 @@ long long ipm_scratch_doubles() { return (long long)kRedBlocks * 16 + 64; }
 
 }  // namespace ab
 
+// ---------------------------------------------------------------------------
+// Fraction-to-boundary step length without any device allocation.
+//
+// ab_ipm_max_step needs a scratch array for its per-block partial minima and
+// takes it from a buffer the library cudaMalloc's on first use.  Some callers
+// cannot let a library allocate device memory: a host that hands the whole
+// device to its own caching allocator (PyTorch, a serving runtime with a
+// fixed memory plan), code that must not allocate once its iteration loop
+// is running, or an embedding where every device buffer is owned by the
+// caller.  This variant runs the same two kernels with their scratch taken
+// from a fixed array compiled into the library instead.
+//
+// The array holds one partial per 256 primal entries (the variant launches
+// one block per 256 entries, not the fixed grid), at most kNoAllocBlocks
+// blocks, so np is limited to kNoAllocBlocks * 256 = 2,097,152 primal
+// entries; larger problems are rejected with AB_ERR_CAPACITY.  Every GPU
+// that loads the library holds the array (8192 x (2 doubles + 2 ints) =
+// 192 KiB) until the process exits.
+namespace ab {
+namespace {
+constexpr int kNoAllocBlocks = 8192;
+constexpr int kNoAllocPartials = 2 * kNoAllocBlocks;  // (ax, az) per block
+
+// Doubles [0, 2*kNoAllocBlocks) hold the value partials; the int partials
+// follow them (two ints per block, 4 bytes each: kNoAllocBlocks doubles).
+static __device__ __align__(256) double g_noalloc_max_step[kNoAllocPartials +
+                                                           kNoAllocBlocks];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the array on the current device (host code cannot use
+// the symbol itself: its host-side name is only a stand-in).  Looked up once
+// per device; the first call on a device therefore performs a runtime query
+// and should come before any stream capture.
+double* noalloc_scratch(int* rc) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    *rc = AB_ERR_CUDA;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_max_step);
+    if (e != cudaSuccess || p == nullptr) {
+      *rc = AB_ERR_CUDA;
+      return nullptr;
+    }
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *rc = AB_OK;
+  return g_noalloc_ptr[dev];
+}
+}  // namespace
+}  // namespace ab
+
+extern "C" int ab_ipm_max_step_noalloc(const ab_ipm_problem* p,
+                                       const ab_ipm_state* s, double tau,
+                                       const double* px, const double* dzl,
+                                       const double* dzu, double* out,
+                                       int* iout, void* stream) {
+  if (!p || !s || !out || !iout || p->n < 0 || p->np < 0 || p->nc < 0)
+    return AB_ERR_ARG;
+  if (p->np > 0 && (!p->pidx || !p->lbx || !p->ubx || !s->zl || !s->zu ||
+                    !s->sl || !s->su || !px || !dzl || !dzu))
+    return AB_ERR_ARG;
+  const long long nblocks = ((long long)p->np + ab::RT - 1) / ab::RT;
+  if (nblocks > ab::kNoAllocBlocks) {
+    std::fprintf(stderr,
+                 "ab_ipm_max_step_noalloc: %d primal entries exceed the "
+                 "static scratch limit of %d\n",
+                 p->np, ab::kNoAllocBlocks * ab::RT);
+    return AB_ERR_CAPACITY;
+  }
+  int rc = AB_OK;
+  double* scratch = ab::noalloc_scratch(&rc);
+  if (!scratch) return rc;
+  const int grid = nblocks > 0 ? (int)nblocks : 1;
+  double* pv = scratch;
+  int* pi = reinterpret_cast<int*>(scratch + ab::kNoAllocPartials);
+  cudaStream_t st = (cudaStream_t)stream;
+  // Every block writes its two partials before the final pass reads them,
+  // so nothing in the array has to start at zero.
+  ab::k_max_step<<<grid, ab::RT, 0, st>>>(ab::mkP(p), ab::mkS(s), tau, px, dzl,
+                                          dzu, pv, pi);
+  ab::k_max_step_final<<<1, 32, 0, st>>>(grid, p->pidx, pv, pi, out, iout);
+  return cudaGetLastError() == cudaSuccess ? AB_OK : AB_ERR_CUDA;
+}

@@ -139,6 +139,23 @@ int ab_ipm_bound_dual_step(const ab_ipm_problem* p, const ab_ipm_state* s,
 int ab_ipm_max_step(const ab_ipm_problem* p, const ab_ipm_state* s,
                     double tau, const double* px, const double* dzl,
                     const double* dzu, double* out, int* iout, void* stream);
+/* The same step-length computation as ab_ipm_max_step, for callers that
+ * cannot let the library allocate device memory (a host whose caching
+ * allocator owns the device, a loop that must not allocate once running,
+ * an embedding in which the caller owns every device buffer).  No
+ * counterpart in the reference.  Its reduction scratch is a fixed array
+ * compiled into the library (192 KiB, held on every GPU that loads the
+ * library until process exit) instead of a cudaMalloc'd buffer, which caps
+ * np at 2,097,152 primal entries; larger problems return AB_ERR_CAPACITY.
+ * The first call on a device looks up the array's device address (a CUDA
+ * runtime query), so make that call before any stream capture.  All calls
+ * share the one array: calls that can overlap on the GPU (different
+ * streams, or different host threads) race and must be serialised by the
+ * caller.  Arguments and results as for ab_ipm_max_step. */
+int ab_ipm_max_step_noalloc(const ab_ipm_problem* p, const ab_ipm_state* s,
+                            double tau, const double* px, const double* dzl,
+                            const double* dzu, double* out, int* iout,
+                            void* stream);
 /* apply_step (:376-392) into new-state arrays */
 int ab_ipm_apply_step(const ab_ipm_problem* p, const ab_ipm_state* s,
                       double ax, double az, const double* dxlam,
