@@ -70,6 +70,10 @@ _SIGS = {
     "ab_ldl_solve": (_i, [_vp, _vp, _i, _i, _vp]),
     "ab_ldl_stats": (_i, [_vp, _vp, _dp, _dp, _ip, _ip, _ip]),
     "ab_ldl_node_pivots": (_i, [_vp, _vp, _ip, _ip]),
+    "ab_ldl_batch_create": (_i, [_i, _ip, ctypes.POINTER(_ip), ctypes.POINTER(_ip),
+                                 _i, _i, _d, _d, _d, ctypes.POINTER(_vp)]),
+    "ab_ldl_batch_inertia": (_i, [_vp, _vp, _ip, _ip]),
+    "ab_ldl_batch_sizes": (_i, [_vp, _ip, _ip, ctypes.POINTER(ctypes.c_longlong)]),
     "ab_ipm_residual": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
                              _d, _vp, _vp, _vp, _vp]),
     "ab_ipm_diagonal": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
@@ -114,6 +118,7 @@ _SIGS = {
     "ab_csr_matvec": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ab_cartpole_gradient": (_i, [ctypes.POINTER(CartPoleStruct), _vp, _d, _vp, _vp]),
     "ab_cartpole_hessian": (_i, [ctypes.POINTER(CartPoleStruct), _vp, _d, _vp, _vp]),
+    "ab_cartpole_objective": (_i, [ctypes.POINTER(CartPoleStruct), _vp, _vp, _vp]),
     "ab_simp2d_gradient": (_i, [ctypes.POINTER(Simp2DStruct), _vp, _d, _vp, _vp]),
     "ab_simp2d_hessian": (_i, [ctypes.POINTER(Simp2DStruct), _vp, _d, _vp, _vp]),
 }

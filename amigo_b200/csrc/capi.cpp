@@ -3,6 +3,7 @@
 
 #include <cstdio>
 #include <new>
+#include <vector>
 
 #include "../../include/amigo_b200.h"
 #include "ldl_internal.h"
@@ -125,21 +126,164 @@ int ab_ldl_factor(ab_ldl_t H, const double* d_vals, void* stream) {
   return ab::factor_numeric(H->h, d_vals, (cudaStream_t)stream);
 }
 
-int ab_ldl_inertia(ab_ldl_t H, void* stream, int* npos, int* nneg) {
+int ab_ldl_batch_inertia(ab_ldl_t H, void* stream, int* npos, int* nneg) {
   if (!H || !npos || !nneg) return AB_ERR_ARG;
   if (!H->h.factored) return AB_ERR_NOT_FACTORED;
+  const int np = H->h.d.nprob;
   if (H->h.sym.n == 0) {
-    *npos = *nneg = 0;
+    for (int p = 0; p < np; p++) npos[p] = nneg[p] = 0;
     return AB_OK;
   }
-  int v[2];
+  std::vector<int> v(2 * (size_t)np);
   cudaStream_t s = (cudaStream_t)stream;
-  if (cudaMemcpyAsync(v, H->h.d.inertia, 2 * sizeof(int),
+  if (cudaMemcpyAsync(v.data(), H->h.d.inertia, 2 * sizeof(int) * np,
                       cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
     return AB_ERR_CUDA;
-  *npos = v[0];
-  *nneg = v[1];
+  for (int p = 0; p < np; p++) {
+    npos[p] = v[2 * p];
+    nneg[p] = v[2 * p + 1];
+  }
+  return AB_OK;
+}
+
+int ab_ldl_inertia(ab_ldl_t H, void* stream, int* npos, int* nneg) {
+  if (!H || !npos || !nneg) return AB_ERR_ARG;
+  if (!H->h.factored) return AB_ERR_NOT_FACTORED;
+  const int np = H->h.has_plan ? H->h.d.nprob : 1;
+  std::vector<int> a(np), b(np);
+  int rc = ab_ldl_batch_inertia(H, stream, a.data(), b.data());
+  if (rc != AB_OK) return rc;
+  *npos = *nneg = 0;
+  for (int p = 0; p < np; p++) {
+    *npos += a[p];
+    *nneg += b[p];
+  }
+  return AB_OK;
+}
+
+// Merge per-problem symbolic trees into one block-diagonal tree: node,
+// variable and contribution indices are offset, every problem keeps its own
+// (reference-identical) ordering and supernodes, and the roots of all
+// problems are listed at the tail of the children array.
+static void merge_trees(const std::vector<ab::SymbolicTree>& P,
+                        ab::SymbolicTree& M, std::vector<int>& node_ptr_p,
+                        std::vector<int>& var_ptr_p) {
+  M = ab::SymbolicTree();
+  int n = 0, nn = 0, nc = 0;
+  node_ptr_p.assign(1, 0);
+  var_ptr_p.assign(1, 0);
+  for (const auto& T : P) {
+    n += T.n;
+    nn += T.num_nodes;
+    nc += (int)T.contrib_rows.size();
+    node_ptr_p.push_back(nn);
+    var_ptr_p.push_back(n);
+  }
+  M.n = n;
+  M.num_nodes = nn;
+  M.permuted = true;
+  M.invperm.reserve(n);
+  M.node_ptr.assign(1, 0);
+  M.node_to_var.reserve(n);
+  M.contrib_ptr.assign(1, 0);
+  M.contrib_rows.reserve(nc);
+  M.node_parent.reserve(nn);
+  std::vector<int> kids_of(nn + 1, 0);  // counts per parent
+  std::vector<int> roots;
+  for (size_t p = 0; p < P.size(); p++) {
+    const auto& T = P[p];
+    const int vo = var_ptr_p[p], no = node_ptr_p[p];
+    for (int i = 0; i < T.n; i++) M.invperm.push_back(vo + T.invperm[i]);
+    for (int k = 0; k < T.num_nodes; k++)
+      M.node_ptr.push_back(vo + T.node_ptr[k + 1]);
+    for (int v : T.node_to_var) M.node_to_var.push_back(vo + v);
+    const int cbase = M.contrib_ptr.back();
+    for (int k = 0; k < T.num_nodes; k++)
+      M.contrib_ptr.push_back(cbase + T.contrib_ptr[k + 1]);
+    for (int r : T.contrib_rows) M.contrib_rows.push_back(vo + r);
+    for (int k = 0; k < T.num_nodes; k++) {
+      const int par = T.node_parent[k];
+      M.node_parent.push_back(par >= 0 ? no + par : -1);
+    }
+  }
+  // children lists: same construction as the per-problem ones
+  M.children_ptr.assign(nn + 2, 0);
+  M.children.assign(nn, 0);
+  for (int i = 0; i < nn; i++)
+    M.children_ptr[(M.node_parent[i] != -1 ? M.node_parent[i] : nn) + 1]++;
+  for (int i = 0; i < nn + 1; i++) M.children_ptr[i + 1] += M.children_ptr[i];
+  std::vector<int> fill(M.children_ptr.begin(), M.children_ptr.end() - 1);
+  for (int i = 0; i < nn; i++) {
+    const int slot = M.node_parent[i] != -1 ? M.node_parent[i] : nn;
+    M.children[fill[slot]++] = i;
+  }
+  (void)kids_of;
+  (void)roots;
+}
+
+int ab_ldl_batch_create(int nprob, const int* n, const int* const* rowp,
+                        const int* const* cols, int order, int solver_type,
+                        double ustab, double pivot_tol, double delay_growth,
+                        ab_ldl_t* out) {
+  if (!out || nprob < 1 || !n || !rowp || !cols) return AB_ERR_ARG;
+  *out = nullptr;
+  if (solver_type != 0) return AB_ERR_UNSUPPORTED;
+  if (order != ab::ORDER_ND && order != ab::ORDER_AMD &&
+      order != ab::ORDER_NATURAL)
+    return AB_ERR_UNSUPPORTED;
+  for (int p = 0; p < nprob; p++) {
+    if (n[p] < 1 || !rowp[p] || !cols[p]) return AB_ERR_ARG;
+    for (int i = 0; i < n[p]; i++)
+      for (int q = rowp[p][i]; q < rowp[p][i + 1]; q++)
+        if (cols[p][q] < 0 || cols[p][q] >= n[p]) return AB_ERR_ARG;
+  }
+  ab_ldl* H = new (std::nothrow) ab_ldl;
+  if (!H) return AB_ERR_CAPACITY;
+  ab::LdlHandle& h = H->h;
+  if (ustab > 0.5) ustab = 0.5;
+  if (ustab < 0.0) ustab = 0.0;
+  if (delay_growth < 1.0) delay_growth = 1.0;
+  if (delay_growth > 10.0) delay_growth = 10.0;
+  h.ustab = ustab;
+  h.pivot_tol = pivot_tol;
+  h.delay_growth = delay_growth;
+  h.order = order;
+  if (cudaGetDevice(&h.device) != cudaSuccess) {
+    delete H;
+    return AB_ERR_CUDA;
+  }
+  std::vector<ab::SymbolicTree> trees(nprob);
+  for (int p = 0; p < nprob; p++)
+    ab::analyze(order, n[p], rowp[p], cols[p], trees[p]);
+  merge_trees(trees, h.sym, h.prob_node_ptr, h.prob_var_ptr);
+  // block-diagonal CSR of all problems
+  std::vector<int> mr(1, 0), mc;
+  h.prob_nnz_ptr.assign(1, 0);
+  for (int p = 0; p < nprob; p++) {
+    const int vo = h.prob_var_ptr[p];
+    const int base = mr.back();
+    for (int i = 0; i < n[p]; i++) mr.push_back(base + rowp[p][i + 1]);
+    for (int q = 0; q < rowp[p][n[p]]; q++) mc.push_back(vo + cols[p][q]);
+    h.prob_nnz_ptr.push_back(mr.back());
+  }
+  h.has_plan = true;
+  int rc = ab::build_plan(h, mr.data(), mc.data());
+  if (rc != 0) {
+    ab::free_plan(h);
+    delete H;
+    return rc;
+  }
+  *out = H;
+  return AB_OK;
+}
+
+int ab_ldl_batch_sizes(ab_ldl_t H, int* nprob, int* n_total,
+                       long long* nnz_total) {
+  if (!H) return AB_ERR_ARG;
+  if (nprob) *nprob = H->h.has_plan ? H->h.d.nprob : 1;
+  if (n_total) *n_total = H->h.sym.n;
+  if (nnz_total) *nnz_total = H->h.has_plan ? H->h.d.nnz : 0;
   return AB_OK;
 }
 

@@ -142,10 +142,36 @@ __global__ void k_cartpole_bc(ab_cartpole m, const double* __restrict__ x,
   }
 }
 
+// Objective alpha * sum_k h/2 (u_k^2 + u_k+1^2), one block, fixed order.
+__global__ void k_cartpole_objective(ab_cartpole m, const double* x,
+                                     double* out) {
+  __shared__ double part[256];
+  double acc = 0.0;
+  for (int k = threadIdx.x; k < m.N; k += blockDim.x) {
+    const int* iv = m.iv + 14 * k;
+    const double u0 = x[iv[4]], u1 = x[iv[9]];
+    acc += 0.5 * m.h * (u0 * u0 + u1 * u1);
+  }
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = part[0];
+}
+
 }  // namespace
 }  // namespace ab
 
 extern "C" {
+
+int ab_cartpole_objective(const ab_cartpole* m, const double* x, double* out,
+                          void* stream) {
+  if (!m || !x || !out) return AB_ERR_ARG;
+  ab::k_cartpole_objective<<<1, 256, 0, (cudaStream_t)stream>>>(*m, x, out);
+  return cudaGetLastError() == cudaSuccess ? AB_OK : AB_ERR_CUDA;
+}
 
 int ab_cartpole_gradient(const ab_cartpole* m, const double* x, double alpha,
                          double* grad, void* stream) {

@@ -33,19 +33,25 @@ namespace {
 constexpr int NT = kThreads;
 constexpr int NB = kPanel;
 constexpr int NWARP = NT / 32;
+// Threads of the one-CTA panel kernel of the large-front path: each
+// candidate column is brought up to date by one thread per row, so more
+// threads shorten every candidate step.
+constexpr int kPanelThreads = 1024;
 constexpr int kTile = 64;
 
-struct Ctl {
+template <int BT>
+struct CtlT {
   double wrow[NB];     // row k (or imax) of W, columns 0..kw-1
-  double red_v[NWARP];
-  int red_i[NWARP];
-  double red_v2[NWARP];
+  double red_v[(BT / 32)];
+  int red_i[(BT / 32)];
+  double red_v2[(BT / 32)];
   double abswik, ctail, rowmax;
   int imax;
   int f, fs, ns, ndin, npiv;
   long long foff, ioff;
   int skip;
 };
+using Ctl = CtlT<NT>;
 
 // Lexicographic "larger |value|, then smaller index" -- the first maximum,
 // which is what BLAS idamax returns.
@@ -59,7 +65,8 @@ __device__ __forceinline__ void argmax_merge(double& v, int& i, double v2,
 
 // Block-wide first-argmax of (v, i) plus a max of v2.  Result is written to
 // ctl.red_v[0], ctl.red_i[0], ctl.red_v2[0].
-__device__ void block_argmax(Ctl& ctl, double v, int i, double v2) {
+template <int BT>
+__device__ void block_argmax(CtlT<BT>& ctl, double v, int i, double v2) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int o = 16; o > 0; o >>= 1) {
     double ov = __shfl_down_sync(0xffffffffu, v, o);
@@ -75,9 +82,9 @@ __device__ void block_argmax(Ctl& ctl, double v, int i, double v2) {
   }
   __syncthreads();
   if (warp == 0) {
-    v = lane < NWARP ? ctl.red_v[lane] : -1.0;
-    i = lane < NWARP ? ctl.red_i[lane] : 0x7fffffff;
-    v2 = lane < NWARP ? ctl.red_v2[lane] : 0.0;
+    v = lane < (BT / 32) ? ctl.red_v[lane] : -1.0;
+    i = lane < (BT / 32) ? ctl.red_i[lane] : 0x7fffffff;
+    v2 = lane < (BT / 32) ? ctl.red_v2[lane] : 0.0;
     for (int o = 16; o > 0; o >>= 1) {
       double ov = __shfl_down_sync(0xffffffffu, v, o);
       int oi = __shfl_down_sync(0xffffffffu, i, o);
@@ -97,23 +104,24 @@ __device__ void block_argmax(Ctl& ctl, double v, int i, double v2) {
 // Symmetric interchange of rows/columns a < b of the lower triangle of F,
 // of the variable list and of the fully-summed permutation record
 // (reference: symm_swap, include/sparse_ldl.h:1252-1274).
+template <int BT>
 __device__ void symm_swap(double* F, int ld, int n, int* vars, int* fsperm,
                           int a, int b) {
   const int tid = threadIdx.x;
   // rows a and b over columns [0, a)
-  for (int j = tid; j < a; j += NT) {
+  for (int j = tid; j < a; j += BT) {
     double t = F[a + (size_t)j * ld];
     F[a + (size_t)j * ld] = F[b + (size_t)j * ld];
     F[b + (size_t)j * ld] = t;
   }
   // F[j, a] <-> F[b, j] for a < j < b
-  for (int j = a + 1 + tid; j < b; j += NT) {
+  for (int j = a + 1 + tid; j < b; j += BT) {
     double t = F[j + (size_t)a * ld];
     F[j + (size_t)a * ld] = F[b + (size_t)j * ld];
     F[b + (size_t)j * ld] = t;
   }
   // F[j, a] <-> F[j, b] for j > b
-  for (int j = b + 1 + tid; j < n; j += NT) {
+  for (int j = b + 1 + tid; j < n; j += BT) {
     double t = F[j + (size_t)a * ld];
     F[j + (size_t)a * ld] = F[j + (size_t)b * ld];
     F[j + (size_t)b * ld] = t;
@@ -132,8 +140,9 @@ __device__ void symm_swap(double* F, int ld, int n, int* vars, int* fsperm,
 }
 
 // Swap rows a and b of W over columns [0, ncol).
+template <int BT>
 __device__ void swap_wrows(double* W, int ldw, int ncol, int a, int b) {
-  for (int j = threadIdx.x; j < ncol; j += NT) {
+  for (int j = threadIdx.x; j < ncol; j += BT) {
     double t = W[a + (size_t)j * ldw];
     W[a + (size_t)j * ldw] = W[b + (size_t)j * ldw];
     W[b + (size_t)j * ldw] = t;
@@ -234,13 +243,14 @@ __device__ void trailing_update(double* F, int ld, const double* W, int ldw,
 //           -> ctl.ctail.
 //   mode 1: column imax; src(r) = F[imax, r] for r < imax else F[r, imax];
 //           reduces max over [k, n) \ {imax} -> ctl.rowmax.
+template <int BT>
 __device__ void build_column(double* F, int ld, double* W, int ldw, int n,
                              int k, int kstart, int kw, int col, int mode,
-                             int imax, int nc, Ctl& ctl, int* status) {
+                             int imax, int nc, CtlT<BT>& ctl, int* status) {
   const int tid = threadIdx.x;
   double bestv = -1.0, tailv = 0.0;
   int besti = 0x7fffffff;
-  for (int r = k + tid; r < n; r += NT) {
+  for (int r = k + tid; r < n; r += BT) {
     double acc;
     if (mode == 0) {
       acc = F[r + (size_t)k * ld];
@@ -258,7 +268,7 @@ __device__ void build_column(double* F, int ld, double* W, int ldw, int n,
       if (r != imax) tailv = fmax(tailv, a);
     }
   }
-  block_argmax(ctl, bestv, besti, tailv);
+  block_argmax<BT>(ctl, bestv, besti, tailv);
   if (tid == 0) {
     if (mode == 0) {
       int im = ctl.red_i[0];
@@ -279,8 +289,9 @@ __device__ void build_column(double* F, int ld, double* W, int ldw, int n,
 }
 
 // Load row `row` of W (columns 0..kw-1) into ctl.wrow.
-__device__ void load_wrow(const double* W, int ldw, int row, int kw, Ctl& ctl) {
-  for (int j = threadIdx.x; j < kw; j += NT) ctl.wrow[j] = W[row + (size_t)j * ldw];
+template <int BT>
+__device__ void load_wrow(const double* W, int ldw, int row, int kw, CtlT<BT>& ctl) {
+  for (int j = threadIdx.x; j < kw; j += BT) ctl.wrow[j] = W[row + (size_t)j * ldw];
   __syncthreads();
 }
 
@@ -289,17 +300,18 @@ __device__ void load_wrow(const double* W, int ldw, int row, int kw, Ctl& ctl) {
 // on while kw < NB - 1, each either eliminated (1x1 or 2x2, its L column(s)
 // written to F and its L*D column(s) kept in W) or delayed to the end of the
 // candidate set.  The trailing update of F[k:, k:] is left to the caller.
+template <int BT>
 __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
                              bool root, int* vars, int* fsperm, double ustab,
-                             double pivot_tol, int* status, Ctl& ctl, int& k_,
+                             double pivot_tol, int* status, CtlT<BT>& ctl, int& k_,
                              int& nc_, int& kw_) {
   const int tid = threadIdx.x;
   const double bk_alpha = (1.0 + sqrt(17.0)) / 8.0;
   int k = k_, nc = nc_, kw = 0;
   const int kstart = k;
   while (kw < NB - 1 && k < nc) {
-    load_wrow(W, ldw, k, kw, ctl);
-    build_column(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status);
+    load_wrow<BT>(W, ldw, k, kw, ctl);
+    build_column<BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status);
     const double wkk = W[k + (size_t)kw * ldw];
     const double abswkk = fabs(wkk);
     const int imax = ctl.imax;
@@ -312,13 +324,13 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
         step = 1;
         kpiv = k;
       } else if (k + 1 < nc) {
-        load_wrow(W, ldw, imax, kw, ctl);
-        build_column(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
+        load_wrow<BT>(W, ldw, imax, kw, ctl);
+        build_column<BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
         const double rowmax = ctl.rowmax;
         const double wii = W[imax + (size_t)(kw + 1) * ldw];
         const double abswii = fabs(wii);
         if (abswii >= pivot_tol && abswii >= ustab * rowmax) {
-          for (int r = k + tid; r < n; r += NT)
+          for (int r = k + tid; r < n; r += BT)
             W[r + (size_t)kw * ldw] = W[r + (size_t)(kw + 1) * ldw];
           __syncthreads();
           step = 1;
@@ -347,15 +359,15 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
         step = 1;
         kpiv = k;
       } else {
-        load_wrow(W, ldw, imax, kw, ctl);
-        build_column(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
+        load_wrow<BT>(W, ldw, imax, kw, ctl);
+        build_column<BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
         const double rowmax = ctl.rowmax;
         const double abswii = fabs(W[imax + (size_t)(kw + 1) * ldw]);
         if (abswkk >= bk_alpha * colmax * (colmax / rowmax)) {
           step = 1;
           kpiv = k;
         } else if (abswii >= bk_alpha * rowmax) {
-          for (int r = k + tid; r < n; r += NT)
+          for (int r = k + tid; r < n; r += BT)
             W[r + (size_t)kw * ldw] = W[r + (size_t)(kw + 1) * ldw];
           __syncthreads();
           step = 1;
@@ -370,8 +382,8 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
     if (step == 0) {
       // Delay candidate k: move it to the end of the candidate set.
       if (k < nc - 1) {
-        symm_swap(F, ld, n, vars, fsperm, k, nc - 1);
-        swap_wrows(W, ldw, kw, k, nc - 1);
+        symm_swap<BT>(F, ld, n, vars, fsperm, k, nc - 1);
+        swap_wrows<BT>(W, ldw, kw, k, nc - 1);
         __syncthreads();
       }
       nc -= 1;
@@ -379,15 +391,16 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
     }
     const int ksrc = k + step - 1;
     if (kpiv != ksrc) {
-      symm_swap(F, ld, n, vars, fsperm, ksrc, kpiv);
-      swap_wrows(W, ldw, kw + step, ksrc, kpiv);
+      symm_swap<BT>(F, ld, n, vars, fsperm, ksrc, kpiv);
+      swap_wrows<BT>(W, ldw, kw + step, ksrc, kpiv);
       __syncthreads();
     }
     if (step == 1) {
       const double d = W[k + (size_t)kw * ldw];
       if (!isfinite(d) && tid == 0) atomicOr(status, ST_NAN);
       const double dinv = zero_pivot ? 0.0 : 1.0 / d;
-      for (int r = k + tid; r < n; r += NT) {
+      if (tid == 0) vars[3 * ld + k] = 0;  // 1x1 pivot
+      for (int r = k + tid; r < n; r += BT) {
         double w = W[r + (size_t)kw * ldw];
         F[r + (size_t)k * ld] = (r == k) ? w : w * dinv;
       }
@@ -399,7 +412,7 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
       if (!isfinite(detinv) && tid == 0) atomicOr(status, ST_NAN);
       const double i00 = d22 * detinv, i10 = -d21 * detinv,
                    i01 = -d21 * detinv, i11 = d11 * detinv;
-      for (int r = k + 2 + tid; r < n; r += NT) {
+      for (int r = k + 2 + tid; r < n; r += BT) {
         double w0 = W[r + (size_t)kw * ldw], w1 = W[r + (size_t)(kw + 1) * ldw];
         F[r + (size_t)k * ld] = w0 * i00 + w1 * i10;
         F[r + (size_t)(k + 1) * ld] = w0 * i01 + w1 * i11;
@@ -410,6 +423,10 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
         F[k + 1 + (size_t)(k + 1) * ld] = d22;
         vars[k] = -(vars[k] + 1);
         vars[k + 1] = -(vars[k + 1] + 1);
+        // pivot kinds (first / second column of a 2x2 block), used by the
+        // inertia count and the solves; vars has ld rows per section
+        vars[3 * ld + k] = 1;
+        vars[3 * ld + k + 1] = 2;
       }
     }
     __syncthreads();
@@ -432,8 +449,8 @@ __device__ int factor_front(double* F, int ld, double* W, int ldw, int n,
   while (k < nc) {
     const int kstart = k;
     int kw = 0;
-    panel_factor(F, ld, W, ldw, n, root, vars, fsperm, ustab, pivot_tol,
-                 status, ctl, k, nc, kw);
+    panel_factor<NT>(F, ld, W, ldw, n, root, vars, fsperm, ustab, pivot_tol,
+                     status, ctl, k, nc, kw);
     trailing_update(F, ld, W, ldw, n, k, kstart, kw, tiles);
     __syncthreads();
   }
@@ -521,42 +538,54 @@ __device__ __forceinline__ int child_row_pos(const DevicePlan& d, int cb,
   return r0 < ns ? r0 : r0 + ndin;
 }
 
-// Inertia of the D blocks, scanned in pivot order as the reference does
-// (include/sparse_ldl.h:1937-1968); also records the pivot kinds (0: 1x1,
-// 1/2: first/second column of a 2x2 block) and the inverse of the
-// fully-summed permutation, both used by the solves.
+// Inertia of the D blocks with the reference's rule
+// (include/sparse_ldl.h:1937-1968), from the pivot kinds recorded when each
+// pivot was accepted (0: 1x1, 1/2: first/second column of a 2x2 block),
+// plus the inverse of the fully-summed permutation used by the solves.
 __device__ void finish_front(const DevicePlan& d, int node, const double* F,
                              int f, int fs, int npiv, int* fvars) {
+  __shared__ int s_pos, s_neg;
   const int tid = threadIdx.x;
   const int* fsperm = fvars + f;
   int* fsinv = fvars + 2 * f;
-  int* kind = fvars + 3 * f;
-  for (int r = tid; r < fs; r += NT) fsinv[fsperm[r]] = r;
+  const int* kind = fvars + 3 * f;
   if (tid == 0) {
-    int pos = 0, neg = 0;
-    for (int j = 0; j < npiv;) {
-      if (fvars[j] >= 0) {
-        if (F[j + (size_t)j * f] >= 0.0) pos++; else neg++;
-        kind[j] = 0;
-        j += 1;
+    s_pos = 0;
+    s_neg = 0;
+  }
+  for (int r = tid; r < fs; r += blockDim.x) fsinv[fsperm[r]] = r;
+  __syncthreads();
+  int pos = 0, neg = 0;
+  for (int j = tid; j < npiv; j += blockDim.x) {
+    const int kd = kind[j];
+    if (kd == 0) {
+      if (F[j + (size_t)j * f] >= 0.0) pos++; else neg++;
+    } else if (kd == 1) {
+      const double d11 = F[j + (size_t)j * f];
+      const double d21 = F[j + 1 + (size_t)j * f];
+      const double d22 = F[j + 1 + (size_t)(j + 1) * f];
+      const double det = d11 * d22 - d21 * d21;
+      if (det >= 0.0) {
+        if (d11 >= 0.0) pos += 2; else neg += 2;
       } else {
-        kind[j] = 1;
-        kind[j + 1] = 2;
-        const double d11 = F[j + (size_t)j * f];
-        const double d21 = F[j + 1 + (size_t)j * f];
-        const double d22 = F[j + 1 + (size_t)(j + 1) * f];
-        const double det = d11 * d22 - d21 * d21;
-        if (det >= 0.0) {
-          if (d11 >= 0.0) pos += 2; else neg += 2;
-        } else {
-          pos++;
-          neg++;
-        }
-        j += 2;
+        pos++;
+        neg++;
       }
     }
-    atomicAdd(&d.inertia[0], pos);
-    atomicAdd(&d.inertia[1], neg);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    pos += __shfl_down_sync(0xffffffffu, pos, o);
+    neg += __shfl_down_sync(0xffffffffu, neg, o);
+  }
+  if ((tid & 31) == 0 && (pos || neg)) {
+    atomicAdd(&s_pos, pos);
+    atomicAdd(&s_neg, neg);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int pb = d.node_prob ? d.node_prob[node] : 0;
+    atomicAdd(&d.inertia[2 * pb], s_pos);
+    atomicAdd(&d.inertia[2 * pb + 1], s_neg);
     d.npiv[node] = npiv;
     d.ndel[node] = fs - npiv;
   }
@@ -699,10 +728,10 @@ k_big_extend(DevicePlan d, const int* __restrict__ nodes, int q) {
   }
 }
 
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(kPanelThreads)
 k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
             double pivot_tol) {
-  __shared__ Ctl ctl;
+  __shared__ CtlT<kPanelThreads> ctl;
   if (big_skip(d)) return;
   const int node = nodes[blockIdx.x];
   int* st = d.pstate + 4 * node;
@@ -718,7 +747,7 @@ k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
   int* fvars = d.ipool + d.ioff[node];
   const int kstart = k;
   int kw = 0;
-  panel_factor(F, f, W, f, f, fs == f, fvars, fvars + f, ustab, pivot_tol,
+  panel_factor<kPanelThreads>(F, f, W, f, f, fs == f, fvars, fvars + f, ustab, pivot_tol,
                d.status, ctl, k, nc, kw);
   if (threadIdx.x == 0) {
     st[0] = k;
@@ -801,7 +830,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     attr_set = true;
   }
   FCUDA(cudaMemsetAsync(d.counters, 0, 2 * sizeof(unsigned long long), s));
-  FCUDA(cudaMemsetAsync(d.inertia, 0, 2 * sizeof(int), s));
+  FCUDA(cudaMemsetAsync(d.inertia, 0, 2 * sizeof(int) * d.nprob, s));
   FCUDA(cudaMemsetAsync(d.status, 0, sizeof(int), s));
   // AMIGO_B200_TRACE=1 prints the device time of every level's small- and
   // large-front phases to stderr (diagnostics only).
@@ -846,7 +875,8 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       for (;;) {
         budget += panels;
         for (int it = 0; it < panels; it++) {
-          k_big_panel<<<B, NT, 0, s>>>(d, nodes, h.ustab, h.pivot_tol);
+          k_big_panel<<<B, kPanelThreads, 0, s>>>(d, nodes, h.ustab,
+                                                  h.pivot_tol);
           k_big_update<<<dim3(B, std::max(gu, 1)), NT, kTileSmem * 8, s>>>(
               d, nodes);
         }

@@ -64,7 +64,9 @@ struct DevicePlan {
   int* ndin = nullptr;         // delayed pivots received from children
   long long* foff = nullptr;   // offset of F in the FP64 pool
   long long* ioff = nullptr;   // offset of the var list in the int pool
-  int* inertia = nullptr;      // [npos, nneg]
+  int* inertia = nullptr;      // [npos, nneg] per problem
+  int* node_prob = nullptr;    // problem of each node (batched handles)
+  int nprob = 1;
   int* status = nullptr;       // ST_* bits
   int* pstate = nullptr;       // per node: k, candidates left, kstart, kw
   int* scratch_int = nullptr;  // small device scratch for host queries
@@ -91,6 +93,10 @@ struct LdlHandle {
   std::vector<int> h_ns, h_nc;    // host copies of static sizes
   std::vector<int> level_max_f;   // static max front per level
   std::vector<LevelSchedule> sched;
+  // Batched handles: node, variable and CSR-entry ranges of every problem
+  // (empty for a single problem).
+  std::vector<int> prob_node_ptr, prob_var_ptr;
+  std::vector<long long> prob_nnz_ptr;
   long long f_static_total = 0;   // sum of static (f^2 + f*kPanel)
   long long i_static_total = 0;
   DevicePlan d;

@@ -51,6 +51,13 @@ int build_plan(LdlHandle& h, const int* rowp, const int* cols) {
   const SymbolicTree& T = h.sym;
   const int n = T.n, nn = T.num_nodes;
   DevicePlan& d = h.d;
+  d.nprob = std::max(1, (int)h.prob_node_ptr.size() - 1);
+  if (d.nprob > 1) {
+    std::vector<int> np(nn);
+    for (int p = 0; p < d.nprob; p++)
+      for (int k = h.prob_node_ptr[p]; k < h.prob_node_ptr[p + 1]; k++) np[k] = p;
+    if (upload(&d.node_prob, np)) return -2;
+  }
   d.n = n;
   d.nn = nn;
   d.nnz = rowp[n];
@@ -204,7 +211,7 @@ int build_plan(LdlHandle& h, const int* rowp, const int* cols) {
   rc |= zalloc(&d.ndin, nn);
   rc |= zalloc(&d.foff, nn);
   rc |= zalloc(&d.ioff, nn);
-  rc |= zalloc(&d.inertia, 2);
+  rc |= zalloc(&d.inertia, 2 * (size_t)std::max(d.nprob, 1));
   rc |= zalloc(&d.status, 1);
   rc |= zalloc(&d.counters, 2);
   if (rc) return -2;
@@ -224,7 +231,8 @@ void free_plan(LdlHandle& h) {
                   d.kid_ptr, d.kids, d.amap_ptr, d.amap_pos, d.amap_row,
                   d.amap_col, d.level_nodes, d.sched_nodes, d.pstate,
                   d.scratch_int, d.f, d.npiv, d.ndel, d.ndin,
-                  d.foff, d.ioff, d.inertia, d.status, d.counters, d.fpool,
+                  d.foff, d.ioff, d.inertia, d.node_prob, d.status,
+                  d.counters, d.fpool,
                   d.ipool, h.ubuf, h.uoff};
   for (void* p : ptrs)
     if (p) cudaFree(p);

@@ -14,7 +14,9 @@
 // of one level run concurrently without atomics.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
+#include <vector>
 
 #include "ldl_internal.h"
 
@@ -36,7 +38,9 @@ __device__ __forceinline__ int block_end(const int* kind, int jb, int npiv) {
 
 __global__ void __launch_bounds__(NT)
 k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
-                int nrhs, int ldx, double* ubuf, const long long* uoff) {
+                int nrhs, int ldx, double* ubuf, const long long* uoff,
+                int smem_doubles) {
+  extern __shared__ double sV[];
   const int node = nodes[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int f = d.f[node], npiv = d.npiv[node];
@@ -47,9 +51,14 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
   const int* kind = fvars + 3 * f;
   const double* L = d.fpool + d.foff[node];
   __shared__ int s_choff;
+  __shared__ double sL[(SB + 1) * (SB + 1)];
 
   for (int rhs = 0; rhs < nrhs; rhs++) {
-    double* V = ubuf + uoff[node] + (long long)rhs * f;
+    // The front vector is worked on in shared memory when it fits (every
+    // step of the in-block triangular solve depends on the previous one);
+    // its tail is stored in ubuf for the parent.
+    double* G = ubuf + uoff[node] + (long long)rhs * f;
+    double* V = f <= smem_doubles ? sV : G;
     double* xr = x + (long long)rhs * ldx;
     for (int r = tid; r < f; r += NT) V[r] = 0.0;
     __syncthreads();
@@ -81,9 +90,17 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
       __syncthreads();
     }
 
-    // Forward elimination with the unit lower factor.
+    // Forward elimination with the unit lower factor.  The diagonal block
+    // of each column block is staged in shared memory first, so that the
+    // dependent steps of the warp's triangular solve read no global memory.
     for (int jb = 0; jb < npiv;) {
       const int je = block_end(kind, jb, npiv);
+      const int bw = je - jb;
+      for (int t = tid; t < bw * bw; t += NT) {
+        const int i = t % bw, j = t / bw;
+        sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
+      }
+      __syncthreads();
       if (warp == 0) {
         for (int j = jb; j < je;) {
           const bool two = kind[j] == 1;
@@ -91,8 +108,8 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
           const double v1 = two ? V[j + 1] : 0.0;
           const int i0 = j + (two ? 2 : 1);
           for (int i = i0 + lane; i < je; i += 32) {
-            double t = L[i + (size_t)j * f] * v0;
-            if (two) t += L[i + (size_t)(j + 1) * f] * v1;
+            double t = sL[(i - jb) + (j - jb) * (SB + 1)] * v0;
+            if (two) t += sL[(i - jb) + (j + 1 - jb) * (SB + 1)] * v1;
             V[i] -= t;
           }
           __syncwarp();
@@ -125,13 +142,17 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
     }
     __syncthreads();
     for (int j = tid; j < npiv; j += NT) xr[decode_var(fvars[j])] = V[j];
+    if (V != G)
+      for (int r = npiv + tid; r < f; r += NT) G[r] = V[r];
     __syncthreads();
   }
 }
 
 __global__ void __launch_bounds__(NT)
 k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
-                 int nrhs, int ldx, double* ubuf, const long long* uoff) {
+                 int nrhs, int ldx, double* ubuf, const long long* uoff,
+                 int smem_doubles) {
+  extern __shared__ double sV[];
   const int node = nodes[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NWARP = NT / 32;
@@ -139,9 +160,13 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
   const int* fvars = d.ipool + d.ioff[node];
   const int* kind = fvars + 3 * f;
   const double* L = d.fpool + d.foff[node];
+  __shared__ double sL[(SB + 1) * (SB + 1)];
   for (int rhs = 0; rhs < nrhs; rhs++) {
-    double* V = ubuf + uoff[node] + (long long)rhs * f;
+    double* V = f <= smem_doubles ? sV : ubuf + uoff[node] + (long long)rhs * f;
     double* xr = x + (long long)rhs * ldx;
+    // pivots: their forward values (written to x by the forward sweep);
+    // delayed and contribution rows: final values of the ancestors
+    for (int r = tid; r < npiv; r += NT) V[r] = xr[decode_var(fvars[r])];
     for (int r = npiv + tid; r < f; r += NT) V[r] = xr[fvars[r]];
     __syncthreads();
     // Column blocks from the last one backwards.
@@ -157,6 +182,11 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
         if (lane == 0) V[j] -= acc;
       }
+      const int bw = je - jb;
+      for (int t = tid; t < bw * bw; t += NT) {
+        const int i = t % bw, j = t / bw;
+        sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
+      }
       __syncthreads();
       if (warp == 0) {
         // within the block, backwards: column j (or pair j-1, j)
@@ -166,8 +196,8 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
           // rows strictly inside the block below this pivot
           double a0 = 0.0, a1 = 0.0;
           for (int i = j + 1 + lane; i < je; i += 32) {
-            a0 += L[i + (size_t)jl * f] * V[i];
-            if (two) a1 += L[i + (size_t)j * f] * V[i];
+            a0 += sL[(i - jb) + (jl - jb) * (SB + 1)] * V[i];
+            if (two) a1 += sL[(i - jb) + (j - jb) * (SB + 1)] * V[i];
           }
           for (int o = 16; o > 0; o >>= 1) {
             a0 += __shfl_down_sync(0xffffffffu, a0, o);
@@ -221,15 +251,37 @@ int solve_numeric(LdlHandle& h, double* d_x, int nrhs, int ldx,
                           cudaMemcpyHostToDevice, s));
     h.uoff_nrhs = nrhs;
   }
+  static bool attr_set = false;
+  if (!attr_set) {
+    SCUDA(cudaFuncSetAttribute(k_solve_forward,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kMaxDynSmem));
+    SCUDA(cudaFuncSetAttribute(k_solve_backward,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kMaxDynSmem));
+    attr_set = true;
+  }
+  // shared memory per level: the largest front vector of the level
+  std::vector<int> smem(d.num_levels, 0);
+  for (int l = 0; l < d.num_levels; l++) {
+    int fm = 0;
+    for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++)
+      fm = std::max(fm, h.h_f[h.level_nodes[q]]);
+    long long bytes = (long long)fm * 8;
+    smem[l] = (int)std::min<long long>(bytes, kMaxDynSmem);
+  }
   for (int l = 0; l < d.num_levels; l++) {
     const int b = h.level_ptr[l], cnt = h.level_ptr[l + 1] - b;
-    if (cnt) k_solve_forward<<<cnt, NT, 0, s>>>(d, d.level_nodes + b, d_x, nrhs,
-                                                ldx, h.ubuf, h.uoff);
+    if (cnt)
+      k_solve_forward<<<cnt, NT, smem[l], s>>>(d, d.level_nodes + b, d_x, nrhs,
+                                               ldx, h.ubuf, h.uoff, smem[l] / 8);
   }
   for (int l = d.num_levels - 1; l >= 0; l--) {
     const int b = h.level_ptr[l], cnt = h.level_ptr[l + 1] - b;
-    if (cnt) k_solve_backward<<<cnt, NT, 0, s>>>(d, d.level_nodes + b, d_x,
-                                                 nrhs, ldx, h.ubuf, h.uoff);
+    if (cnt)
+      k_solve_backward<<<cnt, NT, smem[l], s>>>(d, d.level_nodes + b, d_x,
+                                                nrhs, ldx, h.ubuf, h.uoff,
+                                                smem[l] / 8);
   }
   SCUDA(cudaGetLastError());
   return 0;

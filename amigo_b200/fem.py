@@ -88,3 +88,7 @@ class CartPoleDevice:
     def hessian(self, x, alpha, vals):
         _lib.call("ab_cartpole_hessian", ctypes.byref(self.st), x.data_ptr(),
                   float(alpha), vals.data_ptr(), _stream_ptr(self.device))
+
+    def objective(self, x, out):
+        _lib.call("ab_cartpole_objective", ctypes.byref(self.st), x.data_ptr(),
+                  out.data_ptr(), _stream_ptr(self.device))

@@ -1,0 +1,263 @@
+"""A primal-dual interior-point loop over the device numeric core.
+
+amigo's own driver (amigo/algorithm/ipm_driver.py:109-483) is Python that
+calls its numeric core; this module is a compact driver of the same shape
+for running whole solves on the GPU: residual and KKT error, monotone
+barrier update (the reference's "monotone" strategy: reduce mu when
+E_mu <= kappa_eps mu, mu <- max(mu_min, min(kappa_mu mu, mu^theta_mu))),
+inertia-corrected factorization (Algorithm IC of
+amigo/algorithm/inertia_correction.py: increase delta_w until the inertia is
+(n_primal, n_constraints), delta_c on the multipliers when the matrix is
+singular), Newton direction with 8-block iterative refinement, bound-dual
+back-substitution, fraction-to-boundary step, a backtracking line search on
+an l1 merit function, and the bound-multiplier reset.  It is not a copy of
+amigo's filter line search, watchdog or restoration phase.
+
+The numeric work goes through a backend object; `DeviceBackend` is the
+product path (libamigo_b200.so through torch device buffers).  The same
+driver runs over a host backend made of the reference's own SparseLDL and
+IPM vector functions (oracle/host_backend.py) to compare iteration counts
+and optima.
+"""
+import math
+import time
+
+import numpy as np
+import torch
+
+from .ipm import InteriorPointOptimizer
+from .linalg import OrderingType
+from .solver import B200Solver
+
+
+DEFAULTS = dict(tol=1e-8, max_iter=200, mu0=0.1, mu_min=1e-11,
+                kappa_eps=10.0, kappa_mu=0.2, theta_mu=1.5, tau_min=0.99,
+                kappa_sigma=1e10, dw_first=1e-4, dw_min=1e-20, dw_max=1e40,
+                kw_plus_first=100.0, kw_plus=8.0, kw_minus=1.0 / 3.0,
+                dc=1e-8, kappa_c=0.25, armijo=1e-4, max_ls=40,
+                refine_steps=1)
+
+
+def solve(backend, options=None, verbose=False):
+    """Run the interior-point loop; returns a dict with converged,
+    iterations, objective, kkt_error, time_s, inertia_corrections."""
+    o = dict(DEFAULTS)
+    o.update(options or {})
+    B = backend
+    t0 = time.perf_counter()
+    st = B.initial_state()
+    mu = o["mu0"]
+    dw_last = 0.0
+    nu = 1.0
+    n_ic = 0
+    result = dict(converged=False)
+    for it in range(o["max_iter"]):
+        g = B.gradient(st)
+        d, p, c = B.kkt_error(0.0, st, g)
+        E0 = max(d, p, c)
+        if verbose:
+            print("it %3d  mu %.2e  E0 %.3e  obj %.8e" % (it, mu, E0, B.objective(st)))
+        if E0 <= o["tol"]:
+            result.update(converged=True, iterations=it)
+            break
+        # monotone barrier update
+        while True:
+            Emu = max(B.kkt_error(mu, st, g))
+            if Emu <= o["kappa_eps"] * mu and mu > o["mu_min"]:
+                mu = max(o["mu_min"], min(o["kappa_mu"] * mu, mu ** o["theta_mu"]))
+                continue
+            break
+        # inertia-corrected factorization
+        diag = B.diagonal(st)
+        dw, dc = 0.0, 0.0
+        want = (B.np, B.nc)
+        for attempt in range(41):
+            inertia = B.factor(st, diag, dw, dc)
+            if inertia == want:
+                break
+            n_ic += 1
+            if inertia[0] + inertia[1] < B.n and dc == 0.0:
+                dc = o["dc"] * mu ** o["kappa_c"]
+            if dw == 0.0:
+                dw = o["dw_first"] if dw_last == 0.0 else max(o["dw_min"],
+                                                              o["kw_minus"] * dw_last)
+            else:
+                dw *= o["kw_plus_first"] if dw_last == 0.0 else o["kw_plus"]
+            if dw > o["dw_max"]:
+                break
+        if dw > 0.0:
+            dw_last = dw
+        # Newton direction
+        res = B.residual(mu, st, g)
+        px = B.solve(res)
+        if o["refine_steps"]:
+            B.refine(mu, st, g, res, px, o["refine_steps"])
+        upd = B.update(mu, st, px)
+        tau = max(o["tau_min"], 1.0 - mu)
+        ax, az = B.max_step(tau, st, upd)
+        # l1-merit backtracking line search
+        nu = max(nu, 1.1 * B.max_abs_mult(st, px))
+        gf = B.objective_gradient(st)
+        theta0 = B.cviol(st, g)
+        phi0 = B.objective(st) + B.barrier_log_sum(mu, st) + nu * theta0
+        dphi = B.dphi(mu, st, gf, px) - nu * theta0
+        alpha = ax
+        trial = None
+        for ls in range(o["max_ls"]):
+            trial = B.apply_step(alpha, az, st, upd)
+            gt = B.gradient(trial)
+            phi = B.objective(trial) + B.barrier_log_sum(mu, trial) + nu * B.cviol(trial, gt)
+            if phi <= phi0 + o["armijo"] * alpha * dphi or not math.isfinite(dphi):
+                break
+            alpha *= 0.5
+        st = trial
+        B.reset_bound_multipliers(mu, o["kappa_sigma"], st)
+    else:
+        result.update(iterations=o["max_iter"])
+    g = B.gradient(st)
+    result.update(objective=B.objective(st), kkt_error=max(B.kkt_error(0.0, st, g)),
+                  time_s=time.perf_counter() - t0, inertia_corrections=n_ic,
+                  x=B.solution(st))
+    return result
+
+
+class CartPoleProblem:
+    """Device KKT problem for the cart-pole model (problems/cartpole.py)."""
+
+    def __init__(self, model, device="cuda"):
+        from .linalg import CSRMat
+        self.model = model
+        self.device = torch.device(device)
+        self.dm = model.device_model(self.device)
+        self._csr = CSRMat
+        self._obj = torch.zeros(1, dtype=torch.float64, device=self.device)
+
+    def create_matrix(self):
+        m = self.model
+        return self._csr(m.n, m.n, m.rowp, m.cols, device=self.device)
+
+    def hessian(self, alpha, x, hess):
+        self.dm.hessian(x, alpha, hess.vals)
+
+    def gradient(self, alpha, x, g):
+        self.dm.gradient(x, alpha, g)
+
+    def add_diagonal(self, diag, hess):
+        hess.add_diagonal(diag)
+
+    def objective(self, x):
+        self.dm.objective(x, self._obj)
+        return float(self._obj.item())
+
+
+class DeviceBackend:
+    """Numeric core on the GPU: component kernels, multifrontal LDL^T,
+    IPM vector kernels."""
+
+    def __init__(self, problem, model, device="cuda"):
+        self.P = problem
+        self.m = model
+        self.device = torch.device(device)
+        self.solver = B200Solver(problem, order=OrderingType.AMD)
+        self.opt = InteriorPointOptimizer(model.mult, model.lower, model.upper,
+                                          device=self.device)
+        self.opt.relax_bounds()
+        self.n, self.np, self.nc = model.n, self.opt.np_, self.opt.nc_
+        f64 = dict(dtype=torch.float64, device=self.device)
+        self.g = torch.zeros(self.n, **f64)
+        self.gf = torch.zeros(self.n, **f64)
+        self.res = torch.zeros(self.n, **f64)
+        self.px = torch.zeros(self.n, **f64)
+        self.diag = torch.zeros(self.n, **f64)
+        self.dtot = torch.zeros(self.n, **f64)
+        self.primal = torch.from_numpy(~model.mult).to(self.device).double()
+        self.upd = self.opt.create_opt_vector()
+        self.xtmp = torch.zeros(self.n, **f64)
+        self._hsave = None
+        self._hx = None
+        self.mult_idx = self.opt.cidx.long()
+        self._lbx = self.opt.lbx.cpu().numpy()
+        self._ubx = self.opt.ubx.cpu().numpy()
+
+    def initial_state(self):
+        x = torch.from_numpy(np.ascontiguousarray(self.m.x0)).to(self.device)
+        v = self.opt.create_opt_vector(x)
+        self.opt.initialize_multipliers_and_slacks(0.1, None, v)
+        return v
+
+    def _new_state(self):
+        return self.opt.create_opt_vector()
+
+    def gradient(self, st):
+        out = torch.zeros(self.n, dtype=torch.float64, device=self.device)
+        self.P.gradient(1.0, st.x, out)
+        return out
+
+    def objective_gradient(self, st):
+        self.xtmp.copy_(st.x)
+        self.xtmp[self.mult_idx] = 0.0
+        self.P.gradient(1.0, self.xtmp, self.gf)
+        return self.gf
+
+    def objective(self, st):
+        return self.P.objective(st.x)
+
+    def kkt_error(self, mu, st, g):
+        return self.opt.compute_kkt_error_mu(mu, st, g)
+
+    def diagonal(self, st):
+        self.opt.compute_diagonal(st, self.diag)
+        return self.diag
+
+    def factor(self, st, diag, dw, dc):
+        torch.add(diag, self.primal, alpha=dw, out=self.dtot)
+        if dc:
+            self.dtot.sub_(1.0 - self.primal, alpha=dc)
+        self.solver.factor(1.0, st.x, self.dtot)
+        return self.solver.get_inertia()
+
+    def residual(self, mu, st, g):
+        self.opt.compute_residual(mu, st, g, self.res)
+        return self.res
+
+    def solve(self, res):
+        self.solver.solve(res, self.px)
+        return self.px
+
+    def refine(self, mu, st, g, res, px, steps):
+        self.solver.iterative_refinement(mu, self.m.mult, res, st, g,
+                                         self._lbx, self._ubx, px, None, None,
+                                         max_steps=steps + 1)
+
+    def update(self, mu, st, px):
+        self.opt.compute_update(mu, st, px, self.upd)
+        return self.upd
+
+    def max_step(self, tau, st, upd):
+        ax, xi, az, zi = self.opt.compute_max_step(tau, st, upd)
+        return ax, az
+
+    def apply_step(self, ax, az, st, upd):
+        t = self._new_state()
+        t.copy(st)
+        self.opt.apply_step_update(ax, az, st, upd, t)
+        return t
+
+    def max_abs_mult(self, st, px):
+        lam = st.x[self.mult_idx] + px[self.mult_idx]
+        return float(lam.abs().max().item()) if lam.numel() else 0.0
+
+    def cviol(self, st, g):
+        return self.opt.compute_constraint_violation_1norm(st, g)
+
+    def barrier_log_sum(self, mu, st):
+        return self.opt.compute_barrier_log_sum(mu, st)
+
+    def dphi(self, mu, st, gf, px):
+        return self.opt.compute_barrier_dphi_direct(mu, st, gf, px)
+
+    def reset_bound_multipliers(self, mu, kappa, st):
+        self.opt.reset_bound_multipliers(mu, kappa, st)
+
+    def solution(self, st):
+        return st.x.cpu().numpy()

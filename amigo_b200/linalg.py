@@ -309,3 +309,73 @@ def analyze(n, rowp, cols, order=OrderingType.AMD):
         return symbolic_arrays(h)
     finally:
         _lib.lib().ab_ldl_destroy(h)
+
+
+class BatchedSparseLDL:
+    """Many independent SparseLDL problems factored and solved together:
+    one launch per elimination-tree level covers the fronts of every
+    problem.  `patterns` is a list of (n, rowp, cols); the values passed to
+    factor() and the vectors passed to solve are the problems'
+    concatenation (device tensors).  get_inertia() returns a list of
+    (npos, nneg), one per problem."""
+
+    def __init__(self, patterns, ustab=0.01, pivot_tol=1e-14,
+                 delay_growth=2.0, order=OrderingType.AMD, device=None):
+        self.device = _device(device)
+        self.k = len(patterns)
+        ns = np.array([int(p[0]) for p in patterns], dtype=np.int32)
+        self._rowp = [np.ascontiguousarray(p[1], dtype=np.int32) for p in patterns]
+        self._cols = [np.ascontiguousarray(p[2], dtype=np.int32) for p in patterns]
+        RP = (ctypes.POINTER(ctypes.c_int) * self.k)(*[_iptr(a) for a in self._rowp])
+        CP = (ctypes.POINTER(ctypes.c_int) * self.k)(*[_iptr(a) for a in self._cols])
+        self.n_each = ns
+        self.nnz_each = np.array([int(a[-1]) for a in self._rowp])
+        self.var_off = np.concatenate([[0], np.cumsum(ns)])
+        self.nnz_off = np.concatenate([[0], np.cumsum(self.nnz_each)])
+        self.n = int(self.var_off[-1])
+        self.nnz = int(self.nnz_off[-1])
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.call("ab_ldl_batch_create", self.k, _iptr(ns), RP, CP, int(order),
+                      0, float(ustab), float(pivot_tol), float(delay_growth),
+                      ctypes.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().ab_ldl_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def factor(self, vals):
+        if vals.numel() != self.nnz or vals.dtype != torch.float64:
+            raise ValueError("expected the concatenated float64 values")
+        with torch.cuda.device(self.device):
+            _lib.call("ab_ldl_factor", self._h, vals.data_ptr(),
+                      _stream_ptr(self.device))
+        return 0
+
+    def get_inertia(self):
+        a = np.zeros(self.k, np.int32)
+        b = np.zeros(self.k, np.int32)
+        _lib.call("ab_ldl_batch_inertia", self._h, _stream_ptr(self.device),
+                  _iptr(a), _iptr(b))
+        return list(zip(a.tolist(), b.tolist()))
+
+    def solve_device(self, xd):
+        nrhs = 1 if xd.dim() == 1 else xd.shape[0]
+        with torch.cuda.device(self.device):
+            _lib.call("ab_ldl_solve", self._h, xd.data_ptr(), nrhs, self.n,
+                      _stream_ptr(self.device))
+
+    def stats(self):
+        fl, fe = ctypes.c_double(), ctypes.c_double()
+        mf, nd, lv = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.call("ab_ldl_stats", self._h, _stream_ptr(self.device),
+                  ctypes.byref(fl), ctypes.byref(fe), ctypes.byref(mf),
+                  ctypes.byref(nd), ctypes.byref(lv))
+        return dict(flops=fl.value, factor_entries=fe.value, max_front=mf.value,
+                    num_delayed=nd.value, levels=lv.value)

@@ -76,6 +76,24 @@ int ab_ldl_inertia(ab_ldl_t h, void* stream, int* npos, int* nneg);
  * SparseLDL::solve (include/sparse_ldl.h:162-190). */
 int ab_ldl_solve(ab_ldl_t h, double* d_x, int nrhs, int ldx, void* stream);
 
+/* Batched handle: nprob independent problems factored and solved together,
+ * one launch per elimination-tree level for all of them (fronts of every
+ * problem at the same level share the launch).  Each problem keeps its own
+ * symbolic analysis (identical to the reference's for that problem); the
+ * values and right-hand sides are the concatenation of the problems' in
+ * order (problem p's CSR values start at the sum of the earlier nnz, its
+ * rows at the sum of the earlier n).  ab_ldl_factor / ab_ldl_solve /
+ * ab_ldl_destroy apply to the batch; ab_ldl_inertia returns the sums and
+ * ab_ldl_batch_inertia the per-problem values (arrays of nprob).  No single
+ * reference counterpart: the reference factors one SparseLDL at a time. */
+int ab_ldl_batch_create(int nprob, const int* n, const int* const* rowp,
+                        const int* const* cols, int order, int solver_type,
+                        double ustab, double pivot_tol, double delay_growth,
+                        ab_ldl_t* out);
+int ab_ldl_batch_inertia(ab_ldl_t h, void* stream, int* npos, int* nneg);
+int ab_ldl_batch_sizes(ab_ldl_t h, int* nprob, int* n_total,
+                       long long* nnz_total);
+
 /* Statistics of the last factorization (host values; synchronises).
  * flops: sum over fronts of p^3/3 + p^2 c + p c^2 with p = pivots, c =
  * contribution size; factor_entries: sum f*p; max_front; num_delayed:
@@ -304,6 +322,9 @@ int ab_cartpole_gradient(const ab_cartpole* m, const double* x, double alpha,
                          double* grad, void* stream);
 int ab_cartpole_hessian(const ab_cartpole* m, const double* x, double alpha,
                         double* vals, void* stream);
+/* objective value (trapezoidal integral of u^2) -> out[0] */
+int ab_cartpole_objective(const ab_cartpole* m, const double* x, double* out,
+                          void* stream);
 
 #ifdef __cplusplus
 }

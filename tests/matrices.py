@@ -69,7 +69,7 @@ def kkt_matrix(n_primal, n_con, seed, density=None, delta_c=0.0,
     J = sp.random(n_con, n_primal, density=min(1.0, 4.0 / max(n_primal, 1)),
                   random_state=r).tolil()
     # full row rank: one strong entry per row, in distinct columns
-    strong = r.permutation(n_primal)[:n_con]
+    strong = np.resize(r.permutation(n_primal), n_con)
     for i in range(n_con):
         J[i, strong[i]] = 2.0 + r.rand()
     J = J.tocsr()
