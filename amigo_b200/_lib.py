@@ -29,7 +29,9 @@ _dp = ctypes.POINTER(ctypes.c_double)
 
 class IpmProblem(ctypes.Structure):
     _fields_ = [("n", _i), ("np", _i), ("nc", _i), ("pidx", _vp),
-                ("cidx", _vp), ("lbx", _vp), ("ubx", _vp), ("lbh", _vp)]
+                ("cidx", _vp), ("lbx", _vp), ("ubx", _vp), ("lbh", _vp),
+                ("mu_inst", _vp), ("pinst", _vp), ("vinst", _vp),
+                ("ninst", _i), ("poff", _vp), ("coff", _vp)]
 
 
 class IpmState(ctypes.Structure):
@@ -51,11 +53,26 @@ class Simp2DStruct(ctypes.Structure):
                                      "penalty")])
 
 
+class Simp3DStruct(ctypes.Structure):
+    """Mirror of ab_simp3d (include/amigo_b200.h)."""
+    _fields_ = ([(k, _i) for k in ("n", "nnz", "nelems", "nnodes", "u0", "rt0",
+                                   "re0", "s_index", "lam0", "mu0", "nu_index")]
+                + [("color_ptr", _i * 9)]
+                + [(k, _vp) for k in ("color_elems", "ev", "fv", "epos", "fpos",
+                                      "vpos", "spos", "fixed", "fixed_zero_pos",
+                                      "fixed_diag_pos", "load_idx", "load_val",
+                                      "K0", "A")]
+                + [(k, _i) for k in ("nfixed", "nfixed_zero", "nload")]
+                + [(k, _d) for k in ("Bq", "vcoef", "volfrac", "E0", "Emin",
+                                     "penalty")])
+
+
 class CartPoleStruct(ctypes.Structure):
     """Mirror of ab_cartpole (include/amigo_b200.h)."""
     _fields_ = ([(k, _i) for k in ("n", "nnz", "N")]
                 + [(k, _d) for k in ("h", "M", "m", "l", "g")]
-                + [(k, _vp) for k in ("iv", "ipos", "bv", "bpos")])
+                + [(k, _vp) for k in ("iv", "ipos", "bv", "bpos", "h_iv", "m_iv")]
+                + [("nbc", _i), ("ninst", _i), ("inst_iv", _vp)])
 
 
 # name -> (restype, argtypes)
@@ -106,6 +123,11 @@ _SIGS = {
     "ab_ipm_relax_bounds": (_i, [_i, _vp, _vp, _vp, _vp, _d, _d, _vp]),
     "ab_ipm_initialize": (_i, [ctypes.POINTER(IpmProblem), _vp, _vp, _vp, _vp,
                                _vp, _d, _d, _vp]),
+    "ab_ipm_seg_reduce": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
+                               _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ab_ipm_apply_step_seg": (_i, [ctypes.POINTER(IpmProblem),
+                                   ctypes.POINTER(IpmState), _vp, _vp, _vp, _vp,
+                                   _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ab_ipm_refine_init": (_i, [ctypes.POINTER(IpmProblem), ctypes.POINTER(IpmState),
                                 _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ab_ipm_refine_residual": (_i, [ctypes.POINTER(IpmProblem),
@@ -114,11 +136,24 @@ _SIGS = {
     "ab_ipm_refine_update": (_i, [ctypes.POINTER(IpmProblem),
                                   ctypes.POINTER(IpmState), _vp, _vp, _vp, _vp,
                                   _vp, _vp, _vp]),
+    "ab_ipm_refine_init_seg": (_i, [ctypes.POINTER(IpmProblem),
+                                    ctypes.POINTER(IpmState), _vp, _vp, _vp,
+                                    _vp, _vp, _vp, _vp]),
+    "ab_ipm_refine_residual_seg": (_i, [ctypes.POINTER(IpmProblem),
+                                        ctypes.POINTER(IpmState), _vp, _vp,
+                                        _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                        _vp, _vp]),
+    "ab_ipm_refine_update_seg": (_i, [ctypes.POINTER(IpmProblem),
+                                      ctypes.POINTER(IpmState), _vp, _vp, _vp,
+                                      _vp, _vp, _vp, _vp, _vp]),
+    "ab_launch_count": (ctypes.c_longlong, []),
     "ab_csr_add_diagonal": (_i, [_i, _vp, _vp, _vp, _vp]),
     "ab_csr_matvec": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ab_cartpole_gradient": (_i, [ctypes.POINTER(CartPoleStruct), _vp, _d, _vp, _vp]),
     "ab_cartpole_hessian": (_i, [ctypes.POINTER(CartPoleStruct), _vp, _d, _vp, _vp]),
     "ab_cartpole_objective": (_i, [ctypes.POINTER(CartPoleStruct), _vp, _vp, _vp]),
+    "ab_simp3d_gradient": (_i, [ctypes.POINTER(Simp3DStruct), _vp, _d, _vp, _vp]),
+    "ab_simp3d_hessian": (_i, [ctypes.POINTER(Simp3DStruct), _vp, _d, _vp, _vp]),
     "ab_simp2d_gradient": (_i, [ctypes.POINTER(Simp2DStruct), _vp, _d, _vp, _vp]),
     "ab_simp2d_hessian": (_i, [ctypes.POINTER(Simp2DStruct), _vp, _d, _vp, _vp]),
 }

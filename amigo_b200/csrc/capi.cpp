@@ -1,18 +1,29 @@
 // extern "C" entry points declared in include/amigo_b200.h (LDL part).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <new>
 #include <vector>
 
 #include "../../include/amigo_b200.h"
+#include "launch_count.h"
 #include "ldl_internal.h"
+
+namespace ab {
+namespace {
+std::atomic<long long> g_launches{0};
+}
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace ab
 
 struct ab_ldl {
   ab::LdlHandle h;
 };
 
 extern "C" {
+
+long long ab_launch_count(void) { return ab::g_launches.load(); }
 
 int ab_ldl_create(int n, const int* rowp, const int* cols, int order,
                   int solver_type, double ustab, double pivot_tol,

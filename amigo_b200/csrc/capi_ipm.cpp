@@ -161,6 +161,32 @@ int ab_ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
                             (cudaStream_t)stream);
 }
 
+int ab_ipm_seg_reduce(const ab_ipm_problem* p, const ab_ipm_state* s,
+                      double tau, const double* grad, const double* px,
+                      const double* dzl, const double* dzu, const double* gf,
+                      double* out, void* stream) {
+  if (bad(p, s) || !out || p->ninst < 1 || !p->mu_inst || !p->poff ||
+      !p->coff)
+    return AB_ERR_ARG;
+  return ab::ipm_seg_reduce(p, s, tau, grad, px, dzl, dzu, gf, out,
+                            (cudaStream_t)stream);
+}
+
+int ab_ipm_apply_step_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
+                          const double* ax, const double* az,
+                          const double* dxlam, const double* dzl,
+                          const double* dzu, double* xlam_new, double* zl_new,
+                          double* zu_new, double* sl_new, double* su_new,
+                          void* stream) {
+  if (bad(p, s) || !ax || !az || !p->pinst || !p->vinst || !s->xlam ||
+      !dxlam || !xlam_new ||
+      (p->np > 0 && (!dzl || !dzu || !zl_new || !zu_new || !sl_new || !su_new)))
+    return AB_ERR_ARG;
+  return ab::ipm_apply_step_seg(p, s, ax, az, dxlam, dzl, dzu, xlam_new,
+                                zl_new, zu_new, sl_new, su_new,
+                                (cudaStream_t)stream);
+}
+
 int ab_ipm_refine_init(const ab_ipm_problem* p, const ab_ipm_state* s,
                        double mu, const double* grad, const double* rhs_saved,
                        const double* px, double* dzl, double* dzu, double* out,
@@ -200,6 +226,55 @@ int ab_ipm_refine_update(const ab_ipm_problem* p, const ab_ipm_state* s,
     return AB_ERR_ARG;
   return ab::ipm_refine_update(p, s, corr, e_zl, e_zu, px, dzl, dzu,
                                (cudaStream_t)stream);
+}
+
+static bool bad_seg(const ab_ipm_problem* p) {
+  return p->ninst < 1 || !p->mu_inst || !p->pinst || !p->vinst;
+}
+
+int ab_ipm_refine_init_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
+                           const double* grad, const double* rhs_saved,
+                           const double* px, double* dzl, double* dzu,
+                           double* seg_out, void* stream) {
+  if (bad(p, s) || bad_seg(p) || !seg_out ||
+      (p->n > 0 && (!grad || !rhs_saved || !px)) ||
+      (p->np > 0 && (!dzl || !dzu)))
+    return AB_ERR_ARG;
+  double* scratch = device_scratch();
+  if (!scratch) return AB_ERR_CUDA;
+  return ab::ipm_refine_init(p, s, 0.0, grad, rhs_saved, px, dzl, dzu,
+                             scratch + ab::ipm_scratch_doubles() - 8,
+                             (cudaStream_t)stream, scratch, seg_out);
+}
+
+int ab_ipm_refine_residual_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
+                               const double* grad, const double* rhs_saved,
+                               const double* kpx, const double* px,
+                               const double* dzl, const double* dzu,
+                               double* e_cond, double* e_zl, double* e_zu,
+                               double* seg_out, void* stream) {
+  if (bad(p, s) || bad_seg(p) || !seg_out ||
+      (p->n > 0 && (!grad || !rhs_saved || !kpx || !px || !e_cond)) ||
+      (p->np > 0 && (!dzl || !dzu || !e_zl || !e_zu)))
+    return AB_ERR_ARG;
+  double* scratch = device_scratch();
+  if (!scratch) return AB_ERR_CUDA;
+  return ab::ipm_refine_residual(p, s, 0.0, grad, rhs_saved, kpx, px, dzl,
+                                 dzu, e_cond, e_zl, e_zu,
+                                 scratch + ab::ipm_scratch_doubles() - 8,
+                                 (cudaStream_t)stream, scratch, seg_out);
+}
+
+int ab_ipm_refine_update_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
+                             const int* active, const double* corr,
+                             const double* e_zl, const double* e_zu,
+                             double* px, double* dzl, double* dzu,
+                             void* stream) {
+  if (bad(p, s) || bad_seg(p) || !active || (p->n > 0 && (!corr || !px)) ||
+      (p->np > 0 && (!e_zl || !e_zu || !dzl || !dzu)))
+    return AB_ERR_ARG;
+  return ab::ipm_refine_update(p, s, corr, e_zl, e_zu, px, dzl, dzu,
+                               (cudaStream_t)stream, active);
 }
 
 int ab_csr_add_diagonal(int n, const int* diag_pos, const double* d,

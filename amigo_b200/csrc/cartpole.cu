@@ -9,32 +9,44 @@
 // (include/optimization_problem.h:742-818).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "../../include/amigo_b200.h"
+#include "launch_count.h"
 #include "hyperdual.h"
 
 namespace ab {
 namespace {
 
+// Per-interval constants: step h and pole mass (a batch of instances has
+// one value per interval; a single model uses its scalars).
+struct IvParams {
+  double h, mp;
+};
+__device__ __forceinline__ IvParams iv_params(const ab_cartpole& m, int k) {
+  return IvParams{m.h_iv ? m.h_iv[k] : m.h, m.m_iv ? m.m_iv[k] : m.m};
+}
+
 // Cart-pole dynamics f(q, u) for q = (x, theta, xdot, thetadot).
 template <typename T>
-__device__ __forceinline__ void dynamics(const ab_cartpole& m, const T* q,
-                                         const T& u, T* f) {
+__device__ __forceinline__ void dynamics(const ab_cartpole& m, double mp,
+                                         const T* q, const T& u, T* f) {
   const T s = sin(q[1]), c = cos(q[1]);
   const T td2 = q[3] * q[3];
-  const T den = m.M + m.m * (1.0 - c * c);
+  const T den = m.M + mp * (1.0 - c * c);
   f[0] = q[2];
   f[1] = q[3];
-  f[2] = (m.l * m.m * s * td2 + u + m.m * m.g * c * s) / den;
-  f[3] = -(m.l * m.m * c * s * td2 + u * c + (m.M + m.m) * m.g * s) / (m.l * den);
+  f[2] = (m.l * mp * s * td2 + u + mp * m.g * c * s) / den;
+  f[3] = -(m.l * mp * c * s * td2 + u * c + (m.M + mp) * m.g * s) / (m.l * den);
 }
 
 // phi(z) = alpha h/2 u^2 - h/2 lam^T f(z) for one node z = (q, u):
 // value, gradient (5) and Hessian (5x5, symmetric) and the Jacobian of f
 // (4x5) at z.
-__device__ void node_derivs(const ab_cartpole& m, const double* z,
+__device__ void node_derivs(const ab_cartpole& m, IvParams ip, const double* z,
                             const double* lam, double alpha, double* grad,
                             double* hess, double* jac) {
-  const double hh = 0.5 * m.h;
+  const double hh = 0.5 * ip.h;
   for (int i = 0; i < 5; i++) {
     for (int j = i; j < 5; j++) {
       HD zz[5];
@@ -42,7 +54,7 @@ __device__ void node_derivs(const ab_cartpole& m, const double* z,
       zz[i].b = 1.0;
       zz[j].c += 1.0;
       HD f[4];
-      dynamics(m, zz, zz[4], f);
+      dynamics(m, ip.mp, zz, zz[4], f);
       HD phi = alpha * hh * zz[4] * zz[4];
       for (int t = 0; t < 4; t++) phi = phi - hh * lam[t] * f[t];
       hess[i * 5 + j] = phi.d;
@@ -63,15 +75,16 @@ __device__ void interval_values(const ab_cartpole& m, const double* x, int k,
   for (int t = 0; t < 5; t++) z0[t] = x[iv[t]];
   for (int t = 0; t < 5; t++) z1[t] = x[iv[5 + t]];
   for (int t = 0; t < 4; t++) lam[t] = x[iv[10 + t]];
+  const IvParams ip = iv_params(m, k);
   double g0[5], g1[5], h0[25], h1[25], j0[20], j1[20];
-  node_derivs(m, z0, lam, alpha, g0, h0, j0);
-  node_derivs(m, z1, lam, alpha, g1, h1, j1);
+  node_derivs(m, ip, z0, lam, alpha, g0, h0, j0);
+  node_derivs(m, ip, z1, lam, alpha, g1, h1, j1);
   // defect d = q1 - q0 - h/2 (f(z0) + f(z1))
   double f0[4], f1[4];
-  dynamics(m, z0, z0[4], f0);
-  dynamics(m, z1, z1[4], f1);
+  dynamics(m, ip.mp, z0, z0[4], f0);
+  dynamics(m, ip.mp, z1, z1[4], f1);
   for (int t = 0; t < 4; t++)
-    defect[t] = z1[t] - z0[t] - 0.5 * m.h * (f0[t] + f1[t]);
+    defect[t] = z1[t] - z0[t] - 0.5 * ip.h * (f0[t] + f1[t]);
   // gradient w.r.t. [z0 | z1]: phi terms plus the linear -lam / +lam parts
   for (int t = 0; t < 5; t++) {
     g20[t] = g0[t] - (t < 4 ? lam[t] : 0.0);
@@ -87,8 +100,8 @@ __device__ void interval_values(const ab_cartpole& m, const double* x, int k,
   // Jacobian rows (lam) x cols (z0, z1) and the transposed block
   for (int r = 0; r < 4; r++)
     for (int c = 0; c < 5; c++) {
-      const double a = (c == r ? -1.0 : 0.0) - 0.5 * m.h * j0[r * 5 + c];
-      const double b = (c == r ? 1.0 : 0.0) - 0.5 * m.h * j1[r * 5 + c];
+      const double a = (c == r ? -1.0 : 0.0) - 0.5 * ip.h * j0[r * 5 + c];
+      const double b = (c == r ? 1.0 : 0.0) - 0.5 * ip.h * j1[r * 5 + c];
       blk[(10 + r) * 14 + c] = a;
       blk[c * 14 + 10 + r] = a;
       blk[(10 + r) * 14 + 5 + c] = b;
@@ -124,8 +137,8 @@ __global__ void k_cartpole_gradient(ab_cartpole m, int parity,
 // (mu_j, q_j) = 1.
 __global__ void k_cartpole_bc(ab_cartpole m, const double* __restrict__ x,
                               double* grad, double* vals) {
-  const int b = threadIdx.x;
-  if (b >= 2) return;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= (m.nbc > 0 ? m.nbc : 2)) return;
   const int* bv = m.bv + 8 * b;
   if (grad) {
     for (int t = 0; t < 4; t++) {
@@ -142,15 +155,20 @@ __global__ void k_cartpole_bc(ab_cartpole m, const double* __restrict__ x,
   }
 }
 
-// Objective alpha * sum_k h/2 (u_k^2 + u_k+1^2), one block, fixed order.
+// Objective sum_k h/2 (u_k^2 + u_k+1^2); one block per instance (its
+// intervals [inst_iv[b], inst_iv[b+1]); a single model is one instance),
+// fixed summation order.
 __global__ void k_cartpole_objective(ab_cartpole m, const double* x,
                                      double* out) {
   __shared__ double part[256];
+  const int b = blockIdx.x;
+  const int k0 = m.inst_iv ? m.inst_iv[b] : 0;
+  const int k1 = m.inst_iv ? m.inst_iv[b + 1] : m.N;
   double acc = 0.0;
-  for (int k = threadIdx.x; k < m.N; k += blockDim.x) {
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
     const int* iv = m.iv + 14 * k;
     const double u0 = x[iv[4]], u1 = x[iv[9]];
-    acc += 0.5 * m.h * (u0 * u0 + u1 * u1);
+    acc += 0.5 * iv_params(m, k).h * (u0 * u0 + u1 * u1);
   }
   part[threadIdx.x] = acc;
   __syncthreads();
@@ -158,7 +176,7 @@ __global__ void k_cartpole_objective(ab_cartpole m, const double* x,
     if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[0] = part[0];
+  if (threadIdx.x == 0) out[b] = part[0];
 }
 
 }  // namespace
@@ -169,7 +187,8 @@ extern "C" {
 int ab_cartpole_objective(const ab_cartpole* m, const double* x, double* out,
                           void* stream) {
   if (!m || !x || !out) return AB_ERR_ARG;
-  ab::k_cartpole_objective<<<1, 256, 0, (cudaStream_t)stream>>>(*m, x, out);
+  const int nb = m->inst_iv ? (m->ninst > 0 ? m->ninst : 1) : 1;
+  { ab::k_cartpole_objective<<<nb, 256, 0, (cudaStream_t)stream>>>(*m, x, out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? AB_OK : AB_ERR_CUDA;
 }
 
@@ -180,9 +199,10 @@ int ab_cartpole_gradient(const ab_cartpole* m, const double* x, double alpha,
   cudaMemsetAsync(grad, 0, (size_t)m->n * sizeof(double), s);
   const int half = (m->N + 1) / 2;
   for (int parity = 0; parity < 2; parity++)
-    ab::k_cartpole_gradient<<<(half + 127) / 128, 128, 0, s>>>(*m, parity, x,
-                                                               alpha, grad);
-  ab::k_cartpole_bc<<<1, 32, 0, s>>>(*m, x, grad, nullptr);
+    { ab::k_cartpole_gradient<<<(half + 127) / 128, 128, 0, s>>>(*m, parity, x,
+                                                               alpha, grad); ab::count_launch(); }
+  { ab::k_cartpole_bc<<<(std::max(m->nbc, 2) + 127) / 128, 128, 0, s>>>(
+      *m, x, grad, nullptr); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? AB_OK : AB_ERR_CUDA;
 }
 
@@ -193,9 +213,10 @@ int ab_cartpole_hessian(const ab_cartpole* m, const double* x, double alpha,
   cudaMemsetAsync(vals, 0, (size_t)m->nnz * sizeof(double), s);
   const int half = (m->N + 1) / 2;
   for (int parity = 0; parity < 2; parity++)
-    ab::k_cartpole_hessian<<<(half + 127) / 128, 128, 0, s>>>(*m, parity, x,
-                                                              alpha, vals);
-  ab::k_cartpole_bc<<<1, 32, 0, s>>>(*m, x, nullptr, vals);
+    { ab::k_cartpole_hessian<<<(half + 127) / 128, 128, 0, s>>>(*m, parity, x,
+                                                              alpha, vals); ab::count_launch(); }
+  { ab::k_cartpole_bc<<<(std::max(m->nbc, 2) + 127) / 128, 128, 0, s>>>(
+      *m, x, nullptr, vals); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? AB_OK : AB_ERR_CUDA;
 }
 

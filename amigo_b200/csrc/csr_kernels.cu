@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "ipm_internal.h"
+#include "launch_count.h"
 
 namespace ab {
 namespace {
@@ -39,7 +40,7 @@ int csr_add_diagonal(int n, const int* diag_pos, const double* d,
   if (n <= 0) return 0;
   int g = (n + 255) / 256;
   if (g > 148 * 16) g = 148 * 16;
-  k_add_diagonal<<<g, 256, 0, st>>>(n, diag_pos, d, vals);
+  { k_add_diagonal<<<g, 256, 0, st>>>(n, diag_pos, d, vals); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -48,7 +49,7 @@ int csr_matvec(int n, const int* rowp, const int* cols, const double* vals,
   if (n <= 0) return 0;
   long long g = ((long long)n + 7) / 8;
   if (g > 148 * 32) g = 148 * 32;
-  k_matvec<<<(int)g, 256, 0, st>>>(n, rowp, cols, vals, x, y);
+  { k_matvec<<<(int)g, 256, 0, st>>>(n, rowp, cols, vals, x, y); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 

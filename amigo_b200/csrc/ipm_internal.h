@@ -54,20 +54,30 @@ int ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
                    double* zu, double* sl, double* su, double kappa1,
                    double kappa2, cudaStream_t st);
 
+int ipm_seg_reduce(const ab_ipm_problem* p, const ab_ipm_state* s,
+                   double tau, const double* grad, const double* px,
+                   const double* dzl, const double* dzu, const double* gf,
+                   double* out, cudaStream_t st);
+int ipm_apply_step_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
+                       const double* ax, const double* az, const double* dxlam,
+                       const double* dzl, const double* dzu, double* xlam_new,
+                       double* zl_new, double* zu_new, double* sl_new,
+                       double* su_new, cudaStream_t st);
 int ipm_refine_init(const ab_ipm_problem* p, const ab_ipm_state* s,
                     double mu, const double* grad, const double* rhs_saved,
                     const double* px, double* dzl, double* dzu, double* out,
-                    cudaStream_t st, double* scratch);
+                    cudaStream_t st, double* scratch, double* seg = nullptr);
 int ipm_refine_residual(const ab_ipm_problem* p, const ab_ipm_state* s,
                         double mu, const double* grad, const double* rhs_saved,
                         const double* kpx, const double* px, const double* dzl,
                         const double* dzu, double* e_cond, double* e_zl,
                         double* e_zu, double* out, cudaStream_t st,
-                        double* scratch);
+                        double* scratch, double* seg = nullptr);
 int ipm_refine_update(const ab_ipm_problem* p, const ab_ipm_state* s,
                       const double* corr, const double* e_zl,
                       const double* e_zu, double* px, double* dzl,
-                      double* dzu, cudaStream_t st);
+                      double* dzu, cudaStream_t st,
+                      const int* active = nullptr);
 
 int csr_add_diagonal(int n, const int* diag_pos, const double* d,
                      double* vals, cudaStream_t st);

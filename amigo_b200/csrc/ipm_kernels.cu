@@ -15,6 +15,7 @@
 
 #include "../../include/amigo_b200.h"
 #include "ipm_internal.h"
+#include "launch_count.h"
 
 namespace ab {
 namespace {
@@ -31,7 +32,31 @@ struct P {
   const double* lbx;
   const double* ubx;
   const double* lbh;
+  // batched problems: barrier parameter per instance and the instance of
+  // every primal entry / n-vector entry (null for a single problem)
+  const double* mu_inst;
+  const int* pinst;
+  const int* vinst;
+  int ninst;
+  const int* poff;
+  const int* coff;
 };
+
+// Barrier parameter of primal entry i: the call's scalar, or the entry's
+// instance value in a batched problem.
+__device__ __forceinline__ double mu_at(const P& p, double mu, int i) {
+  return p.mu_inst ? p.mu_inst[p.pinst[i]] : mu;
+}
+// Per-instance maximum of non-negative values: seg[k] = max(seg[k], v).
+// Non-negative doubles order like their bit patterns, so an integer atomic
+// max is exact; the plain read first skips most atomics (the stored value
+// only grows, so a stale read can only let an unneeded atomic through).
+// NaN is skipped, as fmax skips it.
+__device__ __forceinline__ void seg_max(double* seg, int k, double v) {
+  if (v > 0.0 && v > seg[k])
+    atomicMax(reinterpret_cast<unsigned long long*>(seg + k),
+              static_cast<unsigned long long>(__double_as_longlong(v)));
+}
 struct S {
   const double* xlam;
   const double* zl;
@@ -40,7 +65,9 @@ struct S {
   const double* su;
 };
 P mkP(const ab_ipm_problem* p) {
-  return P{p->n, p->np, p->nc, p->pidx, p->cidx, p->lbx, p->ubx, p->lbh};
+  return P{p->n,      p->np,    p->nc,    p->pidx,  p->cidx,
+           p->lbx,    p->ubx,   p->lbh,   p->mu_inst, p->pinst,
+           p->vinst,  p->ninst, p->poff,  p->coff};
 }
 S mkS(const ab_ipm_state* s) { return S{s->xlam, s->zl, s->zu, s->sl, s->su}; }
 
@@ -59,16 +86,17 @@ __global__ void k_residual(P p, S s, double mu, const double* grad,
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
     const int idx = p.pidx[i];
+    const double mu_i = mu_at(p, mu, i);
     const double rhs_stat = grad[idx] - s.zl[i] + s.zu[i];
     dsq += rhs_stat * rhs_stat;
     double aug = rhs_stat;
     if (finite_bound(p.lbx[i])) {
       const double gap = s.sl[i];
-      aug += (gap * s.zl[i] - mu) / gap;
+      aug += (gap * s.zl[i] - mu_i) / gap;
     }
     if (finite_bound(p.ubx[i])) {
       const double gap = s.su[i];
-      aug -= (gap * s.zu[i] - mu) / gap;
+      aug -= (gap * s.zu[i] - mu_i) / gap;
     }
     res[idx] = -aug;
   }
@@ -102,15 +130,16 @@ __global__ void k_bound_dual_step(P p, S s, double mu, const double* px,
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
     const double dx = px[p.pidx[i]];
+    const double mu_i = mu_at(p, mu, i);
     double a = 0.0, b = 0.0;
     if (finite_bound(p.lbx[i])) {
       const double gap = s.sl[i];
-      const double rc = gap * s.zl[i] - mu;
+      const double rc = gap * s.zl[i] - mu_i;
       a = -(rc + s.zl[i] * dx) / gap;
     }
     if (finite_bound(p.ubx[i])) {
       const double gap = s.su[i];
-      const double rc = gap * s.zu[i] - mu;
+      const double rc = gap * s.zu[i] - mu_i;
       b = -(rc - s.zu[i] * dx) / gap;
     }
     dzl[i] = a;
@@ -351,13 +380,14 @@ __global__ void k_reset_bound_multipliers(P p, S s, double mu, double kappa,
                                           double* zl_out, double* zu_out) {
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    const double mu_i = mu_at(p, mu, i);
     if (finite_bound(p.lbx[i])) {
       const double g = s.sl[i];
-      zl_out[i] = fmax(fmin(s.zl[i], kappa * mu / g), mu / (kappa * g));
+      zl_out[i] = fmax(fmin(s.zl[i], kappa * mu_i / g), mu_i / (kappa * g));
     }
     if (finite_bound(p.ubx[i])) {
       const double g = s.su[i];
-      zu_out[i] = fmax(fmin(s.zu[i], kappa * mu / g), mu / (kappa * g));
+      zu_out[i] = fmax(fmin(s.zu[i], kappa * mu_i / g), mu_i / (kappa * g));
     }
   }
 }
@@ -450,7 +480,8 @@ __device__ __forceinline__ void ir_bounds(const P& p, const S& s, int i,
 // four blocks (linear_solver.py:168-191).
 __global__ void k_ir_init(P p, S s, double mu, const double* grad,
                           const double* rhs_saved, const double* px,
-                          double* dzl, double* dzu, double* partial) {
+                          double* dzl, double* dzu, double* partial,
+                          double* seg) {
   double nrm = 0.0;
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
@@ -458,16 +489,23 @@ __global__ void k_ir_init(P p, S s, double mu, const double* grad,
     double gl, gu;
     ir_bounds(p, s, i, fl, fu, gl, gu);
     const int idx = p.pidx[i];
+    const double mu_i = mu_at(p, mu, i);
     const double zl = s.zl[i], zu = s.zu[i], dx = px[idx];
-    dzl[i] = fl ? (mu - gl * zl - zl * dx) / gl : 0.0;
-    dzu[i] = fu ? (mu - gu * zu + zu * dx) / gu : 0.0;
+    dzl[i] = fl ? (mu_i - gl * zl - zl * dx) / gl : 0.0;
+    dzu[i] = fu ? (mu_i - gu * zu + zu * dx) / gu : 0.0;
     const double rx = -(grad[idx] - zl + zu);
-    nrm = fmax(nrm, fabs(rx));
-    if (fl) nrm = fmax(nrm, fabs(mu - gl * zl));
-    if (fu) nrm = fmax(nrm, fabs(mu - gu * zu));
+    double e = fabs(rx);
+    if (fl) e = fmax(e, fabs(mu_i - gl * zl));
+    if (fu) e = fmax(e, fabs(mu_i - gu * zu));
+    nrm = fmax(nrm, e);
+    if (seg) seg_max(seg, p.pinst[i], e);
   }
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p.nc; j += stride)
-    nrm = fmax(nrm, fabs(rhs_saved[p.cidx[j]]));
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p.nc; j += stride) {
+    const int idx = p.cidx[j];
+    const double e = fabs(rhs_saved[idx]);
+    nrm = fmax(nrm, e);
+    if (seg) seg_max(seg, p.vinst[idx], e);
+  }
   block_max2(nrm, 0.0, partial);
 }
 
@@ -478,7 +516,8 @@ __global__ void k_ir_residual(P p, S s, double mu, const double* grad,
                               const double* rhs_saved, const double* kpx,
                               const double* px, const double* dzl,
                               const double* dzu, double* e_cond,
-                              double* e_zl, double* e_zu, double* partial) {
+                              double* e_zl, double* e_zu, double* partial,
+                              double* seg) {
   double nres = 0.0, nsol = 0.0;
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
@@ -490,13 +529,20 @@ __global__ void k_ir_residual(P p, S s, double mu, const double* grad,
     const double sigma = (fl ? zl / gl : 0.0) + (fu ? zu / gu : 0.0);
     const double rx = -(grad[idx] - zl + zu);
     const double ex = rx - kpx[idx] + sigma * dx + dzl[i] - dzu[i];
-    const double ezl = fl ? (mu - gl * zl) - zl * dx - gl * dzl[i] : 0.0;
-    const double ezu = fu ? (mu - gu * zu) + zu * dx - gu * dzu[i] : 0.0;
+    const double mu_i = mu_at(p, mu, i);
+    const double ezl = fl ? (mu_i - gl * zl) - zl * dx - gl * dzl[i] : 0.0;
+    const double ezu = fu ? (mu_i - gu * zu) + zu * dx - gu * dzu[i] : 0.0;
     e_zl[i] = ezl;
     e_zu[i] = ezu;
     e_cond[idx] = ex + (fl ? ezl / gl : 0.0) - (fu ? ezu / gu : 0.0);
-    nres = fmax(nres, fmax(fabs(ex), fmax(fabs(ezl), fabs(ezu))));
-    nsol = fmax(nsol, fmax(fabs(dx), fmax(fabs(dzl[i]), fabs(dzu[i]))));
+    const double r = fmax(fabs(ex), fmax(fabs(ezl), fabs(ezu)));
+    const double x = fmax(fabs(dx), fmax(fabs(dzl[i]), fabs(dzu[i])));
+    nres = fmax(nres, r);
+    nsol = fmax(nsol, x);
+    if (seg) {
+      seg_max(seg, 2 * p.pinst[i], r);
+      seg_max(seg, 2 * p.pinst[i] + 1, x);
+    }
   }
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < p.nc; j += stride) {
     const int idx = p.cidx[j];
@@ -504,6 +550,10 @@ __global__ void k_ir_residual(P p, S s, double mu, const double* grad,
     e_cond[idx] = ec;
     nres = fmax(nres, fabs(ec));
     nsol = fmax(nsol, fabs(px[idx]));
+    if (seg) {
+      seg_max(seg, 2 * p.vinst[idx], fabs(ec));
+      seg_max(seg, 2 * p.vinst[idx] + 1, fabs(px[idx]));
+    }
   }
   block_max2(nres, nsol, partial);
 }
@@ -512,9 +562,10 @@ __global__ void k_ir_residual(P p, S s, double mu, const double* grad,
 // (linear_solver.py:255-262).
 __global__ void k_ir_update(P p, S s, const double* corr, const double* e_zl,
                             const double* e_zu, double* px, double* dzl,
-                            double* dzu) {
+                            double* dzu, const int* active) {
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    if (active && !active[p.pinst[i]]) continue;
     bool fl, fu;
     double gl, gu;
     ir_bounds(p, s, i, fl, fu, gl, gu);
@@ -523,7 +574,7 @@ __global__ void k_ir_update(P p, S s, const double* corr, const double* e_zl,
     if (fu) dzu[i] += (e_zu[i] + s.zu[i] * dc) / gu;
   }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride)
-    px[i] += corr[i];
+    if (!active || active[p.vinst[i]]) px[i] += corr[i];
 }
 
 __global__ void k_max2_final(int nblocks, const double* partial, double* out) {
@@ -535,6 +586,113 @@ __global__ void k_max2_final(int nblocks, const double* partial, double* out) {
   }
   out[0] = a;
   out[1] = b;
+}
+
+// ------------------------------------------------- batched (per instance)
+// One block per instance over its contiguous primal / constraint ranges;
+// every quantity is reduced in a fixed order (deterministic).  Outputs per
+// instance k at out[k * kSegQ + q]:
+//   0 dual inf-norm, 1 primal inf-norm, 2 complementarity inf-norm
+//   (|gap z - mu_k|), 3 constraint violation 1-norm, 4 barrier log-sum,
+//   5 max primal step, 6 max dual step (fraction to the boundary, seeded
+//   at 1), 7 barrier directional derivative, 8 max |lam + dlam|.
+constexpr int kSegQ = 10;
+__global__ void k_seg_reduce(P p, S s, double tau, const double* grad,
+                             const double* px, const double* dzl,
+                             const double* dzu, const double* gf,
+                             double* out) {
+  const int k = blockIdx.x;
+  const double mu = p.mu_inst[k];
+  // tau < 0 selects the per-instance fraction max(-tau, 1 - mu_k)
+  const double tk = tau < 0.0 ? fmax(-tau, 1.0 - mu) : tau;
+  const int p0 = p.poff[k], p1 = p.poff[k + 1];
+  const int c0 = p.coff[k], c1 = p.coff[k + 1];
+  double q[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, 0.0};
+  for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+    const int idx = p.pidx[i];
+    const bool hl = finite_bound(p.lbx[i]), hu = finite_bound(p.ubx[i]);
+    if (grad) q[0] = fmax(q[0], fabs(grad[idx] - s.zl[i] + s.zu[i]));
+    if (hl) {
+      q[2] = fmax(q[2], fabs(s.sl[i] * s.zl[i] - mu));
+      if (s.sl[i] > 0) q[4] -= mu * log(s.sl[i]);
+    }
+    if (hu) {
+      q[2] = fmax(q[2], fabs(s.su[i] * s.zu[i] - mu));
+      if (s.su[i] > 0) q[4] -= mu * log(s.su[i]);
+    }
+    if (px && dzl) {
+      const double dx = px[idx];
+      if (hl) {
+        if (dx < 0.0) q[5] = fmin(q[5], -tk * s.sl[i] / dx);
+        if (dzl[i] < 0.0) q[6] = fmin(q[6], -tk * s.zl[i] / dzl[i]);
+      }
+      if (hu) {
+        if (dx > 0.0) q[5] = fmin(q[5], tk * s.su[i] / dx);
+        if (dzu[i] < 0.0) q[6] = fmin(q[6], -tk * s.zu[i] / dzu[i]);
+      }
+    }
+    if (gf && px) {
+      const double dx = px[idx];
+      q[7] += gf[idx] * dx;
+      if (hl) q[7] -= mu * dx / s.sl[i];
+      if (hu) q[7] += mu * dx / s.su[i];
+    }
+  }
+  for (int j = c0 + threadIdx.x; j < c1; j += blockDim.x) {
+    const int idx = p.cidx[j];
+    if (grad) {
+      const double r = fabs(grad[idx] - p.lbh[j]);
+      q[1] = fmax(q[1], r);
+      q[3] += r;
+    }
+    if (px && s.xlam) q[8] = fmax(q[8], fabs(s.xlam[idx] + px[idx]));
+  }
+  __shared__ double sh[9][RT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t < 9; t++) {
+    double v = q[t];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double w = __shfl_down_sync(0xffffffffu, v, o);
+      if (t == 5 || t == 6) v = fmin(v, w);
+      else if (t == 3 || t == 4 || t == 7) v += w;
+      else v = fmax(v, w);
+    }
+    if (lane == 0) sh[t][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 9) {
+    const int t = threadIdx.x;
+    double v = sh[t][0];
+    for (int w = 1; w < RT / 32; w++) {
+      const double x = sh[t][w];
+      if (t == 5 || t == 6) v = fmin(v, x);
+      else if (t == 3 || t == 4 || t == 7) v += x;
+      else v = fmax(v, x);
+    }
+    out[k * kSegQ + t] = v;
+  }
+}
+
+// apply_step with per-instance step lengths (interior_point_backend.h:
+// 376-392): xlam += ax_k dxlam, z += az_k dz, s +- ax_k dx.
+__global__ void k_apply_step_seg(P p, S s, const double* ax, const double* az,
+                                 const double* dxlam, const double* dzl,
+                                 const double* dzu, double* xlam_new,
+                                 double* zl_new, double* zu_new,
+                                 double* sl_new, double* su_new) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride)
+    xlam_new[i] = s.xlam[i] + ax[p.vinst[i]] * dxlam[i];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.np; i += stride) {
+    const int k = p.pinst[i];
+    const bool hl = finite_bound(p.lbx[i]), hu = finite_bound(p.ubx[i]);
+    if (hl) zl_new[i] = s.zl[i] + az[k] * dzl[i];
+    if (hu) zu_new[i] = s.zu[i] + az[k] * dzu[i];
+    const double dx = ax[k] * dxlam[p.pidx[i]];
+    if (hl) sl_new[i] = s.sl[i] + dx;
+    if (hu) su_new[i] = s.su[i] - dx;
+  }
 }
 
 __global__ void k_sum2_final(int nblocks, const double* partial, double* out) {
@@ -611,11 +769,11 @@ int ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
   P pp = mkP(p);
   S ss = mkS(s);
   if (out2) {
-    k_residual<<<kRedBlocks, RT, 0, st>>>(pp, ss, mu, grad, res, scratch);
-    k_sum2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out2);
+    { k_residual<<<kRedBlocks, RT, 0, st>>>(pp, ss, mu, grad, res, scratch); ab::count_launch(); }
+    { k_sum2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out2); ab::count_launch(); }
   } else {
     long long m = p->np > p->nc ? p->np : p->nc;
-    k_residual<<<grid_for(m), RT, 0, st>>>(pp, ss, mu, grad, res, nullptr);
+    { k_residual<<<grid_for(m), RT, 0, st>>>(pp, ss, mu, grad, res, nullptr); ab::count_launch(); }
   }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
@@ -623,15 +781,15 @@ int ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
 int ipm_diagonal(const ab_ipm_problem* p, const ab_ipm_state* s, double* diag,
                  cudaStream_t st) {
   long long m = p->np > p->nc ? p->np : p->nc;
-  k_diagonal<<<grid_for(m), RT, 0, st>>>(mkP(p), mkS(s), diag);
+  { k_diagonal<<<grid_for(m), RT, 0, st>>>(mkP(p), mkS(s), diag); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
 int ipm_bound_dual_step(const ab_ipm_problem* p, const ab_ipm_state* s,
                         double mu, const double* px, double* dzl, double* dzu,
                         cudaStream_t st) {
-  k_bound_dual_step<<<grid_for(p->np), RT, 0, st>>>(mkP(p), mkS(s), mu, px,
-                                                     dzl, dzu);
+  { k_bound_dual_step<<<grid_for(p->np), RT, 0, st>>>(mkP(p), mkS(s), mu, px,
+                                                     dzl, dzu); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -640,9 +798,9 @@ int ipm_max_step(const ab_ipm_problem* p, const ab_ipm_state* s, double tau,
                  double* out, int* iout, cudaStream_t st, double* scratch) {
   double* pv = scratch;
   int* pi = reinterpret_cast<int*>(scratch + 2 * kRedBlocks);
-  k_max_step<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), tau, px, dzl, dzu, pv,
-                                        pi);
-  k_max_step_final<<<1, 32, 0, st>>>(kRedBlocks, p->pidx, pv, pi, out, iout);
+  { k_max_step<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), tau, px, dzl, dzu, pv,
+                                        pi); ab::count_launch(); }
+  { k_max_step_final<<<1, 32, 0, st>>>(kRedBlocks, p->pidx, pv, pi, out, iout); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -652,26 +810,26 @@ int ipm_apply_step(const ab_ipm_problem* p, const ab_ipm_state* s, double ax,
                    double* zu_new, double* sl_new, double* su_new,
                    cudaStream_t st) {
   long long m = p->n > p->np ? p->n : p->np;
-  k_apply_step<<<grid_for(m), RT, 0, st>>>(mkP(p), mkS(s), ax, az, dxlam, dzl,
+  { k_apply_step<<<grid_for(m), RT, 0, st>>>(mkP(p), mkS(s), ax, az, dxlam, dzl,
                                            dzu, xlam_new, zl_new, zu_new,
-                                           sl_new, su_new);
+                                           sl_new, su_new); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
 int ipm_reductions(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
                    const double* grad, double* out, cudaStream_t st,
                    double* scratch) {
-  k_reductions<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, scratch);
-  k_reductions_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out);
+  { k_reductions<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, scratch); ab::count_launch(); }
+  { k_reductions_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
 int ipm_barrier_dphi(const ab_ipm_problem* p, const ab_ipm_state* s,
                      double mu, const double* grad, const double* px,
                      double* out, cudaStream_t st, double* scratch) {
-  k_barrier_dphi<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, px,
-                                            scratch);
-  k_sum1_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out);
+  { k_barrier_dphi<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, px,
+                                            scratch); ab::count_launch(); }
+  { k_sum1_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -679,8 +837,8 @@ int ipm_reset_bound_multipliers(const ab_ipm_problem* p,
                                 const ab_ipm_state* s, double mu,
                                 double kappa, double* zl_out, double* zu_out,
                                 cudaStream_t st) {
-  k_reset_bound_multipliers<<<grid_for(p->np), RT, 0, st>>>(
-      mkP(p), mkS(s), mu, kappa, zl_out, zu_out);
+  { k_reset_bound_multipliers<<<grid_for(p->np), RT, 0, st>>>(
+      mkP(p), mkS(s), mu, kappa, zl_out, zu_out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -688,8 +846,8 @@ int ipm_affine_start_point(const ab_ipm_problem* p, const ab_ipm_state* s,
                            double beta_min, const double* dzl,
                            const double* dzu, double* zl_out, double* zu_out,
                            cudaStream_t st) {
-  k_affine_start_point<<<grid_for(p->np), RT, 0, st>>>(
-      mkP(p), mkS(s), beta_min, dzl, dzu, zl_out, zu_out);
+  { k_affine_start_point<<<grid_for(p->np), RT, 0, st>>>(
+      mkP(p), mkS(s), beta_min, dzl, dzu, zl_out, zu_out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -697,9 +855,9 @@ int ipm_barrier_dphi_kkt(const ab_ipm_problem* p, const ab_ipm_state* s,
                          const double* res, const double* px,
                          const double* diag, double* out, cudaStream_t st,
                          double* scratch) {
-  k_barrier_dphi_kkt<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), res, px, diag,
-                                                scratch);
-  k_sum1_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out);
+  { k_barrier_dphi_kkt<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), res, px, diag,
+                                                scratch); ab::count_launch(); }
+  { k_sum1_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -707,8 +865,8 @@ int ipm_relax_bounds(int np, const double* lbx, const double* ubx,
                      double* lo, double* hi, double factor, double tol,
                      cudaStream_t st) {
   if (np <= 0) return 0;
-  k_relax_bounds<<<grid_for(np), RT, 0, st>>>(np, lbx, ubx, lo, hi, factor,
-                                               tol);
+  { k_relax_bounds<<<grid_for(np), RT, 0, st>>>(np, lbx, ubx, lo, hi, factor,
+                                               tol); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -716,18 +874,43 @@ int ipm_initialize(const ab_ipm_problem* p, double* xlam, double* zl,
                    double* zu, double* sl, double* su, double kappa1,
                    double kappa2, cudaStream_t st) {
   if (p->np <= 0) return 0;
-  k_initialize<<<grid_for(p->np), RT, 0, st>>>(mkP(p), xlam, zl, zu, sl, su,
-                                                kappa1, kappa2);
+  { k_initialize<<<grid_for(p->np), RT, 0, st>>>(mkP(p), xlam, zl, zu, sl, su,
+                                                kappa1, kappa2); ab::count_launch(); }
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_seg_reduce(const ab_ipm_problem* p, const ab_ipm_state* s,
+                   double tau, const double* grad, const double* px,
+                   const double* dzl, const double* dzu, const double* gf,
+                   double* out, cudaStream_t st) {
+  if (p->ninst <= 0) return 0;
+  { k_seg_reduce<<<p->ninst, RT, 0, st>>>(mkP(p), mkS(s), tau, grad, px, dzl,
+                                        dzu, gf, out); ab::count_launch(); }
+  return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
+}
+
+int ipm_apply_step_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
+                       const double* ax, const double* az, const double* dxlam,
+                       const double* dzl, const double* dzu, double* xlam_new,
+                       double* zl_new, double* zu_new, double* sl_new,
+                       double* su_new, cudaStream_t st) {
+  long long m = p->n > p->np ? p->n : p->np;
+  { k_apply_step_seg<<<grid_for(m), RT, 0, st>>>(mkP(p), mkS(s), ax, az, dxlam,
+                                               dzl, dzu, xlam_new, zl_new,
+                                               zu_new, sl_new, su_new); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
 int ipm_refine_init(const ab_ipm_problem* p, const ab_ipm_state* s,
                     double mu, const double* grad, const double* rhs_saved,
                     const double* px, double* dzl, double* dzu, double* out,
-                    cudaStream_t st, double* scratch) {
-  k_ir_init<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, rhs_saved,
-                                       px, dzl, dzu, scratch);
-  k_max2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out);
+                    cudaStream_t st, double* scratch, double* seg) {
+  if (seg && cudaMemsetAsync(seg, 0, sizeof(double) * p->ninst, st) !=
+                 cudaSuccess)
+    return AB_ERR_CUDA;
+  { k_ir_init<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, rhs_saved,
+                                       px, dzl, dzu, scratch, seg); ab::count_launch(); }
+  { k_max2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -736,21 +919,24 @@ int ipm_refine_residual(const ab_ipm_problem* p, const ab_ipm_state* s,
                         const double* kpx, const double* px, const double* dzl,
                         const double* dzu, double* e_cond, double* e_zl,
                         double* e_zu, double* out, cudaStream_t st,
-                        double* scratch) {
-  k_ir_residual<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, rhs_saved,
+                        double* scratch, double* seg) {
+  if (seg && cudaMemsetAsync(seg, 0, sizeof(double) * 2 * p->ninst, st) !=
+                 cudaSuccess)
+    return AB_ERR_CUDA;
+  { k_ir_residual<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, rhs_saved,
                                            kpx, px, dzl, dzu, e_cond, e_zl,
-                                           e_zu, scratch);
-  k_max2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out);
+                                           e_zu, scratch, seg); ab::count_launch(); }
+  { k_max2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
 int ipm_refine_update(const ab_ipm_problem* p, const ab_ipm_state* s,
                       const double* corr, const double* e_zl,
                       const double* e_zu, double* px, double* dzl,
-                      double* dzu, cudaStream_t st) {
+                      double* dzu, cudaStream_t st, const int* active) {
   long long m = p->n > p->np ? p->n : p->np;
-  k_ir_update<<<grid_for(m), RT, 0, st>>>(mkP(p), mkS(s), corr, e_zl, e_zu,
-                                          px, dzl, dzu);
+  { k_ir_update<<<grid_for(m), RT, 0, st>>>(mkP(p), mkS(s), corr, e_zl, e_zu,
+                                          px, dzl, dzu, active); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -842,8 +1028,8 @@ extern "C" int ab_ipm_max_step_noalloc(const ab_ipm_problem* p,
   cudaStream_t st = (cudaStream_t)stream;
   // Every block writes its two partials before the final pass reads them,
   // so nothing in the array has to start at zero.
-  ab::k_max_step<<<grid, ab::RT, 0, st>>>(ab::mkP(p), ab::mkS(s), tau, px, dzl,
-                                          dzu, pv, pi);
-  ab::k_max_step_final<<<1, 32, 0, st>>>(grid, p->pidx, pv, pi, out, iout);
+  { ab::k_max_step<<<grid, ab::RT, 0, st>>>(ab::mkP(p), ab::mkS(s), tau, px, dzl,
+                                          dzu, pv, pi); ab::count_launch(); }
+  { ab::k_max_step_final<<<1, 32, 0, st>>>(grid, p->pidx, pv, pi, out, iout); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? AB_OK : AB_ERR_CUDA;
 }

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "ldl_internal.h"
+#include "launch_count.h"
 
 namespace ab {
 namespace {
@@ -848,9 +849,9 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       long long bytes = (fm * fm + fm * NB) * 8;
       if (bytes < (long long)kTileSmem * 8) bytes = (long long)kTileSmem * 8;
       if (bytes > kMaxDynSmem) bytes = kMaxDynSmem;
-      k_factor_level<<<L.nsmall, NT, (size_t)bytes, s>>>(
+      { k_factor_level<<<L.nsmall, NT, (size_t)bytes, s>>>(
           d, d.sched_nodes + L.small_begin, L.nsmall, d_vals, h.ustab,
-          h.pivot_tol, (int)(bytes / 8));
+          h.pivot_tol, (int)(bytes / 8)); ab::count_launch(); }
     }
     if (trace) cudaEventRecord(ev[3 * l + 1], s);
     if (L.nbig) {
@@ -860,11 +861,11 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       int gz = (int)std::min<long long>(512, (fm * fm + 4095) / 4096);
       int ga = (int)std::min<long long>(256, (L.big_max_amap + NT - 1) / NT);
       int ge = (int)std::min<long long>(1024, fm);
-      k_big_setup<<<B, NT, 0, s>>>(d, nodes);
-      k_big_zero<<<dim3(B, std::max(gz, 1)), NT, 0, s>>>(d, nodes);
-      k_big_add_A<<<dim3(B, std::max(ga, 1)), NT, 0, s>>>(d, nodes, d_vals);
+      { k_big_setup<<<B, NT, 0, s>>>(d, nodes); ab::count_launch(); }
+      { k_big_zero<<<dim3(B, std::max(gz, 1)), NT, 0, s>>>(d, nodes); ab::count_launch(); }
+      { k_big_add_A<<<dim3(B, std::max(ga, 1)), NT, 0, s>>>(d, nodes, d_vals); ab::count_launch(); }
       for (int q = 0; q < L.big_max_kids; q++)
-        k_big_extend<<<dim3(B, std::max(ge, 1)), NT, 0, s>>>(d, nodes, q);
+        { k_big_extend<<<dim3(B, std::max(ge, 1)), NT, 0, s>>>(d, nodes, q); ab::count_launch(); }
       const long long ntl = (fm + kTile - 1) / kTile;
       int gu = (int)std::min<long long>(4 * 148, ntl * (ntl + 1) / 2);
       int panels = (int)((L.big_max_fs + NB - 2) / (NB - 1)) + 2;
@@ -875,14 +876,14 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       for (;;) {
         budget += panels;
         for (int it = 0; it < panels; it++) {
-          k_big_panel<<<B, kPanelThreads, 0, s>>>(d, nodes, h.ustab,
-                                                  h.pivot_tol);
-          k_big_update<<<dim3(B, std::max(gu, 1)), NT, kTileSmem * 8, s>>>(
-              d, nodes);
+          { k_big_panel<<<B, kPanelThreads, 0, s>>>(d, nodes, h.ustab,
+                                                  h.pivot_tol); ab::count_launch(); }
+          { k_big_update<<<dim3(B, std::max(gu, 1)), NT, kTileSmem * 8, s>>>(
+              d, nodes); ab::count_launch(); }
         }
         // Delayed pivots received from the children can make a front need
         // more panels than its static size implies: check and continue.
-        k_big_remaining<<<1, 32, 0, s>>>(d, nodes, B, d.scratch_int);
+        { k_big_remaining<<<1, 32, 0, s>>>(d, nodes, B, d.scratch_int); ab::count_launch(); }
         int left = 0;
         FCUDA(cudaMemcpyAsync(&left, d.scratch_int, sizeof(int),
                               cudaMemcpyDeviceToHost, s));
@@ -894,7 +895,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
         }
         panels = 4;
       }
-      k_big_finalize<<<B, NT, 0, s>>>(d, nodes);
+      { k_big_finalize<<<B, NT, 0, s>>>(d, nodes); ab::count_launch(); }
     }
     if (trace) cudaEventRecord(ev[3 * l + 2], s);
   }

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "ldl_internal.h"
+#include "launch_count.h"
 
 namespace ab {
 namespace {
@@ -273,15 +274,15 @@ int solve_numeric(LdlHandle& h, double* d_x, int nrhs, int ldx,
   for (int l = 0; l < d.num_levels; l++) {
     const int b = h.level_ptr[l], cnt = h.level_ptr[l + 1] - b;
     if (cnt)
-      k_solve_forward<<<cnt, NT, smem[l], s>>>(d, d.level_nodes + b, d_x, nrhs,
-                                               ldx, h.ubuf, h.uoff, smem[l] / 8);
+      { k_solve_forward<<<cnt, NT, smem[l], s>>>(d, d.level_nodes + b, d_x, nrhs,
+                                               ldx, h.ubuf, h.uoff, smem[l] / 8); ab::count_launch(); }
   }
   for (int l = d.num_levels - 1; l >= 0; l--) {
     const int b = h.level_ptr[l], cnt = h.level_ptr[l + 1] - b;
     if (cnt)
-      k_solve_backward<<<cnt, NT, smem[l], s>>>(d, d.level_nodes + b, d_x,
+      { k_solve_backward<<<cnt, NT, smem[l], s>>>(d, d.level_nodes + b, d_x,
                                                 nrhs, ldx, h.ubuf, h.uoff,
-                                                smem[l] / 8);
+                                                smem[l] / 8); ab::count_launch(); }
   }
   SCUDA(cudaGetLastError());
   return 0;

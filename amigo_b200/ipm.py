@@ -244,3 +244,80 @@ class InteriorPointOptimizer:
                 _dev(res).data_ptr(), _dev(px).data_ptr(),
                 _dev(diag).data_ptr(), self._out.data_ptr(), self._s())
         return float(self._out[0].item())
+
+
+class BatchedInteriorPointOptimizer(InteriorPointOptimizer):
+    """InteriorPointOptimizer over independent instances stored one after
+    another (`vinst[i]` = instance of entry i, non-decreasing).  Every
+    kernel that takes the barrier parameter reads instance k's value from
+    `mu` (a device array set with set_barrier_params); seg_reduce returns
+    per-instance norms, step lengths and merit terms, and
+    apply_step_seg / the *_seg refinement steps act per instance."""
+
+    def __init__(self, mult, lower, upper, vinst, device=None):
+        super().__init__(mult, lower, upper, device=device)
+        vinst = np.ascontiguousarray(vinst, dtype=np.int32)
+        if len(vinst) != self.n or np.any(np.diff(vinst) < 0):
+            raise ValueError("vinst must be non-decreasing with one entry per row")
+        self.ninst = int(vinst[-1]) + 1 if len(vinst) else 0
+        pidx, cidx = self.pidx.cpu().numpy(), self.cidx.cpu().numpy()
+        pinst, cinst = vinst[pidx], vinst[cidx]
+        cnt = lambda a: np.concatenate([[0], np.cumsum(np.bincount(a, minlength=self.ninst))])
+        poff, coff = cnt(pinst).astype(np.int32), cnt(cinst).astype(np.int32)
+        self.np_each = np.diff(poff)
+        self.nc_each = np.diff(coff)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+        self.vinst, self.pinst = t(vinst), t(pinst)
+        self.poff, self.coff = t(poff), t(coff)
+        f64 = dict(dtype=torch.float64, device=self.device)
+        self.mu = torch.zeros(self.ninst, **f64)
+        self.mu0 = torch.zeros(self.ninst, **f64)
+        self._seg = torch.zeros(self.ninst * 10, **f64)
+        self._ir = torch.zeros(self.ninst * 2, **f64)
+        self._p = self._mk(self.mu)
+        self._pz = self._mk(self.mu0)
+
+    def _mk(self, mu):
+        p = _lib.IpmProblem(self.n, self.np_, self.nc_, self.pidx.data_ptr(),
+                            self.cidx.data_ptr(), self.lbx.data_ptr(),
+                            self.ubx.data_ptr(), self.lbh.data_ptr())
+        p.mu_inst, p.pinst, p.vinst = mu.data_ptr(), self.pinst.data_ptr(), self.vinst.data_ptr()
+        p.ninst, p.poff, p.coff = self.ninst, self.poff.data_ptr(), self.coff.data_ptr()
+        return p
+
+    def set_barrier_params(self, mu):
+        self.mu.copy_(torch.as_tensor(np.asarray(mu, dtype=np.float64)))
+
+    def residual(self, vars, grad, res):
+        """compute_residual with each instance's barrier parameter (no
+        norm, no synchronisation)."""
+        r = _dev(res)
+        r.zero_()
+        self._c("ab_ipm_residual", ctypes.byref(self._state(vars)), 0.0,
+                _dev(grad).data_ptr(), r.data_ptr(), None, self._s())
+
+    def seg_reduce(self, vars, grad=None, upd=None, gf=None, tau=0.0,
+                   zero_mu=False):
+        """Per-instance quantities as a (ninst, 10) host array (see
+        ab_ipm_seg_reduce): 0 dual, 1 primal, 2 comp inf-norms, 3 constraint
+        violation 1-norm, 4 barrier log-sum, 5/6 primal/dual step,
+        7 barrier directional derivative, 8 max |lam + dlam|."""
+        p = self._pz if zero_mu else self._p
+        ptr = lambda a: None if a is None else a.data_ptr()
+        _lib.call("ab_ipm_seg_reduce", ctypes.byref(p),
+                  ctypes.byref(self._state(vars)), float(tau),
+                  ptr(None if grad is None else _dev(grad)),
+                  ptr(None if upd is None else upd.x),
+                  ptr(None if upd is None else upd.zl),
+                  ptr(None if upd is None else upd.zu),
+                  ptr(None if gf is None else _dev(gf)),
+                  self._seg.data_ptr(), self._s())
+        return self._seg.view(self.ninst, 10).cpu().numpy()
+
+    def apply_step_seg(self, ax, az, vars, upd, tmp):
+        """tmp = vars + (ax[k], az[k]) * upd per instance; ax, az device."""
+        self._c("ab_ipm_apply_step_seg", ctypes.byref(self._state(vars)),
+                ax.data_ptr(), az.data_ptr(), upd.x.data_ptr(),
+                upd.zl.data_ptr(), upd.zu.data_ptr(), tmp.x.data_ptr(),
+                tmp.zl.data_ptr(), tmp.zu.data_ptr(), tmp.sl.data_ptr(),
+                tmp.su.data_ptr(), self._s())

@@ -111,13 +111,17 @@ class CSRMat:
         self.vals = torch.from_numpy(self.host_data.copy()).to(self.device)
         self.d_rowp = torch.from_numpy(self.rowp).to(self.device)
         self.d_cols = torch.from_numpy(self.cols).to(self.device)
-        diag = np.full(self.nrows, -1, dtype=np.int32)
-        for i in range(self.nrows):
-            row = self.cols[self.rowp[i]:self.rowp[i + 1]]
-            hit = np.nonzero(row == i)[0]
-            if len(hit):
-                diag[i] = self.rowp[i] + hit[0]
-        self.diag = diag
+        # first position of column i in row i, -1 when absent
+        diag = np.full(self.nrows, -1, dtype=np.int64)
+        rows = np.repeat(np.arange(self.nrows), np.diff(self.rowp))
+        hit = np.nonzero(self.cols[: self.nnz] == rows)[0]
+        if len(hit):
+            r = rows[hit]
+            first = np.ones(len(hit), bool)
+            first[1:] = r[1:] != r[:-1]
+            diag[r[first]] = hit[first]
+        self.diag = diag.astype(np.int32)
+        diag = self.diag
         self.d_diag = torch.from_numpy(np.maximum(diag, 0)).to(self.device)
 
     def get_nonzero_structure(self):

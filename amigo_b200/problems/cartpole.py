@@ -107,3 +107,57 @@ class CartPole:
     def device_model(self, device):
         from amigo_b200.fem import CartPoleDevice
         return CartPoleDevice(self, device)
+
+
+class CartPoleBatch:
+    """Independent cart-pole instances stored one after another (the
+    batched-trajectories config: N ~ U{50..400}, pole mass ~ U(0.1, 0.5),
+    final cart position ~ U(-1, 1), from the seed)."""
+
+    def __init__(self, instances):
+        self.inst = list(instances)
+        self.k = len(self.inst)
+        ns = [m.n for m in self.inst]
+        self.var_off = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+        self.nnz_off = np.concatenate([[0], np.cumsum([m.nnz for m in self.inst])])
+        self.n = int(self.var_off[-1])
+        self.nnz = int(self.nnz_off[-1])
+        cat = lambda f: np.concatenate([f(m) for m in self.inst])
+        self.mult = cat(lambda m: m.mult)
+        self.lower = cat(lambda m: m.lower)
+        self.upper = cat(lambda m: m.upper)
+        self.x0 = cat(lambda m: m.x0)
+        self.iv = np.concatenate([m.iv + o for m, o in zip(self.inst, self.var_off)]).astype(np.int32)
+        self.ipos = np.concatenate([m.ipos + o for m, o in zip(self.inst, self.nnz_off)]).astype(np.int32)
+        self.bv = np.concatenate([m.bv + o for m, o in zip(self.inst, self.var_off)]).astype(np.int32)
+        self.bpos = np.concatenate([m.bpos + o for m, o in zip(self.inst, self.nnz_off)]).astype(np.int32)
+        self.h_iv = cat(lambda m: np.full(m.N, m.h))
+        self.m_iv = cat(lambda m: np.full(m.N, m.m_pole))
+        self.inst_iv = np.concatenate([[0], np.cumsum([m.N for m in self.inst])]).astype(np.int32)
+        self.vinst = np.repeat(np.arange(self.k), ns).astype(np.int32)
+        self.diag_pos = np.concatenate([m.diag_pos + o for m, o in zip(self.inst, self.nnz_off)])
+        self.N = int(self.inst_iv[-1])
+        self.npr = int((~self.mult).sum())
+        # block-diagonal CSR of the whole batch
+        self.rowp = np.concatenate([[0]] + [m.rowp[1:] + o for m, o in
+                                            zip(self.inst, self.nnz_off)]).astype(np.int32)
+        self.cols = np.concatenate([m.cols + o for m, o in
+                                    zip(self.inst, self.var_off)]).astype(np.int32)
+
+    def patterns(self):
+        return [(m.n, m.rowp, m.cols) for m in self.inst]
+
+    def device_model(self, device):
+        from amigo_b200.fem import CartPoleDevice
+        return CartPoleDevice(self, device, batch=True)
+
+
+def batch_config(k=512, seed=0, nmin=50, nmax=400):
+    """The batched-trajectories config: k instances from the seed."""
+    r = np.random.RandomState(seed)
+    Ns = r.randint(nmin, nmax + 1, size=k)
+    ms = r.uniform(0.1, 0.5, size=k)
+    xfs = r.uniform(-1.0, 1.0, size=k)
+    return CartPoleBatch([CartPole(N=int(N), m_pole=float(mp), xf=float(xf),
+                                   seed=seed + 1 + i)
+                          for i, (N, mp, xf) in enumerate(zip(Ns, ms, xfs))])

@@ -44,6 +44,10 @@ def parse():
     ap.add_argument("--nx", type=int, default=128)
     ap.add_argument("--ny", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--solves", type=int, default=5)
+    ap.add_argument("--no-ipm-solve", action="store_true")
+    ap.add_argument("--batch", type=int, default=512,
+                    help="instances in the batched cart-pole solve (0: skip)")
     return ap.parse_args()
 
 
@@ -190,18 +194,6 @@ class Core:
         return inertia
 
 
-def count_launches(core):
-    """Kernels of ours launched per step: element kernels, IPM kernels, the
-    factor (one per level) and the solves (two per level, two solves)."""
-    st = core.ldl.stats()
-    L = st["levels"]
-    hess = 4 + 1 + 2          # colours + global + fixed rows/diagonal
-    grad = 4 + 1 + 1
-    ipm = 1 + 1 + 1 + 2 + 1   # diagonal, residual, bound-dual, max-step (2), apply
-    csr = 1 + 1               # add_diagonal, matvec
-    return hess + grad + ipm + csr + L + 2 * (2 * L)
-
-
 def run_ours(args, rank, world, local):
     import torch
     torch.cuda.set_device(local)
@@ -221,6 +213,10 @@ def run_ours(args, rank, world, local):
           for _ in range(args.steps)]
     fev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
+    sev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    from amigo_b200 import _lib
+    launches0 = _lib.lib().ab_launch_count()
     clk = ClockSampler(os.path.join(ROOT, "gpurun_out" if os.path.isdir(
         os.path.join(ROOT, "gpurun_out")) else ".", "clocks_rank%d.csv" % rank), local)
     t0 = time.time()
@@ -240,10 +236,12 @@ def run_ours(args, rank, world, local):
             opt, v = core.opt, core.vars
             opt.compute_residual(core.mu, v, core.grad, core.res)
             core.px.copy_(core.res)
+            sev[k][0].record(stream)
             core.ldl.solve_device(core.px)
             core.K.mult(core.px, core.kp)
             torch.sub(core.res, core.kp, out=core.r2)
             core.ldl.solve_device(core.r2)
+            sev[k][1].record(stream)
             core.px.add_(core.r2)
             opt.compute_update(core.mu, v, core.px, core.upd)
             ax, xi, az, zi = opt.compute_max_step(0.99, v, core.upd)
@@ -252,8 +250,10 @@ def run_ours(args, rank, world, local):
             ev[k][1].record(stream)
         torch.cuda.synchronize()
     wall = time.time() - t0
+    launches = _lib.lib().ab_launch_count() - launches0
     step_ms = [a.elapsed_time(b) for a, b in ev]
     fac_ms = [a.elapsed_time(b) for a, b in fev]
+    sol_ms = [a.elapsed_time(b) for a, b in sev]
     dev_ms = float(np.sum(step_ms))
     fac_tot = float(np.sum(fac_ms))
     dev_ms, fac_tot = max_over_ranks([dev_ms, fac_tot], device)
@@ -281,12 +281,98 @@ def run_ours(args, rank, world, local):
         "ipm_iterations_per_s": round(world * args.steps / (dev_ms * 1e-3), 3),
         "wall_s": round(wall, 3),
         "e2e": e2e,
-        "gpu_launches": count_launches(core) * args.steps,
+        "gpu_launches": int(launches),
+        "solve_ms_per_step": round(float(np.sum(sol_ms)) / args.steps, 4),
         "clocks": clk.summary(),
         "ldl_stats": st,
     }
     out["roofline"] = roofline(core, fac_tot / args.steps)
+    if not args.no_ipm_solve:
+        out["ipm_solve"] = ipm_solve_bench(device, args.solves)
+        if args.batch > 0:
+            out["batch_solve"] = batch_solve_bench(device, args.batch)
     return out
+
+
+def batch_solve_bench(device, k, sequential_sample=8):
+    """The batched-trajectories config: k cart-pole instances (N ~
+    U{50..400}, pole mass ~ U(0.1, 0.5), final position ~ U(-1, 1), seed 0)
+    solved together, one launch per IPM phase over all instances; beside it
+    the same instances solved one after another by the single-problem
+    device path (a sample of `sequential_sample`, extrapolated)."""
+    import torch
+    from amigo_b200 import ipm_driver
+    from amigo_b200.problems.cartpole import batch_config
+    ipm_driver.solve_batch(batch_config(k=4, seed=1), device)   # warm-up
+    B = batch_config(k=k, seed=0)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    r = ipm_driver.solve_batch(B, device)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t
+    seq = []
+    for m in B.inst[:sequential_sample]:
+        t1 = time.perf_counter()
+        one = ipm_driver.solve(ipm_driver.DeviceBackend(
+            ipm_driver.CartPoleProblem(m, device), m, device))
+        torch.cuda.synchronize()
+        seq.append(time.perf_counter() - t1)
+    return {"workload": "%d cart-pole instances, N~U{50..400}, one launch per "
+                        "IPM phase, FP64" % k,
+            "n_total": int(B.n), "nnz_total": int(B.nnz),
+            "solves_per_s": round(k / wall, 3),
+            "wall_s": round(wall, 3), "setup_s": round(float(r["setup_s"]), 3),
+            "converged": int(r["converged"].sum()),
+            "max_iterations": int(r["iterations"].max()),
+            "max_kkt_error": float(r["kkt_error"].max()),
+            "sequential_single_path_solves_per_s":
+                round(len(seq) / float(np.sum(seq)), 3),
+            "sequential_sample": "first %d instances, single-problem device "
+                                 "path, one after another" % len(seq)}
+
+
+def ipm_solve_bench(device, solves):
+    """Whole interior-point solves of the cart-pole config (N = 100, n = 913)
+    on the GPU core: solves/s and latency percentiles over `solves` solves
+    after one warm-up solve."""
+    import torch
+    from amigo_b200 import ipm_driver
+    from amigo_b200.problems.cartpole import CartPole
+    m = CartPole(N=100, seed=0)
+    B = ipm_driver.DeviceBackend(ipm_driver.CartPoleProblem(m, device), m, device)
+    r = ipm_driver.solve(B)
+    lat = []
+    for _ in range(solves):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = ipm_driver.solve(B)
+        torch.cuda.synchronize()
+        lat.append(time.perf_counter() - t)
+    lat = np.array(lat)
+    return {"workload": "cart-pole swing-up N=100 (n=913), full IPM solve, FP64",
+            "solves_per_s": round(float(len(lat) / lat.sum()), 4),
+            "p50_ms": round(1e3 * float(np.percentile(lat, 50)), 2),
+            "p99_ms": round(1e3 * float(np.percentile(lat, 99)), 2),
+            "iterations": int(r["iterations"]), "objective": r["objective"],
+            "kkt_error": r["kkt_error"], "converged": bool(r["converged"]),
+            "solves": int(len(lat))}
+
+
+def ipm_solve_host_baseline():
+    """The same driver over the reference's own SparseLDL + IPM vector code
+    on the host (oracle/host_backend.py): one solve."""
+    from amigo_b200 import ipm_driver
+    from amigo_b200.problems.cartpole import CartPole
+    from oracle.host_backend import HostBackend
+    m = CartPole(N=100, seed=0)
+    t = time.perf_counter()
+    r = ipm_driver.solve(HostBackend(m))
+    dt = time.perf_counter() - t
+    return {"solves_per_s": round(1.0 / dt, 4), "iterations": int(r["iterations"]),
+            "objective": r["objective"], "kkt_error": r["kkt_error"],
+            "kind": "reference", "cores": 1,
+            "sample": "1 cart-pole N=100 solve: same driver, reference SparseLDL "
+                      "and interior_point_backend.h on the host"}
 
 
 def roofline(core, fac_ms):
@@ -480,6 +566,8 @@ def main():
                 from oracle import ref
                 if ref.available():
                     out["cpu_baseline"] = cpu_baseline()
+                    if "ipm_solve" in out:
+                        out["ipm_solve"]["host_reference_core"] = ipm_solve_host_baseline()
         if rank == 0 and out is not None:
             print(json.dumps(out))
     finally:

@@ -94,6 +94,11 @@ int ab_ldl_batch_inertia(ab_ldl_t h, void* stream, int* npos, int* nneg);
 int ab_ldl_batch_sizes(ab_ldl_t h, int* nprob, int* n_total,
                        long long* nnz_total);
 
+/* Number of kernels this library has launched in the process so far (every
+ * kernel of every entry point; library memsets excluded).  No reference
+ * counterpart: it lets callers count the device launches of a region. */
+long long ab_launch_count(void);
+
 /* Statistics of the last factorization (host values; synchronises).
  * flops: sum over fronts of p^3/3 + p^2 c + p c^2 with p = pivots, c =
  * contribution size; factor_entries: sum f*p; max_front; num_delayed:
@@ -127,6 +132,18 @@ typedef struct ab_ipm_problem {
   const double* lbx;
   const double* ubx;
   const double* lbh;
+  /* Batched problems (all NULL / 0 for a single problem): instances are
+   * stored one after another; mu_inst[k] is instance k's barrier parameter
+   * (used instead of the `mu` argument wherever it is set), pinst / vinst
+   * the instance of every primal entry / n-vector entry, and the primal and
+   * constraint entries of instance k are [poff[k], poff[k+1]) and
+   * [coff[k], coff[k+1]). */
+  const double* mu_inst;
+  const int* pinst;
+  const int* vinst;
+  int ninst;
+  const int* poff;
+  const int* coff;
 } ab_ipm_problem;
 
 typedef struct ab_ipm_state {
@@ -241,6 +258,50 @@ int ab_ipm_refine_update(const ab_ipm_problem* p, const ab_ipm_state* s,
                          const double* corr, const double* e_zl,
                          const double* e_zu, double* px, double* dzl,
                          double* dzu, void* stream);
+/* Batched problems: the refinement steps above with the barrier parameter
+ * of each entry's instance (p->mu_inst) and per-instance norms, so every
+ * instance applies the reference's stopping rule
+ * (amigo/algorithm/solvers/linear_solver.py:203-239) on its own:
+ *  refine_init_seg:     seg_out[k] = instance k's right-hand-side norm;
+ *  refine_residual_seg: seg_out[2k] = residual norm, seg_out[2k+1] =
+ *                       solution norm of instance k;
+ *  refine_update_seg:   applies the correction only to instances with
+ *                       active[k] != 0 (device array of ninst ints). */
+int ab_ipm_refine_init_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
+                           const double* grad, const double* rhs_saved,
+                           const double* px, double* dzl, double* dzu,
+                           double* seg_out, void* stream);
+int ab_ipm_refine_residual_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
+                               const double* grad, const double* rhs_saved,
+                               const double* kpx, const double* px,
+                               const double* dzl, const double* dzu,
+                               double* e_cond, double* e_zl, double* e_zu,
+                               double* seg_out, void* stream);
+int ab_ipm_refine_update_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
+                             const int* active, const double* corr,
+                             const double* e_zl, const double* e_zu,
+                             double* px, double* dzl, double* dzu,
+                             void* stream);
+/* Batched problems: per-instance reductions, one block per instance
+ * (deterministic).  out[k * 10 + q] for instance k: 0 dual, 1 primal,
+ * 2 complementarity inf-norms of compute_kkt_error (:450-466, with
+ * mu_inst[k]); 3 constraint violation 1-norm (:565-573); 4 barrier log-sum
+ * (:471-484); 5, 6 primal / dual fraction-to-boundary steps
+ * (compute_max_step :329-369, seeded at 1); 7 barrier directional
+ * derivative (:491-502, with gf); 8 max |lam + dlam| over the
+ * constraints.  Null inputs skip the quantities that need them.  tau < 0
+ * selects the per-instance fraction max(-tau, 1 - mu_inst[k]). */
+int ab_ipm_seg_reduce(const ab_ipm_problem* p, const ab_ipm_state* s,
+                      double tau, const double* grad, const double* px,
+                      const double* dzl, const double* dzu, const double* gf,
+                      double* out, void* stream);
+/* apply_step (:376-392) with step lengths ax[k], az[k] per instance. */
+int ab_ipm_apply_step_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
+                          const double* ax, const double* az,
+                          const double* dxlam, const double* dzl,
+                          const double* dzu, double* xlam_new, double* zl_new,
+                          double* zu_new, double* sl_new, double* su_new,
+                          void* stream);
 /* reset_bound_multipliers (:508-522) */
 int ab_ipm_reset_bound_multipliers(const ab_ipm_problem* p,
                                    const ab_ipm_state* s, double mu,
@@ -303,6 +364,40 @@ int ab_simp2d_gradient(const ab_simp2d* m, const double* x, double alpha,
 int ab_simp2d_hessian(const ab_simp2d* m, const double* x, double alpha,
                       double* vals, void* stream);
 
+/* The 3D SIMP full-space model (48 x 24 x 24 trilinear hexahedra): the
+ * same Lagrangian and field meanings as ab_simp2d with 8-node elements,
+ * 3 displacement components per node and 8 element colours:
+ *   ev   [nelems x 56]   u(24) rt(8) lam(24) indices
+ *   fv   [nelems x 17]   rt(8) re mu(8) indices
+ *   epos [nelems x 3136] CSR positions of ev x ev
+ *   fpos [nelems x 289]  CSR positions of fv x fv
+ *   K0   24 x 24 unit-modulus stiffness, A 8 x 8 filter matrix. */
+typedef struct ab_simp3d {
+  int n, nnz, nelems, nnodes;
+  int u0, rt0, re0, s_index, lam0, mu0, nu_index;
+  int color_ptr[9];
+  const int* color_elems;
+  const int* ev;
+  const int* fv;
+  const int* epos;
+  const int* fpos;
+  const int* vpos;
+  const int* spos;
+  const int* fixed;
+  const int* fixed_zero_pos;
+  const int* fixed_diag_pos;
+  const int* load_idx;
+  const double* load_val;
+  const double* K0;
+  const double* A;
+  int nfixed, nfixed_zero, nload;
+  double Bq, vcoef, volfrac, E0, Emin, penalty;
+} ab_simp3d;
+int ab_simp3d_gradient(const ab_simp3d* m, const double* x, double alpha,
+                       double* grad, void* stream);
+int ab_simp3d_hessian(const ab_simp3d* m, const double* x, double alpha,
+                      double* vals, void* stream);
+
 /* ----------------------------------------------------------------------
  * Component evaluation for the cart-pole trapezoidal-collocation model
  * (gradient and Hessian of the Lagrangian; exact derivatives by hyper-dual
@@ -314,15 +409,25 @@ typedef struct ab_cartpole {
   double h, M, m, l, g;
   const int* iv;    /* [N x 14]: z_k (5), z_k+1 (5), defect multipliers (4) */
   const int* ipos;  /* [N x 196] CSR positions of iv x iv */
-  const int* bv;    /* [2 x 8]: boundary states (4), multipliers (4) */
-  const int* bpos;  /* [2 x 64] CSR positions of bv x bv */
+  const int* bv;    /* [nbc x 8]: boundary states (4), multipliers (4) */
+  const int* bpos;  /* [nbc x 64] CSR positions of bv x bv */
+  /* Batches of instances stored one after another (NULL / 0 for a single
+   * model): per-interval step and pole mass, the number of boundary
+   * components, and each instance's interval range [inst_iv[b],
+   * inst_iv[b+1]) (objective per instance). */
+  const double* h_iv;
+  const double* m_iv;
+  int nbc;
+  int ninst;
+  const int* inst_iv;
 } ab_cartpole;
 
 int ab_cartpole_gradient(const ab_cartpole* m, const double* x, double alpha,
                          double* grad, void* stream);
 int ab_cartpole_hessian(const ab_cartpole* m, const double* x, double alpha,
                         double* vals, void* stream);
-/* objective value (trapezoidal integral of u^2) -> out[0] */
+/* objective value (trapezoidal integral of u^2) -> out[0], or out[b] per
+ * instance of a batch */
 int ab_cartpole_objective(const ab_cartpole* m, const double* x, double* out,
                           void* stream);
 

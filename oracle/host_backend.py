@@ -61,8 +61,9 @@ class HostBackend:
         xp = np.where(both, np.maximum(np.minimum(xp, ub - pu), lb + pl), xp)
         onlyl = hl & ~hu
         onlyu = hu & ~hl
-        xp = np.where(onlyl, np.maximum(xp, lb + 1e-2 * np.maximum(1.0, np.abs(lb))), xp)
-        xp = np.where(onlyu, np.minimum(xp, ub - 1e-2 * np.maximum(1.0, np.abs(ub))), xp)
+        with np.errstate(invalid="ignore"):
+            xp = np.where(onlyl, np.maximum(xp, lb + 1e-2 * np.maximum(1.0, np.abs(lb))), xp)
+            xp = np.where(onlyu, np.minimum(xp, ub - 1e-2 * np.maximum(1.0, np.abs(ub))), xp)
         x[self.pidx] = xp
         zl = np.where(hl, 1.0, 0.0)
         zu = np.where(hu, 1.0, 0.0)

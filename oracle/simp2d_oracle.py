@@ -1,5 +1,8 @@
-"""CPU restatement of the 2D SIMP full-space model's Lagrangian, gradient
-and Hessian (test infrastructure only; numpy).
+"""CPU restatement of the SIMP full-space models' Lagrangian, gradient and
+Hessian (test infrastructure only; numpy).  The same functions serve the 2D
+quad model (problems/simp2d.py) and the 3D hexahedron model
+(problems/simp3d.py): the element sizes come from the model's K0 (ND x ND)
+and filter matrix A (NV x NV).
 
 The reference ships no component code for this exact model (its
 generated per-component derivatives come from the absent A2D library, see
@@ -19,69 +22,74 @@ def _stiffness(m, r):
     return E, dE, d2E
 
 
+def _sizes(m):
+    nd, nv = m.K0.shape[0], m.A.shape[0]
+    return nd, nv, nd // nv
+
+
+def _split(m, x):
+    nd, nv, _ = _sizes(m)
+    return (x[m.ev[:, :nd]], x[m.ev[:, nd:nd + nv]], x[m.ev[:, nd + nv:]],
+            x[m.re0:m.re0 + m.nelems], x[m.fv[:, nv + 1:]])
+
+
 def lagrangian(m, x, alpha=1.0):
-    u = x[m.ev[:, :8]]
-    rt = x[m.ev[:, 8:12]]
-    lam = x[m.ev[:, 12:]]
-    re = x[m.re0:m.re0 + m.nelems]
-    mu = x[m.fv[:, 5:]]
+    nd, nv, dim = _sizes(m)
+    u, rt, lam, re, mu = _split(m, x)
     E, _, _ = _stiffness(m, rt.mean(axis=1))
     Ku = u @ m.K0.T
     L = alpha * (m.f @ x)                    # f^T u (f only has u entries)
     L += np.sum(E * np.sum(lam * Ku, axis=1))
-    L -= x[m.lam0:m.lam0 + 2 * m.nnodes] @ m.f[m.u0:m.u0 + 2 * m.nnodes]
-    L += np.sum(mu * (rt @ m.A.T)) - 0.25 * np.sum(mu.sum(axis=1) * re)
+    L -= x[m.lam0:m.lam0 + dim * m.nnodes] @ m.f[m.u0:m.u0 + dim * m.nnodes]
+    L += np.sum(mu * (rt @ m.A.T)) - np.sum(mu.sum(axis=1) * re) / nv
     L += x[m.nu0] * (re.sum() / m.nelems - m.volfrac - x[m.s0])
     return L
 
 
 def gradient(m, x, alpha=1.0):
+    nd, nv, dim = _sizes(m)
     g = np.zeros(m.n)
-    u = x[m.ev[:, :8]]
-    rt = x[m.ev[:, 8:12]]
-    lam = x[m.ev[:, 12:]]
-    re = x[m.re0:m.re0 + m.nelems]
-    mu = x[m.fv[:, 5:]]
+    u, rt, lam, re, mu = _split(m, x)
     E, dE, _ = _stiffness(m, rt.mean(axis=1))
     Ku = u @ m.K0.T
     Kl = lam @ m.K0.T
     lKu = np.sum(lam * Ku, axis=1)
-    np.add.at(g, m.ev[:, :8], E[:, None] * Kl)
-    np.add.at(g, m.ev[:, 8:12], 0.25 * (dE * lKu)[:, None] + mu @ m.A)
-    np.add.at(g, m.ev[:, 12:], E[:, None] * Ku)
-    np.add.at(g, m.fv[:, 4], -0.25 * mu.sum(axis=1) + x[m.nu0] / m.nelems)
-    np.add.at(g, m.fv[:, 5:], rt @ m.A.T - 0.25 * re[:, None])
-    fu = m.f[m.u0:m.u0 + 2 * m.nnodes]
-    g[m.u0:m.u0 + 2 * m.nnodes] += alpha * fu
-    g[m.lam0:m.lam0 + 2 * m.nnodes] -= fu
+    np.add.at(g, m.ev[:, :nd], E[:, None] * Kl)
+    np.add.at(g, m.ev[:, nd:nd + nv], (dE * lKu)[:, None] / nv + mu @ m.A)
+    np.add.at(g, m.ev[:, nd + nv:], E[:, None] * Ku)
+    np.add.at(g, m.fv[:, nv], -mu.sum(axis=1) / nv + x[m.nu0] / m.nelems)
+    np.add.at(g, m.fv[:, nv + 1:], rt @ m.A.T - re[:, None] / nv)
+    fu = m.f[m.u0:m.u0 + dim * m.nnodes]
+    g[m.u0:m.u0 + dim * m.nnodes] += alpha * fu
+    g[m.lam0:m.lam0 + dim * m.nnodes] -= fu
     g[m.nu0] += re.sum() / m.nelems - m.volfrac - x[m.s0]
     g[m.s0] += -x[m.nu0]
     return g
 
 
 def hessian_dense_blocks(m, x):
-    """Per-element 20x20 elasticity and 9x9 filter blocks."""
-    u = x[m.ev[:, :8]]
-    rt = x[m.ev[:, 8:12]]
-    lam = x[m.ev[:, 12:]]
+    """Per-element (2 ND + NV)^2 elasticity and (2 NV + 1)^2 filter blocks."""
+    nd, nv, _ = _sizes(m)
+    u, rt, lam, _, _ = _split(m, x)
     E, dE, d2E = _stiffness(m, rt.mean(axis=1))
     Ku = u @ m.K0.T
     Kl = lam @ m.K0.T
     lKu = np.sum(lam * Ku, axis=1)
-    ne = m.nelems
-    H = np.zeros((ne, 20, 20))
-    H[:, :8, 8:12] = 0.25 * (dE[:, None] * Kl)[:, :, None]
-    H[:, 8:12, :8] = np.transpose(H[:, :8, 8:12], (0, 2, 1))
-    H[:, :8, 12:] = E[:, None, None] * m.K0[None]
-    H[:, 12:, :8] = E[:, None, None] * m.K0.T[None]
-    H[:, 8:12, 8:12] = (0.0625 * d2E * lKu)[:, None, None]
-    H[:, 12:, 8:12] = 0.25 * (dE[:, None] * Ku)[:, :, None]
-    H[:, 8:12, 12:] = np.transpose(H[:, 12:, 8:12], (0, 2, 1))
-    Fb = np.zeros((9, 9))
-    Fb[5:, :4] = m.A
-    Fb[:4, 5:] = m.A.T
-    Fb[5:, 4] = -0.25
-    Fb[4, 5:] = -0.25
+    ne, k = m.nelems, 2 * nd + nv
+    R, L = slice(nd, nd + nv), slice(nd + nv, k)
+    H = np.zeros((ne, k, k))
+    H[:, :nd, R] = (dE[:, None] * Kl)[:, :, None] / nv
+    H[:, R, :nd] = np.transpose(H[:, :nd, R], (0, 2, 1))
+    H[:, :nd, L] = E[:, None, None] * m.K0[None]
+    H[:, L, :nd] = E[:, None, None] * m.K0.T[None]
+    H[:, R, R] = (d2E * lKu)[:, None, None] / (nv * nv)
+    H[:, L, R] = (dE[:, None] * Ku)[:, :, None] / nv
+    H[:, R, L] = np.transpose(H[:, L, R], (0, 2, 1))
+    Fb = np.zeros((2 * nv + 1, 2 * nv + 1))
+    Fb[nv + 1:, :nv] = m.A
+    Fb[:nv, nv + 1:] = m.A.T
+    Fb[nv + 1:, nv] = -1.0 / nv
+    Fb[nv, nv + 1:] = -1.0 / nv
     return H, Fb
 
 
@@ -90,7 +98,7 @@ def hessian_values(m, x, alpha=1.0):
     vals = np.zeros(m.nnz)
     H, Fb = hessian_dense_blocks(m, x)
     np.add.at(vals, m.epos.ravel(), H.reshape(-1))
-    np.add.at(vals, m.fpos.ravel(), np.broadcast_to(Fb.ravel(), (m.nelems, 81)).ravel())
+    np.add.at(vals, m.fpos.ravel(), np.broadcast_to(Fb.ravel(), (m.nelems, Fb.size)).ravel())
     np.add.at(vals, m.vpos.ravel(), 1.0 / m.nelems)
     np.add.at(vals, m.spos, -1.0)
     vals[m.fixed_zero_pos] = 0.0
