@@ -32,7 +32,7 @@ EXTRA = {"ipm_kernels.cu": ["--fmad=false"]}
 
 SOURCES = ["symbolic.cpp", "ldl_plan.cpp", "ldl_factor.cu", "ldl_solve.cu",
            "capi.cpp", "ipm_kernels.cu", "capi_ipm.cpp", "csr_kernels.cu",
-           "fem_simp.cu", "cartpole.cu"]
+           "fem_simp.cu", "cartpole.cu", "tc_kernels.cu"]
 
 
 def nvcc():

@@ -306,6 +306,25 @@ int ab_ldl_solve(ab_ldl_t H, double* d_x, int nrhs, int ldx, void* stream) {
   return ab::solve_numeric(H->h, d_x, nrhs, ldx, (cudaStream_t)stream);
 }
 
+int ab_ldl_set_precision(ab_ldl_t h, int bits) {
+  if (!h || (bits != 32 && bits != 64)) return AB_ERR_ARG;
+  h->h.precision = bits;
+  return AB_OK;
+}
+
+int ab_ldl_set_tensor_cores(ab_ldl_t h, int on) {
+  if (!h) return AB_ERR_ARG;
+  h->h.tensor_cores = on != 0;
+  return AB_OK;
+}
+
+int ab_ldl_set_wide_threshold(ab_ldl_t h, long long entries) {
+  if (!h || entries < 1) return AB_ERR_ARG;
+  h->h.wide_entries = entries;
+  h->h.solve_epoch = -1;
+  return AB_OK;
+}
+
 int ab_ldl_stats(ab_ldl_t H, void* stream, double* flops,
                  double* factor_entries, int* max_front, int* num_delayed,
                  int* levels) {

@@ -159,6 +159,23 @@ __device__ __forceinline__ void amin(double& v, int& i, double v2, int i2) {
   }
 }
 
+// Final combination of per-block partials by one warp: lane l folds blocks
+// l, l + 32, ... in order, then a fixed shuffle tree; the result (in lane
+// 0) does not depend on timing.  partial[b * stride + q] is block b's value.
+enum class Fold { Sum, Max, Min };
+__device__ __forceinline__ double fold_op(Fold op, double a, double b) {
+  return op == Fold::Sum ? a + b : (op == Fold::Max ? fmax(a, b) : fmin(a, b));
+}
+__device__ double warp_fold(const double* partial, int nblocks, int stride,
+                            int q, Fold op, double init) {
+  const int lane = threadIdx.x & 31;
+  double v = init;
+  for (int b = lane; b < nblocks; b += 32) v = fold_op(op, v, partial[b * stride + q]);
+  for (int o = 16; o > 0; o >>= 1)
+    v = fold_op(op, v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
 __global__ void k_max_step(P p, S s, double tau, const double* px,
                            const double* dzl, const double* dzu,
                            double* pv, int* pi) {
@@ -221,17 +238,21 @@ __global__ void k_max_step(P p, S s, double tau, const double* px,
 __global__ void k_max_step_final(int nblocks, const int* pidx,
                                  const double* pv, const int* pi,
                                  double* out, int* iout) {
-  if (threadIdx.x != 0) return;
-  double ax = 1.0, az = 1.0;
-  int xo = 0x7fffffff, zo = 0x7fffffff;
-  for (int b = 0; b < nblocks; b++) {
-    amin(ax, xo, pv[2 * b], pi[2 * b]);
-    amin(az, zo, pv[2 * b + 1], pi[2 * b + 1]);
+  // warp 0: primal step, warp 1: dual step; (value, first index) minimum
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w > 1) return;
+  double v = 1.0;
+  int o = 0x7fffffff;
+  for (int b = lane; b < nblocks; b += 32) amin(v, o, pv[2 * b + w], pi[2 * b + w]);
+  for (int sh = 16; sh > 0; sh >>= 1) {
+    const double v2 = __shfl_down_sync(0xffffffffu, v, sh);
+    const int o2 = __shfl_down_sync(0xffffffffu, o, sh);
+    amin(v, o, v2, o2);
   }
-  out[0] = ax;
-  out[1] = az;
-  iout[0] = xo == 0x7fffffff ? -1 : pidx[xo];
-  iout[1] = zo == 0x7fffffff ? -1 : pidx[zo];
+  if (lane == 0) {
+    out[w] = v;
+    iout[w] = o == 0x7fffffff ? -1 : pidx[o];
+  }
 }
 
 // ------------------------------------------------------------ apply step
@@ -346,16 +367,14 @@ __global__ void k_reductions(P p, S s, double mu, const double* grad,
 
 __global__ void k_reductions_final(int nblocks, const double* partial,
                                    double* out) {
-  const int t = threadIdx.x;
+  const int t = threadIdx.x >> 5;  // one warp per quantity
   if (t >= NQ) return;
-  double v = partial[t];
-  for (int b = 1; b < nblocks; b++) {
-    double x = partial[b * NQ + t];
-    if (t == 2) v = fmin(v, x);
-    else if (t == 3 || t == 4 || t == 5 || t == 8) v = fmax(v, x);
-    else v += x;
-  }
-  out[t] = v;
+  const Fold op = t == 2 ? Fold::Min
+                         : (t == 3 || t == 4 || t == 5 || t == 8) ? Fold::Max
+                                                                  : Fold::Sum;
+  const double init = t == 2 ? INFINITY : 0.0;
+  const double v = warp_fold(partial, nblocks, NQ, t, op, init);
+  if ((threadIdx.x & 31) == 0) out[t] = v;
 }
 
 // ------------------------------------------------------------ barrier dphi
@@ -578,14 +597,10 @@ __global__ void k_ir_update(P p, S s, const double* corr, const double* e_zl,
 }
 
 __global__ void k_max2_final(int nblocks, const double* partial, double* out) {
-  if (threadIdx.x != 0) return;
-  double a = 0.0, b = 0.0;
-  for (int k = 0; k < nblocks; k++) {
-    a = fmax(a, partial[2 * k]);
-    b = fmax(b, partial[2 * k + 1]);
-  }
-  out[0] = a;
-  out[1] = b;
+  const int t = threadIdx.x >> 5;
+  if (t > 1) return;
+  const double v = warp_fold(partial, nblocks, 2, t, Fold::Max, 0.0);
+  if ((threadIdx.x & 31) == 0) out[t] = v;
 }
 
 // ------------------------------------------------- batched (per instance)
@@ -696,21 +711,15 @@ __global__ void k_apply_step_seg(P p, S s, const double* ax, const double* az,
 }
 
 __global__ void k_sum2_final(int nblocks, const double* partial, double* out) {
-  if (threadIdx.x != 0) return;
-  double a = 0.0, b = 0.0;
-  for (int k = 0; k < nblocks; k++) {
-    a += partial[2 * k];
-    b += partial[2 * k + 1];
-  }
-  out[0] = a;
-  out[1] = b;
+  const int t = threadIdx.x >> 5;
+  if (t > 1) return;
+  const double v = warp_fold(partial, nblocks, 2, t, Fold::Sum, 0.0);
+  if ((threadIdx.x & 31) == 0) out[t] = v;
 }
 
 __global__ void k_sum1_final(int nblocks, const double* partial, double* out) {
-  if (threadIdx.x != 0) return;
-  double a = 0.0;
-  for (int k = 0; k < nblocks; k++) a += partial[2 * k];
-  out[0] = a;
+  const double v = warp_fold(partial, nblocks, 2, 0, Fold::Sum, 0.0);
+  if (threadIdx.x == 0) out[0] = v;
 }
 
 }  // namespace
@@ -770,7 +779,7 @@ int ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
   S ss = mkS(s);
   if (out2) {
     { k_residual<<<kRedBlocks, RT, 0, st>>>(pp, ss, mu, grad, res, scratch); ab::count_launch(); }
-    { k_sum2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out2); ab::count_launch(); }
+    { k_sum2_final<<<1, 64, 0, st>>>(kRedBlocks, scratch, out2); ab::count_launch(); }
   } else {
     long long m = p->np > p->nc ? p->np : p->nc;
     { k_residual<<<grid_for(m), RT, 0, st>>>(pp, ss, mu, grad, res, nullptr); ab::count_launch(); }
@@ -800,7 +809,7 @@ int ipm_max_step(const ab_ipm_problem* p, const ab_ipm_state* s, double tau,
   int* pi = reinterpret_cast<int*>(scratch + 2 * kRedBlocks);
   { k_max_step<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), tau, px, dzl, dzu, pv,
                                         pi); ab::count_launch(); }
-  { k_max_step_final<<<1, 32, 0, st>>>(kRedBlocks, p->pidx, pv, pi, out, iout); ab::count_launch(); }
+  { k_max_step_final<<<1, 64, 0, st>>>(kRedBlocks, p->pidx, pv, pi, out, iout); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -820,7 +829,7 @@ int ipm_reductions(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
                    const double* grad, double* out, cudaStream_t st,
                    double* scratch) {
   { k_reductions<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, scratch); ab::count_launch(); }
-  { k_reductions_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
+  { k_reductions_final<<<1, 32 * NQ, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -910,7 +919,7 @@ int ipm_refine_init(const ab_ipm_problem* p, const ab_ipm_state* s,
     return AB_ERR_CUDA;
   { k_ir_init<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, rhs_saved,
                                        px, dzl, dzu, scratch, seg); ab::count_launch(); }
-  { k_max2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
+  { k_max2_final<<<1, 64, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -926,7 +935,7 @@ int ipm_refine_residual(const ab_ipm_problem* p, const ab_ipm_state* s,
   { k_ir_residual<<<kRedBlocks, RT, 0, st>>>(mkP(p), mkS(s), mu, grad, rhs_saved,
                                            kpx, px, dzl, dzu, e_cond, e_zl,
                                            e_zu, scratch, seg); ab::count_launch(); }
-  { k_max2_final<<<1, 32, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
+  { k_max2_final<<<1, 64, 0, st>>>(kRedBlocks, scratch, out); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? 0 : AB_ERR_CUDA;
 }
 
@@ -1030,6 +1039,6 @@ extern "C" int ab_ipm_max_step_noalloc(const ab_ipm_problem* p,
   // so nothing in the array has to start at zero.
   { ab::k_max_step<<<grid, ab::RT, 0, st>>>(ab::mkP(p), ab::mkS(s), tau, px, dzl,
                                           dzu, pv, pi); ab::count_launch(); }
-  { ab::k_max_step_final<<<1, 32, 0, st>>>(grid, p->pidx, pv, pi, out, iout); ab::count_launch(); }
+  { ab::k_max_step_final<<<1, 64, 0, st>>>(grid, p->pidx, pv, pi, out, iout); ab::count_launch(); }
   return cudaGetLastError() == cudaSuccess ? AB_OK : AB_ERR_CUDA;
 }

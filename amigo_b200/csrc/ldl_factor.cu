@@ -25,8 +25,10 @@
 #include <cstdlib>
 #include <vector>
 
+#include "../../include/amigo_b200.h"
 #include "ldl_internal.h"
 #include "launch_count.h"
+#include "tc_update.cuh"
 
 namespace ab {
 namespace {
@@ -105,30 +107,30 @@ __device__ void block_argmax(CtlT<BT>& ctl, double v, int i, double v2) {
 // Symmetric interchange of rows/columns a < b of the lower triangle of F,
 // of the variable list and of the fully-summed permutation record
 // (reference: symm_swap, include/sparse_ldl.h:1252-1274).
-template <int BT>
-__device__ void symm_swap(double* F, int ld, int n, int* vars, int* fsperm,
+template <class T, int BT>
+__device__ void symm_swap(T* F, int ld, int n, int* vars, int* fsperm,
                           int a, int b) {
   const int tid = threadIdx.x;
   // rows a and b over columns [0, a)
   for (int j = tid; j < a; j += BT) {
-    double t = F[a + (size_t)j * ld];
+    T t = F[a + (size_t)j * ld];
     F[a + (size_t)j * ld] = F[b + (size_t)j * ld];
     F[b + (size_t)j * ld] = t;
   }
   // F[j, a] <-> F[b, j] for a < j < b
   for (int j = a + 1 + tid; j < b; j += BT) {
-    double t = F[j + (size_t)a * ld];
+    T t = F[j + (size_t)a * ld];
     F[j + (size_t)a * ld] = F[b + (size_t)j * ld];
     F[b + (size_t)j * ld] = t;
   }
   // F[j, a] <-> F[j, b] for j > b
   for (int j = b + 1 + tid; j < n; j += BT) {
-    double t = F[j + (size_t)a * ld];
+    T t = F[j + (size_t)a * ld];
     F[j + (size_t)a * ld] = F[j + (size_t)b * ld];
     F[j + (size_t)b * ld] = t;
   }
   if (tid == 0) {
-    double t = F[a + (size_t)a * ld];
+    T t = F[a + (size_t)a * ld];
     F[a + (size_t)a * ld] = F[b + (size_t)b * ld];
     F[b + (size_t)b * ld] = t;
     int tv = vars[a];
@@ -141,10 +143,10 @@ __device__ void symm_swap(double* F, int ld, int n, int* vars, int* fsperm,
 }
 
 // Swap rows a and b of W over columns [0, ncol).
-template <int BT>
-__device__ void swap_wrows(double* W, int ldw, int ncol, int a, int b) {
+template <class T, int BT>
+__device__ void swap_wrows(T* W, int ldw, int ncol, int a, int b) {
   for (int j = threadIdx.x; j < ncol; j += BT) {
-    double t = W[a + (size_t)j * ldw];
+    T t = W[a + (size_t)j * ldw];
     W[a + (size_t)j * ldw] = W[b + (size_t)j * ldw];
     W[b + (size_t)j * ldw] = t;
   }
@@ -158,25 +160,26 @@ constexpr int kTileSmem = 2 * kTile * TP;  // doubles
 // C tile (ti, tj) of the trailing block F[k:, k:] -= A * B^T with
 // A = F[k:, kstart:kstart+kw] (L columns of the panel) and
 // B = W[k:, 0:kw] (their L*D columns); only the lower triangle is written.
-__device__ void update_tile(double* F, int ld, const double* W, int ldw,
+template <class T>
+__device__ void update_tile(T* F, int ld, const T* W, int ldw,
                             int n, int k, int kstart, int kw, int ti, int tj,
-                            double* As, double* Bs) {
+                            T* As, T* Bs) {
   const int tid = threadIdx.x;
   const int r0 = k + ti * kTile, c0 = k + tj * kTile;
   for (int idx = tid; idx < kTile * kw; idx += NT) {
     const int rr = idx % kTile, jj = idx / kTile;
-    As[rr * TP + jj] = (r0 + rr < n) ? F[r0 + rr + (size_t)(kstart + jj) * ld] : 0.0;
-    Bs[rr * TP + jj] = (c0 + rr < n) ? W[c0 + rr + (size_t)jj * ldw] : 0.0;
+    As[rr * TP + jj] = (r0 + rr < n) ? F[r0 + rr + (size_t)(kstart + jj) * ld] : T(0);
+    Bs[rr * TP + jj] = (c0 + rr < n) ? W[c0 + rr + (size_t)jj * ldw] : T(0);
   }
   __syncthreads();
   const int tr = tid % 16, tc = tid / 16;  // 16 x 16 threads, 4 x 4 outputs each
-  double acc[4][4];
+  T acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+    for (int b = 0; b < 4; b++) acc[a][b] = T(0);
   for (int jj = 0; jj < kw; jj++) {
-    double av[4], bv[4];
+    T av[4], bv[4];
 #pragma unroll
     for (int a = 0; a < 4; a++) av[a] = As[(tr + 16 * a) * TP + jj];
 #pragma unroll
@@ -211,17 +214,18 @@ __device__ __forceinline__ void tile_coords(int t, int& ti, int& tj) {
 // doubles of shared memory) selects the tiled form used for fronts kept in
 // HBM; without it the entries are updated directly (fronts in shared
 // memory).
-__device__ void trailing_update(double* F, int ld, const double* W, int ldw,
+template <class T>
+__device__ void trailing_update(T* F, int ld, const T* W, int ldw,
                                 int n, int k, int kstart, int kw,
-                                double* tiles) {
+                                T* tiles) {
   const int m = n - k;
   if (m <= 0 || kw <= 0) return;
   const int tid = threadIdx.x;
   if (tiles == nullptr) {
     for (int c = 0; c < m; c++) {
-      double* Fc = F + (size_t)(k + c) * ld + k;
+      T* Fc = F + (size_t)(k + c) * ld + k;
       for (int r = c + tid; r < m; r += NT) {
-        double acc = Fc[r];
+        T acc = Fc[r];
         for (int j = 0; j < kw; j++)
           acc -= F[k + r + (size_t)(kstart + j) * ld] * W[k + c + (size_t)j * ldw];
         Fc[r] = acc;
@@ -244,24 +248,24 @@ __device__ void trailing_update(double* F, int ld, const double* W, int ldw,
 //           -> ctl.ctail.
 //   mode 1: column imax; src(r) = F[imax, r] for r < imax else F[r, imax];
 //           reduces max over [k, n) \ {imax} -> ctl.rowmax.
-template <int BT>
-__device__ void build_column(double* F, int ld, double* W, int ldw, int n,
+template <class T, int BT>
+__device__ void build_column(T* F, int ld, T* W, int ldw, int n,
                              int k, int kstart, int kw, int col, int mode,
                              int imax, int nc, CtlT<BT>& ctl, int* status) {
   const int tid = threadIdx.x;
   double bestv = -1.0, tailv = 0.0;
   int besti = 0x7fffffff;
   for (int r = k + tid; r < n; r += BT) {
-    double acc;
+    T acc;
     if (mode == 0) {
       acc = F[r + (size_t)k * ld];
     } else {
       acc = (r < imax) ? F[imax + (size_t)r * ld] : F[r + (size_t)imax * ld];
     }
     for (int j = 0; j < kw; j++)
-      acc -= F[r + (size_t)(kstart + j) * ld] * ctl.wrow[j];
+      acc -= F[r + (size_t)(kstart + j) * ld] * T(ctl.wrow[j]);
     W[r + (size_t)col * ldw] = acc;
-    const double a = fabs(acc);
+    const double a = fabs((double)acc);
     if (mode == 0) {
       if (r > k && r < nc) argmax_merge(bestv, besti, a, r);
       if (r >= nc) tailv = fmax(tailv, a);
@@ -290,8 +294,8 @@ __device__ void build_column(double* F, int ld, double* W, int ldw, int n,
 }
 
 // Load row `row` of W (columns 0..kw-1) into ctl.wrow.
-template <int BT>
-__device__ void load_wrow(const double* W, int ldw, int row, int kw, CtlT<BT>& ctl) {
+template <class T, int BT>
+__device__ void load_wrow(const T* W, int ldw, int row, int kw, CtlT<BT>& ctl) {
   for (int j = threadIdx.x; j < kw; j += BT) ctl.wrow[j] = W[row + (size_t)j * ldw];
   __syncthreads();
 }
@@ -301,8 +305,8 @@ __device__ void load_wrow(const double* W, int ldw, int row, int kw, CtlT<BT>& c
 // on while kw < NB - 1, each either eliminated (1x1 or 2x2, its L column(s)
 // written to F and its L*D column(s) kept in W) or delayed to the end of the
 // candidate set.  The trailing update of F[k:, k:] is left to the caller.
-template <int BT>
-__device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
+template <class T, int BT>
+__device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
                              bool root, int* vars, int* fsperm, double ustab,
                              double pivot_tol, int* status, CtlT<BT>& ctl, int& k_,
                              int& nc_, int& kw_) {
@@ -311,8 +315,8 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
   int k = k_, nc = nc_, kw = 0;
   const int kstart = k;
   while (kw < NB - 1 && k < nc) {
-    load_wrow<BT>(W, ldw, k, kw, ctl);
-    build_column<BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status);
+    load_wrow<T, BT>(W, ldw, k, kw, ctl);
+    build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status);
     const double wkk = W[k + (size_t)kw * ldw];
     const double abswkk = fabs(wkk);
     const int imax = ctl.imax;
@@ -325,8 +329,8 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
         step = 1;
         kpiv = k;
       } else if (k + 1 < nc) {
-        load_wrow<BT>(W, ldw, imax, kw, ctl);
-        build_column<BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
+        load_wrow<T, BT>(W, ldw, imax, kw, ctl);
+        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
         const double rowmax = ctl.rowmax;
         const double wii = W[imax + (size_t)(kw + 1) * ldw];
         const double abswii = fabs(wii);
@@ -360,8 +364,8 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
         step = 1;
         kpiv = k;
       } else {
-        load_wrow<BT>(W, ldw, imax, kw, ctl);
-        build_column<BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
+        load_wrow<T, BT>(W, ldw, imax, kw, ctl);
+        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
         const double rowmax = ctl.rowmax;
         const double abswii = fabs(W[imax + (size_t)(kw + 1) * ldw]);
         if (abswkk >= bk_alpha * colmax * (colmax / rowmax)) {
@@ -383,8 +387,8 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
     if (step == 0) {
       // Delay candidate k: move it to the end of the candidate set.
       if (k < nc - 1) {
-        symm_swap<BT>(F, ld, n, vars, fsperm, k, nc - 1);
-        swap_wrows<BT>(W, ldw, kw, k, nc - 1);
+        symm_swap<T, BT>(F, ld, n, vars, fsperm, k, nc - 1);
+        swap_wrows<T, BT>(W, ldw, kw, k, nc - 1);
         __syncthreads();
       }
       nc -= 1;
@@ -392,29 +396,29 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
     }
     const int ksrc = k + step - 1;
     if (kpiv != ksrc) {
-      symm_swap<BT>(F, ld, n, vars, fsperm, ksrc, kpiv);
-      swap_wrows<BT>(W, ldw, kw + step, ksrc, kpiv);
+      symm_swap<T, BT>(F, ld, n, vars, fsperm, ksrc, kpiv);
+      swap_wrows<T, BT>(W, ldw, kw + step, ksrc, kpiv);
       __syncthreads();
     }
     if (step == 1) {
-      const double d = W[k + (size_t)kw * ldw];
-      if (!isfinite(d) && tid == 0) atomicOr(status, ST_NAN);
-      const double dinv = zero_pivot ? 0.0 : 1.0 / d;
+      const T d = W[k + (size_t)kw * ldw];
+      if (!isfinite((double)d) && tid == 0) atomicOr(status, ST_NAN);
+      const T dinv = zero_pivot ? T(0) : T(1) / d;
       if (tid == 0) vars[3 * ld + k] = 0;  // 1x1 pivot
       for (int r = k + tid; r < n; r += BT) {
-        double w = W[r + (size_t)kw * ldw];
+        T w = W[r + (size_t)kw * ldw];
         F[r + (size_t)k * ld] = (r == k) ? w : w * dinv;
       }
     } else {
-      const double d11 = W[k + (size_t)kw * ldw];
-      const double d21 = W[k + 1 + (size_t)kw * ldw];
-      const double d22 = W[k + 1 + (size_t)(kw + 1) * ldw];
-      const double detinv = 1.0 / (d11 * d22 - d21 * d21);
-      if (!isfinite(detinv) && tid == 0) atomicOr(status, ST_NAN);
-      const double i00 = d22 * detinv, i10 = -d21 * detinv,
-                   i01 = -d21 * detinv, i11 = d11 * detinv;
+      const T d11 = W[k + (size_t)kw * ldw];
+      const T d21 = W[k + 1 + (size_t)kw * ldw];
+      const T d22 = W[k + 1 + (size_t)(kw + 1) * ldw];
+      const T detinv = T(1) / (d11 * d22 - d21 * d21);
+      if (!isfinite((double)detinv) && tid == 0) atomicOr(status, ST_NAN);
+      const T i00 = d22 * detinv, i10 = -d21 * detinv,
+              i01 = -d21 * detinv, i11 = d11 * detinv;
       for (int r = k + 2 + tid; r < n; r += BT) {
-        double w0 = W[r + (size_t)kw * ldw], w1 = W[r + (size_t)(kw + 1) * ldw];
+        T w0 = W[r + (size_t)kw * ldw], w1 = W[r + (size_t)(kw + 1) * ldw];
         F[r + (size_t)k * ld] = w0 * i00 + w1 * i10;
         F[r + (size_t)(k + 1) * ld] = w0 * i01 + w1 * i11;
       }
@@ -441,16 +445,17 @@ __device__ void panel_factor(double* F, int ld, double* W, int ldw, int n,
 
 // Factor the fully-summed columns [0, fs) of the n x n front F in one CTA.
 // Returns the number of pivots (== fs for a root front).
-__device__ int factor_front(double* F, int ld, double* W, int ldw, int n,
+template <class T>
+__device__ int factor_front(T* F, int ld, T* W, int ldw, int n,
                             int fs, bool root, int* vars, int* fsperm,
-                            double ustab, double pivot_tol, double* tiles,
+                            double ustab, double pivot_tol, T* tiles,
                             int* status, Ctl& ctl) {
   int nc = fs;
   int k = 0;
   while (k < nc) {
     const int kstart = k;
     int kw = 0;
-    panel_factor<NT>(F, ld, W, ldw, n, root, vars, fsperm, ustab, pivot_tol,
+    panel_factor<T, NT>(F, ld, W, ldw, n, root, vars, fsperm, ustab, pivot_tol,
                      status, ctl, k, nc, kw);
     trailing_update(F, ld, W, ldw, n, k, kstart, kw, tiles);
     __syncthreads();
@@ -461,6 +466,7 @@ __device__ int factor_front(double* F, int ld, double* W, int ldw, int n,
 // Front set-up shared by both paths (thread 0 sizes and allocates; all
 // threads fill the variable list and the fully-summed permutation record).
 // Returns false when the front must be skipped (a pool ran out earlier).
+template <class T>
 __device__ bool setup_front(const DevicePlan& d, int node, Ctl& ctl) {
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -475,13 +481,18 @@ __device__ bool setup_front(const DevicePlan& d, int node, Ctl& ctl) {
     ctl.f = f;
     ctl.fs = ns + ndin;
     if (!ctl.skip) {
-      // F followed by W, rounded to 8 doubles (64-byte alignment)
+      // F followed by W in elements of T, rounded to 64 bytes; the pool
+      // holds fcap doubles
+      constexpr unsigned long long al = 64 / sizeof(T);
       const unsigned long long need =
-          (((unsigned long long)f * f + (unsigned long long)f * NB) + 15) & ~7ull;
+          (((unsigned long long)f * f + (unsigned long long)f * NB) + 2 * al - 1) &
+          ~(al - 1);
+      const unsigned long long cap =
+          (unsigned long long)d.fcap * (sizeof(double) / sizeof(T));
       const unsigned long long ineed = (4ull * f + 15) & ~7ull;
       unsigned long long off = atomicAdd(&d.counters[0], need);
       unsigned long long ioff = atomicAdd(&d.counters[1], ineed);
-      if (off + need > (unsigned long long)d.fcap) {
+      if (off + need > cap) {
         atomicOr(d.status, ST_POOL_F);
         ctl.skip = 1;
       }
@@ -543,7 +554,8 @@ __device__ __forceinline__ int child_row_pos(const DevicePlan& d, int cb,
 // (include/sparse_ldl.h:1937-1968), from the pivot kinds recorded when each
 // pivot was accepted (0: 1x1, 1/2: first/second column of a 2x2 block),
 // plus the inverse of the fully-summed permutation used by the solves.
-__device__ void finish_front(const DevicePlan& d, int node, const double* F,
+template <class T>
+__device__ void finish_front(const DevicePlan& d, int node, const T* F,
                              int f, int fs, int npiv, int* fvars) {
   __shared__ int s_pos, s_neg;
   const int tid = threadIdx.x;
@@ -560,7 +572,7 @@ __device__ void finish_front(const DevicePlan& d, int node, const double* F,
   for (int j = tid; j < npiv; j += blockDim.x) {
     const int kd = kind[j];
     if (kd == 0) {
-      if (F[j + (size_t)j * f] >= 0.0) pos++; else neg++;
+      if ((double)F[j + (size_t)j * f] >= 0.0) pos++; else neg++;
     } else if (kd == 1) {
       const double d11 = F[j + (size_t)j * f];
       const double d21 = F[j + 1 + (size_t)j * f];
@@ -594,33 +606,36 @@ __device__ void finish_front(const DevicePlan& d, int node, const double* F,
 
 // Small/medium fronts: set up, assemble and factor one front per CTA, in
 // shared memory when it fits.
+template <class T>
 __global__ void __launch_bounds__(NT)
 k_factor_level(DevicePlan d, const int* __restrict__ nodes, int count,
                const double* __restrict__ vals, double ustab,
-               double pivot_tol, int smem_doubles) {
-  extern __shared__ double smem[];
+               double pivot_tol, int smem_elems) {
+  extern __shared__ double smem_raw[];
+  T* smem = reinterpret_cast<T*>(smem_raw);
   __shared__ Ctl ctl;
   const int tid = threadIdx.x;
   const int node = nodes[blockIdx.x];
-  if (!setup_front(d, node, ctl)) return;
+  if (!setup_front<T>(d, node, ctl)) return;
+  T* pool = reinterpret_cast<T*>(d.fpool);
 
   const int f = ctl.f, fs = ctl.fs, ns = ctl.ns, ndin = ctl.ndin;
   int* fvars = d.ipool + ctl.ioff;
   int* fsperm = fvars + f;
-  double* Fg = d.fpool + ctl.foff;
-  const bool in_smem = (long long)f * f + (long long)f * NB <= smem_doubles;
-  double* F = in_smem ? smem : Fg;
-  double* W = in_smem ? smem + (size_t)f * f : Fg + (size_t)f * f;
-  double* tiles = nullptr;
-  if (!in_smem && smem_doubles >= kTileSmem) tiles = smem;
+  T* Fg = pool + ctl.foff;
+  const bool in_smem = (long long)f * f + (long long)f * NB <= smem_elems;
+  T* F = in_smem ? smem : Fg;
+  T* W = in_smem ? smem + (size_t)f * f : Fg + (size_t)f * f;
+  T* tiles = nullptr;
+  if (!in_smem && smem_elems >= kTileSmem) tiles = smem;
 
   // Assemble: zero, add A, extend-add the children.
-  for (size_t idx = tid; idx < (size_t)f * f; idx += NT) F[idx] = 0.0;
+  for (size_t idx = tid; idx < (size_t)f * f; idx += NT) F[idx] = T(0);
   __syncthreads();
   for (int t = d.amap_ptr[node] + tid; t < d.amap_ptr[node + 1]; t += NT) {
     const int r0 = d.amap_row[t];
     const int r = r0 < ns ? r0 : r0 + ndin;
-    F[r + (size_t)d.amap_col[t] * f] += vals[d.amap_pos[t]];
+    F[r + (size_t)d.amap_col[t] * f] += T(vals[d.amap_pos[t]]);
   }
   __syncthreads();
   {
@@ -630,17 +645,17 @@ k_factor_level(DevicePlan d, const int* __restrict__ nodes, int count,
       const int c = d.kids[q];
       const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
       const int cc = fc - npc;
-      const double* C = d.fpool + d.foff[c];
+      const T* C = pool + d.foff[c];
       const int cb = d.cptr[c];
       for (int a = tid; a < cc; a += NT)
         rmap[a] = child_row_pos(d, cb, ndc, choff, ns, ndin, a);
       __syncthreads();
       for (int b = 0; b < cc; b++) {
         const int pb = rmap[b];
-        const double* Cb = C + (size_t)(npc + b) * fc + npc;
+        const T* Cb = C + (size_t)(npc + b) * fc + npc;
         for (int a = b + tid; a < cc; a += NT) {
           const int pa = rmap[a];
-          const double v = Cb[a];
+          const T v = Cb[a];
           if (pa >= pb) F[pa + (size_t)pb * f] += v;
           else F[pb + (size_t)pa * f] += v;
         }
@@ -665,44 +680,48 @@ k_factor_level(DevicePlan d, const int* __restrict__ nodes, int count,
 // the factorization alternates a one-CTA panel kernel with a multi-CTA
 // trailing-update kernel over 64 x 64 tiles.
 
+template <class T>
 __global__ void __launch_bounds__(NT)
 k_big_setup(DevicePlan d, const int* __restrict__ nodes) {
   __shared__ Ctl ctl;
-  setup_front(d, nodes[blockIdx.x], ctl);
+  setup_front<T>(d, nodes[blockIdx.x], ctl);
 }
 
 __device__ __forceinline__ bool big_skip(const DevicePlan& d) {
   return (*((volatile int*)d.status) & (ST_POOL_F | ST_POOL_I)) != 0;
 }
 
+template <class T>
 __global__ void __launch_bounds__(NT)
 k_big_zero(DevicePlan d, const int* __restrict__ nodes) {
   if (big_skip(d)) return;
   const int node = nodes[blockIdx.x];
   const size_t f = d.f[node];
-  double* F = d.fpool + d.foff[node];
+  T* F = reinterpret_cast<T*>(d.fpool) + d.foff[node];
   for (size_t idx = (size_t)blockIdx.y * NT + threadIdx.x; idx < f * f;
        idx += (size_t)gridDim.y * NT)
-    F[idx] = 0.0;
+    F[idx] = T(0);
 }
 
+template <class T>
 __global__ void __launch_bounds__(NT)
 k_big_add_A(DevicePlan d, const int* __restrict__ nodes,
             const double* __restrict__ vals) {
   if (big_skip(d)) return;
   const int node = nodes[blockIdx.x];
   const int f = d.f[node], ns = d.ns[node], ndin = d.ndin[node];
-  double* F = d.fpool + d.foff[node];
+  T* F = reinterpret_cast<T*>(d.fpool) + d.foff[node];
   for (int t = d.amap_ptr[node] + blockIdx.y * NT + threadIdx.x;
        t < d.amap_ptr[node + 1]; t += gridDim.y * NT) {
     const int r0 = d.amap_row[t];
     const int r = r0 < ns ? r0 : r0 + ndin;
-    F[r + (size_t)d.amap_col[t] * f] += vals[d.amap_pos[t]];
+    F[r + (size_t)d.amap_col[t] * f] += T(vals[d.amap_pos[t]]);
   }
 }
 
 // Extend-add of the q-th child of every front (one launch per child rank,
 // so that no two writers of a launch touch the same parent entry).
+template <class T>
 __global__ void __launch_bounds__(NT)
 k_big_extend(DevicePlan d, const int* __restrict__ nodes, int q) {
   if (big_skip(d)) return;
@@ -715,20 +734,21 @@ k_big_extend(DevicePlan d, const int* __restrict__ nodes, int q) {
   const int c = d.kids[q0 + q];
   const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
   const int cc = fc - npc, cb = d.cptr[c];
-  const double* C = d.fpool + d.foff[c];
-  double* F = d.fpool + d.foff[node];
+  const T* C = reinterpret_cast<const T*>(d.fpool) + d.foff[c];
+  T* F = reinterpret_cast<T*>(d.fpool) + d.foff[node];
   for (int b = blockIdx.y; b < cc; b += gridDim.y) {
     const int pb = child_row_pos(d, cb, ndc, choff, ns, ndin, b);
-    const double* Cb = C + (size_t)(npc + b) * fc + npc;
+    const T* Cb = C + (size_t)(npc + b) * fc + npc;
     for (int a = b + threadIdx.x; a < cc; a += NT) {
       const int pa = child_row_pos(d, cb, ndc, choff, ns, ndin, a);
-      const double v = Cb[a];
+      const T v = Cb[a];
       if (pa >= pb) F[pa + (size_t)pb * f] += v;
       else F[pb + (size_t)pa * f] += v;
     }
   }
 }
 
+template <class T>
 __global__ void __launch_bounds__(kPanelThreads)
 k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
             double pivot_tol) {
@@ -743,12 +763,12 @@ k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
   }
   const int f = d.f[node];
   const int fs = d.ns[node] + d.ndin[node];
-  double* F = d.fpool + d.foff[node];
-  double* W = F + (size_t)f * f;
+  T* F = reinterpret_cast<T*>(d.fpool) + d.foff[node];
+  T* W = F + (size_t)f * f;
   int* fvars = d.ipool + d.ioff[node];
   const int kstart = k;
   int kw = 0;
-  panel_factor<kPanelThreads>(F, f, W, f, f, fs == f, fvars, fvars + f, ustab, pivot_tol,
+  panel_factor<T, kPanelThreads>(F, f, W, f, f, fs == f, fvars, fvars + f, ustab, pivot_tol,
                d.status, ctl, k, nc, kw);
   if (threadIdx.x == 0) {
     st[0] = k;
@@ -758,9 +778,11 @@ k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
   }
 }
 
+template <class T>
 __global__ void __launch_bounds__(NT)
 k_big_update(DevicePlan d, const int* __restrict__ nodes) {
-  extern __shared__ double tiles[];
+  extern __shared__ double tiles_raw[];
+  T* tiles = reinterpret_cast<T*>(tiles_raw);
   if (big_skip(d)) return;
   const int node = nodes[blockIdx.x];
   const int* st = d.pstate + 4 * node;
@@ -769,8 +791,8 @@ k_big_update(DevicePlan d, const int* __restrict__ nodes) {
   const int f = d.f[node];
   const int m = f - k;
   if (m <= 0) return;
-  double* F = d.fpool + d.foff[node];
-  const double* W = F + (size_t)f * f;
+  T* F = reinterpret_cast<T*>(d.fpool) + d.foff[node];
+  const T* W = F + (size_t)f * f;
   const int nt = (m + kTile - 1) / kTile;
   const int ntiles = nt * (nt + 1) / 2;
   for (int t = blockIdx.y; t < ntiles; t += gridDim.y) {
@@ -781,6 +803,35 @@ k_big_update(DevicePlan d, const int* __restrict__ nodes) {
   }
 }
 
+// The same update for FP32 fronts on the tensor cores (tc_update.cuh):
+// 128 x 128 tiles of the trailing block, 3xTF32 products in TMEM.
+__global__ void __launch_bounds__(tc::kThreads)
+k_big_update_tc(DevicePlan d, const int* __restrict__ nodes) {
+  extern __shared__ __align__(1024) char tc_smem[];
+  if (big_skip(d)) return;
+  const int node = nodes[blockIdx.x];
+  const int* st = d.pstate + 4 * node;
+  const int k = st[0], kstart = st[2], kw = st[3];
+  if (kw == 0) return;
+  const int f = d.f[node];
+  const int m = f - k;
+  if (m <= 0) return;
+  const int nt = (m + tc::TM - 1) / tc::TM;
+  const int ntiles = nt * (nt + 1) / 2;
+  if ((int)blockIdx.y >= ntiles) return;
+  float* F = reinterpret_cast<float*>(d.fpool) + d.foff[node];
+  const float* W = F + (size_t)f * f;
+  tc::TcCta c = tc::tc_begin(tc_smem);
+  for (int t = blockIdx.y; t < ntiles && c.ok; t += gridDim.y) {
+    int ti, tj;
+    tile_coords(t, ti, tj);
+    tc::tc_tile(c, F + k + (size_t)k * f, f, F + k + (size_t)kstart * f, f,
+                W + k, f, m, kw, ti * tc::TM, tj * tc::TN, d.status);
+  }
+  tc::tc_end(c);
+}
+
+template <class T>
 __global__ void __launch_bounds__(NT)
 k_big_finalize(DevicePlan d, const int* __restrict__ nodes) {
   if (big_skip(d)) return;
@@ -788,8 +839,8 @@ k_big_finalize(DevicePlan d, const int* __restrict__ nodes) {
   const int f = d.f[node];
   const int fs = d.ns[node] + d.ndin[node];
   const int npiv = d.pstate[4 * node + 1];
-  finish_front(d, node, d.fpool + d.foff[node], f, fs, npiv,
-               d.ipool + d.ioff[node]);
+  finish_front(d, node, reinterpret_cast<const T*>(d.fpool) + d.foff[node], f,
+               fs, npiv, d.ipool + d.ioff[node]);
 }
 
 // Number of large fronts of the level still holding candidates; 0 when a
@@ -818,16 +869,20 @@ __global__ void k_big_remaining(DevicePlan d, const int* __restrict__ nodes,
     }                                                                     \
   } while (0)
 
+template <class T>
 static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
   DevicePlan& d = h.d;
   static bool attr_set = false;
   if (!attr_set) {
-    FCUDA(cudaFuncSetAttribute(k_factor_level,
+    FCUDA(cudaFuncSetAttribute(k_factor_level<T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kMaxDynSmem));
-    FCUDA(cudaFuncSetAttribute(k_big_update,
+    FCUDA(cudaFuncSetAttribute(k_big_update<T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               kTileSmem * 8));
+                               kTileSmem * sizeof(T)));
+    FCUDA(cudaFuncSetAttribute(k_big_update_tc,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               tc::kSmemBytes));
     attr_set = true;
   }
   FCUDA(cudaMemsetAsync(d.counters, 0, 2 * sizeof(unsigned long long), s));
@@ -846,12 +901,13 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     if (trace) cudaEventRecord(ev[3 * l], s);
     if (L.nsmall) {
       long long fm = L.small_max_f + 16;
-      long long bytes = (fm * fm + fm * NB) * 8;
-      if (bytes < (long long)kTileSmem * 8) bytes = (long long)kTileSmem * 8;
+      long long bytes = (fm * fm + fm * NB) * (long long)sizeof(T);
+      if (bytes < (long long)(kTileSmem * sizeof(T)))
+        bytes = (long long)(kTileSmem * sizeof(T));
       if (bytes > kMaxDynSmem) bytes = kMaxDynSmem;
-      { k_factor_level<<<L.nsmall, NT, (size_t)bytes, s>>>(
+      { k_factor_level<T><<<L.nsmall, NT, (size_t)bytes, s>>>(
           d, d.sched_nodes + L.small_begin, L.nsmall, d_vals, h.ustab,
-          h.pivot_tol, (int)(bytes / 8)); ab::count_launch(); }
+          h.pivot_tol, (int)(bytes / sizeof(T))); ab::count_launch(); }
     }
     if (trace) cudaEventRecord(ev[3 * l + 1], s);
     if (L.nbig) {
@@ -861,13 +917,18 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       int gz = (int)std::min<long long>(512, (fm * fm + 4095) / 4096);
       int ga = (int)std::min<long long>(256, (L.big_max_amap + NT - 1) / NT);
       int ge = (int)std::min<long long>(1024, fm);
-      { k_big_setup<<<B, NT, 0, s>>>(d, nodes); ab::count_launch(); }
-      { k_big_zero<<<dim3(B, std::max(gz, 1)), NT, 0, s>>>(d, nodes); ab::count_launch(); }
-      { k_big_add_A<<<dim3(B, std::max(ga, 1)), NT, 0, s>>>(d, nodes, d_vals); ab::count_launch(); }
+      { k_big_setup<T><<<B, NT, 0, s>>>(d, nodes); ab::count_launch(); }
+      { k_big_zero<T><<<dim3(B, std::max(gz, 1)), NT, 0, s>>>(d, nodes); ab::count_launch(); }
+      { k_big_add_A<T><<<dim3(B, std::max(ga, 1)), NT, 0, s>>>(d, nodes, d_vals); ab::count_launch(); }
       for (int q = 0; q < L.big_max_kids; q++)
-        { k_big_extend<<<dim3(B, std::max(ge, 1)), NT, 0, s>>>(d, nodes, q); ab::count_launch(); }
+        { k_big_extend<T><<<dim3(B, std::max(ge, 1)), NT, 0, s>>>(d, nodes, q); ab::count_launch(); }
       const long long ntl = (fm + kTile - 1) / kTile;
       int gu = (int)std::min<long long>(4 * 148, ntl * (ntl + 1) / 2);
+      // FP32 fronts of at least one 128-row tile: tensor-core update
+      const bool use_tc = sizeof(T) == 4 && h.tensor_cores && fm >= tc::TM;
+      const long long ntc = (fm + tc::TM - 1) / tc::TM;
+      const int gtc = (int)std::max<long long>(
+          1, std::min<long long>(3 * 148, ntc * (ntc + 1) / 2));
       int panels = (int)((L.big_max_fs + NB - 2) / (NB - 1)) + 2;
       // Every panel consumes at least one candidate of every unfinished
       // front, so no front needs more panels than it has rows.
@@ -876,10 +937,15 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       for (;;) {
         budget += panels;
         for (int it = 0; it < panels; it++) {
-          { k_big_panel<<<B, kPanelThreads, 0, s>>>(d, nodes, h.ustab,
-                                                  h.pivot_tol); ab::count_launch(); }
-          { k_big_update<<<dim3(B, std::max(gu, 1)), NT, kTileSmem * 8, s>>>(
-              d, nodes); ab::count_launch(); }
+          { k_big_panel<T><<<B, kPanelThreads, 0, s>>>(d, nodes, h.ustab,
+                                                     h.pivot_tol); ab::count_launch(); }
+          if (use_tc) {
+            { k_big_update_tc<<<dim3(B, gtc), tc::kThreads, tc::kSmemBytes, s>>>(
+                d, nodes); ab::count_launch(); }
+          } else {
+            { k_big_update<T><<<dim3(B, std::max(gu, 1)), NT, kTileSmem * sizeof(T), s>>>(
+                d, nodes); ab::count_launch(); }
+          }
         }
         // Delayed pivots received from the children can make a front need
         // more panels than its static size implies: check and continue.
@@ -895,7 +961,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
         }
         panels = 4;
       }
-      { k_big_finalize<<<B, NT, 0, s>>>(d, nodes); ab::count_launch(); }
+      { k_big_finalize<T><<<B, NT, 0, s>>>(d, nodes); ab::count_launch(); }
     }
     if (trace) cudaEventRecord(ev[3 * l + 2], s);
   }
@@ -924,18 +990,36 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
 int factor_numeric(LdlHandle& h, const double* d_vals, cudaStream_t s) {
   DevicePlan& d = h.d;
   for (int attempt = 0; attempt < 6; attempt++) {
-    int rc = launch_factor(h, d_vals, s);
+    int rc = h.precision == 32 ? launch_factor<float>(h, d_vals, s)
+                               : launch_factor<double>(h, d_vals, s);
     if (rc) return rc;
     int status = 0;
     FCUDA(cudaMemcpyAsync(&status, d.status, sizeof(int),
                           cudaMemcpyDeviceToHost, s));
     FCUDA(cudaStreamSynchronize(s));
     h.last_status = status;
+    if (status & tc::kStatusTimeout) {
+      std::fprintf(stderr, "amigo_b200: tensor-core update wait ran out\n");
+      return AB_ERR_CUDA;
+    }
     if (status & (ST_POOL_F | ST_POOL_I)) {
       // Delayed pivots made fronts larger than the pool allows: grow it.
       if (status & ST_POOL_F) {
+        // double the pool, within what the device has free
         FCUDA(cudaFree(d.fpool));
-        d.fcap = d.fcap * 2;
+        d.fpool = nullptr;
+        size_t free_b = 0, total_b = 0;
+        FCUDA(cudaMemGetInfo(&free_b, &total_b));
+        const long long budget =
+            ((long long)free_b - (long long)(total_b / 20)) / 8;
+        const long long grown = std::min<long long>(2 * d.fcap, budget);
+        if (grown <= d.fcap) {
+          std::fprintf(stderr, "amigo_b200: delayed pivots need more than "
+                               "the %.1f GB front pool\n", d.fcap * 8e-9);
+          FCUDA(cudaMalloc((void**)&d.fpool, (size_t)d.fcap * sizeof(double)));
+          return AB_ERR_CAPACITY;
+        }
+        d.fcap = grown;
         FCUDA(cudaMalloc((void**)&d.fpool, (size_t)d.fcap * sizeof(double)));
       }
       if (status & ST_POOL_I) {
@@ -958,7 +1042,8 @@ int factor_numeric(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                           cudaMemcpyDeviceToHost, s));
     FCUDA(cudaStreamSynchronize(s));
     h.factored = true;
-    h.uoff_nrhs = 0;  // solve offsets must be rebuilt
+    h.factor_epoch++;
+    h.factor_precision = h.precision;
     return (status & ST_NAN) ? -5 : 0;
   }
   return -6;

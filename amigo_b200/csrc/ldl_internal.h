@@ -5,7 +5,8 @@
 //     schedule, the CSR-entry -> front-position map for assembling A, and the
 //     child-contribution-row -> parent-front-position map for extend-add;
 //   * per-factorization pools: every front F (f x f, column-major, ld = f)
-//     plus its panel workspace W (f x NB) is carved from one FP64 pool with
+//     plus its panel workspace W (f x NB) is carved (in FP64 or, for the
+//     mixed-precision form, FP32 elements) from one pool with
 //     an atomic bump pointer, so fronts whose size grows with delayed pivots
 //     need no host round trip; after factorization the first npiv columns of
 //     F hold L (unit lower, D on the diagonal / 2x2 blocks) and the trailing
@@ -111,6 +112,23 @@ struct LdlHandle {
   long long* uoff = nullptr;      // per node offset into ubuf (device)
   std::vector<long long> h_uoff;
   int uoff_nrhs = 0;
+  // solve schedule, rebuilt after each factorization: per level the fronts
+  // solved one per CTA ("narrow") and the wide fronts solved by the
+  // cooperative multi-CTA kernels, concatenated level by level
+  long long factor_epoch = 0, solve_epoch = -1;
+  long long wide_entries = 1 << 18;   // f * npiv from which a front is wide
+  // front storage / arithmetic of the next factorization (64: FP64, 32:
+  // FP32 fronts for mixed precision) and of the last one
+  int precision = 64, factor_precision = 64;
+  bool tensor_cores = true;   // FP32 fronts: Schur updates on tcgen05
+  int* sv_nodes = nullptr;        // device, nn entries
+  int* sv_state = nullptr;        // device, 2 ints per wide front of a level
+  std::vector<int> sv_narrow_ptr, sv_wide_ptr, sv_narrow_smem;
+  std::vector<int> sv_host, sv_f, sv_npiv;   // schedule and the sizes it is for
+  int sv_max_wide = 0, sv_state_cap = 0;
+  long long sv_wide_entries = 0;
+  std::vector<int> sv_fwd_grid, sv_bwd_grid;   // cooperative grid per level
+  int sv_grid_cap = 0;
 };
 
 int build_plan(LdlHandle& h, const int* rowp, const int* cols);

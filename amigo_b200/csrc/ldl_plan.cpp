@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "../../include/amigo_b200.h"
 #include "ldl_internal.h"
 
 namespace ab {
@@ -216,9 +217,23 @@ int build_plan(LdlHandle& h, const int* rowp, const int* cols) {
   rc |= zalloc(&d.counters, 2);
   if (rc) return -2;
 
+  // Pools: delay_growth times the static front sizes, capped by what the
+  // device has free (keeping a reserve for the caller's vectors); the
+  // static size itself must fit.
   double g = std::max(1.0, h.delay_growth);
-  d.fcap = (long long)(g * (double)h.f_static_total) + 4096;
   d.icap = (long long)(g * (double)h.i_static_total) + 4096;
+  size_t free_b = 0, total_b = 0;
+  PLAN_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const long long reserve = (long long)(total_b / 20) + d.icap * 4;
+  const long long budget = ((long long)free_b - reserve) / 8;
+  const long long fmin = h.f_static_total + 4096;
+  if (fmin > budget) {
+    std::fprintf(stderr, "amigo_b200: the fronts need %.1f GB, %.1f GB free\n",
+                 fmin * 8e-9, free_b * 1e-9);
+    return AB_ERR_CAPACITY;
+  }
+  d.fcap = std::min<long long>((long long)(g * (double)h.f_static_total) + 4096,
+                               budget);
   PLAN_CUDA(cudaMalloc((void**)&d.fpool, (size_t)d.fcap * sizeof(double)));
   PLAN_CUDA(cudaMalloc((void**)&d.ipool, (size_t)d.icap * sizeof(int)));
   PLAN_CUDA(cudaMalloc((void**)&h.uoff, (size_t)std::max(nn, 1) * sizeof(long long)));
@@ -233,12 +248,15 @@ void free_plan(LdlHandle& h) {
                   d.scratch_int, d.f, d.npiv, d.ndel, d.ndin,
                   d.foff, d.ioff, d.inertia, d.node_prob, d.status,
                   d.counters, d.fpool,
-                  d.ipool, h.ubuf, h.uoff};
+                  d.ipool, h.ubuf, h.uoff, h.sv_nodes, h.sv_state};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   d = DevicePlan();
   h.ubuf = nullptr;
   h.uoff = nullptr;
+  h.sv_nodes = nullptr;
+  h.sv_state = nullptr;
+  h.solve_epoch = -1;
 }
 
 }  // namespace ab

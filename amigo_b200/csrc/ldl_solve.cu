@@ -12,10 +12,12 @@
 // reference's solve_ldl (include/sparse_ldl.h:1807-1908,
 // solve_pivot_lower/diagonal/transpose 1550-1669) reorganised so that fronts
 // of one level run concurrently without atomics.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "ldl_internal.h"
@@ -37,6 +39,51 @@ __device__ __forceinline__ int block_end(const int* kind, int jb, int npiv) {
   return je;
 }
 
+// Front vector of `node` for one right-hand side: the node's own entries
+// of the right-hand side plus the update vectors of its children, placed
+// by the same row map as the factorization's extend-add.  Called by a
+// whole CTA; V may be shared or global memory.
+__device__ void assemble_front_vector(const DevicePlan& d, int node, double* V,
+                                      const double* xr, const double* ubuf,
+                                      const long long* uoff, int rhs,
+                                      int* s_choff) {
+  const int tid = threadIdx.x;
+  const int f = d.f[node];
+  const int ns = d.ns[node], ndin = d.ndin[node];
+  const int fs = ns + ndin;
+  const int* fsinv = d.ipool + d.ioff[node] + 2 * f;
+  for (int r = tid; r < f; r += NT) V[r] = 0.0;
+  __syncthreads();
+  const int vb = d.var_ptr[node];
+  for (int r = tid; r < ns; r += NT) V[fsinv[r]] = xr[d.vars[vb + r]];
+  __syncthreads();
+  if (tid == 0) *s_choff = ns;
+  __syncthreads();
+  for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
+    const int c = d.kids[q];
+    const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
+    const int cc = fc - npc;
+    const double* uc = ubuf + uoff[c] + (long long)rhs * fc + npc;
+    const int cb = d.cptr[c];
+    const int choff = *s_choff;
+    for (int a = tid; a < cc; a += NT) {
+      int pos;
+      if (a < ndc) {
+        pos = choff + a;
+      } else {
+        int r0 = d.cmap[cb + a - ndc];
+        pos = r0 < ns ? r0 : r0 + ndin;
+      }
+      if (pos < fs) pos = fsinv[pos];
+      V[pos] += uc[a];
+    }
+    __syncthreads();
+    if (tid == 0) *s_choff = choff + ndc;
+    __syncthreads();
+  }
+}
+
+template <class T>
 __global__ void __launch_bounds__(NT)
 k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
                 int nrhs, int ldx, double* ubuf, const long long* uoff,
@@ -45,12 +92,9 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
   const int node = nodes[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int f = d.f[node], npiv = d.npiv[node];
-  const int ns = d.ns[node], ndin = d.ndin[node];
-  const int fs = ns + ndin;
   const int* fvars = d.ipool + d.ioff[node];
-  const int* fsinv = fvars + 2 * f;
   const int* kind = fvars + 3 * f;
-  const double* L = d.fpool + d.foff[node];
+  const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
   __shared__ int s_choff;
   __shared__ double sL[(SB + 1) * (SB + 1)];
 
@@ -61,35 +105,7 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
     double* G = ubuf + uoff[node] + (long long)rhs * f;
     double* V = f <= smem_doubles ? sV : G;
     double* xr = x + (long long)rhs * ldx;
-    for (int r = tid; r < f; r += NT) V[r] = 0.0;
-    __syncthreads();
-    const int vb = d.var_ptr[node];
-    for (int r = tid; r < ns; r += NT) V[fsinv[r]] = xr[d.vars[vb + r]];
-    __syncthreads();
-    if (tid == 0) s_choff = ns;
-    __syncthreads();
-    for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
-      const int c = d.kids[q];
-      const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
-      const int cc = fc - npc;
-      const double* uc = ubuf + uoff[c] + (long long)rhs * fc + npc;
-      const int cb = d.cptr[c];
-      const int choff = s_choff;
-      for (int a = tid; a < cc; a += NT) {
-        int pos;
-        if (a < ndc) {
-          pos = choff + a;
-        } else {
-          int r0 = d.cmap[cb + a - ndc];
-          pos = r0 < ns ? r0 : r0 + ndin;
-        }
-        if (pos < fs) pos = fsinv[pos];
-        V[pos] += uc[a];
-      }
-      __syncthreads();
-      if (tid == 0) s_choff = choff + ndc;
-      __syncthreads();
-    }
+    assemble_front_vector(d, node, V, xr, ubuf, uoff, rhs, &s_choff);
 
     // Forward elimination with the unit lower factor.  The diagonal block
     // of each column block is staged in shared memory first, so that the
@@ -149,6 +165,7 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
   }
 }
 
+template <class T>
 __global__ void __launch_bounds__(NT)
 k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
                  int nrhs, int ldx, double* ubuf, const long long* uoff,
@@ -160,7 +177,7 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
   const int f = d.f[node], npiv = d.npiv[node];
   const int* fvars = d.ipool + d.ioff[node];
   const int* kind = fvars + 3 * f;
-  const double* L = d.fpool + d.foff[node];
+  const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
   __shared__ double sL[(SB + 1) * (SB + 1)];
   for (int rhs = 0; rhs < nrhs; rhs++) {
     double* V = f <= smem_doubles ? sV : ubuf + uoff[node] + (long long)rhs * f;
@@ -220,6 +237,311 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Wide fronts (f * npiv large): one cooperative launch per level solves all
+// of the level's wide fronts with every CTA of the GPU.  The front vectors
+// live in ubuf (global memory).  Each column block of WB pivots alternates
+// a sequential phase (one CTA per front solves the block's diagonal
+// triangle in shared memory) with a parallel phase (all CTAs apply the
+// block to the rows below it, forward, or to the columns left of it,
+// backward), separated by grid-wide barriers.  Values other CTAs wrote
+// since the last barrier are read with ld.global.cg (L2), never through
+// the non-coherent L1.  Sums run in a fixed order: the result does not
+// depend on the grid size.
+constexpr int WB = 64;
+
+__device__ __forceinline__ int block_end_w(const int* kind, int jb, int npiv) {
+  int je = jb + WB < npiv ? jb + WB : npiv;
+  if (je < npiv && kind[je - 1] == 1) je++;
+  return je;
+}
+
+template <class T>
+struct WideFront {
+  int f, npiv;
+  const int* fvars;
+  const int* kind;
+  const T* L;
+  double* G;
+};
+
+template <class T>
+__device__ __forceinline__ WideFront<T> wide_front(const DevicePlan& d, int node,
+                                                double* ubuf,
+                                                const long long* uoff,
+                                                int rhs) {
+  WideFront<T> w;
+  w.f = d.f[node];
+  w.npiv = d.npiv[node];
+  w.fvars = d.ipool + d.ioff[node];
+  w.kind = w.fvars + 3 * w.f;
+  w.L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
+  w.G = ubuf + uoff[node] + (long long)rhs * w.f;
+  return w;
+}
+
+// Flattened work distribution: item g of a sequence in which front c owns
+// cnt_c consecutive items goes to CTA g mod gridDim.x.  Returns this CTA's
+// first item of front c, given the number of items before it.
+__device__ __forceinline__ long long first_item(long long base) {
+  const long long G = gridDim.x;
+  long long r = ((long long)blockIdx.x - base) % G;
+  return r < 0 ? r + G : r;
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT)
+k_wide_forward(DevicePlan d, const int* __restrict__ nodes, int count,
+               double* x, int nrhs, int ldx, double* ubuf,
+               const long long* uoff, int* wst) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ double sm[];
+  double* sL = sm;                         // (WB + 1)^2 diagonal block
+  double* sv = sm + (WB + 1) * (WB + 1);   // WB + 1 block values
+  __shared__ int s_choff;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int rhs = 0; rhs < nrhs; rhs++) {
+    double* xr = x + (long long)rhs * ldx;
+    for (int c = blockIdx.x; c < count; c += gridDim.x) {
+      const WideFront<T> w = wide_front<T>(d, nodes[c], ubuf, uoff, rhs);
+      assemble_front_vector(d, nodes[c], w.G, xr, ubuf, uoff, rhs, &s_choff);
+      if (tid == 0) {
+        wst[2 * c] = 0;
+        wst[2 * c + 1] = 0;
+      }
+    }
+    grid.sync();
+    for (;;) {
+      // sequential phase: next diagonal block of every front
+      for (int c = blockIdx.x; c < count; c += gridDim.x) {
+        const WideFront<T> w = wide_front<T>(d, nodes[c], ubuf, uoff, rhs);
+        const int jb = __ldcg(wst + 2 * c + 1);
+        if (jb >= w.npiv) {
+          if (tid == 0) wst[2 * c] = jb;
+          continue;
+        }
+        const int je = block_end_w(w.kind, jb, w.npiv);
+        const int bw = je - jb;
+        for (int t = tid; t < bw * bw; t += NT) {
+          const int i = t % bw, j = t / bw;
+          sL[i + j * (WB + 1)] = w.L[jb + i + (size_t)(jb + j) * w.f];
+        }
+        for (int t = tid; t < bw; t += NT) sv[t] = __ldcg(w.G + jb + t);
+        __syncthreads();
+        if (warp == 0) {
+          for (int j = 0; j < bw;) {
+            const bool two = w.kind[jb + j] == 1;
+            const double v0 = sv[j];
+            const double v1 = two ? sv[j + 1] : 0.0;
+            const int i0 = j + (two ? 2 : 1);
+            for (int i = i0 + lane; i < bw; i += 32) {
+              double t = sL[i + j * (WB + 1)] * v0;
+              if (two) t += sL[i + (j + 1) * (WB + 1)] * v1;
+              sv[i] -= t;
+            }
+            __syncwarp();
+            j = i0;
+          }
+        }
+        __syncthreads();
+        for (int t = tid; t < bw; t += NT) w.G[jb + t] = sv[t];
+        if (tid == 0) {
+          wst[2 * c] = jb;
+          wst[2 * c + 1] = je;
+        }
+        __syncthreads();
+      }
+      grid.sync();
+      bool any = false;
+      for (int c = 0; c < count && !any; c++)
+        any = __ldcg(wst + 2 * c) < __ldcg(wst + 2 * c + 1);
+      if (!any) break;
+      // parallel phase: rows below the block, NT rows per item
+      long long base = 0;
+      for (int c = 0; c < count; c++) {
+        const int jb = __ldcg(wst + 2 * c), je = __ldcg(wst + 2 * c + 1);
+        if (jb >= je) continue;
+        const WideFront<T> w = wide_front<T>(d, nodes[c], ubuf, uoff, rhs);
+        const long long items = (w.f - je + NT - 1) / NT;
+        const int bw = je - jb;
+        bool staged = false;
+        for (long long it = first_item(base); it < items; it += gridDim.x) {
+          if (!staged) {
+            __syncthreads();
+            for (int t = tid; t < bw; t += NT) sv[t] = __ldcg(w.G + jb + t);
+            __syncthreads();
+            staged = true;
+          }
+          const int i = je + (int)it * NT + tid;
+          if (i < w.f) {
+            const T* Li = w.L + i + (size_t)jb * w.f;
+            double acc = 0.0;
+            for (int j = 0; j < bw; j++) acc += Li[(size_t)j * w.f] * sv[j];
+            w.G[i] = __ldcg(w.G + i) - acc;
+          }
+        }
+        base += items;
+      }
+      grid.sync();
+    }
+    // D^{-1} and the pivots' forward values
+    for (int c = blockIdx.x; c < count; c += gridDim.x) {
+      const WideFront<T> w = wide_front<T>(d, nodes[c], ubuf, uoff, rhs);
+      for (int j = tid; j < w.npiv; j += NT) {
+        const int kd = w.kind[j];
+        const T* L = w.L;
+        const size_t f = w.f;
+        if (kd == 0) {
+          w.G[j] = __ldcg(w.G + j) / L[j + j * f];
+        } else if (kd == 1) {
+          const double d11 = L[j + j * f];
+          const double d21 = L[j + 1 + j * f];
+          const double d22 = L[j + 1 + (j + 1) * f];
+          const double inv = 1.0 / (d11 * d22 - d21 * d21);
+          const double x1 = __ldcg(w.G + j), x2 = __ldcg(w.G + j + 1);
+          w.G[j] = inv * (d22 * x1 - d21 * x2);
+          w.G[j + 1] = inv * (d11 * x2 - d21 * x1);
+        }
+      }
+      __syncthreads();
+      for (int j = tid; j < w.npiv; j += NT)
+        xr[decode_var(w.fvars[j])] = __ldcg(w.G + j);
+    }
+    grid.sync();
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT)
+k_wide_backward(DevicePlan d, const int* __restrict__ nodes, int count,
+                double* x, int nrhs, int ldx, double* ubuf,
+                const long long* uoff, int* wst) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ double sm[];
+  double* sL = sm;
+  double* sv = sm + (WB + 1) * (WB + 1);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NWARP = NT / 32;
+  const long long gwarps = (long long)gridDim.x * NWARP;
+  for (int rhs = 0; rhs < nrhs; rhs++) {
+    double* xr = x + (long long)rhs * ldx;
+    for (int c = blockIdx.x; c < count; c += gridDim.x) {
+      const WideFront<T> w = wide_front<T>(d, nodes[c], ubuf, uoff, rhs);
+      for (int r = tid; r < w.npiv; r += NT) w.G[r] = xr[decode_var(w.fvars[r])];
+      for (int r = w.npiv + tid; r < w.f; r += NT) w.G[r] = xr[w.fvars[r]];
+      if (tid == 0) {
+        wst[2 * c] = w.npiv;
+        wst[2 * c + 1] = w.npiv;
+      }
+    }
+    grid.sync();
+    // t[j] -= sum_{i >= npiv} L[i, j] t[i]: one warp per pivot column
+    {
+      long long base = 0;
+      for (int c = 0; c < count; c++) {
+        const WideFront<T> w = wide_front<T>(d, nodes[c], ubuf, uoff, rhs);
+        const long long gw = (long long)blockIdx.x * NWARP + warp;
+        long long r = (gw - base) % gwarps;
+        if (r < 0) r += gwarps;
+        for (long long j = r; j < w.npiv; j += gwarps) {
+          const T* Lj = w.L + (size_t)j * w.f;
+          double acc = 0.0;
+          for (int i = w.npiv + lane; i < w.f; i += 32)
+            acc += Lj[i] * __ldcg(w.G + i);
+          for (int o = 16; o > 0; o >>= 1)
+            acc += __shfl_down_sync(0xffffffffu, acc, o);
+          if (lane == 0) w.G[j] = __ldcg(w.G + j) - acc;
+        }
+        base += w.npiv;
+      }
+    }
+    grid.sync();
+    for (;;) {
+      // sequential phase: the next diagonal block from the end
+      for (int c = blockIdx.x; c < count; c += gridDim.x) {
+        const WideFront<T> w = wide_front<T>(d, nodes[c], ubuf, uoff, rhs);
+        const int je = __ldcg(wst + 2 * c);
+        if (je <= 0) {
+          if (tid == 0) wst[2 * c + 1] = je;
+          continue;
+        }
+        int jb = je - WB > 0 ? je - WB : 0;
+        if (jb > 0 && w.kind[jb] == 2) jb--;  // keep 2x2 pairs together
+        const int bw = je - jb;
+        for (int t = tid; t < bw * bw; t += NT) {
+          const int i = t % bw, j = t / bw;
+          sL[i + j * (WB + 1)] = w.L[jb + i + (size_t)(jb + j) * w.f];
+        }
+        for (int t = tid; t < bw; t += NT) sv[t] = __ldcg(w.G + jb + t);
+        __syncthreads();
+        if (warp == 0) {
+          for (int j = bw - 1; j >= 0;) {
+            const bool two = w.kind[jb + j] == 2;
+            const int jl = two ? j - 1 : j;
+            double a0 = 0.0, a1 = 0.0;
+            for (int i = j + 1 + lane; i < bw; i += 32) {
+              a0 += sL[i + jl * (WB + 1)] * sv[i];
+              if (two) a1 += sL[i + j * (WB + 1)] * sv[i];
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+              a0 += __shfl_down_sync(0xffffffffu, a0, o);
+              a1 += __shfl_down_sync(0xffffffffu, a1, o);
+            }
+            if (lane == 0) {
+              sv[jl] -= a0;
+              if (two) sv[j] -= a1;
+            }
+            __syncwarp();
+            j = jl - 1;
+          }
+        }
+        __syncthreads();
+        for (int t = tid; t < bw; t += NT) w.G[jb + t] = sv[t];
+        if (tid == 0) {
+          wst[2 * c] = jb;
+          wst[2 * c + 1] = je;
+        }
+        __syncthreads();
+      }
+      grid.sync();
+      bool any = false;
+      for (int c = 0; c < count && !any; c++)
+        any = __ldcg(wst + 2 * c) < __ldcg(wst + 2 * c + 1);
+      if (!any) break;
+      // parallel phase: t[j] -= sum_{i in block} L[i, j] t[i] for j < jb,
+      // one warp per column
+      long long base = 0;
+      for (int c = 0; c < count; c++) {
+        const int jb = __ldcg(wst + 2 * c), je = __ldcg(wst + 2 * c + 1);
+        if (jb >= je) continue;
+        const WideFront<T> w = wide_front<T>(d, nodes[c], ubuf, uoff, rhs);
+        const long long gw = (long long)blockIdx.x * NWARP + warp;
+        long long r = (gw - base) % gwarps;
+        if (r < 0) r += gwarps;
+        for (long long j = r; j < jb; j += gwarps) {
+          const T* Lj = w.L + (size_t)j * w.f;
+          double acc = 0.0;
+          for (int i = jb + lane; i < je; i += 32) acc += Lj[i] * __ldcg(w.G + i);
+          for (int o = 16; o > 0; o >>= 1)
+            acc += __shfl_down_sync(0xffffffffu, acc, o);
+          if (lane == 0) w.G[j] = __ldcg(w.G + j) - acc;
+        }
+        base += jb;
+      }
+      grid.sync();
+    }
+    for (int c = blockIdx.x; c < count; c += gridDim.x) {
+      const WideFront<T> w = wide_front<T>(d, nodes[c], ubuf, uoff, rhs);
+      for (int j = tid; j < w.npiv; j += NT)
+        xr[decode_var(w.fvars[j])] = __ldcg(w.G + j);
+    }
+    grid.sync();
+  }
+}
+
 }  // namespace
 
 #define SCUDA(call)                                                       \
@@ -232,11 +554,194 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
     }                                                                     \
   } while (0)
 
+// Per level: narrow fronts (one CTA each) and wide fronts, from the sizes
+// of the last factorization.
+static int build_solve_schedule(LdlHandle& h, cudaStream_t s) {
+  const int L = h.d.num_levels, nn = h.d.nn;
+  // unchanged front sizes (the usual case between IPM iterations): keep it
+  if (h.sv_f == h.h_f && h.sv_npiv == h.h_npiv && !h.sv_narrow_ptr.empty() &&
+      h.sv_wide_entries == h.wide_entries) {
+    h.solve_epoch = h.factor_epoch;
+    return 0;
+  }
+  std::vector<int>& nodes = h.sv_host;
+  nodes.clear();
+  nodes.reserve(nn);
+  h.sv_narrow_ptr.assign(L + 1, 0);
+  h.sv_wide_ptr.assign(L + 1, 0);
+  h.sv_narrow_smem.assign(L, 0);
+  h.sv_max_wide = 0;
+  for (int l = 0; l < L; l++) {
+    h.sv_narrow_ptr[l] = (int)nodes.size();
+    int fm = 0;
+    for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++) {
+      const int k = h.level_nodes[q];
+      if ((long long)h.h_f[k] * h.h_npiv[k] < h.wide_entries) {
+        nodes.push_back(k);
+        fm = std::max(fm, h.h_f[k]);
+      }
+    }
+    h.sv_narrow_smem[l] =
+        (int)std::min<long long>((long long)fm * 8, kMaxDynSmem);
+    h.sv_wide_ptr[l] = (int)nodes.size();
+    for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++) {
+      const int k = h.level_nodes[q];
+      if ((long long)h.h_f[k] * h.h_npiv[k] >= h.wide_entries) nodes.push_back(k);
+    }
+    h.sv_max_wide = std::max(h.sv_max_wide,
+                             (int)nodes.size() - h.sv_wide_ptr[l]);
+  }
+  h.sv_narrow_ptr[L] = h.sv_wide_ptr[L] = (int)nodes.size();
+  if (!h.sv_nodes) SCUDA(cudaMalloc((void**)&h.sv_nodes, std::max(nn, 1) * sizeof(int)));
+  if (h.sv_max_wide > h.sv_state_cap) {
+    if (h.sv_state) SCUDA(cudaFree(h.sv_state));
+    h.sv_state = nullptr;
+    h.sv_state_cap = std::max(h.sv_max_wide, 16);
+    SCUDA(cudaMalloc((void**)&h.sv_state, 2 * h.sv_state_cap * sizeof(int)));
+  }
+  // nodes is a member: it outlives the asynchronous copy
+  SCUDA(cudaMemcpyAsync(h.sv_nodes, nodes.data(), nodes.size() * sizeof(int),
+                        cudaMemcpyHostToDevice, s));
+  h.sv_f = h.h_f;
+  h.sv_npiv = h.h_npiv;
+  h.sv_fwd_grid.clear();
+  h.sv_wide_entries = h.wide_entries;
+  h.solve_epoch = h.factor_epoch;
+  return 0;
+}
+
+template <class T>
+static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
+                        cudaStream_t s) {
+  DevicePlan& d = h.d;
+  static bool attr_set = false;
+  static int wide_grid = 0;
+  const size_t wide_smem = ((WB + 1) * (WB + 1) + WB + 1) * sizeof(double);
+  if (!attr_set) {
+    SCUDA(cudaFuncSetAttribute(k_solve_forward<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kMaxDynSmem));
+    SCUDA(cudaFuncSetAttribute(k_solve_backward<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kMaxDynSmem));
+    int dev = 0, sms = 0, bf = 0, bb = 0;
+    SCUDA(cudaGetDevice(&dev));
+    SCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_wide_forward<T>, NT,
+                                                        wide_smem));
+    SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_wide_backward<T>,
+                                                        NT, wide_smem));
+    wide_grid = sms * std::max(1, std::min(bf, bb));
+    attr_set = true;
+  }
+  if ((int)h.sv_fwd_grid.size() != d.num_levels || h.sv_grid_cap != wide_grid) {
+    // Cooperative grids sized to the level's work (a grid-wide barrier
+    // costs more the more CTAs it spans): forward, one CTA per NT rows of
+    // the level's wide fronts; backward, one per 8 pivot columns (one warp
+    // each); at least one per front, at most what is co-resident.
+    h.sv_fwd_grid.assign(d.num_levels, 1);
+    h.sv_bwd_grid.assign(d.num_levels, 1);
+    for (int l = 0; l < d.num_levels; l++) {
+      long long fr = 0, bc = 0;
+      const int wc = h.sv_narrow_ptr[l + 1] - h.sv_wide_ptr[l];
+      for (int q = h.sv_wide_ptr[l]; q < h.sv_narrow_ptr[l + 1]; q++) {
+        const int k = h.sv_host[q];
+        fr += (h.h_f[k] + NT - 1) / NT;
+        bc += (h.h_npiv[k] + 7) / 8;
+      }
+      h.sv_fwd_grid[l] = (int)std::min<long long>(wide_grid, std::max<long long>(fr, wc));
+      h.sv_bwd_grid[l] = (int)std::min<long long>(wide_grid, std::max<long long>(bc, wc));
+      h.sv_fwd_grid[l] = std::max(h.sv_fwd_grid[l], 1);
+      h.sv_bwd_grid[l] = std::max(h.sv_bwd_grid[l], 1);
+    }
+    h.sv_grid_cap = wide_grid;
+  }
+  int* wst = h.sv_state;
+  // AMIGO_B200_TRACE=1: device time of every level's sweeps (diagnostics)
+  static const bool trace = std::getenv("AMIGO_B200_TRACE") != nullptr;
+  std::vector<cudaEvent_t> ev;
+  if (trace) {
+    ev.resize(2 * d.num_levels + 2);
+    for (auto& e : ev) cudaEventCreate(&e);
+  }
+  for (int l = 0; l < d.num_levels; l++) {
+    if (trace) cudaEventRecord(ev[l], s);
+    const int b = h.sv_narrow_ptr[l], cnt = h.sv_wide_ptr[l] - b;
+    if (cnt)
+      { k_solve_forward<T><<<cnt, NT, h.sv_narrow_smem[l], s>>>(d, h.sv_nodes + b, d_x, nrhs,
+                                               ldx, h.ubuf, h.uoff, h.sv_narrow_smem[l] / 8); ab::count_launch(); }
+    const int wb = h.sv_wide_ptr[l], wc = h.sv_narrow_ptr[l + 1] - wb;
+    if (wc) {
+      const int* wn = h.sv_nodes + wb;
+      double* ub = h.ubuf;
+      const long long* uo = h.uoff;
+      void* args[] = {(void*)&d, (void*)&wn, (void*)&wc, (void*)&d_x,
+                      (void*)&nrhs, (void*)&ldx, (void*)&ub, (void*)&uo,
+                      (void*)&wst};
+      SCUDA(cudaLaunchCooperativeKernel((const void*)k_wide_forward<T>,
+                                        dim3(h.sv_fwd_grid[l]), dim3(NT), args,
+                                        wide_smem, s));
+      ab::count_launch();
+    }
+  }
+  if (trace) cudaEventRecord(ev[d.num_levels], s);
+  for (int l = d.num_levels - 1; l >= 0; l--) {
+    if (trace) cudaEventRecord(ev[d.num_levels + 1 + (d.num_levels - 1 - l)], s);
+    const int b = h.sv_narrow_ptr[l], cnt = h.sv_wide_ptr[l] - b;
+    if (cnt)
+      { k_solve_backward<T><<<cnt, NT, h.sv_narrow_smem[l], s>>>(d, h.sv_nodes + b, d_x,
+                                                nrhs, ldx, h.ubuf, h.uoff,
+                                                h.sv_narrow_smem[l] / 8); ab::count_launch(); }
+    const int wb = h.sv_wide_ptr[l], wc = h.sv_narrow_ptr[l + 1] - wb;
+    if (wc) {
+      const int* wn = h.sv_nodes + wb;
+      double* ub = h.ubuf;
+      const long long* uo = h.uoff;
+      void* args[] = {(void*)&d, (void*)&wn, (void*)&wc, (void*)&d_x,
+                      (void*)&nrhs, (void*)&ldx, (void*)&ub, (void*)&uo,
+                      (void*)&wst};
+      SCUDA(cudaLaunchCooperativeKernel((const void*)k_wide_backward<T>,
+                                        dim3(h.sv_bwd_grid[l]), dim3(NT), args,
+                                        wide_smem, s));
+      ab::count_launch();
+    }
+  }
+  if (trace) {
+    const int L = d.num_levels;
+    cudaEventRecord(ev[2 * L + 1], s);
+    cudaEventSynchronize(ev[2 * L + 1]);
+    float tf = 0.f, tb = 0.f;
+    for (int l = 0; l < L; l++) {
+      float a = 0.f, b = 0.f;
+      cudaEventElapsedTime(&a, ev[l], ev[l + 1]);
+      const int bi = L + 1 + (L - 1 - l);
+      cudaEventElapsedTime(&b, ev[bi], ev[bi + 1]);
+      tf += a;
+      tb += b;
+      int fm = 0;
+      for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++)
+        fm = std::max(fm, h.h_f[h.level_nodes[q]]);
+      std::fprintf(stderr,
+                   "solve level %d: narrow %d wide %d max f %d  fwd %.3f ms  "
+                   "bwd %.3f ms\n",
+                   l, h.sv_wide_ptr[l] - h.sv_narrow_ptr[l],
+                   h.sv_narrow_ptr[l + 1] - h.sv_wide_ptr[l], fm, a, b);
+    }
+    std::fprintf(stderr, "solve total: fwd %.3f ms, bwd %.3f ms\n", tf, tb);
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  SCUDA(cudaGetLastError());
+  return 0;
+}
+
 int solve_numeric(LdlHandle& h, double* d_x, int nrhs, int ldx,
                   cudaStream_t s) {
   DevicePlan& d = h.d;
   const int nn = d.nn;
-  if (h.uoff_nrhs != nrhs) {
+  if (h.uoff_nrhs != nrhs ||
+      (h.solve_epoch != h.factor_epoch && h.sv_f != h.h_f)) {
+    // offsets of the update vectors (front sizes change with the delayed
+    // pivots of each factorization)
     h.h_uoff.resize(nn);
     long long tot = 0;
     for (int k = 0; k < nn; k++) {
@@ -245,6 +750,7 @@ int solve_numeric(LdlHandle& h, double* d_x, int nrhs, int ldx,
     }
     if (tot + 8 > h.ubuf_cap) {
       if (h.ubuf) SCUDA(cudaFree(h.ubuf));
+      h.ubuf = nullptr;
       h.ubuf_cap = tot + 8;
       SCUDA(cudaMalloc((void**)&h.ubuf, (size_t)h.ubuf_cap * sizeof(double)));
     }
@@ -252,40 +758,12 @@ int solve_numeric(LdlHandle& h, double* d_x, int nrhs, int ldx,
                           cudaMemcpyHostToDevice, s));
     h.uoff_nrhs = nrhs;
   }
-  static bool attr_set = false;
-  if (!attr_set) {
-    SCUDA(cudaFuncSetAttribute(k_solve_forward,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               kMaxDynSmem));
-    SCUDA(cudaFuncSetAttribute(k_solve_backward,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               kMaxDynSmem));
-    attr_set = true;
+  if (h.solve_epoch != h.factor_epoch) {
+    int rc = build_solve_schedule(h, s);
+    if (rc) return rc;
   }
-  // shared memory per level: the largest front vector of the level
-  std::vector<int> smem(d.num_levels, 0);
-  for (int l = 0; l < d.num_levels; l++) {
-    int fm = 0;
-    for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++)
-      fm = std::max(fm, h.h_f[h.level_nodes[q]]);
-    long long bytes = (long long)fm * 8;
-    smem[l] = (int)std::min<long long>(bytes, kMaxDynSmem);
-  }
-  for (int l = 0; l < d.num_levels; l++) {
-    const int b = h.level_ptr[l], cnt = h.level_ptr[l + 1] - b;
-    if (cnt)
-      { k_solve_forward<<<cnt, NT, smem[l], s>>>(d, d.level_nodes + b, d_x, nrhs,
-                                               ldx, h.ubuf, h.uoff, smem[l] / 8); ab::count_launch(); }
-  }
-  for (int l = d.num_levels - 1; l >= 0; l--) {
-    const int b = h.level_ptr[l], cnt = h.level_ptr[l + 1] - b;
-    if (cnt)
-      { k_solve_backward<<<cnt, NT, smem[l], s>>>(d, d.level_nodes + b, d_x,
-                                                nrhs, ldx, h.ubuf, h.uoff,
-                                                smem[l] / 8); ab::count_launch(); }
-  }
-  SCUDA(cudaGetLastError());
-  return 0;
+  return h.factor_precision == 32 ? launch_solve<float>(h, d_x, nrhs, ldx, s)
+                                   : launch_solve<double>(h, d_x, nrhs, ldx, s);
 }
 
 }  // namespace ab

@@ -123,7 +123,8 @@ def solve(backend, options=None, verbose=False):
     return result
 
 
-def solve_batch(model, device="cuda", options=None, verbose=False):
+def solve_batch(model, device="cuda", options=None, verbose=False,
+                precision="fp64"):
     """`solve` for every instance of a batch (problems.cartpole.CartPoleBatch)
     at once: each phase is one launch over all instances (the KKT matrices
     are factored together by the block-diagonal multifrontal LDL^T), while
@@ -133,7 +134,9 @@ def solve_batch(model, device="cuda", options=None, verbose=False):
     converged is frozen (zero step) until the last one converges.  Returns
     a dict of per-instance arrays: converged, iterations, objective,
     kkt_error, inertia_corrections, plus time_s (all of it), setup_s
-    (symbolic analysis, uploads) and x (host)."""
+    (symbolic analysis, uploads), fallbacks (FP64 refactorizations of the
+    mixed-precision form) and x (host).  precision "fp32" factors with FP32
+    fronts and refines every direction against the FP64 KKT."""
     from .ipm import BatchedInteriorPointOptimizer
     from .linalg import BatchedSparseLDL, CSRMat
     o = dict(DEFAULTS)
@@ -178,6 +181,49 @@ def solve_batch(model, device="cuda", options=None, verbose=False):
     def dev_vec(a, dtype=torch.float64):
         return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).to(dev)
 
+    def direction(st, steps, live):
+        """px = K^-1 res with per-instance 8-block refinement; returns each
+        instance's last residual ratio."""
+        opt.residual(st, g, res)
+        px.copy_(res)
+        ldl.solve_device(px)
+        ratio = np.zeros(K)
+        if not steps:
+            return ratio
+        S = ctypes.byref(opt._state(st))
+        _lib.call("ab_ipm_refine_init_seg", P, S, g.data_ptr(), res.data_ptr(),
+                  px.data_ptr(), izl.data_ptr(), izu.data_ptr(), seg.data_ptr(),
+                  stream)
+        nrm_rhs = seg[:K].cpu().numpy()
+        ratio_old = np.full(K, 1e30)
+        on = live.copy()
+        for step in range(steps + 1):
+            H.mult(px, kpx)
+            _lib.call("ab_ipm_refine_residual_seg", P, S, g.data_ptr(),
+                      res.data_ptr(), kpx.data_ptr(), px.data_ptr(),
+                      izl.data_ptr(), izu.data_ptr(), ecnd.data_ptr(),
+                      ezl.data_ptr(), ezu.data_ptr(), seg.data_ptr(), stream)
+            ns = seg.view(K, 2).cpu().numpy()
+            r = ns[:, 0] / (np.minimum(ns[:, 1], 1e6 * nrm_rhs) + nrm_rhs)
+            ratio = np.where(on, r, ratio)
+            if step >= 1:
+                on &= ~((r < 1e-10) | (r > 0.999999999 * ratio_old))
+            if not on.any():
+                break
+            ratio_old = np.where(on, r, ratio_old)
+            corr.copy_(ecnd)
+            ldl.solve_device(corr)
+            act.copy_(dev_vec(on.astype(np.int32), torch.int32))
+            _lib.call("ab_ipm_refine_update_seg", P, S, act.data_ptr(),
+                      corr.data_ptr(), ezl.data_ptr(), ezu.data_ptr(),
+                      px.data_ptr(), izl.data_ptr(), izu.data_ptr(), stream)
+        return ratio
+
+    refine_steps = o["refine_steps"]
+    if precision == "fp32":
+        ldl.set_precision("fp32")
+        refine_steps = max(refine_steps, DeviceBackend.mixed_refine_steps)
+    fallbacks = 0
     mu = np.full(K, o["mu0"])
     dw_last = np.zeros(K)
     nu = np.ones(K)
@@ -236,37 +282,18 @@ def solve_batch(model, device="cuda", options=None, verbose=False):
             if not pending.any():
                 break
         dw_last = np.where(live & (dw > 0.0), dw, dw_last)
-        # Newton direction with per-instance refinement
-        opt.residual(st, g, res)
-        px.copy_(res)
-        ldl.solve_device(px)
-        if o["refine_steps"]:
-            S = ctypes.byref(opt._state(st))
-            _lib.call("ab_ipm_refine_init_seg", P, S, g.data_ptr(), res.data_ptr(),
-                      px.data_ptr(), izl.data_ptr(), izu.data_ptr(), seg.data_ptr(),
-                      stream)
-            nrm_rhs = seg[:K].cpu().numpy()
-            ratio_old = np.full(K, 1e30)
-            on = live.copy()
-            for step in range(o["refine_steps"] + 1):
-                H.mult(px, kpx)
-                _lib.call("ab_ipm_refine_residual_seg", P, S, g.data_ptr(),
-                          res.data_ptr(), kpx.data_ptr(), px.data_ptr(),
-                          izl.data_ptr(), izu.data_ptr(), ecnd.data_ptr(),
-                          ezl.data_ptr(), ezu.data_ptr(), seg.data_ptr(), stream)
-                ns = seg.view(K, 2).cpu().numpy()
-                ratio = ns[:, 0] / (np.minimum(ns[:, 1], 1e6 * nrm_rhs) + nrm_rhs)
-                if step >= 1:
-                    on &= ~((ratio < 1e-10) | (ratio > 0.999999999 * ratio_old))
-                if not on.any():
-                    break
-                ratio_old = np.where(on, ratio, ratio_old)
-                corr.copy_(ecnd)
-                ldl.solve_device(corr)
-                act.copy_(dev_vec(on.astype(np.int32), torch.int32))
-                _lib.call("ab_ipm_refine_update_seg", P, S, act.data_ptr(),
-                          corr.data_ptr(), ezl.data_ptr(), ezu.data_ptr(),
-                          px.data_ptr(), izl.data_ptr(), izu.data_ptr(), stream)
+        # Newton direction with per-instance refinement; on FP32 fronts a
+        # direction whose refinement stalls is recomputed on an FP64
+        # refactorization of the same matrices
+        ratio = direction(st, refine_steps, live)
+        if precision == "fp32" and np.any(live & (ratio > 1e-10)):
+            fallbacks += 1
+            ldl.set_precision("fp64")
+            dm.hessian(st.x, 1.0, H.vals)
+            H.add_diagonal(dtot)
+            ldl.factor(H.vals)
+            direction(st, refine_steps, live)
+            ldl.set_precision("fp32")
         opt.compute_update(0.0, st, px, upd)
         # frozen instances take no step
         lv = dev_vec(live, torch.bool)
@@ -305,7 +332,7 @@ def solve_batch(model, device="cuda", options=None, verbose=False):
     return dict(converged=~live, iterations=iters, objective=objective(st),
                 kkt_error=q[:, :3].max(axis=1), inertia_corrections=n_ic,
                 time_s=time.perf_counter() - t0, setup_s=t_setup,
-                x=st.x.cpu().numpy())
+                fallbacks=fallbacks, x=st.x.cpu().numpy())
 
 
 class CartPoleProblem:
@@ -339,13 +366,25 @@ class CartPoleProblem:
 
 class DeviceBackend:
     """Numeric core on the GPU: component kernels, multifrontal LDL^T,
-    IPM vector kernels."""
+    IPM vector kernels.
 
-    def __init__(self, problem, model, device="cuda"):
+    precision "fp32" is the mixed-precision form: the KKT is factored with
+    FP32 fronts (tensor-core Schur updates on large fronts), every Newton
+    direction gets at least `mixed_refine_steps` steps of the 8-block
+    iterative refinement against the FP64 KKT, and an iteration whose
+    refinement stalls above 1e-10 is refactored in FP64 and solved again
+    (counted in `fallbacks`)."""
+
+    mixed_refine_steps = 4
+
+    def __init__(self, problem, model, device="cuda", precision="fp64"):
         self.P = problem
         self.m = model
         self.device = torch.device(device)
-        self.solver = B200Solver(problem, order=OrderingType.AMD)
+        self.precision = precision
+        self.fallbacks = 0
+        self.solver = B200Solver(problem, order=OrderingType.AMD,
+                                 precision=precision)
         self.opt = InteriorPointOptimizer(model.mult, model.lower, model.upper,
                                           device=self.device)
         self.opt.relax_bounds()
@@ -400,6 +439,7 @@ class DeviceBackend:
         torch.add(diag, self.primal, alpha=dw, out=self.dtot)
         if dc:
             self.dtot.sub_(1.0 - self.primal, alpha=dc)
+        self._fx = st.x
         self.solver.factor(1.0, st.x, self.dtot)
         return self.solver.get_inertia()
 
@@ -412,9 +452,21 @@ class DeviceBackend:
         return self.px
 
     def refine(self, mu, st, g, res, px, steps):
+        if self.precision == "fp32":
+            steps = max(steps, self.mixed_refine_steps)
         self.solver.iterative_refinement(mu, self.m.mult, res, st, g,
                                          self._lbx, self._ubx, px, None, None,
                                          max_steps=steps + 1)
+        if self.precision == "fp32" and self.solver.last_refinement[1] > 1e-10:
+            # refinement stalled on the FP32 factor: refactor in FP64
+            self.fallbacks += 1
+            self.solver.set_precision("fp64")
+            self.solver.factor(1.0, self._fx, self.dtot)
+            self.solver.solve(res, px)
+            self.solver.iterative_refinement(mu, self.m.mult, res, st, g,
+                                             self._lbx, self._ubx, px, None,
+                                             None, max_steps=steps + 1)
+            self.solver.set_precision("fp32")
 
     def update(self, mu, st, px):
         self.opt.compute_update(mu, st, px, self.upd)

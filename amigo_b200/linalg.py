@@ -175,7 +175,7 @@ class SparseLDL:
 
     def __init__(self, mat, solver_type=SolverType.LDL, ustab=0.01,
                  pivot_tol=1e-14, delay_growth=2.0,
-                 order=OrderingType.NATURAL):
+                 order=OrderingType.NATURAL, precision="fp64"):
         if int(solver_type) != int(SolverType.LDL):
             raise NotImplementedError(
                 "SolverType.CHOLESKY is not provided by amigo_b200")
@@ -189,6 +189,9 @@ class SparseLDL:
                       float(pivot_tol), float(delay_growth), ctypes.byref(h))
         self._h = h
         self._factored = False
+        self.precision = "fp64"
+        if precision != "fp64":
+            self.set_precision(precision)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -214,6 +217,24 @@ class SparseLDL:
         _lib.call("ab_ldl_inertia", self._h, _stream_ptr(self.device),
                   ctypes.byref(p), ctypes.byref(q))
         return p.value, q.value
+
+    def set_precision(self, precision):
+        """Front precision of the next factorizations: "fp64" (default) or
+        "fp32" (mixed precision: FP32 fronts, FP64 pivot tests and solve
+        accumulation; pair with FP64 iterative refinement)."""
+        bits = {"fp64": 64, "fp32": 32, 64: 64, 32: 32}[precision]
+        _lib.call("ab_ldl_set_precision", self._h, bits)
+        self.precision = "fp64" if bits == 64 else "fp32"
+
+    def set_tensor_cores(self, on):
+        """FP32 fronts: Schur updates of the large fronts on the tensor
+        cores (3xTF32, default) or on the CUDA cores."""
+        _lib.call("ab_ldl_set_tensor_cores", self._h, int(bool(on)))
+
+    def set_wide_threshold(self, entries):
+        """Fronts with f * npiv >= entries are solved by the multi-CTA
+        kernels (default 2^18)."""
+        _lib.call("ab_ldl_set_wide_threshold", self._h, int(entries))
 
     def stats(self):
         fl, fe = ctypes.c_double(), ctypes.c_double()
@@ -353,6 +374,14 @@ class BatchedSparseLDL:
             except Exception:
                 pass
             self._h = None
+
+    def set_precision(self, precision):
+        """Front precision ("fp64" default, or "fp32" mixed)."""
+        bits = {"fp64": 64, "fp32": 32, 64: 64, 32: 32}[precision]
+        _lib.call("ab_ldl_set_precision", self._h, bits)
+
+    def set_tensor_cores(self, on):
+        _lib.call("ab_ldl_set_tensor_cores", self._h, int(bool(on)))
 
     def factor(self, vals):
         if vals.numel() != self.nnz or vals.dtype != torch.float64:

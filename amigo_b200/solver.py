@@ -33,7 +33,10 @@ class B200Solver:
     supports_inertia = True
 
     def __init__(self, problem, ustab=0.01, pivot_tol=1e-14, delay_growth=2.0,
-                 order=OrderingType.DEFAULT):
+                 order=OrderingType.DEFAULT, precision="fp64"):
+        """precision "fp32" factors with FP32 fronts (mixed precision); the
+        caller's iterative refinement against the FP64 KKT recovers FP64
+        accuracy (see ipm_driver.DeviceBackend for the FP64 fallback)."""
         self.problem = problem
         self.hess = problem.create_matrix()
         (self.nrows, self.ncols, self.nnz, self.rowp,
@@ -41,7 +44,9 @@ class B200Solver:
         self._diag_indices = self.hess.diag
         self.device = self.hess.device
         self.ldl = SparseLDL(self.hess, ustab=ustab, pivot_tol=pivot_tol,
-                             delay_growth=delay_growth, order=order)
+                             delay_growth=delay_growth, order=order,
+                             precision=precision)
+        self.precision = precision
         self._ir = None
         self.last_refinement = None
 
@@ -52,6 +57,10 @@ class B200Solver:
             post_hessian(self.hess)
         self.problem.add_diagonal(diag, self.hess)
         self.ldl.factor()
+
+    def set_precision(self, precision):
+        self.ldl.set_precision(precision)
+        self.precision = precision
 
     def add_diagonal_and_factor(self, diag):
         self.problem.add_diagonal(diag, self.hess)

@@ -94,6 +94,35 @@ int ab_ldl_batch_inertia(ab_ldl_t h, void* stream, int* npos, int* nneg);
 int ab_ldl_batch_sizes(ab_ldl_t h, int* nprob, int* n_total,
                        long long* nnz_total);
 
+/* Precision of the fronts of the following factorizations: 64 (default,
+ * FP64, the reference's arithmetic) or 32 (mixed precision: fronts
+ * assembled from the FP64 values, stored and updated in FP32; the pivot
+ * tests compare FP64 copies of the FP32 values and the solves accumulate in
+ * FP64 while reading the FP32 factor.  Accuracy is recovered by iterative
+ * refinement against the FP64 KKT).  No reference counterpart. */
+int ab_ldl_set_precision(ab_ldl_t h, int bits);
+
+/* FP32 fronts only: 1 (default) applies the large fronts' Schur updates on
+ * the tensor cores (3xTF32 tcgen05, see ab_tc_syrk_tf32x3), 0 on the FP32
+ * CUDA cores.  No reference counterpart. */
+int ab_ldl_set_tensor_cores(ab_ldl_t h, int on);
+
+/* Solve schedule knob: fronts with f * npiv >= entries (default 2^18) are
+ * solved by the cooperative multi-CTA kernels, smaller ones one CTA per
+ * front.  Both give the same result to rounding.  No reference
+ * counterpart (the reference solves every front on one thread). */
+int ab_ldl_set_wide_threshold(ab_ldl_t h, long long entries);
+
+/* The tensor-core Schur update on plain device arrays (column-major, FP32):
+ * lower(C) -= A B^T for n x kw panels A, B (kw <= 31), as 3xTF32 tcgen05
+ * products accumulated in FP32 in tensor memory -- the update the
+ * mixed-precision factorization applies to its large fronts.  *d_status
+ * (device int) gets bit 8 if an MMA completion wait ran out.  No reference
+ * counterpart (the reference updates fronts with FP64 dgemm,
+ * include/sparse_ldl.h:1172-1197). */
+int ab_tc_syrk_tf32x3(int n, int kw, const float* A, int lda, const float* B,
+                      int ldb, float* C, int ldc, int* d_status, void* stream);
+
 /* Number of kernels this library has launched in the process so far (every
  * kernel of every entry point; library memsets excluded).  No reference
  * counterpart: it lets callers count the device launches of a region. */
