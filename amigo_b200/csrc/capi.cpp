@@ -1,7 +1,10 @@
 // extern "C" entry points declared in include/amigo_b200.h (LDL part).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
+#include <mutex>
+#include <unordered_map>
 #include <cstdio>
 #include <new>
 #include <vector>
@@ -20,6 +23,69 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 struct ab_ldl {
   ab::LdlHandle h;
 };
+
+// Symbolic analyses of the batched handles are cached by pattern: a
+// request stream of problems that share a pattern (e.g. trajectories with
+// the same number of intervals) analyses each pattern once.  Keyed by the
+// ordering, n, nnz and a 64-bit FNV-1a hash of rowp and cols; the stored
+// pattern is compared in full before a hit is used.
+namespace {
+struct SymKey {
+  int order, n;
+  long long nnz;
+  unsigned long long hash;
+  bool operator==(const SymKey& o) const {
+    return order == o.order && n == o.n && nnz == o.nnz && hash == o.hash;
+  }
+};
+struct SymKeyHash {
+  size_t operator()(const SymKey& k) const {
+    return (size_t)(k.hash ^ ((unsigned long long)k.n << 1) ^
+                    (unsigned long long)k.order);
+  }
+};
+struct SymEntry {
+  std::vector<int> rowp, cols;
+  ab::SymbolicTree tree;
+};
+std::mutex g_sym_mutex;
+std::unordered_map<SymKey, SymEntry, SymKeyHash> g_sym_cache;
+constexpr size_t kSymCacheMax = 4096;
+
+unsigned long long fnv1a(const int* a, long long len, unsigned long long h) {
+  for (long long i = 0; i < len; i++) {
+    h ^= (unsigned int)a[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+void cached_analyze(int order, int n, const int* rowp, const int* cols,
+                    ab::SymbolicTree& out) {
+  const long long nnz = rowp[n];
+  unsigned long long hh = fnv1a(rowp, n + 1, 1469598103934665603ull);
+  hh = fnv1a(cols, nnz, hh);
+  const SymKey key{order, n, nnz, hh};
+  {
+    std::lock_guard<std::mutex> lock(g_sym_mutex);
+    auto it = g_sym_cache.find(key);
+    if (it != g_sym_cache.end() &&
+        std::equal(rowp, rowp + n + 1, it->second.rowp.begin()) &&
+        std::equal(cols, cols + nnz, it->second.cols.begin())) {
+      out = it->second.tree;
+      return;
+    }
+  }
+  ab::analyze(order, n, rowp, cols, out);
+  std::lock_guard<std::mutex> lock(g_sym_mutex);
+  if (g_sym_cache.size() >= kSymCacheMax) g_sym_cache.clear();
+  SymEntry e;
+  e.rowp.assign(rowp, rowp + n + 1);
+  e.cols.assign(cols, cols + nnz);
+  e.tree = out;
+  g_sym_cache[key] = std::move(e);
+}
+}  // namespace
 
 extern "C" {
 
@@ -266,7 +332,7 @@ int ab_ldl_batch_create(int nprob, const int* n, const int* const* rowp,
   }
   std::vector<ab::SymbolicTree> trees(nprob);
   for (int p = 0; p < nprob; p++)
-    ab::analyze(order, n[p], rowp[p], cols[p], trees[p]);
+    cached_analyze(order, n[p], rowp[p], cols[p], trees[p]);
   merge_trees(trees, h.sym, h.prob_node_ptr, h.prob_var_ptr);
   // block-diagonal CSR of all problems
   std::vector<int> mr(1, 0), mc;

@@ -40,6 +40,9 @@ constexpr int NWARP = NT / 32;
 // candidate column is brought up to date by one thread per row, so more
 // threads shorten every candidate step.
 constexpr int kPanelThreads = 1024;
+// Shared memory of the large-front panel kernel for its copy of the
+// panel's L columns (the static control block aside).
+constexpr int kPanelCacheBytes = 200 * 1024;
 constexpr int kTile = 64;
 
 template <int BT>
@@ -251,7 +254,8 @@ __device__ void trailing_update(T* F, int ld, const T* W, int ldw,
 template <class T, int BT>
 __device__ void build_column(T* F, int ld, T* W, int ldw, int n,
                              int k, int kstart, int kw, int col, int mode,
-                             int imax, int nc, CtlT<BT>& ctl, int* status) {
+                             int imax, int nc, CtlT<BT>& ctl, int* status,
+                             const T* cache, int cld) {
   const int tid = threadIdx.x;
   double bestv = -1.0, tailv = 0.0;
   int besti = 0x7fffffff;
@@ -262,8 +266,10 @@ __device__ void build_column(T* F, int ld, T* W, int ldw, int n,
     } else {
       acc = (r < imax) ? F[imax + (size_t)r * ld] : F[r + (size_t)imax * ld];
     }
-    for (int j = 0; j < kw; j++)
-      acc -= F[r + (size_t)(kstart + j) * ld] * T(ctl.wrow[j]);
+    // the panel's L columns: from the shared-memory copy when there is one
+    const T* Lr = cache ? cache + (r - kstart) : F + r + (size_t)kstart * ld;
+    const size_t ls = cache ? (size_t)cld : (size_t)ld;
+    for (int j = 0; j < kw; j++) acc -= Lr[j * ls] * T(ctl.wrow[j]);
     W[r + (size_t)col * ldw] = acc;
     const double a = fabs((double)acc);
     if (mode == 0) {
@@ -305,18 +311,23 @@ __device__ void load_wrow(const T* W, int ldw, int row, int kw, CtlT<BT>& ctl) {
 // on while kw < NB - 1, each either eliminated (1x1 or 2x2, its L column(s)
 // written to F and its L*D column(s) kept in W) or delayed to the end of the
 // candidate set.  The trailing update of F[k:, k:] is left to the caller.
+// `cache` (shared memory, (n - k_) x NB, leading dimension n - k_) keeps a
+// copy of the panel's L columns for the column builds; nullptr reads them
+// from F.
 template <class T, int BT>
 __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
                              bool root, int* vars, int* fsperm, double ustab,
                              double pivot_tol, int* status, CtlT<BT>& ctl, int& k_,
-                             int& nc_, int& kw_) {
+                             int& nc_, int& kw_, T* cache = nullptr) {
   const int tid = threadIdx.x;
   const double bk_alpha = (1.0 + sqrt(17.0)) / 8.0;
   int k = k_, nc = nc_, kw = 0;
   const int kstart = k;
+  const int cld = n - kstart;
   while (kw < NB - 1 && k < nc) {
     load_wrow<T, BT>(W, ldw, k, kw, ctl);
-    build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status);
+    build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status,
+                        cache, cld);
     const double wkk = W[k + (size_t)kw * ldw];
     const double abswkk = fabs(wkk);
     const int imax = ctl.imax;
@@ -330,7 +341,8 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
         kpiv = k;
       } else if (k + 1 < nc) {
         load_wrow<T, BT>(W, ldw, imax, kw, ctl);
-        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
+        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status,
+                            cache, cld);
         const double rowmax = ctl.rowmax;
         const double wii = W[imax + (size_t)(kw + 1) * ldw];
         const double abswii = fabs(wii);
@@ -365,7 +377,8 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
         kpiv = k;
       } else {
         load_wrow<T, BT>(W, ldw, imax, kw, ctl);
-        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status);
+        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status,
+                            cache, cld);
         const double rowmax = ctl.rowmax;
         const double abswii = fabs(W[imax + (size_t)(kw + 1) * ldw]);
         if (abswkk >= bk_alpha * colmax * (colmax / rowmax)) {
@@ -389,6 +402,7 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
       if (k < nc - 1) {
         symm_swap<T, BT>(F, ld, n, vars, fsperm, k, nc - 1);
         swap_wrows<T, BT>(W, ldw, kw, k, nc - 1);
+        if (cache) swap_wrows<T, BT>(cache, cld, kw, k - kstart, nc - 1 - kstart);
         __syncthreads();
       }
       nc -= 1;
@@ -398,6 +412,7 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
     if (kpiv != ksrc) {
       symm_swap<T, BT>(F, ld, n, vars, fsperm, ksrc, kpiv);
       swap_wrows<T, BT>(W, ldw, kw + step, ksrc, kpiv);
+      if (cache) swap_wrows<T, BT>(cache, cld, kw, ksrc - kstart, kpiv - kstart);
       __syncthreads();
     }
     if (step == 1) {
@@ -407,7 +422,9 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
       if (tid == 0) vars[3 * ld + k] = 0;  // 1x1 pivot
       for (int r = k + tid; r < n; r += BT) {
         T w = W[r + (size_t)kw * ldw];
-        F[r + (size_t)k * ld] = (r == k) ? w : w * dinv;
+        const T l = (r == k) ? w : w * dinv;
+        F[r + (size_t)k * ld] = l;
+        if (cache) cache[(r - kstart) + (size_t)kw * cld] = l;
       }
     } else {
       const T d11 = W[k + (size_t)kw * ldw];
@@ -419,8 +436,13 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
               i01 = -d21 * detinv, i11 = d11 * detinv;
       for (int r = k + 2 + tid; r < n; r += BT) {
         T w0 = W[r + (size_t)kw * ldw], w1 = W[r + (size_t)(kw + 1) * ldw];
-        F[r + (size_t)k * ld] = w0 * i00 + w1 * i10;
-        F[r + (size_t)(k + 1) * ld] = w0 * i01 + w1 * i11;
+        const T l0 = w0 * i00 + w1 * i10, l1 = w0 * i01 + w1 * i11;
+        F[r + (size_t)k * ld] = l0;
+        F[r + (size_t)(k + 1) * ld] = l1;
+        if (cache) {
+          cache[(r - kstart) + (size_t)kw * cld] = l0;
+          cache[(r - kstart) + (size_t)(kw + 1) * cld] = l1;
+        }
       }
       if (tid == 0) {
         F[k + (size_t)k * ld] = d11;
@@ -751,8 +773,9 @@ k_big_extend(DevicePlan d, const int* __restrict__ nodes, int q) {
 template <class T>
 __global__ void __launch_bounds__(kPanelThreads)
 k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
-            double pivot_tol) {
+            double pivot_tol, int cache_bytes) {
   __shared__ CtlT<kPanelThreads> ctl;
+  extern __shared__ double cache_raw[];
   if (big_skip(d)) return;
   const int node = nodes[blockIdx.x];
   int* st = d.pstate + 4 * node;
@@ -768,8 +791,12 @@ k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
   int* fvars = d.ipool + d.ioff[node];
   const int kstart = k;
   int kw = 0;
+  // the panel's L columns in shared memory when the remaining rows fit
+  T* cache = (long long)(f - k) * NB * (long long)sizeof(T) <= cache_bytes
+                 ? reinterpret_cast<T*>(cache_raw)
+                 : nullptr;
   panel_factor<T, kPanelThreads>(F, f, W, f, f, fs == f, fvars, fvars + f, ustab, pivot_tol,
-               d.status, ctl, k, nc, kw);
+               d.status, ctl, k, nc, kw, cache);
   if (threadIdx.x == 0) {
     st[0] = k;
     st[1] = nc;
@@ -880,6 +907,9 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     FCUDA(cudaFuncSetAttribute(k_big_update<T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kTileSmem * sizeof(T)));
+    FCUDA(cudaFuncSetAttribute(k_big_panel<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kPanelCacheBytes));
     FCUDA(cudaFuncSetAttribute(k_big_update_tc,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::kSmemBytes));
@@ -924,6 +954,9 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
         { k_big_extend<T><<<dim3(B, std::max(ge, 1)), NT, 0, s>>>(d, nodes, q); ab::count_launch(); }
       const long long ntl = (fm + kTile - 1) / kTile;
       int gu = (int)std::min<long long>(4 * 148, ntl * (ntl + 1) / 2);
+      // shared-memory copy of the panel's L columns: as many rows as fit
+      const int panel_cache = (int)std::min<long long>(
+          kPanelCacheBytes, (long long)fm * NB * (long long)sizeof(T));
       // FP32 fronts of at least one 128-row tile: tensor-core update
       const bool use_tc = sizeof(T) == 4 && h.tensor_cores && fm >= tc::TM;
       const long long ntc = (fm + tc::TM - 1) / tc::TM;
@@ -937,8 +970,8 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       for (;;) {
         budget += panels;
         for (int it = 0; it < panels; it++) {
-          { k_big_panel<T><<<B, kPanelThreads, 0, s>>>(d, nodes, h.ustab,
-                                                     h.pivot_tol); ab::count_launch(); }
+          { k_big_panel<T><<<B, kPanelThreads, panel_cache, s>>>(d, nodes, h.ustab,
+                                                     h.pivot_tol, panel_cache); ab::count_launch(); }
           if (use_tc) {
             { k_big_update_tc<<<dim3(B, gtc), tc::kThreads, tc::kSmemBytes, s>>>(
                 d, nodes); ab::count_launch(); }

@@ -19,16 +19,14 @@ driver runs over a host backend made of the reference's own SparseLDL and
 IPM vector functions (oracle/host_backend.py) to compare iteration counts
 and optima.
 """
-import ctypes
 import math
 import time
 
 import numpy as np
 import torch
 
-from . import _lib
 from .ipm import InteriorPointOptimizer
-from .linalg import OrderingType, _stream_ptr
+from .linalg import OrderingType
 from .solver import B200Solver
 
 
@@ -126,213 +124,39 @@ def solve(backend, options=None, verbose=False):
 def solve_batch(model, device="cuda", options=None, verbose=False,
                 precision="fp64"):
     """`solve` for every instance of a batch (problems.cartpole.CartPoleBatch)
-    at once: each phase is one launch over all instances (the KKT matrices
-    are factored together by the block-diagonal multifrontal LDL^T), while
-    the barrier parameter, inertia correction, refinement stopping rule,
-    step lengths and line search are kept per instance, so each instance
-    takes the decisions it would take alone.  An instance that has
-    converged is frozen (zero step) until the last one converges.  Returns
-    a dict of per-instance arrays: converged, iterations, objective,
-    kkt_error, inertia_corrections, plus time_s (all of it), setup_s
-    (symbolic analysis, uploads), fallbacks (FP64 refactorizations of the
-    mixed-precision form) and x (host).  precision "fp32" factors with FP32
-    fronts and refines every direction against the FP64 KKT."""
-    from .ipm import BatchedInteriorPointOptimizer
-    from .linalg import BatchedSparseLDL, CSRMat
-    o = dict(DEFAULTS)
-    o.update(options or {})
+    at once, on batch_engine.BatchEngine: each phase is one launch over all
+    instances (the KKT matrices are factored together by the block-diagonal
+    multifrontal LDL^T), while the barrier parameter, inertia correction,
+    refinement stopping rule, step lengths and line search are kept per
+    instance, so each instance takes the decisions it would take alone.  An
+    instance that has converged takes no further steps.  Returns a dict of
+    per-instance arrays: converged, iterations, objective, kkt_error,
+    inertia_corrections, plus time_s (all of it), setup_s (symbolic
+    analysis, uploads), fallbacks (FP64 refactorizations of the
+    mixed-precision form) and x (host, concatenated).  precision "fp32"
+    factors with FP32 fronts and refines every direction against the FP64
+    KKT."""
+    from .batch_engine import BatchEngine
     dev = torch.device(device)
     t0 = time.perf_counter()
-    K = model.k
-    n = model.n
-    dm = model.device_model(dev)
-    H = CSRMat(n, n, model.rowp, model.cols, device=dev)
-    ldl = BatchedSparseLDL(model.patterns(), order=OrderingType.AMD, device=dev)
-    opt = BatchedInteriorPointOptimizer(model.mult, model.lower, model.upper,
-                                        model.vinst, device=dev)
-    opt.relax_bounds()
-    f64 = dict(dtype=torch.float64, device=dev)
-    vinst = opt.vinst.long()
-    pinst = opt.pinst.long()
-    primal = torch.from_numpy(~model.mult).to(dev).double()
-    mult_idx = opt.cidx.long()
-    g, gf, res, px, diag, dtot, xtmp, kpx, ecnd, corr = (
-        torch.zeros(n, **f64) for _ in range(10))
-    ezl, ezu, izl, izu = (torch.zeros(opt.np_, **f64) for _ in range(4))
-    seg = torch.zeros(2 * K, **f64)
-    act = torch.zeros(K, dtype=torch.int32, device=dev)
-    obj = torch.zeros(K, **f64)
-    upd = opt.create_opt_vector()
-    trial = opt.create_opt_vector()
-    st = opt.create_opt_vector(torch.from_numpy(np.ascontiguousarray(model.x0)).to(dev))
-    opt.initialize_multipliers_and_slacks(0.1, None, st)
-    stream = _stream_ptr(dev)
-    P = ctypes.byref(opt._p)
+    eng = BatchEngine(dev, options, precision)
+    eng.admit(enumerate(model.inst))
+    eng._build()
     torch.cuda.synchronize(dev)
     t_setup = time.perf_counter() - t0
-
-    def grad(x, out):
-        dm.gradient(x, 1.0, out)
-
-    def objective(v):
-        dm.objective(v.x, obj)
-        return obj.cpu().numpy()
-
-    def dev_vec(a, dtype=torch.float64):
-        return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).to(dev)
-
-    def direction(st, steps, live):
-        """px = K^-1 res with per-instance 8-block refinement; returns each
-        instance's last residual ratio."""
-        opt.residual(st, g, res)
-        px.copy_(res)
-        ldl.solve_device(px)
-        ratio = np.zeros(K)
-        if not steps:
-            return ratio
-        S = ctypes.byref(opt._state(st))
-        _lib.call("ab_ipm_refine_init_seg", P, S, g.data_ptr(), res.data_ptr(),
-                  px.data_ptr(), izl.data_ptr(), izu.data_ptr(), seg.data_ptr(),
-                  stream)
-        nrm_rhs = seg[:K].cpu().numpy()
-        ratio_old = np.full(K, 1e30)
-        on = live.copy()
-        for step in range(steps + 1):
-            H.mult(px, kpx)
-            _lib.call("ab_ipm_refine_residual_seg", P, S, g.data_ptr(),
-                      res.data_ptr(), kpx.data_ptr(), px.data_ptr(),
-                      izl.data_ptr(), izu.data_ptr(), ecnd.data_ptr(),
-                      ezl.data_ptr(), ezu.data_ptr(), seg.data_ptr(), stream)
-            ns = seg.view(K, 2).cpu().numpy()
-            r = ns[:, 0] / (np.minimum(ns[:, 1], 1e6 * nrm_rhs) + nrm_rhs)
-            ratio = np.where(on, r, ratio)
-            if step >= 1:
-                on &= ~((r < 1e-10) | (r > 0.999999999 * ratio_old))
-            if not on.any():
-                break
-            ratio_old = np.where(on, r, ratio_old)
-            corr.copy_(ecnd)
-            ldl.solve_device(corr)
-            act.copy_(dev_vec(on.astype(np.int32), torch.int32))
-            _lib.call("ab_ipm_refine_update_seg", P, S, act.data_ptr(),
-                      corr.data_ptr(), ezl.data_ptr(), ezu.data_ptr(),
-                      px.data_ptr(), izl.data_ptr(), izu.data_ptr(), stream)
-        return ratio
-
-    refine_steps = o["refine_steps"]
-    if precision == "fp32":
-        ldl.set_precision("fp32")
-        refine_steps = max(refine_steps, DeviceBackend.mixed_refine_steps)
-    fallbacks = 0
-    mu = np.full(K, o["mu0"])
-    dw_last = np.zeros(K)
-    nu = np.ones(K)
-    n_ic = np.zeros(K, np.int64)
-    iters = np.full(K, o["max_iter"], np.int64)
-    live = np.ones(K, bool)
-    opt.set_barrier_params(mu)
-    for it in range(o["max_iter"]):
-        grad(st.x, g)
-        q = opt.seg_reduce(st, grad=g, zero_mu=True)
-        E0 = q[:, :3].max(axis=1)
-        conv = live & (E0 <= o["tol"])
-        iters[conv] = it
-        live &= ~conv
+    results = {}
+    while len(results) < model.k:
+        for r in eng.step(rebuild=False):
+            results[r["id"]] = r
         if verbose:
-            print("it %3d  live %d" % (it, live.sum()))
-        if not live.any():
-            break
-        # monotone barrier update, per instance
-        while True:
-            q = opt.seg_reduce(st, grad=g)
-            Emu = q[:, :3].max(axis=1)
-            dec = live & (Emu <= o["kappa_eps"] * mu) & (mu > o["mu_min"])
-            if not dec.any():
-                break
-            mu[dec] = np.maximum(o["mu_min"], np.minimum(o["kappa_mu"] * mu[dec],
-                                                         mu[dec] ** o["theta_mu"]))
-            opt.set_barrier_params(mu)
-        # inertia-corrected factorization, per instance
-        opt.compute_diagonal(st, diag)
-        dw, dc = np.zeros(K), np.zeros(K)
-        dwf, dcf = dw.copy(), dc.copy()     # values the factor was made with
-        pending = live.copy()
-        for attempt in range(41):
-            dwv, dcv = dev_vec(dwf)[vinst], dev_vec(dcf)[vinst]
-            torch.addcmul(diag, dwv, primal, out=dtot)
-            dtot.sub_(dcv * (1.0 - primal))
-            dm.hessian(st.x, 1.0, H.vals)
-            H.add_diagonal(dtot)
-            ldl.factor(H.vals)
-            inertia = np.array(ldl.get_inertia())
-            ok = (inertia[:, 0] == opt.np_each) & (inertia[:, 1] == opt.nc_each)
-            bad = pending & ~ok
-            if not bad.any():
-                break
-            n_ic[bad] += 1
-            sing = bad & (inertia.sum(axis=1) < ldl.n_each) & (dc == 0.0)
-            dc[sing] = o["dc"] * mu[sing] ** o["kappa_c"]
-            first = bad & (dw == 0.0)
-            dw[first] = np.where(dw_last[first] == 0.0, o["dw_first"],
-                                 np.maximum(o["dw_min"], o["kw_minus"] * dw_last[first]))
-            grow = bad & ~first
-            dw[grow] *= np.where(dw_last[grow] == 0.0, o["kw_plus_first"], o["kw_plus"])
-            pending = bad & (dw <= o["dw_max"])
-            dwf[pending], dcf[pending] = dw[pending], dc[pending]
-            if not pending.any():
-                break
-        dw_last = np.where(live & (dw > 0.0), dw, dw_last)
-        # Newton direction with per-instance refinement; on FP32 fronts a
-        # direction whose refinement stalls is recomputed on an FP64
-        # refactorization of the same matrices
-        ratio = direction(st, refine_steps, live)
-        if precision == "fp32" and np.any(live & (ratio > 1e-10)):
-            fallbacks += 1
-            ldl.set_precision("fp64")
-            dm.hessian(st.x, 1.0, H.vals)
-            H.add_diagonal(dtot)
-            ldl.factor(H.vals)
-            direction(st, refine_steps, live)
-            ldl.set_precision("fp32")
-        opt.compute_update(0.0, st, px, upd)
-        # frozen instances take no step
-        lv = dev_vec(live, torch.bool)
-        upd.x.copy_(torch.where(lv[vinst], upd.x, 0.0))
-        upd.duals.view(2, -1).copy_(torch.where(lv[pinst], upd.duals.view(2, -1), 0.0))
-        # fraction to the boundary and merit terms
-        xtmp.copy_(st.x)
-        xtmp[mult_idx] = 0.0
-        grad(xtmp, gf)
-        q = opt.seg_reduce(st, grad=g, upd=upd, gf=gf, tau=-o["tau_min"])
-        ax, az = q[:, 5].copy(), q[:, 6].copy()
-        nu = np.where(live, np.maximum(nu, 1.1 * q[:, 8]), nu)
-        theta0 = q[:, 3]
-        phi0 = objective(st) + q[:, 4] + nu * theta0
-        dphi = q[:, 7] - nu * theta0
-        alpha = np.where(live, ax, 0.0)
-        az = np.where(live, az, 0.0)
-        az_d = dev_vec(az)
-        search = live.copy()
-        gt = torch.zeros(n, **f64)
-        trial.copy(st)
-        for ls in range(o["max_ls"]):
-            opt.apply_step_seg(dev_vec(alpha), az_d, st, upd, trial)
-            grad(trial.x, gt)
-            qt = opt.seg_reduce(trial, grad=gt)
-            phi = objective(trial) + qt[:, 4] + nu * qt[:, 3]
-            accept = (phi <= phi0 + o["armijo"] * alpha * dphi) | ~np.isfinite(dphi)
-            search &= ~accept
-            if not search.any():
-                break
-            alpha = np.where(search, 0.5 * alpha, alpha)
-        st, trial = trial, st
-        opt.reset_bound_multipliers(0.0, o["kappa_sigma"], st)
-    grad(st.x, g)
-    q = opt.seg_reduce(st, grad=g, zero_mu=True)
-    return dict(converged=~live, iterations=iters, objective=objective(st),
-                kkt_error=q[:, :3].max(axis=1), inertia_corrections=n_ic,
+            print("live %d" % (model.k - len(results)))
+    R = [results[k] for k in range(model.k)]
+    col = lambda key, dt: np.array([r[key] for r in R], dtype=dt)
+    return dict(converged=col("converged", bool), iterations=col("iterations", np.int64),
+                objective=col("objective", float), kkt_error=col("kkt_error", float),
+                inertia_corrections=col("inertia_corrections", np.int64),
                 time_s=time.perf_counter() - t0, setup_s=t_setup,
-                fallbacks=fallbacks, x=st.x.cpu().numpy())
+                fallbacks=eng.fallbacks, x=np.concatenate([r["x"] for r in R]))
 
 
 class CartPoleProblem:

@@ -3,10 +3,14 @@ library once or a few times; used for profiler captures of single kernels.
 
     python -m amigo_b200.workloads simp2d [nx ny]   # KKT assembly, factor, solve, IPM vectors
     python -m amigo_b200.workloads cartpole [N]     # one whole IPM solve
+    python -m amigo_b200.workloads simp3d [nx ny nz [fp32|fp64]]
+                                   # 3D KKT factor (tensor-core updates in
+                                   # fp32) and solve
 """
 import sys
 import time
 
+import numpy as np
 import torch
 
 
@@ -64,12 +68,39 @@ def cartpole(N=100):
           (N, r["iterations"], r["objective"], r["kkt_error"], r["time_s"]))
 
 
+def simp3d(nx=16, ny=8, nz=8, precision="fp32", reps=2):
+    from . import linalg
+    from .problems.simp3d import Simp3D
+    dev = torch.device("cuda", 0)
+    m = Simp3D(nx, ny, nz)
+    dm = m.device_model(dev)
+    K = linalg.CSRMat(m.n, m.n, m.rowp, m.cols, device=dev)
+    ldl = linalg.SparseLDL(K, order=linalg.OrderingType.AMD, precision=precision)
+    x = torch.from_numpy(m.initial_point()).to(dev)
+    dm.hessian(x, 1.0, K.vals)
+    d = torch.from_numpy(np.where(~m.mult, 1.0, 0.0)).to(dev)
+    K.add_diagonal(d)
+    b = torch.ones(m.n, dtype=torch.float64, device=dev)
+    for _ in range(reps):
+        t = time.perf_counter()
+        ldl.factor()
+        xs = b.clone()
+        ldl.solve_device(xs)
+        torch.cuda.synchronize()
+        print("simp3d %dx%dx%d n=%d %s inertia=%s %.2f ms" %
+              (nx, ny, nz, m.n, precision, ldl.get_inertia(),
+               1e3 * (time.perf_counter() - t)))
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "simp2d"
-    args = [int(a) for a in sys.argv[2:]]
+    args = [int(a) for a in sys.argv[2:] if a.isdigit()]
     if which == "simp2d":
         simp2d(*args)
     elif which == "cartpole":
         cartpole(*args)
+    elif which == "simp3d":
+        prec = sys.argv[5] if len(sys.argv) > 5 else "fp32"
+        simp3d(*[int(a) for a in sys.argv[2:5]], precision=prec)
     else:
         raise SystemExit("unknown workload " + which)

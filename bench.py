@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-ipm-solve", action="store_true")
     ap.add_argument("--batch", type=int, default=512,
                     help="instances in the batched cart-pole solve (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=600,
+                    help="requests in the serving run (0: skip)")
     ap.add_argument("--no-3d", action="store_true",
                     help="skip the 3D SIMP 48x24x24 factorization")
     return ap.parse_args()
@@ -298,7 +300,26 @@ def run_ours(args, rank, world, local):
         out["ipm_solve"] = ipm_solve_bench(device, args.solves)
         if args.batch > 0:
             out["batch_solve"] = batch_solve_bench(device, args.batch)
+            if args.serve_requests > 0:
+                cap = out["batch_solve"]["solves_per_s"]
+                out["serve"] = serve_bench(device, args.serve_requests, cap)
     return out
+
+
+def serve_bench(device, n_requests, capacity):
+    """Serving: a stream of cart-pole solve requests (N ~ U{50..400}) with
+    Poisson arrivals at 80% of the measured batched capacity, continuous
+    batching (serve.Server: admission at iteration boundaries by slots and a
+    150 GB device-memory budget from symbolic workspace estimates)."""
+    from amigo_b200 import serve
+    rate = 0.8 * capacity
+    reqs = serve.make_stream(n_requests, rate, seed=11)
+    srv = serve.Server(device, mem_budget=150e9, max_batch=512)
+    _, summ = srv.run(reqs, time_limit=240)
+    summ = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in summ.items()}
+    summ.update(arrival_rate_per_s=round(rate, 3), capacity_per_s=capacity,
+                mix="cart-pole requests only (the 70% class of the serving mix)")
+    return summ
 
 
 def simp3d_bench(device, reps=2):
@@ -345,16 +366,42 @@ def simp3d_bench(device, reps=2):
     K.mult(xs, kx)
     res = (kx - b).abs().max().item()
     st = ldl.stats()
+    inertia = list(ldl.get_inertia())
     fac_s = float(np.median(fac)) * 1e-3
+    # mixed precision: FP32 fronts, tensor-core Schur updates, FP64
+    # refinement of the solve against the FP64 matrix
+    ldl.set_precision("fp32")
+    ldl.factor()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    xm = b.clone()
+    r = torch.empty_like(b)
+    e[0].record(stream)
+    ldl.factor()
+    e[1].record(stream)
+    ldl.solve_device(xm)
+    for _ in range(3):
+        K.mult(xm, r)
+        r.sub_(b).neg_()
+        ldl.solve_device(r)
+        xm.add_(r)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    K.mult(xm, kx)
+    mixed = {"factor_s": round(e[0].elapsed_time(e[1]) * 1e-3, 4),
+             "solve_refine3_s": round(e[1].elapsed_time(e[2]) * 1e-3, 4),
+             "inertia": list(ldl.get_inertia()),
+             "residual_inf": (kx - b).abs().max().item(),
+             "note": "FP32 fronts, 3xTF32 tcgen05 Schur updates, 3 steps of "
+                     "FP64 refinement"}
     return {"workload": "3D SIMP cantilever 48x24x24 full-space KKT, FP64 "
                         "factor + solve",
             "n": int(m.n), "nnz": int(m.nnz), "flops": st["flops"],
             "factor_s": round(fac_s, 4), "solve_s": round(float(np.median(sol)) * 1e-3, 4),
             "tflops": round(st["flops"] / fac_s / 1e12, 3),
-            "inertia": list(ldl.get_inertia()), "inertia_expected": list(want),
+            "inertia": inertia, "inertia_expected": list(want),
             "residual_inf": res, "max_front": st["max_front"],
             "num_delayed": st["num_delayed"], "factor_entries": st["factor_entries"],
-            "host_setup_s": round(setup_s, 2), "reps": reps}
+            "host_setup_s": round(setup_s, 2), "reps": reps, "mixed": mixed}
 
 
 def batch_solve_bench(device, k, sequential_sample=8):
@@ -373,6 +420,21 @@ def batch_solve_bench(device, k, sequential_sample=8):
     r = ipm_driver.solve_batch(B, device)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    rm = ipm_driver.solve_batch(B, device, precision="fp32")
+    torch.cuda.synchronize()
+    wall_m = time.perf_counter() - t
+    same = rm["converged"] & r["converged"]
+    obj_dev = (float(np.max(np.abs(rm["objective"][same] - r["objective"][same]) /
+                            np.maximum(1.0, np.abs(r["objective"][same]))))
+               if same.any() else None)
+    mixed = {"solves_per_s": round(int(rm["converged"].sum()) / wall_m, 3),
+             "wall_s": round(wall_m, 3), "converged": int(rm["converged"].sum()),
+             "fp64_fallbacks": int(rm["fallbacks"]),
+             "max_rel_objective_diff_vs_fp64": obj_dev,
+             "max_kkt_error_converged": (float(rm["kkt_error"][rm["converged"]].max())
+                                         if rm["converged"].any() else None)}
     seq = []
     for m in B.inst[:sequential_sample]:
         t1 = time.perf_counter()
@@ -391,6 +453,7 @@ def batch_solve_bench(device, k, sequential_sample=8):
                                 "line search) does not solve in 200 iterations",
             "max_iterations": int(r["iterations"].max()),
             "max_kkt_error": float(r["kkt_error"].max()),
+            "mixed": mixed,
             "sequential_single_path_solves_per_s":
                 round(len(seq) / float(np.sum(seq)), 3),
             "sequential_sample": "first %d instances, single-problem device "
