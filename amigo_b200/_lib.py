@@ -150,6 +150,7 @@ _SIGS = {
     "ab_ldl_set_wide_threshold": (_i, [_vp, ctypes.c_longlong]),
     "ab_ldl_set_precision": (_i, [_vp, _i]),
     "ab_ldl_set_tensor_cores": (_i, [_vp, _i]),
+    "ab_ldl_set_panel_cache": (_i, [_vp, _i]),
     "ab_tc_syrk_tf32x3": (_i, [_i, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _vp]),
     "ab_csr_add_diagonal": (_i, [_i, _vp, _vp, _vp, _vp]),
     "ab_csr_matvec": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -56,6 +56,7 @@ class BatchEngine:
         self.waiting = []      # admitted, not yet in the layout
         self.fallbacks = 0
         self.rebuilds = 0
+        self.rebuild_s = 0.0   # host + device time spent rebuilding layouts
         self._built = False
 
     # -- membership ------------------------------------------------------
@@ -93,6 +94,15 @@ class BatchEngine:
         from .ipm import BatchedInteriorPointOptimizer
         from .linalg import BatchedSparseLDL, CSRMat
         from .problems.cartpole import CartPoleBatch
+        t0 = time.perf_counter()
+        try:
+            self._build_layout(BatchedInteriorPointOptimizer, BatchedSparseLDL,
+                               CSRMat, CartPoleBatch)
+        finally:
+            self.rebuild_s += time.perf_counter() - t0
+
+    def _build_layout(self, BatchedInteriorPointOptimizer, BatchedSparseLDL,
+                      CSRMat, CartPoleBatch):
         self._save_states()
         self.insts = [r for r in self.insts if not r.done] + self.waiting
         self.waiting = []
@@ -105,7 +115,7 @@ class BatchEngine:
         self.B = B
         self.K, self.n = B.k, B.n
         self.dm = B.device_model(dev)
-        self.H = CSRMat(B.n, B.n, B.rowp, B.cols, device=dev)
+        self.H = CSRMat(B.n, B.n, B.rowp, B.cols, device=dev, diag_pos=B.diag_pos)
         self.ldl = BatchedSparseLDL(B.patterns(), order=OrderingType.AMD, device=dev)
         if self.precision == "fp32":
             self.ldl.set_precision("fp32")

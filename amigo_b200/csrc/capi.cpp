@@ -384,6 +384,12 @@ int ab_ldl_set_tensor_cores(ab_ldl_t h, int on) {
   return AB_OK;
 }
 
+int ab_ldl_set_panel_cache(ab_ldl_t h, int bytes) {
+  if (!h || bytes < 0 || bytes > 200 * 1024) return AB_ERR_ARG;
+  h->h.panel_cache_bytes = bytes;
+  return AB_OK;
+}
+
 int ab_ldl_set_wide_threshold(ab_ldl_t h, long long entries) {
   if (!h || entries < 1) return AB_ERR_ARG;
   h->h.wide_entries = entries;

@@ -266,9 +266,10 @@ __device__ void build_column(T* F, int ld, T* W, int ldw, int n,
     } else {
       acc = (r < imax) ? F[imax + (size_t)r * ld] : F[r + (size_t)imax * ld];
     }
-    // the panel's L columns: from the shared-memory copy when there is one
-    const T* Lr = cache ? cache + (r - kstart) : F + r + (size_t)kstart * ld;
-    const size_t ls = cache ? (size_t)cld : (size_t)ld;
+    // the panel's L columns: from the shared-memory copy for its rows
+    const bool inc = cache && (r - kstart) < cld;
+    const T* Lr = inc ? cache + (r - kstart) : F + r + (size_t)kstart * ld;
+    const size_t ls = inc ? (size_t)cld : (size_t)ld;
     for (int j = 0; j < kw; j++) acc -= Lr[j * ls] * T(ctl.wrow[j]);
     W[r + (size_t)col * ldw] = acc;
     const double a = fabs((double)acc);
@@ -311,19 +312,31 @@ __device__ void load_wrow(const T* W, int ldw, int row, int kw, CtlT<BT>& ctl) {
 // on while kw < NB - 1, each either eliminated (1x1 or 2x2, its L column(s)
 // written to F and its L*D column(s) kept in W) or delayed to the end of the
 // candidate set.  The trailing update of F[k:, k:] is left to the caller.
-// `cache` (shared memory, (n - k_) x NB, leading dimension n - k_) keeps a
-// copy of the panel's L columns for the column builds; nullptr reads them
-// from F.
+// `cache` (shared memory, cache_rows x NB, leading dimension cache_rows)
+// keeps a copy of the panel's L columns for rows [k_, k_ + cache_rows) for
+// the column builds; the other rows (and all rows when cache is nullptr)
+// are read from F, which always holds the values.
+template <class T, int BT>
+__device__ void refresh_cache_rows(const T* F, int ld, T* cache, int cld,
+                                   int kstart, int kw, int a, int b) {
+  for (int t = threadIdx.x; t < 2 * kw; t += BT) {
+    const int row = (t & 1) ? b : a, j = t >> 1;
+    if (row - kstart < cld)
+      cache[(row - kstart) + (size_t)j * cld] = F[row + (size_t)(kstart + j) * ld];
+  }
+}
+
 template <class T, int BT>
 __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
                              bool root, int* vars, int* fsperm, double ustab,
                              double pivot_tol, int* status, CtlT<BT>& ctl, int& k_,
-                             int& nc_, int& kw_, T* cache = nullptr) {
+                             int& nc_, int& kw_, T* cache = nullptr,
+                             int cache_rows = 0) {
   const int tid = threadIdx.x;
   const double bk_alpha = (1.0 + sqrt(17.0)) / 8.0;
   int k = k_, nc = nc_, kw = 0;
   const int kstart = k;
-  const int cld = n - kstart;
+  const int cld = cache ? (n - kstart < cache_rows ? n - kstart : cache_rows) : 0;
   while (kw < NB - 1 && k < nc) {
     load_wrow<T, BT>(W, ldw, k, kw, ctl);
     build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status,
@@ -402,8 +415,11 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
       if (k < nc - 1) {
         symm_swap<T, BT>(F, ld, n, vars, fsperm, k, nc - 1);
         swap_wrows<T, BT>(W, ldw, kw, k, nc - 1);
-        if (cache) swap_wrows<T, BT>(cache, cld, kw, k - kstart, nc - 1 - kstart);
         __syncthreads();
+        if (cache) {
+          refresh_cache_rows<T, BT>(F, ld, cache, cld, kstart, kw, k, nc - 1);
+          __syncthreads();
+        }
       }
       nc -= 1;
       continue;
@@ -412,8 +428,11 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
     if (kpiv != ksrc) {
       symm_swap<T, BT>(F, ld, n, vars, fsperm, ksrc, kpiv);
       swap_wrows<T, BT>(W, ldw, kw + step, ksrc, kpiv);
-      if (cache) swap_wrows<T, BT>(cache, cld, kw, ksrc - kstart, kpiv - kstart);
       __syncthreads();
+      if (cache) {
+        refresh_cache_rows<T, BT>(F, ld, cache, cld, kstart, kw, ksrc, kpiv);
+        __syncthreads();
+      }
     }
     if (step == 1) {
       const T d = W[k + (size_t)kw * ldw];
@@ -424,7 +443,7 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
         T w = W[r + (size_t)kw * ldw];
         const T l = (r == k) ? w : w * dinv;
         F[r + (size_t)k * ld] = l;
-        if (cache) cache[(r - kstart) + (size_t)kw * cld] = l;
+        if (r - kstart < cld) cache[(r - kstart) + (size_t)kw * cld] = l;
       }
     } else {
       const T d11 = W[k + (size_t)kw * ldw];
@@ -439,7 +458,7 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
         const T l0 = w0 * i00 + w1 * i10, l1 = w0 * i01 + w1 * i11;
         F[r + (size_t)k * ld] = l0;
         F[r + (size_t)(k + 1) * ld] = l1;
-        if (cache) {
+        if (r - kstart < cld) {
           cache[(r - kstart) + (size_t)kw * cld] = l0;
           cache[(r - kstart) + (size_t)(kw + 1) * cld] = l1;
         }
@@ -791,12 +810,11 @@ k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
   int* fvars = d.ipool + d.ioff[node];
   const int kstart = k;
   int kw = 0;
-  // the panel's L columns in shared memory when the remaining rows fit
-  T* cache = (long long)(f - k) * NB * (long long)sizeof(T) <= cache_bytes
-                 ? reinterpret_cast<T*>(cache_raw)
-                 : nullptr;
+  // the panel's L columns in shared memory for as many rows as fit
+  const int cache_rows = cache_bytes / (NB * (int)sizeof(T));
+  T* cache = cache_rows > 0 ? reinterpret_cast<T*>(cache_raw) : nullptr;
   panel_factor<T, kPanelThreads>(F, f, W, f, f, fs == f, fvars, fvars + f, ustab, pivot_tol,
-               d.status, ctl, k, nc, kw, cache);
+               d.status, ctl, k, nc, kw, cache, cache_rows);
   if (threadIdx.x == 0) {
     st[0] = k;
     st[1] = nc;
@@ -956,7 +974,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       int gu = (int)std::min<long long>(4 * 148, ntl * (ntl + 1) / 2);
       // shared-memory copy of the panel's L columns: as many rows as fit
       const int panel_cache = (int)std::min<long long>(
-          kPanelCacheBytes, (long long)fm * NB * (long long)sizeof(T));
+          h.panel_cache_bytes, (long long)fm * NB * (long long)sizeof(T));
       // FP32 fronts of at least one 128-row tile: tensor-core update
       const bool use_tc = sizeof(T) == 4 && h.tensor_cores && fm >= tc::TM;
       const long long ntc = (fm + tc::TM - 1) / tc::TM;

@@ -121,6 +121,9 @@ struct LdlHandle {
   // FP32 fronts for mixed precision) and of the last one
   int precision = 64, factor_precision = 64;
   bool tensor_cores = true;   // FP32 fronts: Schur updates on tcgen05
+  // large-front panel: bytes of shared memory for a copy of the panel's L
+  // columns (0: read them from HBM; measured faster on the 2D KKT)
+  int panel_cache_bytes = 0;
   int* sv_nodes = nullptr;        // device, nn entries
   int* sv_state = nullptr;        // device, 2 ints per wide front of a level
   std::vector<int> sv_narrow_ptr, sv_wide_ptr, sv_narrow_smem;

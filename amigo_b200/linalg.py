@@ -98,19 +98,28 @@ class CSRMat:
     authoritative copy; ``get_data()`` returns the host mirror.
     """
 
-    def __init__(self, nrows, ncols, rowp, cols, vals=None, device=None):
+    def __init__(self, nrows, ncols, rowp, cols, vals=None, device=None,
+                 diag_pos=None):
+        """diag_pos: the position of each row's diagonal entry when the
+        caller already knows it (otherwise found from the pattern)."""
         self.device = _device(device)
         self.nrows = int(nrows)
         self.ncols = int(ncols)
         self.rowp = np.ascontiguousarray(rowp, dtype=np.int32)
         self.cols = np.ascontiguousarray(cols, dtype=np.int32)
         self.nnz = int(self.rowp[-1])
-        self.host_data = np.zeros(self.nnz)
+        self._host = None          # host mirror, made on first use
         if vals is not None:
             self.host_data[:] = np.asarray(vals, dtype=np.float64)
-        self.vals = torch.from_numpy(self.host_data.copy()).to(self.device)
+            self.vals = torch.from_numpy(self.host_data.copy()).to(self.device)
+        else:
+            self.vals = torch.zeros(self.nnz, dtype=torch.float64, device=self.device)
         self.d_rowp = torch.from_numpy(self.rowp).to(self.device)
         self.d_cols = torch.from_numpy(self.cols).to(self.device)
+        if diag_pos is not None:
+            self.diag = np.ascontiguousarray(diag_pos, dtype=np.int32)
+            self.d_diag = torch.from_numpy(np.maximum(self.diag, 0)).to(self.device)
+            return
         # first position of column i in row i, -1 when absent
         diag = np.full(self.nrows, -1, dtype=np.int64)
         rows = np.repeat(np.arange(self.nrows), np.diff(self.rowp))
@@ -123,6 +132,12 @@ class CSRMat:
         self.diag = diag.astype(np.int32)
         diag = self.diag
         self.d_diag = torch.from_numpy(np.maximum(diag, 0)).to(self.device)
+
+    @property
+    def host_data(self):
+        if self._host is None:
+            self._host = np.zeros(self.nnz)
+        return self._host
 
     def get_nonzero_structure(self):
         return self.nrows, self.ncols, self.nnz, self.rowp, self.cols
@@ -230,6 +245,12 @@ class SparseLDL:
         """FP32 fronts: Schur updates of the large fronts on the tensor
         cores (3xTF32, default) or on the CUDA cores."""
         _lib.call("ab_ldl_set_tensor_cores", self._h, int(bool(on)))
+
+    def set_panel_cache(self, nbytes):
+        """Shared memory of the large-front panel kernel for a copy of the
+        panel's L columns (0 .. 204800 bytes; default 0 reads them from
+        HBM)."""
+        _lib.call("ab_ldl_set_panel_cache", self._h, int(nbytes))
 
     def set_wide_threshold(self, entries):
         """Fronts with f * npiv >= entries are solved by the multi-CTA

@@ -127,22 +127,37 @@ class CartPoleBatch:
         self.lower = cat(lambda m: m.lower)
         self.upper = cat(lambda m: m.upper)
         self.x0 = cat(lambda m: m.x0)
-        self.iv = np.concatenate([m.iv + o for m, o in zip(self.inst, self.var_off)]).astype(np.int32)
-        self.ipos = np.concatenate([m.ipos + o for m, o in zip(self.inst, self.nnz_off)]).astype(np.int32)
-        self.bv = np.concatenate([m.bv + o for m, o in zip(self.inst, self.var_off)]).astype(np.int32)
-        self.bpos = np.concatenate([m.bpos + o for m, o in zip(self.inst, self.nnz_off)]).astype(np.int32)
+        voff = self.var_off.astype(np.int32)
+        zoff = self.nnz_off.astype(np.int32)
+
+        def shifted(name, offs, rows_of=None):
+            # concatenation of each instance's int32 index array + its offset
+            parts = [getattr(m, name) for m in self.inst]
+            shape = (sum(a.shape[0] for a in parts),) + parts[0].shape[1:]
+            out = np.empty(shape, np.int32)
+            r = 0
+            for a, o in zip(parts, offs):
+                np.add(a, o, out=out[r:r + a.shape[0]], casting="unsafe")
+                r += a.shape[0]
+            return out
+
+        self.iv = shifted("iv", voff)
+        self.ipos = shifted("ipos", zoff)
+        self.bv = shifted("bv", voff)
+        self.bpos = shifted("bpos", zoff)
         self.h_iv = cat(lambda m: np.full(m.N, m.h))
         self.m_iv = cat(lambda m: np.full(m.N, m.m_pole))
         self.inst_iv = np.concatenate([[0], np.cumsum([m.N for m in self.inst])]).astype(np.int32)
-        self.vinst = np.repeat(np.arange(self.k), ns).astype(np.int32)
-        self.diag_pos = np.concatenate([m.diag_pos + o for m, o in zip(self.inst, self.nnz_off)])
+        self.vinst = np.repeat(np.arange(self.k, dtype=np.int32), ns)
+        self.diag_pos = shifted("diag_pos", zoff)
         self.N = int(self.inst_iv[-1])
         self.npr = int((~self.mult).sum())
         # block-diagonal CSR of the whole batch
-        self.rowp = np.concatenate([[0]] + [m.rowp[1:] + o for m, o in
-                                            zip(self.inst, self.nnz_off)]).astype(np.int32)
-        self.cols = np.concatenate([m.cols + o for m, o in
-                                    zip(self.inst, self.var_off)]).astype(np.int32)
+        self.rowp = np.empty(self.n + 1, np.int32)
+        self.rowp[0] = 0
+        for m, a, o in zip(self.inst, self.var_off, zoff):
+            np.add(m.rowp[1:], o, out=self.rowp[a + 1:a + 1 + m.n], casting="unsafe")
+        self.cols = shifted("cols", voff)
 
     def patterns(self):
         return [(m.n, m.rowp, m.cols) for m in self.inst]

@@ -71,7 +71,7 @@ def workspace_bytes(model, delay_growth=2.0):
 
 class Server:
     def __init__(self, device="cuda", mem_budget=150e9, max_batch=512,
-                 admit_min=32, max_wait_s=0.25, options=None, precision="fp64"):
+                 admit_min=64, max_wait_s=0.5, options=None, precision="fp64"):
         self.device = torch.device(device)
         self.mem_budget = mem_budget
         self.max_batch = max_batch
@@ -144,5 +144,6 @@ class Server:
                        p95_ms=1e3 * float(np.percentile(lat, 95)),
                        p99_ms=1e3 * float(np.percentile(lat, 99)),
                        iterations=steps, rebuilds=eng.rebuilds,
+                       rebuild_s=eng.rebuild_s,
                        fp64_fallbacks=eng.fallbacks)
         return results, summary

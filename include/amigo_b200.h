@@ -107,6 +107,13 @@ int ab_ldl_set_precision(ab_ldl_t h, int bits);
  * CUDA cores.  No reference counterpart. */
 int ab_ldl_set_tensor_cores(ab_ldl_t h, int on);
 
+/* Large-front panel knob: bytes of shared memory (0 .. 204800, default 0)
+ * for a copy of the panel's L columns that the pivot-column builds read;
+ * 0 reads them from the front in HBM (on the 2D SIMP KKT the copy measured
+ * 7% slower: the shared-memory carve-out takes L1 from the other reads).
+ * No reference counterpart. */
+int ab_ldl_set_panel_cache(ab_ldl_t h, int bytes);
+
 /* Solve schedule knob: fronts with f * npiv >= entries (default 2^18) are
  * solved by the cooperative multi-CTA kernels, smaller ones one CTA per
  * front.  Both give the same result to rounding.  No reference
