@@ -249,7 +249,7 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
 // since the last barrier are read with ld.global.cg (L2), never through
 // the non-coherent L1.  Sums run in a fixed order: the result does not
 // depend on the grid size.
-constexpr int WB = 64;
+constexpr int WB = 128;
 
 __device__ __forceinline__ int block_end_w(const int* kind, int jb, int npiv) {
   int je = jb + WB < npiv ? jb + WB : npiv;
@@ -624,6 +624,12 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
     SCUDA(cudaFuncSetAttribute(k_solve_backward<T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kMaxDynSmem));
+    SCUDA(cudaFuncSetAttribute(k_wide_forward<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)wide_smem));
+    SCUDA(cudaFuncSetAttribute(k_wide_backward<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)wide_smem));
     int dev = 0, sms = 0, bf = 0, bb = 0;
     SCUDA(cudaGetDevice(&dev));
     SCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

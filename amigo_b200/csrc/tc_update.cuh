@@ -14,9 +14,10 @@
 //      layout the MMA descriptors describe;
 //   2. one thread issues 3 x 4 tcgen05.mma (K = 8 each) and commits them to
 //      an mbarrier;
-//   3. after the (bounded) wait, each warp reads its 32 TMEM lanes with
-//      tcgen05.ld and subtracts the tile from C in global memory, lower
-//      triangle only.
+//   3. while the MMAs run, every thread loads the first 32 entries of its
+//      row of the C tile; after the (bounded) wait each warp reads its 32
+//      TMEM lanes with tcgen05.ld chunk by chunk (the next chunk of C
+//      already loading) and writes C - A B^T, lower triangle only.
 // Descriptor encodings follow the sm_100 shared-memory and instruction
 // descriptor formats (PTX ISA, tcgen05 "Matrix Descriptors" / "Instruction
 // Descriptor"; the same fields as CUTLASS's UMMA::SmemDescriptor and
@@ -193,18 +194,23 @@ __device__ __forceinline__ bool tc_tile(TcCta& c, float* C, long long ldc,
   char* Bhi = c.tiles + 2 * kTileBytes;
   char* Blo = c.tiles + 3 * kTileBytes;
   {
+    // all 64 loads first (in flight together), then split and store
     const int ra = r0 + t, rb = c0 + t;
-#pragma unroll 4
+    float av[TK], bv[TK];
+#pragma unroll
     for (int j = 0; j < TK; j++) {
-      const float a = (ra < n && j < kw) ? A[ra + (long long)j * lda] : 0.f;
-      const float b = (rb < n && j < kw) ? B[rb + (long long)j * ldb] : 0.f;
-      const float ah = __uint_as_float(__float_as_uint(a) & 0xffffe000u);
-      const float bh = __uint_as_float(__float_as_uint(b) & 0xffffe000u);
+      av[j] = (ra < n && j < kw) ? A[ra + (long long)j * lda] : 0.f;
+      bv[j] = (rb < n && j < kw) ? B[rb + (long long)j * ldb] : 0.f;
+    }
+#pragma unroll
+    for (int j = 0; j < TK; j++) {
+      const float ah = __uint_as_float(__float_as_uint(av[j]) & 0xffffe000u);
+      const float bh = __uint_as_float(__float_as_uint(bv[j]) & 0xffffe000u);
       const uint32_t o = sw128(t, j);
       *reinterpret_cast<float*>(Ahi + o) = ah;
-      *reinterpret_cast<float*>(Alo + o) = a - ah;
+      *reinterpret_cast<float*>(Alo + o) = av[j] - ah;
       *reinterpret_cast<float*>(Bhi + o) = bh;
-      *reinterpret_cast<float*>(Blo + o) = b - bh;
+      *reinterpret_cast<float*>(Blo + o) = bv[j] - bh;
     }
   }
   // make the generic-proxy stores visible to the tensor core's async proxy
@@ -224,6 +230,19 @@ __device__ __forceinline__ bool tc_tile(TcCta& c, float* C, long long ldc,
                  (p | kk) ? 1u : 0u);
     mma_commit(c.mbar);
   }
+  // this thread's row of the C tile: chunk 0 is loaded while the MMAs run,
+  // each later chunk while the previous one is updated
+  const int warp = t >> 5, lane = t & 31;
+  const int r = r0 + warp * 32 + lane;
+  float cv[32];
+  auto load_chunk = [&](int cc, float* dst) {
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      const int col = c0 + cc * 32 + j;
+      dst[j] = (r < n && col < n && r >= col) ? C[r + (long long)col * ldc] : 0.f;
+    }
+  };
+  load_chunk(0, cv);
   bool done = false;
   for (long long it = 0; it < kWaitLimit && !done; it++)
     done = mbar_try_wait(c.mbar, c.phase);
@@ -236,18 +255,20 @@ __device__ __forceinline__ bool tc_tile(TcCta& c, float* C, long long ldc,
     c.ok = false;
     return false;
   }
-  const int warp = t >> 5, lane = t & 31;
-  const int r = r0 + warp * 32 + lane;
 #pragma unroll 1
   for (int cc = 0; cc < TN / 32; cc++) {
+    float nv[32];
+    if (cc + 1 < TN / 32) load_chunk(cc + 1, nv);
     float v[32];
     tmem_ld32(c.tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc * 32), v);
-    if (r < n) {
 #pragma unroll
-      for (int j = 0; j < 32; j++) {
-        const int col = c0 + cc * 32 + j;
-        if (col < n && r >= col) C[r + (long long)col * ldc] -= v[j];
-      }
+    for (int j = 0; j < 32; j++) {
+      const int col = c0 + cc * 32 + j;
+      if (r < n && col < n && r >= col) C[r + (long long)col * ldc] = cv[j] - v[j];
+    }
+    if (cc + 1 < TN / 32) {
+#pragma unroll
+      for (int j = 0; j < 32; j++) cv[j] = nv[j];
     }
   }
   fence_before_sync();
