@@ -35,6 +35,7 @@ namespace {
 
 constexpr int NT = kThreads;
 constexpr int NB = kPanel;
+constexpr int NWARP = NT / 32;
 // Threads of the one-CTA panel kernel of the large-front path: each
 // candidate column is brought up to date by one thread per row, so more
 // threads shorten every candidate step.
@@ -46,11 +47,12 @@ constexpr int kTile = 64;
 
 template <int BT>
 struct CtlT {
-  // per-warp partials of the column reductions, two buffers used in turn
-  // (a warp can only be one reduction ahead of the slowest one)
-  double red_v[2][(BT / 32)];
-  int red_i[2][(BT / 32)];
-  double red_v2[2][(BT / 32)];
+  double wrow[NB];     // row k (or imax) of W, columns 0..kw-1
+  double red_v[(BT / 32)];
+  int red_i[(BT / 32)];
+  double red_v2[(BT / 32)];
+  double abswik, ctail, rowmax;
+  int imax;
   int f, fs, ns, ndin, npiv;
   long long foff, ioff;
   int skip;
@@ -67,14 +69,10 @@ __device__ __forceinline__ void argmax_merge(double& v, int& i, double v2,
   }
 }
 
-// Block-wide first-argmax of (v, i) plus a max of v2, returned to every
-// thread with one barrier: each warp reduces its lanes, lane 0 posts the
-// warp's partial to buffer `buf`, and after the barrier every warp reduces
-// the posted partials itself (the merge is a total order, so every warp
-// obtains the same result).
+// Block-wide first-argmax of (v, i) plus a max of v2.  Result is written to
+// ctl.red_v[0], ctl.red_i[0], ctl.red_v2[0].
 template <int BT>
-__device__ void block_argmax(CtlT<BT>& ctl, int buf, double& v, int& i,
-                             double& v2) {
+__device__ void block_argmax(CtlT<BT>& ctl, double v, int i, double v2) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int o = 16; o > 0; o >>= 1) {
     double ov = __shfl_down_sync(0xffffffffu, v, o);
@@ -84,21 +82,29 @@ __device__ void block_argmax(CtlT<BT>& ctl, int buf, double& v, int& i,
     v2 = fmax(v2, ov2);
   }
   if (lane == 0) {
-    ctl.red_v[buf][warp] = v;
-    ctl.red_i[buf][warp] = i;
-    ctl.red_v2[buf][warp] = v2;
+    ctl.red_v[warp] = v;
+    ctl.red_i[warp] = i;
+    ctl.red_v2[warp] = v2;
   }
   __syncthreads();
-  v = lane < (BT / 32) ? ctl.red_v[buf][lane] : -1.0;
-  i = lane < (BT / 32) ? ctl.red_i[buf][lane] : 0x7fffffff;
-  v2 = lane < (BT / 32) ? ctl.red_v2[buf][lane] : 0.0;
-  for (int o = 16; o > 0; o >>= 1) {
-    double ov = __shfl_xor_sync(0xffffffffu, v, o);
-    int oi = __shfl_xor_sync(0xffffffffu, i, o);
-    double ov2 = __shfl_xor_sync(0xffffffffu, v2, o);
-    argmax_merge(v, i, ov, oi);
-    v2 = fmax(v2, ov2);
+  if (warp == 0) {
+    v = lane < (BT / 32) ? ctl.red_v[lane] : -1.0;
+    i = lane < (BT / 32) ? ctl.red_i[lane] : 0x7fffffff;
+    v2 = lane < (BT / 32) ? ctl.red_v2[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      double ov = __shfl_down_sync(0xffffffffu, v, o);
+      int oi = __shfl_down_sync(0xffffffffu, i, o);
+      double ov2 = __shfl_down_sync(0xffffffffu, v2, o);
+      argmax_merge(v, i, ov, oi);
+      v2 = fmax(v2, ov2);
+    }
+    if (lane == 0) {
+      ctl.red_v[0] = v;
+      ctl.red_i[0] = i;
+      ctl.red_v2[0] = v2;
+    }
   }
+  __syncthreads();
 }
 
 // Symmetric interchange of rows/columns a < b of the lower triangle of F,
@@ -238,61 +244,67 @@ __device__ void trailing_update(T* F, int ld, const T* W, int ldw,
                   tiles + kTile * TP);
 }
 
-// W[r, col] = src(r) - F[r, kstart:kstart+kw] . W[row, 0:kw]  for r in
-// [k, n), and the reductions the pivot tests need, returned to every thread
-// (one barrier):
-//   mode 0: candidate column k (row = k); src(r) = F[r, k]; first-argmax of
-//           |W| over (k, nc) -> imax, abswik, and max over [nc, n) -> tail.
-//   mode 1: column imax_in (row = imax_in); src(r) = F[imax_in, r] for
-//           r < imax_in else F[r, imax_in]; max over [k, n) \ {imax_in}
-//           -> tail (the row maximum).
+// W[r, col] = src(r) - F[r, kstart:kstart+kw] . ctl.wrow  for r in [k, n),
+// and the reductions the pivot tests need.
+//   mode 0: candidate column k; src(r) = F[r, k]; reduces first-argmax of
+//           |W| over (k, nc) -> ctl.imax / ctl.abswik and max over [nc, n)
+//           -> ctl.ctail.
+//   mode 1: column imax; src(r) = F[imax, r] for r < imax else F[r, imax];
+//           reduces max over [k, n) \ {imax} -> ctl.rowmax.
 template <class T, int BT>
 __device__ void build_column(T* F, int ld, T* W, int ldw, int n,
                              int k, int kstart, int kw, int col, int mode,
-                             int imax_in, int nc, CtlT<BT>& ctl, int& buf,
-                             int* status, const T* cache, int cld,
-                             int& imax, double& abswik, double& tail) {
+                             int imax, int nc, CtlT<BT>& ctl, int* status,
+                             const T* cache, int cld) {
   const int tid = threadIdx.x;
   double bestv = -1.0, tailv = 0.0;
   int besti = 0x7fffffff;
-  // row k (mode 0) or imax (mode 1) of W, columns 0..kw-1, read by every
-  // thread (a broadcast through L1)
-  const T* wr = W + (mode == 0 ? k : imax_in);
   for (int r = k + tid; r < n; r += BT) {
     T acc;
     if (mode == 0) {
       acc = F[r + (size_t)k * ld];
     } else {
-      acc = (r < imax_in) ? F[imax_in + (size_t)r * ld] : F[r + (size_t)imax_in * ld];
+      acc = (r < imax) ? F[imax + (size_t)r * ld] : F[r + (size_t)imax * ld];
     }
     // the panel's L columns: from the shared-memory copy for its rows
     const bool inc = cache && (r - kstart) < cld;
     const T* Lr = inc ? cache + (r - kstart) : F + r + (size_t)kstart * ld;
     const size_t ls = inc ? (size_t)cld : (size_t)ld;
-    for (int j = 0; j < kw; j++) acc -= Lr[j * ls] * wr[(size_t)j * ldw];
+    for (int j = 0; j < kw; j++) acc -= Lr[j * ls] * T(ctl.wrow[j]);
     W[r + (size_t)col * ldw] = acc;
     const double a = fabs((double)acc);
     if (mode == 0) {
       if (r > k && r < nc) argmax_merge(bestv, besti, a, r);
       if (r >= nc) tailv = fmax(tailv, a);
     } else {
-      if (r != imax_in) tailv = fmax(tailv, a);
+      if (r != imax) tailv = fmax(tailv, a);
     }
   }
-  block_argmax<BT>(ctl, buf, bestv, besti, tailv);
-  buf ^= 1;
-  tail = tailv;
-  if (mode == 0) {
-    int im = besti;
-    if (im >= nc || im <= k) {
-      // No finite candidate entry (all NaN, or no candidates): keep the
-      // index in range; NaN is reported through the status word.
-      if (k + 1 < nc && tid == 0) atomicOr(status, ST_NAN);
-      im = (k + 1 < n) ? k + 1 : k;
+  block_argmax<BT>(ctl, bestv, besti, tailv);
+  if (tid == 0) {
+    if (mode == 0) {
+      int im = ctl.red_i[0];
+      if (im >= nc || im <= k) {
+        // No finite candidate entry (all NaN, or no candidates): keep the
+        // index in range; NaN is reported through the status word.
+        if (k + 1 < nc) atomicOr(status, ST_NAN);
+        im = (k + 1 < n) ? k + 1 : k;
+      }
+      ctl.imax = im;
+      ctl.abswik = ctl.red_v[0] < 0.0 ? 0.0 : ctl.red_v[0];
+      ctl.ctail = ctl.red_v2[0];
+    } else {
+      ctl.rowmax = ctl.red_v2[0];
     }
-    imax = im;
-    abswik = bestv < 0.0 ? 0.0 : bestv;
   }
+  __syncthreads();
+}
+
+// Load row `row` of W (columns 0..kw-1) into ctl.wrow.
+template <class T, int BT>
+__device__ void load_wrow(const T* W, int ldw, int row, int kw, CtlT<BT>& ctl) {
+  for (int j = threadIdx.x; j < kw; j += BT) ctl.wrow[j] = W[row + (size_t)j * ldw];
+  __syncthreads();
 }
 
 // One panel of the blocked factorization of the fully-summed columns of the
@@ -325,26 +337,26 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
   int k = k_, nc = nc_, kw = 0;
   const int kstart = k;
   const int cld = cache ? (n - kstart < cache_rows ? n - kstart : cache_rows) : 0;
-  int buf = 0;
   while (kw < NB - 1 && k < nc) {
-    int imax;
-    double abswik, ctail, rowmax;
-    build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, buf,
-                        status, cache, cld, imax, abswik, ctail);
+    load_wrow<T, BT>(W, ldw, k, kw, ctl);
+    build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status,
+                        cache, cld);
     const double wkk = W[k + (size_t)kw * ldw];
     const double abswkk = fabs(wkk);
+    const int imax = ctl.imax;
+    const double abswik = ctl.abswik;
     int step = 0, kpiv = -1;
     bool zero_pivot = false;
     if (!root) {
-      const double colmax = fmax(abswik, ctail);
+      const double colmax = fmax(abswik, ctl.ctail);
       if (abswkk >= pivot_tol && abswkk >= ustab * colmax) {
         step = 1;
         kpiv = k;
       } else if (k + 1 < nc) {
-        int im2;
-        double aw2;
-        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl,
-                            buf, status, cache, cld, im2, aw2, rowmax);
+        load_wrow<T, BT>(W, ldw, imax, kw, ctl);
+        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status,
+                            cache, cld);
+        const double rowmax = ctl.rowmax;
         const double wii = W[imax + (size_t)(kw + 1) * ldw];
         const double abswii = fabs(wii);
         if (abswii >= pivot_tol && abswii >= ustab * rowmax) {
@@ -377,10 +389,10 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
         step = 1;
         kpiv = k;
       } else {
-        int im2;
-        double aw2;
-        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl,
-                            buf, status, cache, cld, im2, aw2, rowmax);
+        load_wrow<T, BT>(W, ldw, imax, kw, ctl);
+        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status,
+                            cache, cld);
+        const double rowmax = ctl.rowmax;
         const double abswii = fabs(W[imax + (size_t)(kw + 1) * ldw]);
         if (abswkk >= bk_alpha * colmax * (colmax / rowmax)) {
           step = 1;

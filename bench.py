@@ -523,9 +523,11 @@ def ipm_solve_host_baseline():
 
 
 def roofline(core, fac_ms):
-    """Dominant kernel: the per-level front factorization.  Algorithmic
-    bytes of one factorization: 8 (c(c+1)/2 child-contribution read +
-    f p factor write + c(c+1)/2 contribution write) per front + 12 nnz(A)."""
+    """The factorization as one unit (its kernels: per-level small fronts,
+    large-front set-up, extend-add, panel and trailing update; the panel
+    kernel is the largest share).  Algorithmic bytes of one factorization:
+    8 (c(c+1)/2 child-contribution read + f p factor write + c(c+1)/2
+    contribution write) per front + 12 nnz(A), over its CUDA-event time."""
     ldl = core.ldl
     h = ldl._h
     npiv, ndel = ldl.node_pivots()
@@ -550,7 +552,8 @@ def roofline(core, fac_ms):
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = bytes_ / (fac_ms * 1e-3) / 1e9
     del h
-    return {"kernel": "k_factor_level (all levels of one factorization)",
+    return {"kernel": "multifrontal factorization (k_factor_level, k_big_panel, "
+                      "k_big_update, k_big_extend, ...; one factorization)",
             "bound": "hbm", "achieved": round(achieved, 2),
             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5),
             "traffic": None,
