@@ -35,7 +35,6 @@ namespace {
 
 constexpr int NT = kThreads;
 constexpr int NB = kPanel;
-constexpr int NWARP = NT / 32;
 // Threads of the one-CTA panel kernel of the large-front path: each
 // candidate column is brought up to date by one thread per row, so more
 // threads shorten every candidate step.
@@ -44,6 +43,11 @@ constexpr int kPanelThreads = 1024;
 // panel's L columns (the static control block aside).
 constexpr int kPanelCacheBytes = 200 * 1024;
 constexpr int kTile = 64;
+// Right-looking small-front kernel: rows of room for delayed pivots, and
+// its block size (measured on 68-row fronts: 32 threads 11.9 ms, 64 9.7,
+// 128 8.5, 256 8.25 for one factorization of 512 cart-pole problems).
+constexpr int kRlSlack = 8;
+constexpr int kRlThreads = 256;
 
 template <int BT>
 struct CtlT {
@@ -213,35 +217,86 @@ __device__ __forceinline__ void tile_coords(int t, int& ti, int& tj) {
   tj = t - i * (i + 1) / 2;
 }
 
-// Trailing update of the whole block by one CTA.  `tiles` (kTileSmem
-// doubles of shared memory) selects the tiled form used for fronts kept in
-// HBM; without it the entries are updated directly (fronts in shared
-// memory).
-template <class T>
-__device__ void trailing_update(T* F, int ld, const T* W, int ldw,
-                                int n, int k, int kstart, int kw,
-                                T* tiles) {
-  const int m = n - k;
-  if (m <= 0 || kw <= 0) return;
-  const int tid = threadIdx.x;
-  if (tiles == nullptr) {
-    for (int c = 0; c < m; c++) {
-      T* Fc = F + (size_t)(k + c) * ld + k;
-      for (int r = c + tid; r < m; r += NT) {
-        T acc = Fc[r];
-        for (int j = 0; j < kw; j++)
-          acc -= F[k + r + (size_t)(kstart + j) * ld] * W[k + c + (size_t)j * ldw];
-        Fc[r] = acc;
+// Column imax as the pivot search sees it: the largest |entry| off its
+// diagonal over rows [k, n), its diagonal and its entry in row k.
+struct ImaxColumn {
+  double rowmax, wii, wik;
+};
+
+struct PivotChoice {
+  int step;       // 0: delay candidate k; 1 or 2: size of the pivot block
+  int kpiv;       // k or imax
+  bool zero;      // Bunch-Kaufman zero column: D = 0, L column 0
+  bool imax_1x1;  // 1x1 pivot on column imax
+};
+
+// The pivot rule for candidate k of a front (reference: the 1x1 / 2x2
+// threshold tests of the front factorization, include/sparse_ldl.h, and
+// LAPACK dsytf2 Bunch-Kaufman for the root front): `wkk` is the candidate's
+// current diagonal, `abswik` = |entry| at imax (largest over the other
+// candidates), `ctail` = largest |entry| over the non-candidate rows.
+// `imax_column()` evaluates column imax; it is called only when the 1x1
+// test on k fails, and by every thread of the block together.
+template <class ImaxFn>
+__device__ __forceinline__ PivotChoice choose_pivot(bool root, int k, int nc,
+                                                    double wkk, int imax,
+                                                    double abswik, double ctail,
+                                                    double ustab, double pivot_tol,
+                                                    ImaxFn imax_column) {
+  const double bk_alpha = (1.0 + sqrt(17.0)) / 8.0;
+  const double abswkk = fabs(wkk);
+  PivotChoice p{0, -1, false, false};
+  if (!root) {
+    const double colmax = fmax(abswik, ctail);
+    if (abswkk >= pivot_tol && abswkk >= ustab * colmax) {
+      p.step = 1;
+      p.kpiv = k;
+    } else if (k + 1 < nc) {
+      const ImaxColumn c = imax_column();
+      const double abswii = fabs(c.wii);
+      if (abswii >= pivot_tol && abswii >= ustab * c.rowmax) {
+        p.step = 1;
+        p.kpiv = imax;
+        p.imax_1x1 = true;
+      } else {
+        const double det = fabs(wkk * c.wii - c.wik * c.wik);
+        if (det >= pivot_tol) {
+          const double delta = det / fmax(abswii + abswik, abswkk + abswik);
+          if (delta >= ustab * colmax && delta >= ustab * c.rowmax) {
+            p.step = 2;
+            p.kpiv = imax;
+          }
+        }
       }
     }
-    __syncthreads();
-    return;
+  } else {
+    // Bunch-Kaufman (LAPACK dsytf2/dlasyf, lower): every column is
+    // eliminated, by a 1x1 or a 2x2 pivot.
+    const double colmax = abswik;  // nc == n: all rows are candidates
+    if (!(fmax(abswkk, colmax) > 0.0)) {
+      p.step = 1;
+      p.kpiv = k;
+      p.zero = true;
+    } else if (abswkk >= bk_alpha * colmax) {
+      p.step = 1;
+      p.kpiv = k;
+    } else {
+      const ImaxColumn c = imax_column();
+      const double abswii = fabs(c.wii);
+      if (abswkk >= bk_alpha * colmax * (colmax / c.rowmax)) {
+        p.step = 1;
+        p.kpiv = k;
+      } else if (abswii >= bk_alpha * c.rowmax) {
+        p.step = 1;
+        p.kpiv = imax;
+        p.imax_1x1 = true;
+      } else {
+        p.step = 2;
+        p.kpiv = imax;
+      }
+    }
   }
-  const int nt = (m + kTile - 1) / kTile;
-  for (int tj = 0; tj < nt; tj++)
-    for (int ti = tj; ti < nt; ti++)
-      update_tile(F, ld, W, ldw, n, k, kstart, kw, ti, tj, tiles,
-                  tiles + kTile * TP);
+  return p;
 }
 
 // W[r, col] = src(r) - F[r, kstart:kstart+kw] . ctl.wrow  for r in [k, n),
@@ -333,7 +388,6 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
                              int& nc_, int& kw_, T* cache = nullptr,
                              int cache_rows = 0) {
   const int tid = threadIdx.x;
-  const double bk_alpha = (1.0 + sqrt(17.0)) / 8.0;
   int k = k_, nc = nc_, kw = 0;
   const int kstart = k;
   const int cld = cache ? (n - kstart < cache_rows ? n - kstart : cache_rows) : 0;
@@ -342,73 +396,28 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
     build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status,
                         cache, cld);
     const double wkk = W[k + (size_t)kw * ldw];
-    const double abswkk = fabs(wkk);
     const int imax = ctl.imax;
-    const double abswik = ctl.abswik;
-    int step = 0, kpiv = -1;
-    bool zero_pivot = false;
-    if (!root) {
-      const double colmax = fmax(abswik, ctl.ctail);
-      if (abswkk >= pivot_tol && abswkk >= ustab * colmax) {
-        step = 1;
-        kpiv = k;
-      } else if (k + 1 < nc) {
-        load_wrow<T, BT>(W, ldw, imax, kw, ctl);
-        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status,
-                            cache, cld);
-        const double rowmax = ctl.rowmax;
-        const double wii = W[imax + (size_t)(kw + 1) * ldw];
-        const double abswii = fabs(wii);
-        if (abswii >= pivot_tol && abswii >= ustab * rowmax) {
-          for (int r = k + tid; r < n; r += BT)
-            W[r + (size_t)kw * ldw] = W[r + (size_t)(kw + 1) * ldw];
-          __syncthreads();
-          step = 1;
-          kpiv = imax;
-        } else {
+    const PivotChoice pc = choose_pivot(
+        root, k, nc, wkk, imax, ctl.abswik, ctl.ctail, ustab, pivot_tol, [&]() {
           const double wik = W[imax + (size_t)kw * ldw];
-          const double det = fabs(wkk * wii - wik * wik);
-          if (det >= pivot_tol) {
-            const double delta = det / fmax(abswii + abswik, abswkk + abswik);
-            if (delta >= ustab * colmax && delta >= ustab * rowmax) {
-              step = 2;
-              kpiv = imax;
-            }
-          }
-        }
-      }
-    } else {
-      // Bunch-Kaufman (LAPACK dsytf2/dlasyf, lower): every column is
-      // eliminated, by a 1x1 or a 2x2 pivot.
-      const double colmax = abswik;  // nc == n: all rows are candidates
-      if (!(fmax(abswkk, colmax) > 0.0)) {
-        step = 1;
-        kpiv = k;
-        zero_pivot = true;
-      } else if (abswkk >= bk_alpha * colmax) {
-        step = 1;
-        kpiv = k;
-      } else {
-        load_wrow<T, BT>(W, ldw, imax, kw, ctl);
-        build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax, nc, ctl, status,
-                            cache, cld);
-        const double rowmax = ctl.rowmax;
-        const double abswii = fabs(W[imax + (size_t)(kw + 1) * ldw]);
-        if (abswkk >= bk_alpha * colmax * (colmax / rowmax)) {
-          step = 1;
-          kpiv = k;
-        } else if (abswii >= bk_alpha * rowmax) {
-          for (int r = k + tid; r < n; r += BT)
-            W[r + (size_t)kw * ldw] = W[r + (size_t)(kw + 1) * ldw];
+          load_wrow<T, BT>(W, ldw, imax, kw, ctl);
+          build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax,
+                              nc, ctl, status, cache, cld);
+          const ImaxColumn c{ctl.rowmax, (double)W[imax + (size_t)(kw + 1) * ldw],
+                             wik};
+          // every thread holds its decision inputs before the interchange
+          // or the column copy that follow rewrite them
           __syncthreads();
-          step = 1;
-          kpiv = imax;
-        } else {
-          step = 2;
-          kpiv = imax;
-        }
-      }
+          return c;
+        });
+    if (pc.imax_1x1) {
+      // column imax is the pivot column: its W column replaces column k's
+      for (int r = k + tid; r < n; r += BT)
+        W[r + (size_t)kw * ldw] = W[r + (size_t)(kw + 1) * ldw];
+      __syncthreads();
     }
+    const int step = pc.step, kpiv = pc.kpiv;
+    const bool zero_pivot = pc.zero;
 
     if (step == 0) {
       // Delay candidate k: move it to the end of the candidate set.
@@ -484,31 +493,273 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
   kw_ = kw;
 }
 
-// Factor the fully-summed columns [0, fs) of the n x n front F in one CTA.
-// Returns the number of pivots (== fs for a root front).
-template <class T>
-__device__ int factor_front(T* F, int ld, T* W, int ldw, int n,
-                            int fs, bool root, int* vars, int* fsperm,
-                            double ustab, double pivot_tol, T* tiles,
-                            int* status, Ctl& ctl) {
-  int nc = fs;
-  int k = 0;
-  while (k < nc) {
-    const int kstart = k;
-    int kw = 0;
-    panel_factor<T, NT>(F, ld, W, ldw, n, root, vars, fsperm, ustab, pivot_tol,
-                     status, ctl, k, nc, kw);
-    trailing_update(F, ld, W, ldw, n, k, kstart, kw, tiles);
-    __syncthreads();
+// ---------------------------------------------------------------------------
+// Unblocked right-looking factorization for fronts held in shared memory.
+// Every pivot's rank-1 (2x2: rank-2) update is applied to the trailing
+// lower triangle at once, so each candidate column is current when it is
+// examined: a pivot step is one column scan with a block reduction, the
+// pivot rule, an optional interchange and the update -- two barriers for
+// the common 1x1 case and no W panel.  Entries are updated as
+// F[r, c] -= L[r, j] * W[c, j] in pivot order, the operands and order of
+// the blocked factorization's updates.
+
+// Reduction slots: two sets, so the column-imax reduction can follow the
+// column-k one without a barrier between them; and the next candidate
+// column's scan, made during the update, by step parity.
+template <int BT>
+struct RedSlots {
+  double v[2][BT / 32];
+  int i[2][BT / 32];
+  double v2[2][BT / 32];
+  double nv[2], nt[2];
+  int ni[2];
+};
+
+// Block-wide first-argmax of (v, i) and max of v2, result in every thread.
+// Per-thread inputs are never NaN (they start at -1 / 0 and only take
+// larger values), so the merge is commutative and all threads agree.
+template <int BT>
+__device__ __forceinline__ void block_argmax_all(RedSlots<BT>& rs, int set,
+                                                 double& v, int& i, double& v2) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    const double ov2 = __shfl_xor_sync(0xffffffffu, v2, o);
+    argmax_merge(v, i, ov, oi);
+    v2 = fmax(v2, ov2);
   }
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    rs.v[set][warp] = v;
+    rs.i[set][warp] = i;
+    rs.v2[set][warp] = v2;
+  }
+  __syncthreads();
+  v = rs.v[set][0];
+  i = rs.i[set][0];
+  v2 = rs.v2[set][0];
+  for (int w = 1; w < BT / 32; w++) {
+    argmax_merge(v, i, rs.v[set][w], rs.i[set][w]);
+    v2 = fmax(v2, rs.v2[set][w]);
+  }
+}
+
+// L column(s) of the pivot at k: rows (k + step, n) of column k (and k+1)
+// scaled by D^-1 from the unscaled L*D values left there by the update.
+template <class T, int BT>
+__device__ __forceinline__ void rl_scale(T* F, int ld, int n, int k, int step,
+                                         T dinv, T i00, T i10, T i01, T i11) {
+  if (step == 1) {
+    T* Fk = F + (size_t)k * ld;
+    for (int r = k + 1 + threadIdx.x; r < n; r += BT) Fk[r] = Fk[r] * dinv;
+  } else {
+    T* F0 = F + (size_t)k * ld;
+    T* F1 = F0 + ld;
+    for (int r = k + 2 + threadIdx.x; r < n; r += BT) {
+      const T w0 = F0[r], w1 = F1[r];
+      F0[r] = w0 * i00 + w1 * i10;
+      F1[r] = w0 * i01 + w1 * i11;
+    }
+  }
+}
+
+// Rank-1 (STEP 1) or rank-2 (STEP 2) update of the trailing triangle
+// F[c0:, c0:] by the pivot at k: F[r, c] -= L[r, j] * W[c, j], j = k (and
+// k+1), with L = W D^-1 (coefficients d00..d11).  Threads form a 16 x TC
+// grid: thread (tr, tc) takes columns c0 + tc + TC j and, in each, the rows
+// on or below the diagonal that are congruent to c0 + tr modulo 16.  Lanes
+// 0..15 of warp 0 (tc == 0) hold column c0 and leave its scan for the next
+// pivot search (first-argmax over the candidates c0 < r < nc, max over
+// r >= nc) in slot `par`.  Returns whether they did (c0 < n).
+constexpr int kRlRows = 16;
+
+template <class T, int BT, int STEP>
+__device__ __forceinline__ bool rl_update(T* F, int ld, int n, int k, int c0,
+                                          int nc, T d00, T d10, T d01, T d11,
+                                          int par, RedSlots<BT>& rs) {
+  constexpr int TR = kRlRows, TC = BT / TR;
+  const int tr = threadIdx.x % TR, tc = threadIdx.x / TR;
+  const T* W0 = F + (size_t)k * ld;
+  const T* W1 = W0 + ld;
+  if (c0 >= n) return false;
+  int c = c0 + tc;
+  if (tc == 0) {
+    double bv = -1.0, tv = 0.0;
+    int bi = 0x7fffffff;
+    const T y0 = W0[c0];
+    const T y1 = STEP == 2 ? W1[c0] : T(0);
+    T* Fc = F + (size_t)c0 * ld;
+    for (int r = c0 + tr; r < n; r += TR) {
+      T acc = Fc[r];
+      if (STEP == 1) {
+        acc -= (W0[r] * d00) * y0;
+      } else {
+        const T w0 = W0[r], w1 = W1[r];
+        const T l0 = w0 * d00 + w1 * d10, l1 = w0 * d01 + w1 * d11;
+        acc -= l0 * y0;
+        acc -= l1 * y1;
+      }
+      Fc[r] = acc;
+      const double av = fabs((double)acc);
+      if (r > c0 && r < nc) argmax_merge(bv, bi, av, r);
+      else if (r >= nc) tv = fmax(tv, av);
+    }
+    for (int o = TR / 2; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0x0000ffffu, bv, o);
+      const int oi = __shfl_xor_sync(0x0000ffffu, bi, o);
+      const double ot = __shfl_xor_sync(0x0000ffffu, tv, o);
+      argmax_merge(bv, bi, ov, oi);
+      tv = fmax(tv, ot);
+    }
+    if (tr == 0) {
+      rs.nv[par] = bv;
+      rs.ni[par] = bi;
+      rs.nt[par] = tv;
+    }
+    c += TC;
+  }
+  for (; c < n; c += TC) {
+    const T y0 = W0[c];
+    const T y1 = STEP == 2 ? W1[c] : T(0);
+    T* Fc = F + (size_t)c * ld;
+    int r = c0 + tr;
+    if (r < c) r += ((c - r + TR - 1) / TR) * TR;
+    for (; r < n; r += TR) {
+      T acc = Fc[r];
+      if (STEP == 1) {
+        acc -= (W0[r] * d00) * y0;
+      } else {
+        const T w0 = W0[r], w1 = W1[r];
+        const T l0 = w0 * d00 + w1 * d10, l1 = w0 * d01 + w1 * d11;
+        acc -= l0 * y0;
+        acc -= l1 * y1;
+      }
+      Fc[r] = acc;
+    }
+  }
+  return true;
+}
+
+// Factor the fully-summed columns [0, fs) of the n x n front F (lower
+// triangle, leading dimension ld) in one CTA; `vars` holds 4 sections of ld
+// ints (variables, fully-summed permutation, -, pivot kinds).  Same pivot
+// rule, interchanges and output layout as the blocked panel factorization
+// of the large fronts.  Returns the number of pivots.
+template <class T, int BT>
+__device__ int factor_front_rl(T* F, int ld, int n, int fs, bool root,
+                               int* vars, int* fsperm, double ustab,
+                               double pivot_tol, int* status, RedSlots<BT>& rs) {
+  const int tid = threadIdx.x;
+  int k = 0, nc = fs;
+  int par = 0;          // parity of the scan slot the next step reads
+  bool have = false;    // the update left the scan of column k in slot par
+  // the last pivot, whose L column(s) are scaled at the next step
+  int pk = -1, pstep = 0;
+  T pd = T(0), p00 = T(0), p10 = T(0), p01 = T(0), p11 = T(0);
+  while (k < nc) {
+    if (pk >= 0) {
+      rl_scale<T, BT>(F, ld, n, pk, pstep, pd, p00, p10, p01, p11);
+      pk = -1;
+    }
+    const T* Fk = F + (size_t)k * ld;
+    double bv, tv;
+    int bi;
+    if (have) {
+      bv = rs.nv[par];
+      bi = rs.ni[par];
+      tv = rs.nt[par];
+    } else {
+      // candidate column k: first-argmax of |F[r, k]| over candidates
+      // r > k, max over the non-candidate rows
+      bv = -1.0;
+      tv = 0.0;
+      bi = 0x7fffffff;
+      for (int r = k + 1 + tid; r < n; r += BT) {
+        const double a = fabs((double)Fk[r]);
+        if (r < nc) argmax_merge(bv, bi, a, r);
+        else tv = fmax(tv, a);
+      }
+      block_argmax_all<BT>(rs, 0, bv, bi, tv);
+    }
+    int imax = bi;
+    if (imax >= nc || imax <= k) {
+      // no finite candidate entry (all NaN, or no candidates)
+      if (k + 1 < nc && tid == 0) atomicOr(status, ST_NAN);
+      imax = (k + 1 < n) ? k + 1 : k;
+    }
+    const PivotChoice pc = choose_pivot(
+        root, k, nc, (double)Fk[k], imax, bv < 0.0 ? 0.0 : bv, tv, ustab,
+        pivot_tol, [&]() {
+          // read before the reduction's barrier: past it, other threads may
+          // interchange or update these entries
+          const double wii = F[imax + (size_t)imax * ld], wik = F[imax + (size_t)k * ld];
+          double rv = -1.0, rt = 0.0;
+          int ri = 0x7fffffff;
+          for (int r = k + tid; r < n; r += BT) {
+            if (r == imax) continue;
+            const T x = r < imax ? F[imax + (size_t)r * ld] : F[r + (size_t)imax * ld];
+            rt = fmax(rt, fabs((double)x));
+          }
+          block_argmax_all<BT>(rs, 1, rv, ri, rt);
+          return ImaxColumn{rt, wii, wik};
+        });
+    if (pc.step == 0) {
+      // delay candidate k: move it to the end of the candidate set
+      if (k < nc - 1) {
+        symm_swap<T, BT>(F, ld, n, vars, fsperm, k, nc - 1);
+        __syncthreads();
+      }
+      nc -= 1;
+      have = false;
+      continue;
+    }
+    const int step = pc.step;
+    const int ksrc = k + step - 1;
+    if (pc.kpiv != ksrc) {
+      symm_swap<T, BT>(F, ld, n, vars, fsperm, ksrc, pc.kpiv);
+      __syncthreads();
+    }
+    const int c0 = k + step;
+    const int npar = par ^ 1;
+    if (step == 1) {
+      const T d = Fk[k];
+      if (!isfinite((double)d) && tid == 0) atomicOr(status, ST_NAN);
+      const T dinv = pc.zero ? T(0) : T(1) / d;
+      if (tid == 0) vars[3 * ld + k] = 0;  // 1x1 pivot
+      have = rl_update<T, BT, 1>(F, ld, n, k, c0, nc, dinv, T(0), T(0), T(0), npar, rs);
+      pd = dinv;
+    } else {
+      const T* W1 = Fk + ld;
+      const T d11 = Fk[k], d21 = Fk[k + 1], d22 = W1[k + 1];
+      const T detinv = T(1) / (d11 * d22 - d21 * d21);
+      if (!isfinite((double)detinv) && tid == 0) atomicOr(status, ST_NAN);
+      const T i00 = d22 * detinv, i10 = -d21 * detinv,
+              i01 = -d21 * detinv, i11 = d11 * detinv;
+      if (tid == 0) {
+        vars[k] = -(vars[k] + 1);
+        vars[k + 1] = -(vars[k + 1] + 1);
+        vars[3 * ld + k] = 1;
+        vars[3 * ld + k + 1] = 2;
+      }
+      have = rl_update<T, BT, 2>(F, ld, n, k, c0, nc, i00, i10, i01, i11, npar, rs);
+      p00 = i00; p10 = i10; p01 = i01; p11 = i11;
+    }
+    pk = k;
+    pstep = step;
+    par = npar;
+    __syncthreads();
+    k += step;
+  }
+  if (pk >= 0) rl_scale<T, BT>(F, ld, n, pk, pstep, pd, p00, p10, p01, p11);
+  __syncthreads();
   return nc;
 }
 
 // Front set-up shared by both paths (thread 0 sizes and allocates; all
 // threads fill the variable list and the fully-summed permutation record).
 // Returns false when the front must be skipped (a pool ran out earlier).
-template <class T>
-__device__ bool setup_front(const DevicePlan& d, int node, Ctl& ctl) {
+template <class T, int BT>
+__device__ bool setup_front(const DevicePlan& d, int node, CtlT<BT>& ctl) {
   const int tid = threadIdx.x;
   if (tid == 0) {
     ctl.skip = (*((volatile int*)d.status) & (ST_POOL_F | ST_POOL_I)) ? 1 : 0;
@@ -566,18 +817,18 @@ __device__ bool setup_front(const DevicePlan& d, int node, Ctl& ctl) {
   // Variable list: node vars, delayed pivots of the children, contribution
   // rows (include/sparse_ldl.h:957-987, 596-616).
   const int vbase = d.var_ptr[node];
-  for (int r = tid; r < ns; r += NT) fvars[r] = d.vars[vbase + r];
+  for (int r = tid; r < ns; r += BT) fvars[r] = d.vars[vbase + r];
   int choff = ns;
   for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
     const int c = d.kids[q];
     const int ndc = d.ndel[c];
     const int* cv = d.ipool + d.ioff[c] + d.npiv[c];
-    for (int t = tid; t < ndc; t += NT) fvars[choff + t] = cv[t];
+    for (int t = tid; t < ndc; t += BT) fvars[choff + t] = cv[t];
     choff += ndc;
   }
   const int cb = d.cptr[node];
-  for (int t = tid; t < d.nc[node]; t += NT) fvars[fs + t] = d.crows[cb + t];
-  for (int r = tid; r < fs; r += NT) fsperm[r] = r;
+  for (int t = tid; t < d.nc[node]; t += BT) fvars[fs + t] = d.crows[cb + t];
+  for (int r = tid; r < fs; r += BT) fsperm[r] = r;
   __syncthreads();
   return true;
 }
@@ -645,72 +896,103 @@ __device__ void finish_front(const DevicePlan& d, int node, const T* F,
   }
 }
 
-// Small/medium fronts: set up, assemble and factor one front per CTA, in
-// shared memory when it fits.
-template <class T>
-__global__ void __launch_bounds__(NT)
-k_factor_level(DevicePlan d, const int* __restrict__ nodes, int count,
-               const double* __restrict__ vals, double ustab,
-               double pivot_tol, int smem_elems) {
-  extern __shared__ double smem_raw[];
-  T* smem = reinterpret_cast<T*>(smem_raw);
-  __shared__ Ctl ctl;
+// Assemble front `node` (f x f, leading dimension f) in F: zero, add the
+// entries of A, extend-add the children's contribution blocks.  `rmap`
+// holds f ints of scratch.
+template <class T, int BT>
+__device__ void assemble_front(const DevicePlan& d, int node, T* F, int f,
+                               int ns, int ndin, const double* __restrict__ vals,
+                               int* rmap) {
   const int tid = threadIdx.x;
-  const int node = nodes[blockIdx.x];
-  if (!setup_front<T>(d, node, ctl)) return;
-  T* pool = reinterpret_cast<T*>(d.fpool);
-
-  const int f = ctl.f, fs = ctl.fs, ns = ctl.ns, ndin = ctl.ndin;
-  int* fvars = d.ipool + ctl.ioff;
-  int* fsperm = fvars + f;
-  T* Fg = pool + ctl.foff;
-  const bool in_smem = (long long)f * f + (long long)f * NB <= smem_elems;
-  T* F = in_smem ? smem : Fg;
-  T* W = in_smem ? smem + (size_t)f * f : Fg + (size_t)f * f;
-  T* tiles = nullptr;
-  if (!in_smem && smem_elems >= kTileSmem) tiles = smem;
-
-  // Assemble: zero, add A, extend-add the children.
-  for (size_t idx = tid; idx < (size_t)f * f; idx += NT) F[idx] = T(0);
+  const T* pool = reinterpret_cast<const T*>(d.fpool);
+  for (size_t idx = tid; idx < (size_t)f * f; idx += BT) F[idx] = T(0);
   __syncthreads();
-  for (int t = d.amap_ptr[node] + tid; t < d.amap_ptr[node + 1]; t += NT) {
-    const int r0 = d.amap_row[t];
-    const int r = r0 < ns ? r0 : r0 + ndin;
-    F[r + (size_t)d.amap_col[t] * f] += T(vals[d.amap_pos[t]]);
-  }
-  __syncthreads();
+  // each entry of A lands on its own front position: the index loads of a
+  // thread's next entries are issued before its adds
   {
-    int* rmap = reinterpret_cast<int*>(W);  // W is free until factoring
-    int choff = ns;
-    for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
-      const int c = d.kids[q];
-      const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
-      const int cc = fc - npc;
-      const T* C = pool + d.foff[c];
-      const int cb = d.cptr[c];
-      for (int a = tid; a < cc; a += NT)
-        rmap[a] = child_row_pos(d, cb, ndc, choff, ns, ndin, a);
-      __syncthreads();
-      for (int b = 0; b < cc; b++) {
-        const int pb = rmap[b];
-        const T* Cb = C + (size_t)(npc + b) * fc + npc;
-        for (int a = b + tid; a < cc; a += NT) {
-          const int pa = rmap[a];
-          const T v = Cb[a];
-          if (pa >= pb) F[pa + (size_t)pb * f] += v;
-          else F[pb + (size_t)pa * f] += v;
+    const int a0 = d.amap_ptr[node], a1 = d.amap_ptr[node + 1];
+    for (int t0 = a0 + tid; t0 < a1; t0 += 4 * BT) {
+      long long pos[4];
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int t = t0 + u * BT;
+        pos[u] = -1;
+        if (t < a1) {
+          const int r0 = d.amap_row[t];
+          const int r = r0 < ns ? r0 : r0 + ndin;
+          pos[u] = r + (long long)d.amap_col[t] * f;
+          v[u] = vals[d.amap_pos[t]];
         }
       }
-      __syncthreads();
-      choff += ndc;
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (pos[u] >= 0) F[pos[u]] += T(v[u]);
     }
   }
+  __syncthreads();
+  int choff = ns;
+  for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
+    const int c = d.kids[q];
+    const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
+    const int cc = fc - npc;
+    const T* C = pool + d.foff[c];
+    const int cb = d.cptr[c];
+    for (int a = tid; a < cc; a += BT)
+      rmap[a] = child_row_pos(d, cb, ndc, choff, ns, ndin, a);
+    __syncthreads();
+    for (int b = 0; b < cc; b++) {
+      const int pb = rmap[b];
+      const T* Cb = C + (size_t)(npc + b) * fc + npc;
+      for (int a = b + tid; a < cc; a += BT) {
+        const int pa = rmap[a];
+        const T v = Cb[a];
+        if (pa >= pb) F[pa + (size_t)pb * f] += v;
+        else F[pb + (size_t)pa * f] += v;
+      }
+    }
+    __syncthreads();
+    choff += ndc;
+  }
+}
 
-  const bool root = (fs == f);
-  const int npiv = factor_front(F, f, W, f, f, fs, root, fvars, fsperm, ustab,
-                                pivot_tol, tiles, d.status, ctl);
+// Small fronts with the unblocked right-looking factorization: the front
+// and its four integer sections (variables, fully-summed permutation,
+// inverse permutation, pivot kinds) in shared memory when they fit, else in
+// the pools; `smem_bytes` is the dynamic shared memory of the launch.
+// Four CTAs per SM (64 registers a thread at 256 threads): as many fronts
+// as shared memory holds for 70-row fronts.
+template <class T, int BT>
+__global__ void __launch_bounds__(BT, 4)
+k_factor_level_rl(DevicePlan d, const int* __restrict__ nodes, int count,
+                  const double* __restrict__ vals, double ustab,
+                  double pivot_tol, int smem_bytes) {
+  extern __shared__ double smem_raw[];
+  __shared__ CtlT<BT> ctl;
+  __shared__ RedSlots<BT> rs;
+  const int tid = threadIdx.x;
+  const int node = nodes[blockIdx.x];
+  if (!setup_front<T, BT>(d, node, ctl)) return;
+  T* pool = reinterpret_cast<T*>(d.fpool);
+  const int f = ctl.f, fs = ctl.fs, ns = ctl.ns, ndin = ctl.ndin;
+  int* fvars = d.ipool + ctl.ioff;
+  T* Fg = pool + ctl.foff;
+  const long long fbytes = ((long long)f * f * (long long)sizeof(T) + 15) & ~15ll;
+  const bool in_smem = fbytes + 5ll * f * (long long)sizeof(int) <= smem_bytes;
+  T* F = in_smem ? reinterpret_cast<T*>(smem_raw) : Fg;
+  int* iv = in_smem ? reinterpret_cast<int*>(reinterpret_cast<char*>(smem_raw) + fbytes)
+                    : fvars;
+  // scratch for the child row map: shared memory, or the front's W area
+  int* rmap = in_smem ? iv + 4 * f : reinterpret_cast<int*>(Fg + (size_t)f * f);
+  if (in_smem)
+    for (int t = tid; t < 2 * f; t += BT) iv[t] = fvars[t];
+  assemble_front<T, BT>(d, node, F, f, ns, ndin, vals, rmap);
+  const int npiv = factor_front_rl<T, BT>(F, f, f, fs, fs == f, iv, iv + f,
+                                          ustab, pivot_tol, d.status, rs);
   if (in_smem) {
-    for (size_t idx = tid; idx < (size_t)f * f; idx += NT) Fg[idx] = F[idx];
+    for (size_t idx = tid; idx < (size_t)f * f; idx += BT) Fg[idx] = F[idx];
+    for (int t = tid; t < 2 * f; t += BT) fvars[t] = iv[t];
+    for (int t = tid; t < npiv; t += BT) fvars[3 * f + t] = iv[3 * f + t];
   }
   __syncthreads();
   finish_front(d, node, F, f, fs, npiv, fvars);
@@ -725,7 +1007,7 @@ template <class T>
 __global__ void __launch_bounds__(NT)
 k_big_setup(DevicePlan d, const int* __restrict__ nodes) {
   __shared__ Ctl ctl;
-  setup_front<T>(d, nodes[blockIdx.x], ctl);
+  setup_front<T, NT>(d, nodes[blockIdx.x], ctl);
 }
 
 __device__ __forceinline__ bool big_skip(const DevicePlan& d) {
@@ -919,7 +1201,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
   DevicePlan& d = h.d;
   static bool attr_set = false;
   if (!attr_set) {
-    FCUDA(cudaFuncSetAttribute(k_factor_level<T>,
+    FCUDA(cudaFuncSetAttribute(k_factor_level_rl<T, 256>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kMaxDynSmem));
     FCUDA(cudaFuncSetAttribute(k_big_update<T>,
@@ -948,14 +1230,15 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     const LevelSchedule& L = h.sched[l];
     if (trace) cudaEventRecord(ev[3 * l], s);
     if (L.nsmall) {
-      long long fm = L.small_max_f + 16;
-      long long bytes = (fm * fm + fm * NB) * (long long)sizeof(T);
-      if (bytes < (long long)(kTileSmem * sizeof(T)))
-        bytes = (long long)(kTileSmem * sizeof(T));
+      // front + 5 int sections, sized for a few delayed pivots more than
+      // the static front; larger fronts run in the pools
+      const long long fm = L.small_max_f + kRlSlack;
+      long long bytes = ((fm * fm * (long long)sizeof(T) + 15) & ~15ll) + 5 * fm * 4;
       if (bytes > kMaxDynSmem) bytes = kMaxDynSmem;
-      { k_factor_level<T><<<L.nsmall, NT, (size_t)bytes, s>>>(
+      k_factor_level_rl<T, kRlThreads><<<L.nsmall, kRlThreads, (size_t)bytes, s>>>(
           d, d.sched_nodes + L.small_begin, L.nsmall, d_vals, h.ustab,
-          h.pivot_tol, (int)(bytes / sizeof(T))); ab::count_launch(); }
+          h.pivot_tol, (int)bytes);
+      ab::count_launch();
     }
     if (trace) cudaEventRecord(ev[3 * l + 1], s);
     if (L.nbig) {

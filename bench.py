@@ -13,6 +13,17 @@ by the device time of the whole step.  `e2e` is the same metric through the
 public SparseLDL API with the KKT values and right-hand side starting in
 host memory and the solution copied back every step.
 
+Extra fields of the same JSON line (1 GPU): `simp3d_factor` (3D SIMP
+cantilever 48x24x24 KKT: FP64 factor + solve, and the mixed-precision form
+with FP32 fronts, tensor-core Schur updates and FP64 refinement),
+`ipm_solve` (the cart-pole N = 100 problem solved end to end, p50/p99, with
+the same driver over the reference's host core beside it), `batch_solve`
+(512 cart-pole problems solved together, FP64 and mixed, with the
+single-problem device path beside it), `serve` (a Poisson request stream at
+80% of the serving loop's measured capacity, continuous batching,
+p50/p95/p99 latency).  `--no-3d`, `--no-ipm-solve`, `--batch 0`,
+`--serve-requests 0` skip them.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 Under torchrun each rank runs an independent replica on its own GPU
