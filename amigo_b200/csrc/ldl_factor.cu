@@ -35,10 +35,17 @@ namespace {
 
 constexpr int NT = kThreads;
 constexpr int NB = kPanel;
-// Threads of the one-CTA panel kernel of the large-front path: each
-// candidate column is brought up to date by one thread per row, so more
-// threads shorten every candidate step.
-constexpr int kPanelThreads = 1024;
+// Threads of the one-CTA panel kernel of the large-front path.  Each
+// candidate column is brought up to date by one thread per row.  Measured
+// on the 2D SIMP 128x64 KKT (fronts up to 1221 rows) one factorization
+// takes 31.4 ms with 256 threads, 27.2 ms with 512 and 31.3 ms with 1024;
+// the 3D SIMP 48x24x24 KKT (fronts up to 25216 rows) takes 4.9 s with 1024
+// and 5.75 s with 512 (the same from 1280 to 4096 rows as the switch
+// point).  Levels whose largest front has more than kPanelWideRows rows
+// take the wide kernel.
+constexpr int kPanelThreads = 512;
+constexpr int kPanelThreadsWide = 1024;
+constexpr int kPanelWideRows = 2048;
 // Shared memory of the large-front panel kernel for its copy of the
 // panel's L columns (the static control block aside).
 constexpr int kPanelCacheBytes = 200 * 1024;
@@ -71,44 +78,6 @@ __device__ __forceinline__ void argmax_merge(double& v, int& i, double v2,
     v = v2;
     i = i2;
   }
-}
-
-// Block-wide first-argmax of (v, i) plus a max of v2.  Result is written to
-// ctl.red_v[0], ctl.red_i[0], ctl.red_v2[0].
-template <int BT>
-__device__ void block_argmax(CtlT<BT>& ctl, double v, int i, double v2) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) {
-    double ov = __shfl_down_sync(0xffffffffu, v, o);
-    int oi = __shfl_down_sync(0xffffffffu, i, o);
-    double ov2 = __shfl_down_sync(0xffffffffu, v2, o);
-    argmax_merge(v, i, ov, oi);
-    v2 = fmax(v2, ov2);
-  }
-  if (lane == 0) {
-    ctl.red_v[warp] = v;
-    ctl.red_i[warp] = i;
-    ctl.red_v2[warp] = v2;
-  }
-  __syncthreads();
-  if (warp == 0) {
-    v = lane < (BT / 32) ? ctl.red_v[lane] : -1.0;
-    i = lane < (BT / 32) ? ctl.red_i[lane] : 0x7fffffff;
-    v2 = lane < (BT / 32) ? ctl.red_v2[lane] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) {
-      double ov = __shfl_down_sync(0xffffffffu, v, o);
-      int oi = __shfl_down_sync(0xffffffffu, i, o);
-      double ov2 = __shfl_down_sync(0xffffffffu, v2, o);
-      argmax_merge(v, i, ov, oi);
-      v2 = fmax(v2, ov2);
-    }
-    if (lane == 0) {
-      ctl.red_v[0] = v;
-      ctl.red_i[0] = i;
-      ctl.red_v2[0] = v2;
-    }
-  }
-  __syncthreads();
 }
 
 // Symmetric interchange of rows/columns a < b of the lower triangle of F,
@@ -300,21 +269,29 @@ __device__ __forceinline__ PivotChoice choose_pivot(bool root, int k, int nc,
 }
 
 // W[r, col] = src(r) - F[r, kstart:kstart+kw] . ctl.wrow  for r in [k, n),
-// and the reductions the pivot tests need.
-//   mode 0: candidate column k; src(r) = F[r, k]; reduces first-argmax of
-//           |W| over (k, nc) -> ctl.imax / ctl.abswik and max over [nc, n)
-//           -> ctl.ctail.
+// and the reductions the pivot tests need, returned to every thread.
+//   mode 0: candidate column k; src(r) = F[r, k]; first-argmax of |W| over
+//           (k, nc) -> imax / abswik, max over [nc, n) -> ctail.
 //   mode 1: column imax; src(r) = F[imax, r] for r < imax else F[r, imax];
-//           reduces max over [k, n) \ {imax} -> ctl.rowmax.
+//           max over [k, n) \ {imax} -> rowmax.
+// Below 1024 threads the W values of the thread's first two rows
+// (k + tid, k + tid + BT) are also left in keep0 / keep1 (at 1024 threads
+// the registers go to the memory-bound row loop).  One barrier, after all
+// W stores.
+struct ColScan {
+  int imax;
+  double abswik, ctail, rowmax;
+};
 template <class T, int BT>
-__device__ void build_column(T* F, int ld, T* W, int ldw, int n,
-                             int k, int kstart, int kw, int col, int mode,
-                             int imax, int nc, CtlT<BT>& ctl, int* status,
-                             const T* cache, int cld) {
+__device__ ColScan build_column(T* F, int ld, T* W, int ldw, int n,
+                                int k, int kstart, int kw, int col, int mode,
+                                int imax, int nc, CtlT<BT>& ctl, int* status,
+                                const T* cache, int cld, T& keep0, T& keep1) {
   const int tid = threadIdx.x;
   double bestv = -1.0, tailv = 0.0;
   int besti = 0x7fffffff;
-  for (int r = k + tid; r < n; r += BT) {
+  int it = 0;
+  for (int r = k + tid; r < n; r += BT, it++) {
     T acc;
     if (mode == 0) {
       acc = F[r + (size_t)k * ld];
@@ -325,8 +302,35 @@ __device__ void build_column(T* F, int ld, T* W, int ldw, int n,
     const bool inc = cache && (r - kstart) < cld;
     const T* Lr = inc ? cache + (r - kstart) : F + r + (size_t)kstart * ld;
     const size_t ls = inc ? (size_t)cld : (size_t)ld;
-    for (int j = 0; j < kw; j++) acc -= Lr[j * ls] * T(ctl.wrow[j]);
+    // the row's panel entries QB at a time, all loads before the FMAs
+    // (same summation order as one at a time).  The 1024-thread kernel
+    // (64 registers a thread) keeps the plain loop, which the compiler
+    // unrolls with its loads ahead on its own.
+    constexpr int QB = BT >= 1024 ? 1 : 8;
+    int j = 0;
+    if (QB == 1)
+      for (; j < kw; j++) acc -= Lr[j * ls] * T(ctl.wrow[j]);
+    for (; j + QB <= kw; j += QB) {
+      T v[QB];
+#pragma unroll
+      for (int u = 0; u < QB; u++) v[u] = Lr[(j + u) * ls];
+#pragma unroll
+      for (int u = 0; u < QB; u++) acc -= v[u] * T(ctl.wrow[j + u]);
+    }
+    if (j < kw) {
+      T v[QB];
+#pragma unroll
+      for (int u = 0; u < QB; u++)
+        if (j + u < kw) v[u] = Lr[(j + u) * ls];
+#pragma unroll
+      for (int u = 0; u < QB; u++)
+        if (j + u < kw) acc -= v[u] * T(ctl.wrow[j + u]);
+    }
     W[r + (size_t)col * ldw] = acc;
+    if (BT < 1024) {
+      if (it == 0) keep0 = acc;
+      else if (it == 1) keep1 = acc;
+    }
     const double a = fabs((double)acc);
     if (mode == 0) {
       if (r > k && r < nc) argmax_merge(bestv, besti, a, r);
@@ -335,24 +339,48 @@ __device__ void build_column(T* F, int ld, T* W, int ldw, int n,
       if (r != imax) tailv = fmax(tailv, a);
     }
   }
-  block_argmax<BT>(ctl, bestv, besti, tailv);
-  if (tid == 0) {
-    if (mode == 0) {
-      int im = ctl.red_i[0];
-      if (im >= nc || im <= k) {
-        // No finite candidate entry (all NaN, or no candidates): keep the
-        // index in range; NaN is reported through the status word.
-        if (k + 1 < nc) atomicOr(status, ST_NAN);
-        im = (k + 1 < n) ? k + 1 : k;
-      }
-      ctl.imax = im;
-      ctl.abswik = ctl.red_v[0] < 0.0 ? 0.0 : ctl.red_v[0];
-      ctl.ctail = ctl.red_v2[0];
-    } else {
-      ctl.rowmax = ctl.red_v2[0];
-    }
+  // warp trees, then every warp folds the warp results itself (inputs are
+  // never NaN, so all threads agree)
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, bestv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, besti, o);
+    const double ov2 = __shfl_xor_sync(0xffffffffu, tailv, o);
+    argmax_merge(bestv, besti, ov, oi);
+    tailv = fmax(tailv, ov2);
+  }
+  const int lane = tid & 31, warp = tid >> 5;
+  if (lane == 0) {
+    ctl.red_v[warp] = bestv;
+    ctl.red_i[warp] = besti;
+    ctl.red_v2[warp] = tailv;
   }
   __syncthreads();
+  bestv = lane < BT / 32 ? ctl.red_v[lane] : -1.0;
+  besti = lane < BT / 32 ? ctl.red_i[lane] : 0x7fffffff;
+  tailv = lane < BT / 32 ? ctl.red_v2[lane] : 0.0;
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, bestv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, besti, o);
+    const double ov2 = __shfl_xor_sync(0xffffffffu, tailv, o);
+    argmax_merge(bestv, besti, ov, oi);
+    tailv = fmax(tailv, ov2);
+  }
+  ColScan cs{0, 0.0, 0.0, 0.0};
+  if (mode == 0) {
+    int im = besti;
+    if (im >= nc || im <= k) {
+      // No finite candidate entry (all NaN, or no candidates): keep the
+      // index in range; NaN is reported through the status word.
+      if (k + 1 < nc && tid == 0) atomicOr(status, ST_NAN);
+      im = (k + 1 < n) ? k + 1 : k;
+    }
+    cs.imax = im;
+    cs.abswik = bestv < 0.0 ? 0.0 : bestv;
+    cs.ctail = tailv;
+  } else {
+    cs.rowmax = tailv;
+  }
+  return cs;
 }
 
 // Load row `row` of W (columns 0..kw-1) into ctl.wrow.
@@ -391,19 +419,23 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
   int k = k_, nc = nc_, kw = 0;
   const int kstart = k;
   const int cld = cache ? (n - kstart < cache_rows ? n - kstart : cache_rows) : 0;
+  // ctl.wrow holds row k of W: staged by the previous pivot step
+  bool wrow_ready = true;  // kw == 0: no columns
   while (kw < NB - 1 && k < nc) {
-    load_wrow<T, BT>(W, ldw, k, kw, ctl);
-    build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0, nc, ctl, status,
-                        cache, cld);
+    if (!wrow_ready) load_wrow<T, BT>(W, ldw, k, kw, ctl);
+    T keep0 = T(0), keep1 = T(0), spare0, spare1;
+    const ColScan cs = build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw, 0, 0,
+                                           nc, ctl, status, cache, cld, keep0, keep1);
     const double wkk = W[k + (size_t)kw * ldw];
-    const int imax = ctl.imax;
+    const int imax = cs.imax;
     const PivotChoice pc = choose_pivot(
-        root, k, nc, wkk, imax, ctl.abswik, ctl.ctail, ustab, pivot_tol, [&]() {
+        root, k, nc, wkk, imax, cs.abswik, cs.ctail, ustab, pivot_tol, [&]() {
           const double wik = W[imax + (size_t)kw * ldw];
           load_wrow<T, BT>(W, ldw, imax, kw, ctl);
-          build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw, kw + 1, 1, imax,
-                              nc, ctl, status, cache, cld);
-          const ImaxColumn c{ctl.rowmax, (double)W[imax + (size_t)(kw + 1) * ldw],
+          const ColScan c1 = build_column<T, BT>(F, ld, W, ldw, n, k, kstart, kw,
+                                                 kw + 1, 1, imax, nc, ctl, status,
+                                                 cache, cld, spare0, spare1);
+          const ImaxColumn c{c1.rowmax, (double)W[imax + (size_t)(kw + 1) * ldw],
                              wik};
           // every thread holds its decision inputs before the interchange
           // or the column copy that follow rewrite them
@@ -431,6 +463,7 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
         }
       }
       nc -= 1;
+      wrow_ready = false;
       continue;
     }
     const int ksrc = k + step - 1;
@@ -448,8 +481,12 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
       if (!isfinite((double)d) && tid == 0) atomicOr(status, ST_NAN);
       const T dinv = zero_pivot ? T(0) : T(1) / d;
       if (tid == 0) vars[3 * ld + k] = 0;  // 1x1 pivot
-      for (int r = k + tid; r < n; r += BT) {
-        T w = W[r + (size_t)kw * ldw];
+      // column k as built: no interchange or copy since, so this thread's
+      // first two rows are still in keep0 / keep1
+      const bool kept = BT < 1024 && kpiv == k;
+      int it = 0;
+      for (int r = k + tid; r < n; r += BT, it++) {
+        T w = (kept && it < 2) ? (it == 0 ? keep0 : keep1) : W[r + (size_t)kw * ldw];
         const T l = (r == k) ? w : w * dinv;
         F[r + (size_t)k * ld] = l;
         if (r - kstart < cld) cache[(r - kstart) + (size_t)kw * cld] = l;
@@ -484,6 +521,12 @@ __device__ void panel_factor(T* F, int ld, T* W, int ldw, int n,
         vars[3 * ld + k + 1] = 2;
       }
     }
+    // stage row k + step of W for the next candidate; published by the
+    // barrier below (nothing reads ctl.wrow between here and there)
+    if (k + step < n)
+      for (int j = tid; j < kw + step; j += BT)
+        ctl.wrow[j] = W[(k + step) + (size_t)j * ldw];
+    wrow_ready = true;
     __syncthreads();
     k += step;
     kw += step;
@@ -1071,11 +1114,11 @@ k_big_extend(DevicePlan d, const int* __restrict__ nodes, int q) {
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(kPanelThreads)
+template <class T, int PT>
+__global__ void __launch_bounds__(PT)
 k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
             double pivot_tol, int cache_bytes) {
-  __shared__ CtlT<kPanelThreads> ctl;
+  __shared__ CtlT<PT> ctl;
   extern __shared__ double cache_raw[];
   if (big_skip(d)) return;
   const int node = nodes[blockIdx.x];
@@ -1095,7 +1138,7 @@ k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
   // the panel's L columns in shared memory for as many rows as fit
   const int cache_rows = cache_bytes / (NB * (int)sizeof(T));
   T* cache = cache_rows > 0 ? reinterpret_cast<T*>(cache_raw) : nullptr;
-  panel_factor<T, kPanelThreads>(F, f, W, f, f, fs == f, fvars, fvars + f, ustab, pivot_tol,
+  panel_factor<T, PT>(F, f, W, f, f, fs == f, fvars, fvars + f, ustab, pivot_tol,
                d.status, ctl, k, nc, kw, cache, cache_rows);
   if (threadIdx.x == 0) {
     st[0] = k;
@@ -1207,7 +1250,10 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     FCUDA(cudaFuncSetAttribute(k_big_update<T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kTileSmem * sizeof(T)));
-    FCUDA(cudaFuncSetAttribute(k_big_panel<T>,
+    FCUDA(cudaFuncSetAttribute(k_big_panel<T, kPanelThreads>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kPanelCacheBytes));
+    FCUDA(cudaFuncSetAttribute(k_big_panel<T, kPanelThreadsWide>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kPanelCacheBytes));
     FCUDA(cudaFuncSetAttribute(k_big_update_tc,
@@ -1271,8 +1317,13 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       for (;;) {
         budget += panels;
         for (int it = 0; it < panels; it++) {
-          { k_big_panel<T><<<B, kPanelThreads, panel_cache, s>>>(d, nodes, h.ustab,
-                                                     h.pivot_tol, panel_cache); ab::count_launch(); }
+          if (fm > kPanelWideRows)
+            k_big_panel<T, kPanelThreadsWide><<<B, kPanelThreadsWide, panel_cache, s>>>(
+                d, nodes, h.ustab, h.pivot_tol, panel_cache);
+          else
+            k_big_panel<T, kPanelThreads><<<B, kPanelThreads, panel_cache, s>>>(
+                d, nodes, h.ustab, h.pivot_tol, panel_cache);
+          ab::count_launch();
           if (use_tc) {
             { k_big_update_tc<<<dim3(B, gtc), tc::kThreads, tc::kSmemBytes, s>>>(
                 d, nodes); ab::count_launch(); }
