@@ -97,6 +97,7 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
   const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
   __shared__ int s_choff;
   __shared__ double sL[(SB + 1) * (SB + 1)];
+  __shared__ int sK[SB + 1];  // the block's pivot kinds
 
   for (int rhs = 0; rhs < nrhs; rhs++) {
     // The front vector is worked on in shared memory when it fits (every
@@ -117,10 +118,11 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
         const int i = t % bw, j = t / bw;
         sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
       }
+      for (int t = tid; t < bw; t += NT) sK[t] = kind[jb + t];
       __syncthreads();
       if (warp == 0) {
         for (int j = jb; j < je;) {
-          const bool two = kind[j] == 1;
+          const bool two = sK[j - jb] == 1;
           const double v0 = V[j];
           const double v1 = two ? V[j + 1] : 0.0;
           const int i0 = j + (two ? 2 : 1);
@@ -179,6 +181,7 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
   const int* kind = fvars + 3 * f;
   const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
   __shared__ double sL[(SB + 1) * (SB + 1)];
+  __shared__ int sK[SB + 1];  // the block's pivot kinds
   for (int rhs = 0; rhs < nrhs; rhs++) {
     double* V = f <= smem_doubles ? sV : ubuf + uoff[node] + (long long)rhs * f;
     double* xr = x + (long long)rhs * ldx;
@@ -205,11 +208,12 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
         const int i = t % bw, j = t / bw;
         sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
       }
+      for (int t = tid; t < bw; t += NT) sK[t] = kind[jb + t];
       __syncthreads();
       if (warp == 0) {
         // within the block, backwards: column j (or pair j-1, j)
         for (int j = je - 1; j >= jb;) {
-          const bool two = kind[j] == 2;
+          const bool two = sK[j - jb] == 2;
           const int jl = two ? j - 1 : j;
           // rows strictly inside the block below this pivot
           double a0 = 0.0, a1 = 0.0;
@@ -300,6 +304,7 @@ k_wide_forward(DevicePlan d, const int* __restrict__ nodes, int count,
   extern __shared__ double sm[];
   double* sL = sm;                         // (WB + 1)^2 diagonal block
   double* sv = sm + (WB + 1) * (WB + 1);   // WB + 1 block values
+  __shared__ int sK[WB + 1];               // the block's pivot kinds
   __shared__ int s_choff;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int rhs = 0; rhs < nrhs; rhs++) {
@@ -328,11 +333,14 @@ k_wide_forward(DevicePlan d, const int* __restrict__ nodes, int count,
           const int i = t % bw, j = t / bw;
           sL[i + j * (WB + 1)] = w.L[jb + i + (size_t)(jb + j) * w.f];
         }
-        for (int t = tid; t < bw; t += NT) sv[t] = __ldcg(w.G + jb + t);
+        for (int t = tid; t < bw; t += NT) {
+          sv[t] = __ldcg(w.G + jb + t);
+          sK[t] = w.kind[jb + t];
+        }
         __syncthreads();
         if (warp == 0) {
           for (int j = 0; j < bw;) {
-            const bool two = w.kind[jb + j] == 1;
+            const bool two = sK[j] == 1;
             const double v0 = sv[j];
             const double v1 = two ? sv[j + 1] : 0.0;
             const int i0 = j + (two ? 2 : 1);
@@ -423,6 +431,7 @@ k_wide_backward(DevicePlan d, const int* __restrict__ nodes, int count,
   extern __shared__ double sm[];
   double* sL = sm;
   double* sv = sm + (WB + 1) * (WB + 1);
+  __shared__ int sK[WB + 1];  // the block's pivot kinds
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NWARP = NT / 32;
   const long long gwarps = (long long)gridDim.x * NWARP;
@@ -475,11 +484,14 @@ k_wide_backward(DevicePlan d, const int* __restrict__ nodes, int count,
           const int i = t % bw, j = t / bw;
           sL[i + j * (WB + 1)] = w.L[jb + i + (size_t)(jb + j) * w.f];
         }
-        for (int t = tid; t < bw; t += NT) sv[t] = __ldcg(w.G + jb + t);
+        for (int t = tid; t < bw; t += NT) {
+          sv[t] = __ldcg(w.G + jb + t);
+          sK[t] = w.kind[jb + t];
+        }
         __syncthreads();
         if (warp == 0) {
           for (int j = bw - 1; j >= 0;) {
-            const bool two = w.kind[jb + j] == 2;
+            const bool two = sK[j] == 2;
             const int jl = two ? j - 1 : j;
             double a0 = 0.0, a1 = 0.0;
             for (int i = j + 1 + lane; i < bw; i += 32) {
