@@ -563,7 +563,7 @@ def roofline(core, fac_ms):
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = bytes_ / (fac_ms * 1e-3) / 1e9
     del h
-    return {"kernel": "multifrontal factorization (k_factor_level, k_big_panel, "
+    return {"kernel": "multifrontal factorization (k_factor_level_rl, k_big_panel, "
                       "k_big_update, k_big_extend, ...; one factorization)",
             "bound": "hbm", "achieved": round(achieved, 2),
             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5),
