@@ -608,31 +608,33 @@ __device__ __forceinline__ void rl_scale(T* F, int ld, int n, int k, int step,
 
 // Rank-1 (STEP 1) or rank-2 (STEP 2) update of the trailing triangle
 // F[c0:, c0:] by the pivot at k: F[r, c] -= L[r, j] * W[c, j], j = k (and
-// k+1), with L = W D^-1 (coefficients d00..d11).  Threads form a 16 x TC
-// grid: thread (tr, tc) takes columns c0 + tc + TC j and, in each, the rows
-// on or below the diagonal that are congruent to c0 + tr modulo 16.  Lanes
-// 0..15 of warp 0 (tc == 0) hold column c0 and leave its scan for the next
-// pivot search (first-argmax over the candidates c0 < r < nc, max over
-// r >= nc) in slot `par`.  Returns whether they did (c0 < n).
+// k+1), with L = W D^-1 (coefficients d00..d11).  Warp 0 takes column c0,
+// one lane per row, and leaves its scan for the next pivot search
+// (first-argmax over the candidates c0 < r < nc, max over r >= nc) in slot
+// `par`: that column is the next step's critical path, so no other work
+// shares the warp.  The other warps form a 16 x TC grid over columns
+// c0+1 .. n-1: thread (tr, tc) takes columns c0 + 1 + tc + TC j and, in
+// each, the rows on or below the diagonal congruent to c0 + 1 + tr modulo
+// 16.  Returns whether the scan was left (c0 < n).
 constexpr int kRlRows = 16;
 
 template <class T, int BT, int STEP>
 __device__ __forceinline__ bool rl_update(T* F, int ld, int n, int k, int c0,
                                           int nc, T d00, T d10, T d01, T d11,
                                           int par, RedSlots<BT>& rs) {
-  constexpr int TR = kRlRows, TC = BT / TR;
-  const int tr = threadIdx.x % TR, tc = threadIdx.x / TR;
+  static_assert(BT >= 64, "one warp for column c0 and at least one more");
+  constexpr int TR = kRlRows, TC = (BT - 32) / TR;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const T* W0 = F + (size_t)k * ld;
   const T* W1 = W0 + ld;
   if (c0 >= n) return false;
-  int c = c0 + tc;
-  if (tc == 0) {
+  if (warp == 0) {
     double bv = -1.0, tv = 0.0;
     int bi = 0x7fffffff;
     const T y0 = W0[c0];
     const T y1 = STEP == 2 ? W1[c0] : T(0);
     T* Fc = F + (size_t)c0 * ld;
-    for (int r = c0 + tr; r < n; r += TR) {
+    for (int r = c0 + lane; r < n; r += 32) {
       T acc = Fc[r];
       if (STEP == 1) {
         acc -= (W0[r] * d00) * y0;
@@ -647,25 +649,28 @@ __device__ __forceinline__ bool rl_update(T* F, int ld, int n, int k, int c0,
       if (r > c0 && r < nc) argmax_merge(bv, bi, av, r);
       else if (r >= nc) tv = fmax(tv, av);
     }
-    for (int o = TR / 2; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0x0000ffffu, bv, o);
-      const int oi = __shfl_xor_sync(0x0000ffffu, bi, o);
-      const double ot = __shfl_xor_sync(0x0000ffffu, tv, o);
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      const double ot = __shfl_xor_sync(0xffffffffu, tv, o);
       argmax_merge(bv, bi, ov, oi);
       tv = fmax(tv, ot);
     }
-    if (tr == 0) {
+    if (lane == 0) {
       rs.nv[par] = bv;
       rs.ni[par] = bi;
       rs.nt[par] = tv;
     }
-    c += TC;
+    return true;
   }
-  for (; c < n; c += TC) {
+  const int t = threadIdx.x - 32;
+  const int tr = t % TR, tc = t / TR;
+  const int b0 = c0 + 1;
+  for (int c = b0 + tc; c < n; c += TC) {
     const T y0 = W0[c];
     const T y1 = STEP == 2 ? W1[c] : T(0);
     T* Fc = F + (size_t)c * ld;
-    int r = c0 + tr;
+    int r = b0 + tr;
     if (r < c) r += ((c - r + TR - 1) / TR) * TR;
     for (; r < n; r += TR) {
       T acc = Fc[r];
