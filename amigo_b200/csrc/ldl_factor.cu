@@ -59,12 +59,10 @@ constexpr int kRlThreads = 256;
 template <int BT>
 struct CtlT {
   double wrow[NB];     // row k (or imax) of W, columns 0..kw-1
-  double red_v[(BT / 32)];
+  double red_v[(BT / 32)];   // per-warp results of the column reductions
   int red_i[(BT / 32)];
   double red_v2[(BT / 32)];
-  double abswik, ctail, rowmax;
-  int imax;
-  int f, fs, ns, ndin, npiv;
+  int f, fs, ns, ndin;       // front set-up (setup_front)
   long long foff, ioff;
   int skip;
 };
