@@ -31,13 +31,7 @@ double* device_scratch() {
 }
 
 bool bad(const ab_ipm_problem* p, const ab_ipm_state* s) {
-  if (!p || !s) return true;
-  if (p->n < 0 || p->np < 0 || p->nc < 0) return true;
-  if (p->np > 0 && (!p->pidx || !p->lbx || !p->ubx || !s->zl || !s->zu ||
-                    !s->sl || !s->su))
-    return true;
-  if (p->nc > 0 && (!p->cidx || !p->lbh)) return true;
-  return false;
+  return ab::ipm_args_bad(p, s);
 }
 
 }  // namespace

@@ -8,6 +8,18 @@
 
 namespace ab {
 
+// Argument check shared by every IPM entry point: sizes non-negative and
+// the index, bound and state arrays present for the sizes given.
+inline bool ipm_args_bad(const ab_ipm_problem* p, const ab_ipm_state* s) {
+  if (!p || !s) return true;
+  if (p->n < 0 || p->np < 0 || p->nc < 0) return true;
+  if (p->np > 0 && (!p->pidx || !p->lbx || !p->ubx || !s->zl || !s->zu ||
+                    !s->sl || !s->su))
+    return true;
+  if (p->nc > 0 && (!p->cidx || !p->lbh)) return true;
+  return false;
+}
+
 __device__ void block_sum2(double a, double b, double* partial);
 __device__ void block_max2(double a, double b, double* partial);
 

@@ -1015,10 +1015,9 @@ extern "C" int ab_ipm_max_step_noalloc(const ab_ipm_problem* p,
                                        const double* px, const double* dzl,
                                        const double* dzu, double* out,
                                        int* iout, void* stream) {
-  if (!p || !s || !out || !iout || p->n < 0 || p->np < 0 || p->nc < 0)
-    return AB_ERR_ARG;
-  if (p->np > 0 && (!p->pidx || !p->lbx || !p->ubx || !s->zl || !s->zu ||
-                    !s->sl || !s->su || !px || !dzl || !dzu))
+  // the same argument check as ab_ipm_max_step
+  if (ab::ipm_args_bad(p, s) || !out || !iout ||
+      (p->np > 0 && (!px || !dzl || !dzu)))
     return AB_ERR_ARG;
   const long long nblocks = ((long long)p->np + ab::RT - 1) / ab::RT;
   if (nblocks > ab::kNoAllocBlocks) {

@@ -34,6 +34,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -61,6 +62,8 @@ def parse():
                     help="instances in the batched cart-pole solve (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=600,
                     help="requests in the serving run (0: skip)")
+    ap.add_argument("--clock-dir", default=tempfile.gettempdir(),
+                    help="folder for the nvidia-smi clock samples of the timed region")
     ap.add_argument("--no-3d", action="store_true",
                     help="skip the 3D SIMP 48x24x24 factorization")
     return ap.parse_args()
@@ -216,8 +219,9 @@ def run_ours(args, rank, world, local):
     core = Core(device, args.nx, args.ny)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
     for _ in range(args.warmup):
-        core.step()
+        inertia = core.step()
     torch.cuda.synchronize()
+    npiv_ours, _ = core.ldl.node_pivots()
     st = core.ldl.stats()
     flops = st["flops"]
     if world > 1:
@@ -232,8 +236,7 @@ def run_ours(args, rank, world, local):
            for _ in range(args.steps)]
     from amigo_b200 import _lib
     launches0 = _lib.lib().ab_launch_count()
-    clk = ClockSampler(os.path.join(ROOT, "gpurun_out" if os.path.isdir(
-        os.path.join(ROOT, "gpurun_out")) else ".", "clocks_rank%d.csv" % rank), local)
+    clk = ClockSampler(os.path.join(args.clock_dir, "clocks_rank%d.csv" % rank), local)
     t0 = time.time()
     with clk:
         for k in range(args.steps):
@@ -300,8 +303,12 @@ def run_ours(args, rank, world, local):
         "solve_ms_per_step": round(float(np.sum(sol_ms)) / args.steps, 4),
         "clocks": clk.summary(),
         "ldl_stats": st,
+        "inertia": [int(inertia[0]), int(inertia[1])],
+        "threads": threads_env(),
     }
+    core_npiv = npiv_ours
     out["roofline"] = roofline(core, fac_tot / args.steps)
+    out["_npiv"] = core_npiv
     if not args.no_3d and world == 1:
         del core, flush
         torch.cuda.empty_cache()
@@ -528,9 +535,12 @@ def ipm_solve_host_baseline():
     dt = time.perf_counter() - t
     return {"solves_per_s": round(1.0 / dt, 4), "iterations": int(r["iterations"]),
             "objective": r["objective"], "kkt_error": r["kkt_error"],
-            "kind": "reference", "cores": 1,
-            "sample": "1 cart-pole N=100 solve: same driver, reference SparseLDL "
-                      "and interior_point_backend.h on the host"}
+            "kind": "port", "cores": 1,
+            "sample": "1 cart-pole N=100 solve with this repository's IPM driver "
+                      "(ipm_driver.solve) over a host numeric core: the "
+                      "reference's SparseLDL and interior_point_backend.h "
+                      "(oracle/_ref) with the numpy restatement of the model's "
+                      "derivatives; not the reference's own Optimizer loop"}
 
 
 def roofline(core, fac_ms):
@@ -672,12 +682,24 @@ def factor_flops_from_ref(R):
     return float((p ** 3 / 3 + p * p * c + p * c * c).sum())
 
 
-def cpu_baseline():
-    m, times, R, cores = run_reference_timed(128, 64, max_seconds=12.0)
+def threads_env():
+    """Thread settings of this process (the reference arm's OpenMP tree tasks
+    use every core; its BLAS calls are pinned to one thread)."""
+    return {"nproc": os.cpu_count(),
+            "OMP_NUM_THREADS": os.environ.get("OMP_NUM_THREADS"),
+            "OPENBLAS_NUM_THREADS": os.environ.get("OPENBLAS_NUM_THREADS"),
+            "reference_blas_threads": 1,
+            "reference_openmp": "-fopenmp -DAMIGO_USE_OPENMP"}
+
+
+def cpu_baseline(nx=128, ny=64):
+    m, times, R, cores = run_reference_timed(nx, ny, max_seconds=12.0)
     flops = factor_flops_from_ref(R)
     med = float(np.median(times))
+    npiv, _ = R.node_pivots()
     return {"value": round(flops / med / 1e12, 6), "unit": "TFLOP/s",
             "cores": cores, "kind": "reference",
+            "inertia": [int(v) for v in R.inertia()], "_npiv": npiv,
             "sample": "%d factor+solve runs of the 2D SIMP 128x64 KKT with the "
                       "reference SparseLDL (AMD, OpenMP tree tasks, 1 BLAS "
                       "thread), median %.3f s" % (len(times), med)}
@@ -699,6 +721,8 @@ def run_reference(args, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic: 2D SIMP KKT at the seeded initial point",
         "config": dict(config(args, 1), n=m.n, nnz=m.nnz),
+        "inertia": [int(v) for v in R.inertia()],
+        "threads": threads_env(),
         "cpu_baseline": {"value": round(value, 6), "unit": "TFLOP/s",
                          "cores": cores, "kind": "reference",
                          "sample": "reference SparseLDL factor+solve of the full "
@@ -726,10 +750,20 @@ def main():
             if rank == 0 and world == 1 and not args.no_cpu_baseline:
                 from oracle import ref
                 if ref.available():
-                    out["cpu_baseline"] = cpu_baseline()
+                    cb = cpu_baseline(args.nx, args.ny)
+                    rnp = cb.pop("_npiv")
+                    out["cpu_baseline"] = cb
+                    # parity of the headline KKT: the same matrix factored by
+                    # the reference's SparseLDL on the host
+                    out["reference_inertia"] = cb["inertia"]
+                    out["inertia_equals_reference"] = out["inertia"] == cb["inertia"]
+                    if len(rnp) == len(out["_npiv"]):
+                        out["pivot_counts_equal_frac"] = round(
+                            float(np.mean(rnp == out["_npiv"])), 4)
                     if "ipm_solve" in out:
-                        out["ipm_solve"]["host_reference_core"] = ipm_solve_host_baseline()
+                        out["ipm_solve"]["host_core_same_driver"] = ipm_solve_host_baseline()
         if rank == 0 and out is not None:
+            out.pop("_npiv", None)
             print(json.dumps(out))
     finally:
         if world > 1:

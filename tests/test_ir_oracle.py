@@ -13,7 +13,8 @@ import scipy.sparse.linalg as spla
 
 from oracle import ir_oracle
 
-REF = "/root/reference/amigo/algorithm/solvers/linear_solver.py"
+REF = os.path.join(os.environ.get("AMIGO_REF_ROOT", "/root/reference"),
+                   "amigo", "algorithm", "solvers", "linear_solver.py")
 
 
 class _Arr:

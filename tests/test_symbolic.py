@@ -85,3 +85,32 @@ def test_bad_arguments():
     with pytest.raises(Exception):
         linalg.analyze(2, np.array([0, 1, 2]), np.array([0, 1]),
                        linalg.OrderingType.MULTI_COLOR)
+
+
+def _config_pattern(name):
+    """KKT sparsity patterns of the benchmarked configurations: the cart-pole
+    collocation problem (N = 100), the 2D SIMP 128 x 64 and the 3D SIMP
+    48 x 24 x 24 compliance KKTs."""
+    if name == "cartpole_N100":
+        from amigo_b200.problems.cartpole import CartPole
+        m = CartPole(N=100, seed=0)
+    elif name == "simp2d_128x64":
+        from amigo_b200.problems.simp2d import Simp2D
+        m = Simp2D(128, 64)
+    else:
+        from amigo_b200.problems.simp3d import Simp3D
+        m = Simp3D(48, 24, 24)
+    return m.n, m.rowp, m.cols
+
+
+@pytest.mark.parametrize("name", ["cartpole_N100", "simp2d_128x64", "simp3d_48x24x24"])
+def test_config_patterns_match_reference(oracle_ref, name):
+    """Ordering, elimination tree, supernodes and contribution rows of the
+    benchmarked KKT patterns equal the reference SparseLDL's (AMD, its
+    default ordering here) bit for bit."""
+    n, rp, ci = _config_pattern(name)
+    want = oracle_ref.RefSparseLDL(n, rp, ci, order="AMD").symbolic()
+    got = linalg.analyze(n, rp, ci, linalg.OrderingType.AMD)
+    assert got["num_nodes"] == want["num_nodes"]
+    for k in KEYS:
+        np.testing.assert_array_equal(got[k], want[k], err_msg="%s %s" % (name, k))

@@ -17,8 +17,6 @@ import torch
 
 from amigo_b200 import _lib
 
-pytestmark = pytest.mark.gpu
-
 
 def problem(np_, seed):
     r = np.random.RandomState(seed)
@@ -53,7 +51,9 @@ def run(name, P, S, t, tau):
     return out.cpu().numpy(), iout.cpu().numpy()
 
 
-@pytest.mark.parametrize("np_", [1, 1000, 300001])
+# 8192 * 256 fills the static array: every block partial is written and read
+@pytest.mark.gpu
+@pytest.mark.parametrize("np_", [1, 1000, 300001, 8192 * 256])
 def test_noalloc_matches_allocating_entry_point(np_):
     for call, seed in enumerate((5, 6)):  # two calls in a row share the array
         P, S, t = problem(np_, seed + np_)
@@ -63,6 +63,7 @@ def test_noalloc_matches_allocating_entry_point(np_):
         assert np.array_equal(got_i, want_i), (call, got_i, want_i)
 
 
+@pytest.mark.gpu
 def test_noalloc_rejects_oversize():
     P, S, t = problem(8, 1)
     P.np = 8192 * 256 + 1  # beyond the static scratch (never launched)
@@ -73,3 +74,16 @@ def test_noalloc_rejects_oversize():
         t["dzl"].data_ptr(), t["dzu"].data_ptr(), out.data_ptr(),
         iout.data_ptr(), None)
     assert rc == -6
+
+
+def test_noalloc_checks_arguments_like_allocating_entry_point():
+    """Both entry points reject the same malformed arguments (no launch is
+    reached, so this runs without a GPU)."""
+    P, S = _lib.IpmProblem(), _lib.IpmState()
+    P.n, P.np, P.nc = 4, 0, 4   # constraints without their index/bound arrays
+    out = (ctypes.c_double * 2)()
+    iout = (ctypes.c_int * 2)()
+    for name in ("ab_ipm_max_step", "ab_ipm_max_step_noalloc"):
+        rc = getattr(_lib.lib(), name)(ctypes.byref(P), ctypes.byref(S), 0.99,
+                                       None, None, None, out, iout, None)
+        assert rc == -1, (name, rc)
