@@ -153,6 +153,14 @@ _SIGS = {
     "ab_ldl_set_panel_cache": (_i, [_vp, _i]),
     "ab_tc_syrk_tf32x3": (_i, [_i, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _vp]),
     "ab_csr_add_diagonal": (_i, [_i, _vp, _vp, _vp, _vp]),
+    "ab_vec_absmax_gather": (_i, [_i, _vp, _vp, _vp, _vp]),
+    "ab_ipm_constraint_scale": (_i, [_i, _i, _vp, _vp, _vp, _d, _d, _vp, _vp,
+                                     _vp, _vp]),
+    "ab_csr_scale_symmetric": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
+    "ab_vec_scale_gather": (_i, [_i, _vp, _vp, _vp, _i, _vp]),
+    "ab_ipm_initialize_slacks": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
+    "ab_ipm_dual_residual_vector": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ab_vec_copy_gather": (_i, [_i, _vp, _vp, _vp, _vp]),
     "ab_csr_matvec": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "ab_cartpole_gradient": (_i, [ctypes.POINTER(CartPoleStruct), _vp, _d, _vp, _vp]),
     "ab_cartpole_hessian": (_i, [ctypes.POINTER(CartPoleStruct), _vp, _d, _vp, _vp]),

@@ -77,6 +77,17 @@ def _dev(v):
     return v
 
 
+def _host(v):
+    """numpy view of an array-like, a Vector's host array or a tensor."""
+    if isinstance(v, Vector):
+        return v.get_array()
+    if isinstance(v, torch.Tensor):
+        return v.cpu().numpy()
+    if hasattr(v, "get_array"):
+        return v.get_array()
+    return v
+
+
 class InteriorPointOptimizer:
     """Device IPM vector operations over a fixed primal/multiplier split.
 
@@ -86,11 +97,21 @@ class InteriorPointOptimizer:
     [lower, upper] as bounds, multiplier entries take lower as lbh.
     """
 
-    def __init__(self, mult, lower, upper, device=None):
+    def __init__(self, problem, lower, upper, device=None):
+        """problem: the reference's first argument, an object with
+        get_multiplier_indicator() (and, for compute_nlp_scaling,
+        create_matrix() / hessian(alpha, x, hess)), or the multiplier
+        indicator itself; lower / upper: arrays or Vector objects."""
         self.device = _device(device)
-        mult = np.asarray(mult).astype(bool)
-        lower = np.asarray(lower, dtype=np.float64)
-        upper = np.asarray(upper, dtype=np.float64)
+        if hasattr(problem, "get_multiplier_indicator"):
+            self.problem = problem
+            mult = problem.get_multiplier_indicator()
+        else:
+            self.problem = None
+            mult = problem
+        mult = np.asarray(_host(mult)).astype(bool)
+        lower = np.asarray(_host(lower), dtype=np.float64)
+        upper = np.asarray(_host(upper), dtype=np.float64)
         self.n = len(mult)
         pidx = np.nonzero(~mult)[0].astype(np.int32)
         cidx = np.nonzero(mult)[0].astype(np.int32)
@@ -99,6 +120,15 @@ class InteriorPointOptimizer:
         self.pidx, self.cidx = t(pidx), t(cidx)
         self.lbx, self.ubx = t(lower[pidx]), t(upper[pidx])
         self.lbh = t(lower[cidx])
+        # the unrelaxed bounds (get_lbx / get_ubx); relax_bounds moves
+        # self.lbx / self.ubx, which the kernels use
+        self.lbx0, self.ubx0 = self.lbx.clone(), self.ubx.clone()
+        self._relaxed = False
+        self._nslack = 0
+        self._obj_scale = 1.0
+        self._scaling = False
+        self._dc = None
+        self._scale = None
         self._out = torch.zeros(16, dtype=torch.float64, device=self.device)
         self._iout = torch.zeros(4, dtype=torch.int32, device=self.device)
         self._p = _lib.IpmProblem(self.n, self.np_, self.nc_,
@@ -125,12 +155,144 @@ class InteriorPointOptimizer:
     def get_num_design_variables(self):
         return self.np_
 
+    def get_num_constraints(self):
+        return self.nc_
+
+    def get_num_equalities(self):
+        return self.nc_
+
+    def get_num_inequalities(self):
+        return 0
+
+    def get_lbx(self):
+        """Primal lower bounds as given (device tensor, n_primal)."""
+        return self.lbx0
+
+    def get_ubx(self):
+        return self.ubx0
+
+    def get_lbx_relaxed(self):
+        """The bounds the IPM kernels use: relaxed once relax_bounds ran."""
+        return self.lbx if self._relaxed else self.lbx0
+
+    def get_ubx_relaxed(self):
+        return self.ubx if self._relaxed else self.ubx0
+
+    def get_kkt_element_counts(self):
+        """(n_d, n_p, n_c): dual-stationarity rows, primal-feasibility rows
+        and finite bounds (interior_point_optimizer.h:441-449)."""
+        n_c = int(torch.isfinite(self.lbx0).sum().item() +
+                  torch.isfinite(self.ubx0).sum().item())
+        return self.np_, self.nc_, n_c
+
     # -- setup -----------------------------------------------------------
     def relax_bounds(self, factor=1e-8, constr_viol_tol=1e-4):
-        _lib.call("ab_ipm_relax_bounds", self.np_, self.lbx.data_ptr(),
-                  self.ubx.data_ptr(), self.lbx.data_ptr(),
+        if factor <= 0:
+            return
+        _lib.call("ab_ipm_relax_bounds", self.np_, self.lbx0.data_ptr(),
+                  self.ubx0.data_ptr(), self.lbx.data_ptr(),
                   self.ubx.data_ptr(), float(factor), float(constr_viol_tol),
                   self._s())
+        self._relaxed = True
+
+    # -- slacks (interior_point_optimizer.h:462-494) ----------------------
+    def set_slack_mapping(self, slack_indices, constr_indices):
+        si = np.ascontiguousarray(slack_indices, dtype=np.int32)
+        ci = np.ascontiguousarray(constr_indices, dtype=np.int32)
+        if si.shape != ci.shape:
+            raise ValueError("slack and constraint index arrays differ in length")
+        t = lambda a: torch.from_numpy(a).to(self.device)
+        self._sidx, self._scidx = t(si), t(ci)
+        self._nslack = len(si)
+
+    def has_slacks(self):
+        return self._nslack > 0
+
+    def get_num_slacks(self):
+        return self._nslack
+
+    def initialize_slacks(self, grad, vars):
+        """Slacks to the constraint bodies: s_k = (c_k(x) - s_k) + s_k from
+        the gradient's constraint rows (evaluated at the current point)."""
+        if self._nslack == 0:
+            return
+        _lib.call("ab_ipm_initialize_slacks", self._nslack, self._sidx.data_ptr(),
+                  self._scidx.data_ptr(), _dev(grad).data_ptr(),
+                  _dev(vars).data_ptr(), self._s())
+
+    # -- NLP scaling (interior_point_optimizer.h:502-598) ------------------
+    def compute_nlp_scaling(self, x, grad, max_gradient=100.0, min_value=1e-8):
+        """Objective scale min(1, max_gradient / ||grad_f||_inf) and, per
+        constraint row j of the KKT at x, dc_j = min(1, max_gradient /
+        ||J_j||_inf) (both floored at min_value); the constraint targets
+        are scaled by dc."""
+        out = torch.zeros(1, dtype=torch.float64, device=self.device)
+        _lib.call("ab_vec_absmax_gather", self.np_, self.pidx.data_ptr(),
+                  _dev(grad).data_ptr(), out.data_ptr(), self._s())
+        gmax = float(out.item())
+        scale = max_gradient / gmax if gmax > max_gradient else 1.0
+        self._obj_scale = max(scale, min_value)
+        if self.problem is None:
+            raise RuntimeError("compute_nlp_scaling needs the problem object "
+                               "(create_matrix / hessian)")
+        hess = self.problem.create_matrix()
+        self.problem.hessian(1.0, x, hess)
+        self._dc = torch.zeros(self.nc_, dtype=torch.float64, device=self.device)
+        self._scale = torch.ones(self.n, dtype=torch.float64, device=self.device)
+        _lib.call("ab_ipm_constraint_scale", self.n, self.nc_, self.cidx.data_ptr(),
+                  hess.d_rowp.data_ptr(), hess.vals.data_ptr(), float(max_gradient),
+                  float(min_value), self._dc.data_ptr(), self.lbh.data_ptr(),
+                  self._scale.data_ptr(), self._s())
+        self._scaling = True
+
+    def apply_gradient_scaling(self, grad):
+        if self._scaling:
+            _lib.call("ab_vec_scale_gather", self.nc_, self.cidx.data_ptr(),
+                      self._dc.data_ptr(), _dev(grad).data_ptr(), 0, self._s())
+
+    def apply_hessian_scaling(self, hess):
+        """D H D with D = 1 on primals and dc on the constraint rows."""
+        if self._scaling:
+            _lib.call("ab_csr_scale_symmetric", hess.nrows, hess.d_rowp.data_ptr(),
+                      hess.d_cols.data_ptr(), self._scale.data_ptr(),
+                      hess.vals.data_ptr(), self._s())
+
+    def scale_multipliers(self, x):
+        if self._scaling:
+            _lib.call("ab_vec_scale_gather", self.nc_, self.cidx.data_ptr(),
+                      self._dc.data_ptr(), _dev(x).data_ptr(), 0, self._s())
+
+    def unscale_multipliers(self, x):
+        if self._scaling:
+            _lib.call("ab_vec_scale_gather", self.nc_, self.cidx.data_ptr(),
+                      self._dc.data_ptr(), _dev(x).data_ptr(), 1, self._s())
+
+    def get_obj_scale(self):
+        return self._obj_scale
+
+    def has_scaling(self):
+        return self._scaling
+
+    # -- copies and debug hooks --------------------------------------------
+    def copy_multipliers(self, d, s):
+        """d[constraint rows] = s[constraint rows]."""
+        _lib.call("ab_vec_copy_gather", self.nc_, self.cidx.data_ptr(),
+                  _dev(s).data_ptr(), _dev(d).data_ptr(), self._s())
+
+    def copy_design_vars(self, d, s):
+        _lib.call("ab_vec_copy_gather", self.np_, self.pidx.data_ptr(),
+                  _dev(s).data_ptr(), _dev(d).data_ptr(), self._s())
+
+    def compute_dual_residual_vector(self, vars, grad, out):
+        """out = grad - zl + zu on the primals, 0 on the multipliers."""
+        _lib.call("ab_ipm_dual_residual_vector", self.n, self.np_,
+                  self.pidx.data_ptr(), _dev(grad).data_ptr(), vars.zl.data_ptr(),
+                  vars.zu.data_ptr(), _dev(out).data_ptr(), self._s())
+
+    def check_update(self, mu, grad, vars, update, hess):
+        """Debug hook; a no-op, as in the reference
+        (interior_point_optimizer.h:451-457)."""
+        return None
 
     def initialize_multipliers_and_slacks(self, mu, grad, vars, kappa1=1e-2,
                                           kappa2=1e-2):

@@ -167,6 +167,9 @@ class Simp2DProblem:
         self._csr = CSRMat
         self.n = model.n
 
+    def get_multiplier_indicator(self):
+        return self.model.mult
+
     def create_matrix(self):
         m = self.model
         return self._csr(m.n, m.n, m.rowp, m.cols, device=self.device)

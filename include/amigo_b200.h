@@ -353,6 +353,46 @@ int ab_ipm_affine_start_point(const ab_ipm_problem* p, const ab_ipm_state* s,
  * KKT matrix utilities (CSR values on the device)
  * -------------------------------------------------------------------- */
 
+/* ---- NLP scaling, slacks, dual residual (InteriorPointOptimizer,
+ * include/interior_point_optimizer.h:476-598; interior_point_backend.h:
+ * 99-121, 579-586).  Device pointers; asynchronous on `stream`. ---- */
+
+/* *d_out = max_j |x[idx[j]]| (0 for m = 0): the objective-gradient norm of
+ * compute_nlp_scaling (interior_point_optimizer.h:508-518). */
+int ab_vec_absmax_gather(int m, const int* idx, const double* x,
+                         double* d_out, void* stream);
+/* Constraint scaling of compute_nlp_scaling (interior_point_optimizer.h:
+ * 520-560): dc[j] = min(1, max_gradient / max_k |H[cidx[j], k]|) floored
+ * at min_value, lbh[j] *= dc[j] where dc[j] != 1, scale[i] = 1 for every
+ * variable and dc[j] at cidx[j] (the D of D H D). */
+int ab_ipm_constraint_scale(int n, int nc, const int* cidx, const int* rowp,
+                            const double* hess_vals, double max_gradient,
+                            double min_value, double* dc, double* lbh,
+                            double* scale, void* stream);
+/* vals[k] *= scale[i] * scale[cols[k]] (apply_hessian_scaling,
+ * interior_point_optimizer.h:573-584). */
+int ab_csr_scale_symmetric(int n, const int* rowp, const int* cols,
+                           const double* scale, double* vals, void* stream);
+/* x[idx[j]] *= s[j], or /= s[j] when divide != 0 (apply_gradient_scaling,
+ * scale_multipliers, unscale_multipliers, interior_point_optimizer.h:
+ * 566-597). */
+int ab_vec_scale_gather(int m, const int* idx, const double* s, double* x,
+                        int divide, void* stream);
+/* xlam[slack_idx[k]] = grad[constr_idx[k]] + xlam[slack_idx[k]]
+ * (initialize_slacks, interior_point_optimizer.h:476-489). */
+int ab_ipm_initialize_slacks(int nslack, const int* slack_idx,
+                             const int* constr_idx, const double* grad,
+                             double* xlam, void* stream);
+/* out = 0, then out[pidx[i]] = grad[pidx[i]] - zl[i] + zu[i]
+ * (compute_dual_residual_vector, interior_point_backend.h:579-586). */
+int ab_ipm_dual_residual_vector(int n, int np, const int* pidx,
+                                const double* grad, const double* zl,
+                                const double* zu, double* out, void* stream);
+/* dst[idx[j]] = src[idx[j]] (copy_primals / copy_constraints,
+ * interior_point_backend.h:106-121). */
+int ab_vec_copy_gather(int m, const int* idx, const double* src, double* dst,
+                       void* stream);
+
 /* vals[diag_pos[i]] += d[i] for i < n.  Replaces CSRMat::add_diagonal
  * (include/csr_matrix.h:508-528). */
 int ab_csr_add_diagonal(int n, const int* diag_pos, const double* d,
