@@ -89,6 +89,38 @@ def max_over_ranks(values, device=None):
     return [float(v) for v in t.cpu()]
 
 
+def sum_over_ranks(values, device=None):
+    """Element-wise sum of a list of floats over all ranks (work counts of
+    the replicas)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64,
+                     device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return [float(v) for v in t.cpu()]
+
+
+def relaunch_under_torchrun(args):
+    """`python bench.py --gpus N` (N > 1) outside torchrun: start N ranks on
+    this node with torch.distributed.run (replicas, one per GPU)."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node", str(args.gpus), "--master-addr", "127.0.0.1",
+           "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    os.execv(sys.executable, cmd)
+
+
+def shard(items, rank, world):
+    """This rank's contiguous share of a list of independent problems."""
+    b0, b1 = replica_items(len(items), rank, world)
+    return items[b0:b1]
+
+
 def replica_items(n_items, rank, world):
     """Independent problems are split over ranks in contiguous blocks (the
     replicas-only decomposition): returns this rank's [begin, end)."""
@@ -309,7 +341,8 @@ def run_ours(args, rank, world, local):
     core_npiv = npiv_ours
     out["roofline"] = roofline(core, fac_tot / args.steps)
     out["_npiv"] = core_npiv
-    if not args.no_3d and world == 1:
+    if not args.no_3d:
+        # one factorization per GPU: every replica runs it on its own device
         del core, flush
         torch.cuda.empty_cache()
         out["simp3d_factor"] = simp3d_bench(device)
@@ -317,14 +350,24 @@ def run_ours(args, rank, world, local):
     if not args.no_ipm_solve:
         out["ipm_solve"] = ipm_solve_bench(device, args.solves)
         if args.batch > 0:
-            out["batch_solve"] = batch_solve_bench(device, args.batch)
+            out["batch_solve"] = batch_solve_bench(device, args.batch, rank=rank,
+                                                   world=world)
             if args.serve_requests > 0:
-                cap = out["batch_solve"]["solves_per_s"]
-                out["serve"] = serve_bench(device, args.serve_requests, cap)
+                cap = out["batch_solve"]["solves_per_s"] / world
+                out["serve"] = serve_bench(device, args.serve_requests, cap,
+                                           rank=rank, world=world)
     return out
 
 
-def serve_bench(device, n_requests, batch_capacity):
+def barrier(device):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.synchronize(device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.barrier()
+
+
+def serve_bench(device, n_requests, batch_capacity, rank=0, world=1):
     """Serving: a stream of cart-pole solve requests (N ~ U{50..400}) with
     Poisson arrivals at 80% of the serving loop's own capacity, continuous
     batching (serve.Server: admission at iteration boundaries by slots and a
@@ -335,9 +378,20 @@ def serve_bench(device, n_requests, batch_capacity):
         serve.make_stream(256, rate=1e6, seed=12), time_limit=120)
     capacity = sat["solves_per_s"]
     rate = 0.8 * capacity
-    reqs = serve.make_stream(n_requests, rate, seed=11)
+    # replicas: rank r serves its contiguous share of the request stream
+    # (each GPU its own queue and memory budget), at its share of the rate
+    b0, b1 = replica_items(n_requests, rank, world)
+    reqs = serve.make_stream(n_requests, rate * world, seed=11)[b0:b1]
     srv = serve.Server(device, mem_budget=150e9, max_batch=512)
+    barrier(device)
     _, summ = srv.run(reqs, time_limit=240)
+    if world > 1:
+        # whole-job throughput; latency percentiles are the slowest rank's
+        summ["solves_per_s"], = sum_over_ranks([summ["solves_per_s"]], device)
+        for key in ("p50_ms", "p95_ms", "p99_ms"):
+            if key in summ:
+                summ[key], = max_over_ranks([summ[key]], device)
+        summ["replicas"] = world
     summ = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in summ.items()}
     summ.update(arrival_rate_per_s=round(rate, 3),
                 serving_capacity_per_s=round(capacity, 3),
@@ -440,7 +494,7 @@ def simp3d_bench(device, reps=2):
             "host_setup_s": round(setup_s, 2), "reps": reps, "mixed": mixed}
 
 
-def batch_solve_bench(device, k, sequential_sample=8):
+def batch_solve_bench(device, k, sequential_sample=8, rank=0, world=1):
     """The batched-trajectories config: k cart-pole instances (N ~
     U{50..400}, pole mass ~ U(0.1, 0.5), final position ~ U(-1, 1), seed 0)
     solved together, one launch per IPM phase over all instances; beside it
@@ -449,23 +503,28 @@ def batch_solve_bench(device, k, sequential_sample=8):
     import torch
     from amigo_b200 import ipm_driver
     from amigo_b200.problems.cartpole import batch_config
+    from amigo_b200.problems.cartpole import CartPoleBatch
     ipm_driver.solve_batch(batch_config(k=4, seed=1), device)   # warm-up
-    B = batch_config(k=k, seed=0)
-    torch.cuda.synchronize()
+    full = batch_config(k=k, seed=0)
+    B = full if world == 1 else CartPoleBatch(shard(full.inst, rank, world))
+    barrier(device)
     t = time.perf_counter()
     r = ipm_driver.solve_batch(B, device)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t
-    torch.cuda.synchronize()
+    barrier(device)
     t = time.perf_counter()
     rm = ipm_driver.solve_batch(B, device, precision="fp32")
     torch.cuda.synchronize()
     wall_m = time.perf_counter() - t
+    wall, wall_m = max_over_ranks([wall, wall_m], device)
+    conv_all, conv_m_all = sum_over_ranks([int(r["converged"].sum()),
+                                           int(rm["converged"].sum())], device)
     same = rm["converged"] & r["converged"]
     obj_dev = (float(np.max(np.abs(rm["objective"][same] - r["objective"][same]) /
                             np.maximum(1.0, np.abs(r["objective"][same]))))
                if same.any() else None)
-    mixed = {"solves_per_s": round(int(rm["converged"].sum()) / wall_m, 3),
+    mixed = {"solves_per_s": round(conv_m_all / wall_m, 3),
              "wall_s": round(wall_m, 3), "converged": int(rm["converged"].sum()),
              "fp64_fallbacks": int(rm["fallbacks"]),
              "max_rel_objective_diff_vs_fp64": obj_dev,
@@ -480,8 +539,9 @@ def batch_solve_bench(device, k, sequential_sample=8):
         seq.append(time.perf_counter() - t1)
     return {"workload": "%d cart-pole instances, N~U{50..400}, one launch per "
                         "IPM phase, FP64" % k,
+            "replicas": world, "instances_per_rank": int(B.k),
             "n_total": int(B.n), "nnz_total": int(B.nnz),
-            "solves_per_s": round(int(r["converged"].sum()) / wall, 3),
+            "solves_per_s": round(conv_all / wall, 3),
             "wall_s": round(wall, 3), "setup_s": round(float(r["setup_s"]), 3),
             "converged": int(r["converged"].sum()),
             "unconverged": [int(i) for i in np.nonzero(~r["converged"])[0]],
@@ -735,6 +795,10 @@ def run_reference(args, rank, world):
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        relaunch_under_torchrun(args)
+    if world != args.gpus:
+        raise SystemExit("bench.py: --gpus %d but WORLD_SIZE=%d" % (args.gpus, world))
     if world > 1:
         import datetime
 
