@@ -80,6 +80,7 @@ _SIGS = {
     "ab_ldl_create": (_i, [_i, _ip, _ip, _i, _i, _d, _d, _d, ctypes.POINTER(_vp)]),
     "ab_ldl_analyze": (_i, [_i, _ip, _ip, _i, ctypes.POINTER(_vp)]),
     "ab_ldl_destroy": (_i, [_vp]),
+    "ab_ldl_mem_estimate": (_i, [_vp, _i, _d, _i, ctypes.POINTER(ctypes.c_longlong)]),
     "ab_ldl_symbolic_sizes": (_i, [_vp, _ip, _ip]),
     "ab_ldl_symbolic_arrays": (_i, [_vp, _ip, _ip, _ip, _ip, _ip, _ip, _ip]),
     "ab_ldl_factor": (_i, [_vp, _vp, _vp]),

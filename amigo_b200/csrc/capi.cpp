@@ -153,6 +153,42 @@ int ab_ldl_analyze(int n, const int* rowp, const int* cols, int order,
   return AB_OK;
 }
 
+int ab_ldl_mem_estimate(ab_ldl_t H, int precision, double delay_growth,
+                        int nrhs, long long* bytes) {
+  if (!H || !bytes || (precision != 32 && precision != 64) || nrhs < 0)
+    return AB_ERR_ARG;
+  const ab::SymbolicTree& T = H->h.sym;
+  const double g = delay_growth > 1.0 ? delay_growth : 1.0;
+  const long long el = precision == 32 ? 4 : 8;
+  long long fronts = 0, ints = 0, fsum = 0, csum = 0;
+  for (int k = 0; k < T.num_nodes; k++) {
+    const long long ns = T.node_ptr[k + 1] - T.node_ptr[k];
+    const long long nc = T.contrib_ptr[k + 1] - T.contrib_ptr[k];
+    const long long f = ns + nc;
+    fronts += f * f + f * ab::kPanel + 8;
+    ints += 4 * f + 16;
+    fsum += f;
+    csum += nc;
+  }
+  // front pool (in its element size, with room for delayed pivots), the
+  // int pool, the static plan (per-node arrays, contribution rows and their
+  // parent map, the assembly map of A: three ints per entry of the
+  // supernodes' columns, bounded by the fronts' fully-summed areas) and
+  // the solve's update vectors
+  long long plan = 64LL * (T.num_nodes + 1) + 8LL * csum + 4LL * T.n;
+  long long amap = 0;
+  for (int k = 0; k < T.num_nodes; k++) {
+    const long long ns = T.node_ptr[k + 1] - T.node_ptr[k];
+    const long long nc = T.contrib_ptr[k + 1] - T.contrib_ptr[k];
+    amap += ns * (ns + nc);
+  }
+  plan += 12LL * amap;
+  const long long solve = 8LL * fsum * (nrhs > 0 ? nrhs : 1);
+  *bytes = (long long)(g * (double)(fronts * el)) + (long long)(g * (double)(ints * 4)) +
+           plan + solve;
+  return AB_OK;
+}
+
 int ab_ldl_destroy(ab_ldl_t H) {
   if (!H) return AB_OK;
   if (H->h.has_plan) {

@@ -357,6 +357,24 @@ def analyze(n, rowp, cols, order=OrderingType.AMD):
         _lib.lib().ab_ldl_destroy(h)
 
 
+def mem_estimate(n, rowp, cols, precision=64, delay_growth=2.0, nrhs=1,
+                 order=OrderingType.AMD):
+    """Device bytes a factorization of this pattern needs (ab_ldl_mem_estimate),
+    from its symbolic analysis on the host."""
+    rowp = np.ascontiguousarray(rowp, dtype=np.int32)
+    cols = np.ascontiguousarray(cols, dtype=np.int32)
+    h = ctypes.c_void_p()
+    _lib.call("ab_ldl_analyze", int(n), _iptr(rowp), _iptr(cols), int(order),
+              ctypes.byref(h))
+    try:
+        out = ctypes.c_longlong()
+        _lib.call("ab_ldl_mem_estimate", h, int(precision), float(delay_growth),
+                  int(nrhs), ctypes.byref(out))
+        return int(out.value)
+    finally:
+        _lib.lib().ab_ldl_destroy(h)
+
+
 class BatchedSparseLDL:
     """Many independent SparseLDL problems factored and solved together:
     one launch per elimination-tree level covers the fronts of every

@@ -52,20 +52,18 @@ def make_stream(n_requests, rate, seed=0, nmin=50, nmax=400):
 _EST = {}
 
 
-def workspace_bytes(model, delay_growth=2.0):
-    """Device bytes one problem needs, from its symbolic analysis: the front
-    pool (sum over fronts of f^2 + 32 f doubles, times the delay growth),
-    the CSR values and index maps, and ~24 n-vectors of iterate and work
-    space.  Cached per pattern size (n, nnz)."""
-    from .linalg import OrderingType, analyze
-    key = (model.n, model.nnz)
+def workspace_bytes(model, delay_growth=2.0, precision=64):
+    """Device bytes one problem needs: the factorization's workspace from its
+    symbolic analysis (linalg.mem_estimate, the library's
+    ab_ldl_mem_estimate: front pool with room for delayed pivots, integer
+    pools, plan, solve vectors), plus the CSR values and ~24 n-vectors of
+    iterate and work space.  Cached per pattern (n, nnz, precision)."""
+    from .linalg import mem_estimate
+    key = (model.n, model.nnz, precision)
     if key not in _EST:
-        S = analyze(model.n, model.rowp, model.cols, OrderingType.AMD)
-        p = np.diff(S["node_ptr"]).astype(np.int64)
-        c = np.diff(S["contrib_ptr"]).astype(np.int64)
-        f = p + c
-        fronts = 8.0 * delay_growth * float(np.sum(f * f + 32 * f))
-        _EST[key] = fronts + 20.0 * model.nnz + 8.0 * 24 * model.n
+        ws = mem_estimate(model.n, model.rowp, model.cols, precision=precision,
+                          delay_growth=delay_growth)
+        _EST[key] = ws + 20.0 * model.nnz + 8.0 * 24 * model.n
     return _EST[key]
 
 

@@ -45,6 +45,17 @@ int ab_ldl_create(int n, const int* rowp, const int* cols, int order,
                   double delay_growth, ab_ldl_t* out);
 int ab_ldl_destroy(ab_ldl_t h);
 
+/* Device bytes a factorization of this pattern needs, from its symbolic
+ * analysis alone (works on analysis-only handles, no GPU needed): the front
+ * pool at `precision` (64 or 32) bits times delay_growth (room for fronts
+ * grown by delayed pivots), the integer pools, the static plan and the
+ * solve's update vectors for nrhs right-hand sides.  The admission budget
+ * of a request loop adds the caller's own vectors.  No counterpart call in
+ * the reference, whose SparseLDL sizes its pools from the same symbolic
+ * data (include/sparse_ldl.h:62-93, 3162-3220). */
+int ab_ldl_mem_estimate(ab_ldl_t h, int precision, double delay_growth,
+                        int nrhs, long long* bytes);
+
 /* Symbolic analysis only (host; makes no CUDA call).  The handle answers
  * ab_ldl_symbolic_sizes / ab_ldl_symbolic_arrays and must be released with
  * ab_ldl_destroy; ab_ldl_factor on it returns AB_ERR_UNSUPPORTED.  Mirrors

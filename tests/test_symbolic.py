@@ -114,3 +114,21 @@ def test_config_patterns_match_reference(oracle_ref, name):
     assert got["num_nodes"] == want["num_nodes"]
     for k in KEYS:
         np.testing.assert_array_equal(got[k], want[k], err_msg="%s %s" % (name, k))
+
+
+def test_mem_estimate_from_symbolic_analysis():
+    """The workspace estimate (ab_ldl_mem_estimate) covers the fronts'
+    static sizes times the delay growth, halves the front pool for FP32
+    fronts, and grows with the number of right-hand sides; no GPU needed."""
+    M = kkt_matrix(500, 300, 5)
+    n, rp, ci, _ = csr_arrays(M)
+    S = linalg.analyze(n, rp, ci, linalg.OrderingType.AMD)
+    f = (np.diff(S["node_ptr"]) + np.diff(S["contrib_ptr"])).astype(np.int64)
+    fronts = 8 * np.sum(f * f + 32 * f)
+    e64 = linalg.mem_estimate(n, rp, ci, precision=64, delay_growth=2.0)
+    e64_1 = linalg.mem_estimate(n, rp, ci, precision=64, delay_growth=1.0)
+    e32 = linalg.mem_estimate(n, rp, ci, precision=32, delay_growth=2.0)
+    e64_4 = linalg.mem_estimate(n, rp, ci, precision=64, delay_growth=2.0, nrhs=4)
+    assert e64 >= 2 * fronts and e64_1 >= fronts
+    assert e32 < e64 and e64 - e32 >= fronts * 0.99
+    assert e64_4 > e64
