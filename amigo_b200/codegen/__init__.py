@@ -1,0 +1,16 @@
+"""Device code generation for component groups.
+
+`Component` declares a component the way amigo does (inputs, data,
+constants, constraints, objective, compute()); `GeneratedModel` assembles
+groups of component instances into a KKT problem and compiles straight-line
+CUDA evaluators of each component's Lagrangian gradient and Hessian, with
+the gradient and the CSR Hessian scatter on the device.
+"""
+from .component import Component
+from .expr import (acos, asin, atan, cos, cosh, exp, fabs, log, log10, sin,
+                   sinh, sqrt, tan, tanh)
+from .model import GeneratedModel, Group, host_evaluator
+
+__all__ = ["Component", "GeneratedModel", "Group", "host_evaluator", "sin", "cos",
+           "tan", "exp", "log", "log10", "sqrt", "tanh", "sinh", "cosh", "asin",
+           "acos", "atan", "fabs"]

@@ -69,29 +69,42 @@ def solve(backend, options=None, verbose=False):
             break
         # inertia-corrected factorization
         diag = B.diagonal(st)
-        dw, dc = 0.0, 0.0
         want = (B.np, B.nc)
-        for attempt in range(41):
-            inertia = B.factor(st, diag, dw, dc)
-            if inertia == want:
-                break
-            n_ic += 1
-            if inertia[0] + inertia[1] < B.n and dc == 0.0:
-                dc = o["dc"] * mu ** o["kappa_c"]
-            if dw == 0.0:
-                dw = o["dw_first"] if dw_last == 0.0 else max(o["dw_min"],
-                                                              o["kw_minus"] * dw_last)
-            else:
-                dw *= o["kw_plus_first"] if dw_last == 0.0 else o["kw_plus"]
-            if dw > o["dw_max"]:
-                break
-        if dw > 0.0:
-            dw_last = dw
+
+        def factorize(force_fp64):
+            dw, dc, n = 0.0, 0.0, 0
+            for attempt in range(41):
+                inertia = (B.factor(st, diag, dw, dc, force_fp64=True) if force_fp64
+                           else B.factor(st, diag, dw, dc))
+                if inertia == want:
+                    break
+                n += 1
+                if inertia[0] + inertia[1] < B.n and dc == 0.0:
+                    dc = o["dc"] * mu ** o["kappa_c"]
+                if dw == 0.0:
+                    dw = o["dw_first"] if dw_last == 0.0 else max(o["dw_min"],
+                                                                  o["kw_minus"] * dw_last)
+                else:
+                    dw *= o["kw_plus_first"] if dw_last == 0.0 else o["kw_plus"]
+                if dw > o["dw_max"]:
+                    break
+            return dw, n
+
+        dw, n = factorize(False)
+        n_ic += n
         # Newton direction
         res = B.residual(mu, st, g)
         px = B.solve(res)
-        if o["refine_steps"]:
+        if o["refine_steps"] and not B.refine(mu, st, g, res, px, o["refine_steps"]):
+            # the FP32 factor's inertia was accepted but the FP64 factor of
+            # the same matrix has another one: correct the inertia in FP64
+            dw, n = factorize(True)
+            n_ic += n
+            res = B.residual(mu, st, g)
+            px = B.solve(res)
             B.refine(mu, st, g, res, px, o["refine_steps"])
+        if dw > 0.0:
+            dw_last = dw
         upd = B.update(mu, st, px)
         tau = max(o["tau_min"], 1.0 - mu)
         ax, az = B.max_step(tau, st, upd)
@@ -160,7 +173,10 @@ def solve_batch(model, device="cuda", options=None, verbose=False,
 
 
 class CartPoleProblem:
-    """Device KKT problem for the cart-pole model (problems/cartpole.py)."""
+    """Device KKT problem for a model whose device_model() gives gradient,
+    hessian and objective(x, out) kernels: the cart-pole model
+    (problems/cartpole.py) or a generated component model
+    (codegen.GeneratedModel)."""
 
     def __init__(self, model, device="cuda"):
         from .linalg import CSRMat
@@ -169,6 +185,9 @@ class CartPoleProblem:
         self.dm = model.device_model(self.device)
         self._csr = CSRMat
         self._obj = torch.zeros(1, dtype=torch.float64, device=self.device)
+
+    def get_multiplier_indicator(self):
+        return self.model.mult
 
     def create_matrix(self):
         m = self.model
@@ -186,6 +205,42 @@ class CartPoleProblem:
     def objective(self, x):
         self.dm.objective(x, self._obj)
         return float(self._obj.item())
+
+
+GeneratedProblem = CartPoleProblem
+
+
+class SimpProblem:
+    """Device KKT problem for the SIMP compliance models (problems/simp2d.py,
+    problems/simp3d.py); the objective is the compliance f^T u."""
+
+    def __init__(self, model, device="cuda"):
+        from .linalg import CSRMat
+        self.model = model
+        self.device = torch.device(device)
+        self.dm = model.device_model(self.device)
+        self._csr = CSRMat
+        self._f = torch.from_numpy(np.ascontiguousarray(model.f)).to(self.device)
+
+    def get_multiplier_indicator(self):
+        return self.model.mult
+
+    def create_matrix(self):
+        m = self.model
+        return self._csr(m.n, m.n, m.rowp, m.cols, device=self.device,
+                         diag_pos=m.diag_pos)
+
+    def hessian(self, alpha, x, hess):
+        self.dm.hessian(x, alpha, hess.vals)
+
+    def gradient(self, alpha, x, g):
+        self.dm.gradient(x, alpha, g)
+
+    def add_diagonal(self, diag, hess):
+        hess.add_diagonal(diag)
+
+    def objective(self, x):
+        return float(torch.dot(self._f, x).item())
 
 
 class DeviceBackend:
@@ -206,7 +261,9 @@ class DeviceBackend:
         self.m = model
         self.device = torch.device(device)
         self.precision = precision
-        self.fallbacks = 0
+        self.fallbacks = 0          # stalled FP32 refinements redone in FP64
+        self.inertia_fallbacks = 0  # FP32 inertia mismatches refactored in FP64
+        self.fp64_now = precision != "fp32"
         self.solver = B200Solver(problem, order=OrderingType.AMD,
                                  precision=precision)
         self.opt = InteriorPointOptimizer(model.mult, model.lower, model.upper,
@@ -259,13 +316,31 @@ class DeviceBackend:
         self.opt.compute_diagonal(st, self.diag)
         return self.diag
 
-    def factor(self, st, diag, dw, dc):
+    def factor(self, st, diag, dw, dc, force_fp64=False):
+        """Factor K + diag(diag + dw on primals - dc on multipliers); returns
+        the inertia.  FP32 fronts are kept only when their inertia is the
+        one the inertia correction wants, (n_primal, n_constraints): a
+        mismatch may be an FP32 artefact (eigenvalues below FP32
+        resolution), so the correction loop decides on the FP64 factor's
+        inertia instead."""
         torch.add(diag, self.primal, alpha=dw, out=self.dtot)
         if dc:
             self.dtot.sub_(1.0 - self.primal, alpha=dc)
         self._fx = st.x
+        self.fp64_now = self.precision != "fp32" or force_fp64
+        if self.precision == "fp32" and force_fp64:
+            self.solver.set_precision("fp64")
         self.solver.factor(1.0, st.x, self.dtot)
-        return self.solver.get_inertia()
+        inertia = self.solver.get_inertia()
+        if self.precision == "fp32" and not force_fp64 and inertia != (self.np, self.nc):
+            self.inertia_fallbacks += 1
+            self.solver.set_precision("fp64")
+            self.solver.factor(1.0, st.x, self.dtot)
+            inertia = self.solver.get_inertia()
+            self.fp64_now = True
+        if self.precision == "fp32":
+            self.solver.set_precision("fp32")
+        return inertia
 
     def residual(self, mu, st, g):
         self.opt.compute_residual(mu, st, g, self.res)
@@ -276,21 +351,31 @@ class DeviceBackend:
         return self.px
 
     def refine(self, mu, st, g, res, px, steps):
-        if self.precision == "fp32":
+        """Iterative refinement of the Newton direction px.  Returns False
+        when the FP32 factor's refinement stalled and the FP64
+        refactorization of the same matrix has an inertia other than
+        (n_primal, n_constraints): the caller then redoes the inertia
+        correction on FP64 factors."""
+        mixed = self.precision == "fp32" and not self.fp64_now
+        if mixed:
             steps = max(steps, self.mixed_refine_steps)
         self.solver.iterative_refinement(mu, self.m.mult, res, st, g,
                                          self._lbx, self._ubx, px, None, None,
                                          max_steps=steps + 1)
-        if self.precision == "fp32" and self.solver.last_refinement[1] > 1e-10:
+        if mixed and self.solver.last_refinement[1] > 1e-10:
             # refinement stalled on the FP32 factor: refactor in FP64
             self.fallbacks += 1
             self.solver.set_precision("fp64")
             self.solver.factor(1.0, self._fx, self.dtot)
+            self.fp64_now = True
+            self.solver.set_precision("fp32")
+            if self.solver.get_inertia() != (self.np, self.nc):
+                return False
             self.solver.solve(res, px)
             self.solver.iterative_refinement(mu, self.m.mult, res, st, g,
                                              self._lbx, self._ubx, px, None,
                                              None, max_steps=steps + 1)
-            self.solver.set_precision("fp32")
+        return True
 
     def update(self, mu, st, px):
         self.opt.compute_update(mu, st, px, self.upd)

@@ -189,6 +189,11 @@ class Simp2D:
         self.fixed_zero_pos = np.nonzero(zero)[0].astype(np.int32)
         self.fixed_diag_pos = self.diag_pos[self.fixed].astype(np.int32)
 
+    @property
+    def x0(self):
+        """The initial point (initial_point()), as the IPM driver reads it."""
+        return self.initial_point()
+
     def initial_point(self):
         """x0: u = 0, rt from the element densities averaged to nodes,
         re = 0.4 + U(-0.01, 0.01), s = v^T re - 0.4 clipped below 0,

@@ -195,6 +195,11 @@ class Simp3D:
         self.fixed_zero_pos = np.nonzero(zero)[0].astype(np.int32)
         self.fixed_diag_pos = self.diag_pos[self.fixed].astype(np.int32)
 
+    @property
+    def x0(self):
+        """The initial point (initial_point()), as the IPM driver reads it."""
+        return self.initial_point()
+
     def initial_point(self):
         x = np.zeros(self.n)
         cnt = np.zeros(self.nnodes)

@@ -88,7 +88,7 @@ class HostBackend:
     def diagonal(self, st):
         return self.ipm.compute_diagonal(st.tup(), self.n)
 
-    def factor(self, st, diag, dw, dc):
+    def factor(self, st, diag, dw, dc, force_fp64=False):
         vals = self.D.hessian_values(self.m, st.x, 1.0)
         vals[self.m.diag_pos] += diag + dw * self.primal - dc * (1.0 - self.primal)
         self.vals = vals
@@ -107,6 +107,7 @@ class HostBackend:
             K, self.ldl.solve, mu, self.m.mult, res, g, st.zl, st.zu, st.sl,
             st.su, self.lbx, self.ubx, px, max_steps=steps + 1)
         px[:] = out
+        return True
 
     def update(self, mu, st, px):
         dzl, dzu = self.ipm.compute_bound_dual_step(mu, st.tup(), px)
