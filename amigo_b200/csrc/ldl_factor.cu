@@ -49,6 +49,12 @@ constexpr int kPanelWideRows = 2048;
 // Shared memory of the large-front panel kernel for its copy of the
 // panel's L columns (the static control block aside).
 constexpr int kPanelCacheBytes = 200 * 1024;
+// Shared-W panel (k_big_panel_sw): threads, rows per thread, and the
+// dynamic shared memory for the panel's W columns.  Levels whose largest
+// static front has at most kSwThreads * kSwRows rows take it.
+constexpr int kSwThreads = 512;
+constexpr int kSwRows = 4;
+constexpr int kSwSmemBytes = 200 * 1024;
 constexpr int kTile = 64;
 // Right-looking small-front kernel: rows of room for delayed pivots, and
 // its block size (measured on 68-row fronts: 32 threads 11.9 ms, 64 9.7,
@@ -171,6 +177,72 @@ __device__ void update_tile(T* F, int ld, const T* W, int ldw,
       const int c = c0 + tc + 16 * b;
       if (r < n && c < n && r >= c) F[r + (size_t)c * ld] -= acc[a][b];
     }
+  }
+  __syncthreads();
+}
+
+// FP64 C tile on the FP64 tensor path: mma.sync m8n8k4 (DMMA), the same
+// tile and operands as update_tile.  A and B are staged row-major with a
+// row stride of TPD = 36 doubles, which puts the 4 x 4 (row, k) pattern of
+// each half-warp's fragment loads on 16 distinct bank pairs; k is padded
+// with zeros to a multiple of 4.  8 warps as 2 x 4, each a 32 x 16 block of
+// the 64 x 64 tile: 4 x 2 MMA tiles of 8 x 8.  Fragment layouts (PTX ISA,
+// mma.m8n8k4 .f64): a0 at (lane / 4, lane % 4), b0 at (k = lane % 4,
+// n = lane / 4), c0 / c1 at (lane / 4, 2 (lane % 4) + 0 / 1).
+constexpr int TPD = 36;
+constexpr int kTileSmemD = 2 * kTile * TPD;  // doubles
+
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a,
+                                           double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, "
+      "{%0, %1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+__device__ void update_tile_dmma(double* F, int ld, const double* W, int ldw,
+                                 int n, int k, int kstart, int kw, int ti,
+                                 int tj, double* As, double* Bs) {
+  const int tid = threadIdx.x;
+  const int r0 = k + ti * kTile, c0 = k + tj * kTile;
+  const int kp = (kw + 3) & ~3;
+  for (int idx = tid; idx < kTile * kp; idx += NT) {
+    const int rr = idx % kTile, jj = idx / kTile;
+    const bool in = jj < kw;
+    As[rr * TPD + jj] = (in && r0 + rr < n) ? F[r0 + rr + (size_t)(kstart + jj) * ld] : 0.0;
+    Bs[rr * TPD + jj] = (in && c0 + rr < n) ? W[c0 + rr + (size_t)jj * ldw] : 0.0;
+  }
+  __syncthreads();
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;
+  const int g = lane >> 2, q = lane & 3;
+  double acc[4][2][2];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 2; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+  for (int kk = 0; kk < kp; kk += 4) {
+    double af[4], bf[2];
+#pragma unroll
+    for (int a = 0; a < 4; a++) af[a] = As[(wr + 8 * a + g) * TPD + kk + q];
+#pragma unroll
+    for (int b = 0; b < 2; b++) bf[b] = Bs[(wc + 8 * b + g) * TPD + kk + q];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 2; b++) dmma_8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    const int r = r0 + wr + 8 * a + g;
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int c = c0 + wc + 8 * b + 2 * q + e;
+        if (r < n && c < n && r >= c) F[r + (size_t)c * ld] -= acc[a][b][e];
+      }
   }
   __syncthreads();
 }
@@ -1151,6 +1223,356 @@ k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Large-front panel with the panel's W columns in shared memory.
+//
+// The same pivot rule, candidate order, interchanges and outputs as
+// panel_factor (the reference's left-looking-in-panel scheme), arranged so
+// that one candidate column costs one block reduction and one barrier in
+// the common case (a 1x1 pivot without interchange):
+//   * W[kstart:, 0:kw] (the panel's unscaled L*D columns) lives in shared
+//     memory, column-major with leading dimension cld = f - kstart, so a
+//     column build reads only shared memory: L[r, j] is recomputed from W
+//     with the same expression that writes it to F (W[r, j] * dinv_j for a
+//     1x1 pivot; the D^-1 combination of the two W columns of a 2x2 pivot);
+//   * each thread owns the rows kstart + tid + PT * i (i < RPT) for the
+//     whole panel and keeps their entries of the next candidate column of
+//     F, loaded one step ahead (reloaded after an interchange or a delay);
+//   * the L columns are written to F and the W rows to HBM once, at the end
+//     of the panel (the trailing-update kernel reads both there).
+// The panel width adapts to the shared memory: nbe = min(kPanel,
+// smem / (cld * sizeof(T))) columns, at least 4.
+template <int PT>
+struct SwCtl {
+  // reduction slots by step parity and kind (candidate column, column
+  // imax): a step's slots are written again two steps later, after the
+  // next step's barrier, so no barrier is needed at the end of a step
+  double red_v[4][PT / 32];
+  int red_i[4][PT / 32];
+  double red_v2[4][PT / 32];
+  double wkk[2], wii;
+  double cA[NB], cB[NB];   // L[r, j] = W[r, j] cA[j] + W[r, partner] cB[j]
+  int kind[NB];            // 0: 1x1, 1 / 2: first / second column of a 2x2
+};
+
+// Block-wide first-argmax of (v, i) and max of v2 in every thread, in
+// reduction slot `set`.
+template <int PT>
+__device__ __forceinline__ void sw_reduce(SwCtl<PT>& c, int set, double& v,
+                                          int& i, double& v2) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    const double ov2 = __shfl_xor_sync(0xffffffffu, v2, o);
+    argmax_merge(v, i, ov, oi);
+    v2 = fmax(v2, ov2);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    c.red_v[set][warp] = v;
+    c.red_i[set][warp] = i;
+    c.red_v2[set][warp] = v2;
+  }
+  __syncthreads();
+  v = lane < PT / 32 ? c.red_v[set][lane] : -1.0;
+  i = lane < PT / 32 ? c.red_i[set][lane] : 0x7fffffff;
+  v2 = lane < PT / 32 ? c.red_v2[set][lane] : 0.0;
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    const double ov2 = __shfl_xor_sync(0xffffffffu, v2, o);
+    argmax_merge(v, i, ov, oi);
+    v2 = fmax(v2, ov2);
+  }
+}
+
+// acc[i] -= sum_j L[r_i, j] * y[j] over the panel's columns j < kw, with
+// L recomputed from the shared W columns; y[j] = W[yrow, j] of the column
+// being built.
+template <class T, int PT, int RPT>
+__device__ __forceinline__ void sw_apply_panel(const T* __restrict__ Ws, int cld,
+                                               int kw, int yrow, const SwCtl<PT>& c,
+                                               const int (&rr)[RPT],
+                                               const bool (&on)[RPT], T (&acc)[RPT]) {
+  for (int j = 0; j < kw;) {
+    const T* w0 = Ws + (size_t)j * cld;
+    if (c.kind[j] == 0) {
+      const T a = T(c.cA[j]), y = w0[yrow];
+#pragma unroll
+      for (int i = 0; i < RPT; i++)
+        if (on[i]) acc[i] -= (w0[rr[i]] * a) * y;
+      j += 1;
+    } else {
+      const T* w1 = w0 + cld;
+      const T i00 = T(c.cA[j]), i10 = T(c.cB[j]);
+      const T i11 = T(c.cA[j + 1]), i01 = T(c.cB[j + 1]);
+      const T y0 = w0[yrow], y1 = w1[yrow];
+#pragma unroll
+      for (int i = 0; i < RPT; i++)
+        if (on[i]) {
+          const T a0 = w0[rr[i]], a1 = w1[rr[i]];
+          const T l0 = a0 * i00 + a1 * i10, l1 = a0 * i01 + a1 * i11;
+          acc[i] -= l0 * y0;
+          acc[i] -= l1 * y1;
+        }
+      j += 2;
+    }
+  }
+}
+
+// Rows a and b interchanged in the shared W columns [0, ncol).
+template <class T, int PT>
+__device__ __forceinline__ void sw_swap_rows(T* Ws, int cld, int ncol, int a,
+                                             int b) {
+  for (int j = threadIdx.x; j < ncol; j += PT) {
+    T t = Ws[a + (size_t)j * cld];
+    Ws[a + (size_t)j * cld] = Ws[b + (size_t)j * cld];
+    Ws[b + (size_t)j * cld] = t;
+  }
+}
+
+template <class T, int PT, int RPT>
+__device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
+                                int* vars, int* fsperm, double ustab,
+                                double pivot_tol, int* status, SwCtl<PT>& c,
+                                T* Ws, int nbe, int& k_, int& nc_, int& kw_) {
+  const int tid = threadIdx.x;
+  int k = k_, nc = nc_, kw = 0;
+  const int kstart = k;
+  const int cld = n - kstart;
+  int rr[RPT];       // owned rows relative to kstart
+  bool on[RPT];
+  T cur[RPT];        // F[r, k] of the candidate column
+#pragma unroll
+  for (int i = 0; i < RPT; i++) rr[i] = tid + PT * i;
+  auto load_col = [&](int col, T (&dst)[RPT]) {
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+      const int r = kstart + rr[i];
+      dst[i] = (r >= col && r < n) ? F[r + (size_t)col * ld] : T(0);
+    }
+  };
+  load_col(k, cur);
+  int par = 0;
+  while (kw < nbe - 1 && k < nc) {
+    par ^= 1;
+    // F[r, k + 1] for the next step, valid unless this step interchanges
+    // rows or delays the candidate
+    T nxt[RPT];
+    load_col(k + 1, nxt);
+    // --- candidate column k: W[:, kw] = F[:, k] - L_panel W[k, :]^T
+    T acc[RPT];
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+      acc[i] = cur[i];
+      on[i] = kstart + rr[i] >= k && kstart + rr[i] < n;
+    }
+    const int krow = k - kstart;
+    sw_apply_panel<T, PT, RPT>(Ws, cld, kw, krow, c, rr, on, acc);
+    double bv = -1.0, tv = 0.0;
+    int bi = 0x7fffffff;
+    T* wcol = Ws + (size_t)kw * cld;
+#pragma unroll
+    for (int i = 0; i < RPT; i++)
+      if (on[i]) {
+        const int r = kstart + rr[i];
+        wcol[rr[i]] = acc[i];
+        const double a = fabs((double)acc[i]);
+        if (r == k) c.wkk[par] = (double)acc[i];
+        else if (r < nc) argmax_merge(bv, bi, a, r);
+        else tv = fmax(tv, a);
+      }
+    sw_reduce<PT>(c, 2 * par, bv, bi, tv);
+    int imax = bi;
+    if (imax >= nc || imax <= k) {
+      if (k + 1 < nc && tid == 0) atomicOr(status, ST_NAN);
+      imax = (k + 1 < n) ? k + 1 : k;
+    }
+    const double wkk = c.wkk[par];
+    const PivotChoice pc = choose_pivot(
+        root, k, nc, wkk, imax, bv < 0.0 ? 0.0 : bv, tv, ustab, pivot_tol, [&]() {
+          // column imax: F[imax, r] for r < imax, F[r, imax] below, minus
+          // the panel's update with W row imax, into W[:, kw + 1]
+          const double wik = (double)wcol[imax - kstart];
+          T a2[RPT];
+#pragma unroll
+          for (int i = 0; i < RPT; i++) {
+            const int r = kstart + rr[i];
+            a2[i] = !on[i] ? T(0)
+                           : (r < imax ? F[imax + (size_t)r * ld] : F[r + (size_t)imax * ld]);
+          }
+          sw_apply_panel<T, PT, RPT>(Ws, cld, kw, imax - kstart, c, rr, on, a2);
+          double rv = -1.0, rt = 0.0;
+          int ri = 0x7fffffff;
+          T* w2 = Ws + (size_t)(kw + 1) * cld;
+#pragma unroll
+          for (int i = 0; i < RPT; i++)
+            if (on[i]) {
+              const int r = kstart + rr[i];
+              w2[rr[i]] = a2[i];
+              if (r == imax) c.wii = (double)a2[i];
+              else rt = fmax(rt, fabs((double)a2[i]));
+            }
+          sw_reduce<PT>(c, 2 * par + 1, rv, ri, rt);
+          return ImaxColumn{rt, c.wii, wik};
+        });
+    // every thread holds its decision inputs: the writes below may follow
+    if (pc.step == 0) {
+      // delay candidate k: move it to the end of the candidate set
+      if (k < nc - 1) {
+        __syncthreads();
+        symm_swap<T, PT>(F, ld, n, vars, fsperm, k, nc - 1);
+        sw_swap_rows<T, PT>(Ws, cld, kw, krow, nc - 1 - kstart);
+        __syncthreads();
+      }
+      nc -= 1;
+      load_col(k, cur);
+      continue;
+    }
+    const int step = pc.step, kpiv = pc.kpiv;
+    const int ksrc = k + step - 1;
+    bool swapped = false;
+    if (pc.imax_1x1) {
+      // column imax is the pivot column: its W column replaces column k's
+      __syncthreads();
+      T* w2 = Ws + (size_t)(kw + 1) * cld;
+#pragma unroll
+      for (int i = 0; i < RPT; i++)
+        if (on[i]) wcol[rr[i]] = w2[rr[i]];
+    }
+    if (kpiv != ksrc) {
+      __syncthreads();
+      symm_swap<T, PT>(F, ld, n, vars, fsperm, ksrc, kpiv);
+      sw_swap_rows<T, PT>(Ws, cld, kw + step, ksrc - kstart, kpiv - kstart);
+      swapped = true;
+    }
+    if (swapped || step == 2 || pc.imax_1x1) __syncthreads();
+    if (step == 1 && !swapped) {
+      // the common step: every thread sets the column's coefficients (the
+      // same value), so the next step needs no barrier before reading them
+      const T d = Ws[(size_t)kw * cld + krow];
+      if (!isfinite((double)d) && tid == 0) atomicOr(status, ST_NAN);
+      c.kind[kw] = 0;
+      c.cA[kw] = pc.zero ? 0.0 : (double)(T(1) / d);
+      c.cB[kw] = 0.0;
+      if (tid == 0) vars[3 * ld + k] = 0;
+    } else if (tid == 0) {
+      if (step == 1) {
+        const T d = Ws[(size_t)kw * cld + krow];
+        if (!isfinite((double)d)) atomicOr(status, ST_NAN);
+        c.kind[kw] = 0;
+        c.cA[kw] = pc.zero ? 0.0 : (double)(T(1) / d);
+        c.cB[kw] = 0.0;
+        vars[3 * ld + k] = 0;
+      } else {
+        const T d11 = Ws[(size_t)kw * cld + krow];
+        const T d21 = Ws[(size_t)kw * cld + krow + 1];
+        const T d22 = Ws[(size_t)(kw + 1) * cld + krow + 1];
+        const T detinv = T(1) / (d11 * d22 - d21 * d21);
+        if (!isfinite((double)detinv)) atomicOr(status, ST_NAN);
+        c.kind[kw] = 1;
+        c.kind[kw + 1] = 2;
+        c.cA[kw] = (double)(d22 * detinv);       // i00
+        c.cB[kw] = (double)(-d21 * detinv);      // i10
+        c.cA[kw + 1] = (double)(d11 * detinv);   // i11
+        c.cB[kw + 1] = (double)(-d21 * detinv);  // i01
+        vars[k] = -(vars[k] + 1);
+        vars[k + 1] = -(vars[k + 1] + 1);
+        vars[3 * ld + k] = 1;
+        vars[3 * ld + k + 1] = 2;
+      }
+    }
+    if (swapped || step == 2) __syncthreads();
+    k += step;
+    kw += step;
+    if (!swapped && step == 1) {
+#pragma unroll
+      for (int i = 0; i < RPT; i++) cur[i] = nxt[i];
+    } else {
+      load_col(k, cur);
+    }
+  }
+  // --- write the panel's L columns to F and its W rows below k to HBM
+  __syncthreads();
+  for (int j = 0; j < kw; j++) {
+    const int col = kstart + j;
+    const int kd = c.kind[j];
+    const T* w0 = Ws + (size_t)j * cld;
+    T* Fc = F + (size_t)col * ld;
+    if (kd == 0) {
+      const T a = T(c.cA[j]);
+      if (tid == 0) Fc[col] = w0[j];
+      for (int r = col + 1 + tid; r < n; r += PT) Fc[r] = w0[r - kstart] * a;
+    } else {
+      const int j0 = kd == 1 ? j : j - 1;
+      const T* wa = Ws + (size_t)j0 * cld;
+      const T* wb = wa + cld;
+      const T i00 = T(c.cA[j0]), i10 = T(c.cB[j0]);
+      const T i11 = T(c.cA[j0 + 1]), i01 = T(c.cB[j0 + 1]);
+      const int c0 = kstart + j0;
+      if (tid == 0) {
+        if (kd == 1) {
+          Fc[col] = wa[j0];
+          Fc[col + 1] = wa[j0 + 1];
+        } else {
+          Fc[col] = wb[j0 + 1];
+        }
+      }
+      for (int r = c0 + 2 + tid; r < n; r += PT) {
+        const T a0 = wa[r - kstart], a1 = wb[r - kstart];
+        Fc[r] = kd == 1 ? a0 * i00 + a1 * i10 : a0 * i01 + a1 * i11;
+      }
+    }
+    for (int r = k + tid; r < n; r += PT) Wg[r + (size_t)j * ld] = w0[r - kstart];
+  }
+  k_ = k;
+  nc_ = nc;
+  kw_ = kw;
+}
+
+template <class T, int PT, int RPT>
+__global__ void __launch_bounds__(PT)
+k_big_panel_sw(DevicePlan d, const int* __restrict__ nodes, double ustab,
+               double pivot_tol, int smem_bytes) {
+  __shared__ SwCtl<PT> c;
+  __shared__ CtlT<PT> ctl;
+  extern __shared__ double sw_raw[];
+  if (big_skip(d)) return;
+  const int node = nodes[blockIdx.x];
+  int* st = d.pstate + 4 * node;
+  int k = st[0], nc = st[1];
+  if (k >= nc) {
+    if (threadIdx.x == 0) st[3] = 0;
+    return;
+  }
+  const int f = d.f[node];
+  const int fs = d.ns[node] + d.ndin[node];
+  T* F = reinterpret_cast<T*>(d.fpool) + d.foff[node];
+  T* W = F + (size_t)f * f;
+  int* fvars = d.ipool + d.ioff[node];
+  const int kstart = k;
+  int kw = 0;
+  const long long cld = f - kstart;
+  const long long fit = (long long)smem_bytes / (cld * (long long)sizeof(T));
+  const int nbe = (int)(fit < NB ? fit : NB);
+  if (nbe >= 4 && cld <= (long long)PT * RPT) {
+    panel_factor_sw<T, PT, RPT>(F, f, W, f, fs == f, fvars, fvars + f, ustab,
+                                pivot_tol, d.status, c, reinterpret_cast<T*>(sw_raw),
+                                nbe, k, nc, kw);
+  } else {
+    // front grown past what this launch's shared memory holds (delayed
+    // pivots): the HBM-panel form
+    panel_factor<T, PT>(F, f, W, f, f, fs == f, fvars, fvars + f, ustab,
+                        pivot_tol, d.status, ctl, k, nc, kw);
+  }
+  if (threadIdx.x == 0) {
+    st[0] = k;
+    st[1] = nc;
+    st[2] = kstart;
+    st[3] = kw;
+  }
+}
+
 template <class T>
 __global__ void __launch_bounds__(NT)
 k_big_update(DevicePlan d, const int* __restrict__ nodes) {
@@ -1171,8 +1593,12 @@ k_big_update(DevicePlan d, const int* __restrict__ nodes) {
   for (int t = blockIdx.y; t < ntiles; t += gridDim.y) {
     int ti, tj;
     tile_coords(t, ti, tj);
-    update_tile(F, f, W, f, f, k, kstart, kw, ti, tj, tiles,
-                tiles + kTile * TP);
+    if constexpr (sizeof(T) == 8)
+      update_tile_dmma(F, f, W, f, f, k, kstart, kw, ti, tj, tiles,
+                       tiles + kTile * TPD);
+    else
+      update_tile(F, f, W, f, f, k, kstart, kw, ti, tj, tiles,
+                  tiles + kTile * TP);
   }
 }
 
@@ -1252,13 +1678,16 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                                kMaxDynSmem));
     FCUDA(cudaFuncSetAttribute(k_big_update<T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               kTileSmem * sizeof(T)));
+                               (sizeof(T) == 8 ? kTileSmemD : kTileSmem) * sizeof(T)));
     FCUDA(cudaFuncSetAttribute(k_big_panel<T, kPanelThreads>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kPanelCacheBytes));
     FCUDA(cudaFuncSetAttribute(k_big_panel<T, kPanelThreadsWide>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kPanelCacheBytes));
+    FCUDA(cudaFuncSetAttribute(k_big_panel_sw<T, kSwThreads, kSwRows>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kSwSmemBytes));
     FCUDA(cudaFuncSetAttribute(k_big_update_tc,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::kSmemBytes));
@@ -1312,7 +1741,26 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       const long long ntc = (fm + tc::TM - 1) / tc::TM;
       const int gtc = (int)std::max<long long>(
           1, std::min<long long>(3 * 148, ntc * (ntc + 1) / 2));
-      int panels = (int)((L.big_max_fs + NB - 2) / (NB - 1)) + 2;
+      // shared-W panel for levels whose fronts fit its rows; its shared
+      // memory holds up to NB columns of W for the largest static front
+      // (fronts grown by delayed pivots get fewer columns)
+      const bool use_sw = fm <= (long long)kSwThreads * kSwRows;
+      const int sw_smem = (int)std::min<long long>(
+          kSwSmemBytes, (fm + kRlSlack) * NB * (long long)sizeof(T));
+      // panels a front of big_max_fs candidates needs without delays: each
+      // takes nbe - 1 pivots, nbe growing as the remaining rows shrink
+      int panels = 0;
+      if (use_sw) {
+        for (long long kk = 0; kk < L.big_max_fs; panels++) {
+          const long long rows = std::max<long long>(fm - kk, 1);
+          const long long nbe = std::min<long long>(
+              NB, sw_smem / (rows * (long long)sizeof(T)));
+          kk += std::max<long long>(nbe - 1, 1);
+        }
+        panels += 2;
+      } else {
+        panels = (int)((L.big_max_fs + NB - 2) / (NB - 1)) + 2;
+      }
       // Every panel consumes at least one candidate of every unfinished
       // front, so no front needs more panels than it has rows.
       long long budget = 0;
@@ -1320,7 +1768,10 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       for (;;) {
         budget += panels;
         for (int it = 0; it < panels; it++) {
-          if (fm > kPanelWideRows)
+          if (use_sw)
+            k_big_panel_sw<T, kSwThreads, kSwRows><<<B, kSwThreads, sw_smem, s>>>(
+                d, nodes, h.ustab, h.pivot_tol, sw_smem);
+          else if (fm > kPanelWideRows)
             k_big_panel<T, kPanelThreadsWide><<<B, kPanelThreadsWide, panel_cache, s>>>(
                 d, nodes, h.ustab, h.pivot_tol, panel_cache);
           else
@@ -1331,7 +1782,8 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
             { k_big_update_tc<<<dim3(B, gtc), tc::kThreads, tc::kSmemBytes, s>>>(
                 d, nodes); ab::count_launch(); }
           } else {
-            { k_big_update<T><<<dim3(B, std::max(gu, 1)), NT, kTileSmem * sizeof(T), s>>>(
+            { k_big_update<T><<<dim3(B, std::max(gu, 1)), NT,
+                                (sizeof(T) == 8 ? kTileSmemD : kTileSmem) * sizeof(T), s>>>(
                 d, nodes); ab::count_launch(); }
           }
         }
