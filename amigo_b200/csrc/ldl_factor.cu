@@ -1253,7 +1253,88 @@ struct SwCtl {
   double wkk[2], wii;
   double cA[NB], cB[NB];   // L[r, j] = W[r, j] cA[j] + W[r, partner] cB[j]
   int kind[NB];            // 0: 1x1, 1 / 2: first / second column of a 2x2
+  // row interchanges of the panel's pivots not yet applied to the columns
+  // left of the panel, and their composition (rows[t] <- src[t])
+  int swa[NB], swb[NB], nsw;
+  int rows[2 * NB], src[2 * NB], nrows;
 };
+
+// Apply the pending interchanges to the columns [0, kstart) left of the
+// panel: thread 0 composes them into one row map, then each warp takes
+// columns and its lanes move the rows of the map (loads before stores).
+template <class T, int PT>
+__device__ void sw_flush_left(T* F, int ld, int kstart, SwCtl<PT>& c) {
+  __syncthreads();
+  if (c.nsw == 0) return;
+  if (threadIdx.x == 0) {
+    int nr = 0;
+    for (int s = 0; s < c.nsw; s++) {
+      const int pr[2] = {c.swa[s], c.swb[s]};
+      int at[2];
+      for (int u = 0; u < 2; u++) {
+        at[u] = -1;
+        for (int t = 0; t < nr; t++)
+          if (c.rows[t] == pr[u]) at[u] = t;
+        if (at[u] < 0) {
+          c.rows[nr] = pr[u];
+          c.src[nr] = pr[u];
+          at[u] = nr++;
+        }
+      }
+      const int tmp = c.src[at[0]];
+      c.src[at[0]] = c.src[at[1]];
+      c.src[at[1]] = tmp;
+    }
+    c.nrows = nr;
+    c.nsw = 0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nr = c.nrows;
+  for (int j = warp; j < kstart; j += PT / 32) {
+    T* Fj = F + (size_t)j * ld;
+    const T v0 = lane < nr ? Fj[c.src[lane]] : T(0);
+    const T v1 = lane + 32 < nr ? Fj[c.src[lane + 32]] : T(0);
+    __syncwarp();
+    if (lane < nr) Fj[c.rows[lane]] = v0;
+    if (lane + 32 < nr) Fj[c.rows[lane + 32]] = v1;
+  }
+  __syncthreads();
+}
+
+// Interchange a < b for a pivot taken at position a (an imax 1x1 pivot,
+// or the second column of a 2x2 pivot): only the entries that stay live
+// are written -- column b and row b of the trailing part from column a's
+// values, which each thread holds for its rows in colA -- since column a
+// becomes a pivot column whose values come from the shared W.  The row
+// interchange of the columns left of the panel is recorded for
+// sw_flush_left; the panel's own columns are written at its end from W.
+template <class T, int PT, int RPT>
+__device__ __forceinline__ void sw_pivot_swap(T* F, int ld, int n, int kstart,
+                                              int a, int b, const int (&rr)[RPT],
+                                              const bool (&on)[RPT],
+                                              const T (&colA)[RPT], int* vars,
+                                              int* fsperm, SwCtl<PT>& c) {
+#pragma unroll
+  for (int i = 0; i < RPT; i++) {
+    if (!on[i]) continue;
+    const int r = kstart + rr[i];
+    if (r > a && r < b) F[b + (size_t)r * ld] = colA[i];
+    else if (r > b) F[r + (size_t)b * ld] = colA[i];
+    else if (r == a) F[b + (size_t)b * ld] = colA[i];
+  }
+  if (threadIdx.x == 0) {
+    int tv = vars[a];
+    vars[a] = vars[b];
+    vars[b] = tv;
+    tv = fsperm[a];
+    fsperm[a] = fsperm[b];
+    fsperm[b] = tv;
+    c.swa[c.nsw] = a;
+    c.swb[c.nsw] = b;
+    c.nsw++;
+  }
+}
 
 // Block-wide first-argmax of (v, i) and max of v2 in every thread, in
 // reduction slot `set`.
@@ -1335,8 +1416,10 @@ template <class T, int PT, int RPT>
 __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
                                 int* vars, int* fsperm, double ustab,
                                 double pivot_tol, int* status, SwCtl<PT>& c,
-                                T* Ws, int nbe, int& k_, int& nc_, int& kw_) {
+                                T* Ws, int nbe, int& k_, int& nc_, int& kw_,
+                                int* dbg) {
   const int tid = threadIdx.x;
+  if (tid == 0) c.nsw = 0;
   int k = k_, nc = nc_, kw = 0;
   const int kstart = k;
   const int cld = n - kstart;
@@ -1418,9 +1501,11 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
         });
     // every thread holds its decision inputs: the writes below may follow
     if (pc.step == 0) {
-      // delay candidate k: move it to the end of the candidate set
+      if (dbg && tid == 0) atomicAdd(dbg + 4, 1);
+      // delay candidate k: move it to the end of the candidate set (both
+      // positions stay live: the full interchange, after the pending ones)
       if (k < nc - 1) {
-        __syncthreads();
+        sw_flush_left<T, PT>(F, ld, kstart, c);
         symm_swap<T, PT>(F, ld, n, vars, fsperm, k, nc - 1);
         sw_swap_rows<T, PT>(Ws, cld, kw, krow, nc - 1 - kstart);
         __syncthreads();
@@ -1432,17 +1517,25 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
     const int step = pc.step, kpiv = pc.kpiv;
     const int ksrc = k + step - 1;
     bool swapped = false;
+    if (dbg && tid == 0)
+      atomicAdd(dbg + (step == 1 ? (pc.imax_1x1 ? 1 : 0) : (kpiv != ksrc ? 3 : 2)), 1);
     if (pc.imax_1x1) {
       // column imax is the pivot column: its W column replaces column k's
-      __syncthreads();
+      // (own rows; the imax build's reduction already separated every read
+      // of W from these writes)
       T* w2 = Ws + (size_t)(kw + 1) * cld;
 #pragma unroll
       for (int i = 0; i < RPT; i++)
         if (on[i]) wcol[rr[i]] = w2[rr[i]];
     }
     if (kpiv != ksrc) {
-      __syncthreads();
-      symm_swap<T, PT>(F, ld, n, vars, fsperm, ksrc, kpiv);
+      // the global interchange from column ksrc's values (cur for a 1x1 at
+      // k, nxt for the second column of a 2x2)
+      if (step == 1) sw_pivot_swap<T, PT, RPT>(F, ld, n, kstart, ksrc, kpiv, rr, on, cur,
+                                               vars, fsperm, c);
+      else sw_pivot_swap<T, PT, RPT>(F, ld, n, kstart, ksrc, kpiv, rr, on, nxt,
+                                     vars, fsperm, c);
+      __syncthreads();   // the W copy above, before the W row interchange
       sw_swap_rows<T, PT>(Ws, cld, kw + step, ksrc - kstart, kpiv - kstart);
       swapped = true;
     }
@@ -1492,8 +1585,9 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
       load_col(k, cur);
     }
   }
-  // --- write the panel's L columns to F and its W rows below k to HBM
-  __syncthreads();
+  // --- the pending interchanges left of the panel; the panel's L columns
+  // to F and its W rows below k to HBM
+  sw_flush_left<T, PT>(F, ld, kstart, c);
   for (int j = 0; j < kw; j++) {
     const int col = kstart + j;
     const int kd = c.kind[j];
@@ -1533,7 +1627,7 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
 template <class T, int PT, int RPT>
 __global__ void __launch_bounds__(PT)
 k_big_panel_sw(DevicePlan d, const int* __restrict__ nodes, double ustab,
-               double pivot_tol, int smem_bytes) {
+               double pivot_tol, int smem_bytes, int* dbg) {
   __shared__ SwCtl<PT> c;
   __shared__ CtlT<PT> ctl;
   extern __shared__ double sw_raw[];
@@ -1552,13 +1646,17 @@ k_big_panel_sw(DevicePlan d, const int* __restrict__ nodes, double ustab,
   int* fvars = d.ipool + d.ioff[node];
   const int kstart = k;
   int kw = 0;
+  // the panel width depends on the front alone (not on the launch), so a
+  // front is factored the same way alone and in a batch
   const long long cld = f - kstart;
-  const long long fit = (long long)smem_bytes / (cld * (long long)sizeof(T));
+  const long long fit = (long long)kSwSmemBytes / (cld * (long long)sizeof(T));
   const int nbe = (int)(fit < NB ? fit : NB);
-  if (nbe >= 4 && cld <= (long long)PT * RPT) {
+  if (nbe >= 4 && cld <= (long long)PT * RPT &&
+      (long long)nbe * cld * (long long)sizeof(T) <= smem_bytes) {
+    if (dbg && threadIdx.x == 0) atomicAdd(dbg + 5, 1);
     panel_factor_sw<T, PT, RPT>(F, f, W, f, fs == f, fvars, fvars + f, ustab,
                                 pivot_tol, d.status, c, reinterpret_cast<T*>(sw_raw),
-                                nbe, k, nc, kw);
+                                nbe, k, nc, kw, dbg);
   } else {
     // front grown past what this launch's shared memory holds (delayed
     // pivots): the HBM-panel form
@@ -1700,9 +1798,16 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
   // large-front phases to stderr (diagnostics only).
   static const bool trace = std::getenv("AMIGO_B200_TRACE") != nullptr;
   std::vector<cudaEvent_t> ev;
+  // trace only: per level, counts of the shared-W panel's steps (fast 1x1,
+  // imax 1x1, 2x2 in place, 2x2 with interchange, delay, panels)
+  int* dbg = nullptr;
+  std::vector<int> dbg_h;
   if (trace) {
     ev.resize(3 * d.num_levels);
     for (auto& e : ev) cudaEventCreate(&e);
+    cudaMalloc((void**)&dbg, 8 * sizeof(int) * (size_t)d.num_levels);
+    cudaMemsetAsync(dbg, 0, 8 * sizeof(int) * (size_t)d.num_levels, s);
+    dbg_h.assign(8 * d.num_levels, 0);
   }
   for (int l = 0; l < d.num_levels; l++) {
     const LevelSchedule& L = h.sched[l];
@@ -1720,6 +1825,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     }
     if (trace) cudaEventRecord(ev[3 * l + 1], s);
     if (L.nbig) {
+      int* dbg_l = dbg ? dbg + 8 * l : nullptr;
       const int* nodes = d.sched_nodes + L.big_begin;
       const int B = L.nbig;
       const long long fm = L.big_max_f;
@@ -1745,8 +1851,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       // memory holds up to NB columns of W for the largest static front
       // (fronts grown by delayed pivots get fewer columns)
       const bool use_sw = fm <= (long long)kSwThreads * kSwRows;
-      const int sw_smem = (int)std::min<long long>(
-          kSwSmemBytes, (fm + kRlSlack) * NB * (long long)sizeof(T));
+      const int sw_smem = kSwSmemBytes;
       // panels a front of big_max_fs candidates needs without delays: each
       // takes nbe - 1 pivots, nbe growing as the remaining rows shrink
       int panels = 0;
@@ -1770,7 +1875,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
         for (int it = 0; it < panels; it++) {
           if (use_sw)
             k_big_panel_sw<T, kSwThreads, kSwRows><<<B, kSwThreads, sw_smem, s>>>(
-                d, nodes, h.ustab, h.pivot_tol, sw_smem);
+                d, nodes, h.ustab, h.pivot_tol, sw_smem, dbg_l);
           else if (fm > kPanelWideRows)
             k_big_panel<T, kPanelThreadsWide><<<B, kPanelThreadsWide, panel_cache, s>>>(
                 d, nodes, h.ustab, h.pivot_tol, panel_cache);
@@ -1807,6 +1912,9 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
   }
   if (trace) {
     cudaStreamSynchronize(s);
+    cudaMemcpy(dbg_h.data(), dbg, 8 * sizeof(int) * (size_t)d.num_levels,
+               cudaMemcpyDeviceToHost);
+    cudaFree(dbg);
     float tot_s = 0.f, tot_b = 0.f;
     for (int l = 0; l < d.num_levels; l++) {
       float a = 0.f, b = 0.f;
@@ -1819,6 +1927,11 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                    "(fmax %5d) %8.3f ms\n",
                    l, h.sched[l].nsmall, h.sched[l].small_max_f, a,
                    h.sched[l].nbig, h.sched[l].big_max_f, b);
+      const int* q = dbg_h.data() + 8 * l;
+      if (q[5])
+        std::fprintf(stderr, "           panel steps: fast %d imax %d 2x2 %d "
+                             "2x2-swap %d delay %d panels %d\n",
+                     q[0], q[1], q[2], q[3], q[4], q[5]);
     }
     std::fprintf(stderr, "total: small %.3f ms, large %.3f ms\n", tot_s, tot_b);
     for (auto& e : ev) cudaEventDestroy(e);
