@@ -433,6 +433,13 @@ int ab_ldl_set_wide_threshold(ab_ldl_t h, long long entries) {
   return AB_OK;
 }
 
+int ab_ldl_set_cluster_threshold(ab_ldl_t h, long long entries) {
+  if (!h || entries < 1) return AB_ERR_ARG;
+  h->h.cluster_entries = entries;
+  h->h.solve_epoch = -1;
+  return AB_OK;
+}
+
 int ab_ldl_stats(ab_ldl_t H, void* stream, double* flops,
                  double* factor_entries, int* max_front, int* num_delayed,
                  int* levels) {

@@ -1437,7 +1437,11 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
   };
   load_col(k, cur);
   int par = 0;
+  unsigned long long* cyc =
+      dbg ? reinterpret_cast<unsigned long long*>(dbg + 8) : nullptr;
+  long long tc0 = 0, tc1 = 0, tc2 = 0, tc3 = 0;
   while (kw < nbe - 1 && k < nc) {
+    if (cyc && tid == 0) tc0 = clock64();
     par ^= 1;
     // F[r, k + 1] for the next step, valid unless this step interchanges
     // rows or delays the candidate
@@ -1465,7 +1469,9 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
         else if (r < nc) argmax_merge(bv, bi, a, r);
         else tv = fmax(tv, a);
       }
+    if (cyc && tid == 0) tc1 = clock64();
     sw_reduce<PT>(c, 2 * par, bv, bi, tv);
+    if (cyc && tid == 0) tc2 = clock64();
     int imax = bi;
     if (imax >= nc || imax <= k) {
       if (k + 1 < nc && tid == 0) atomicOr(status, ST_NAN);
@@ -1500,6 +1506,12 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
           return ImaxColumn{rt, c.wii, wik};
         });
     // every thread holds its decision inputs: the writes below may follow
+    if (cyc && tid == 0) {
+      tc3 = clock64();
+      atomicAdd(cyc + 0, (unsigned long long)(tc1 - tc0));
+      atomicAdd(cyc + 1, (unsigned long long)(tc2 - tc1));
+      atomicAdd(cyc + 2, (unsigned long long)(tc3 - tc2));
+    }
     if (pc.step == 0) {
       if (dbg && tid == 0) atomicAdd(dbg + 4, 1);
       // delay candidate k: move it to the end of the candidate set (both
@@ -1584,9 +1596,11 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
     } else {
       load_col(k, cur);
     }
+    if (cyc && tid == 0) atomicAdd(cyc + 3, (unsigned long long)(clock64() - tc3));
   }
   // --- the pending interchanges left of the panel; the panel's L columns
   // to F and its W rows below k to HBM
+  if (cyc && tid == 0) tc0 = clock64();
   sw_flush_left<T, PT>(F, ld, kstart, c);
   for (int j = 0; j < kw; j++) {
     const int col = kstart + j;
@@ -1619,6 +1633,7 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
     }
     for (int r = k + tid; r < n; r += PT) Wg[r + (size_t)j * ld] = w0[r - kstart];
   }
+  if (cyc && tid == 0) atomicAdd(cyc + 4, (unsigned long long)(clock64() - tc0));
   k_ = k;
   nc_ = nc;
   kw_ = kw;
@@ -1653,10 +1668,17 @@ k_big_panel_sw(DevicePlan d, const int* __restrict__ nodes, double ustab,
   const int nbe = (int)(fit < NB ? fit : NB);
   if (nbe >= 4 && cld <= (long long)PT * RPT &&
       (long long)nbe * cld * (long long)sizeof(T) <= smem_bytes) {
-    if (dbg && threadIdx.x == 0) atomicAdd(dbg + 5, 1);
+    long long tk0 = 0;
+    if (dbg && threadIdx.x == 0) {
+      atomicAdd(dbg + 5, 1);
+      tk0 = clock64();
+    }
     panel_factor_sw<T, PT, RPT>(F, f, W, f, fs == f, fvars, fvars + f, ustab,
                                 pivot_tol, d.status, c, reinterpret_cast<T*>(sw_raw),
                                 nbe, k, nc, kw, dbg);
+    if (dbg && threadIdx.x == 0)
+      atomicAdd(reinterpret_cast<unsigned long long*>(dbg + 8) + 5,
+                (unsigned long long)(clock64() - tk0));
   } else {
     // front grown past what this launch's shared memory holds (delayed
     // pivots): the HBM-panel form
@@ -1802,12 +1824,16 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
   // imax 1x1, 2x2 in place, 2x2 with interchange, delay, panels)
   int* dbg = nullptr;
   std::vector<int> dbg_h;
+  std::vector<float> tpan(d.num_levels, 0.f), tupd(d.num_levels, 0.f);
+  cudaEvent_t te[3];
+  if (trace)
+    for (auto& e : te) cudaEventCreate(&e);
   if (trace) {
     ev.resize(3 * d.num_levels);
     for (auto& e : ev) cudaEventCreate(&e);
-    cudaMalloc((void**)&dbg, 8 * sizeof(int) * (size_t)d.num_levels);
-    cudaMemsetAsync(dbg, 0, 8 * sizeof(int) * (size_t)d.num_levels, s);
-    dbg_h.assign(8 * d.num_levels, 0);
+    cudaMalloc((void**)&dbg, 32 * sizeof(int) * (size_t)d.num_levels);
+    cudaMemsetAsync(dbg, 0, 32 * sizeof(int) * (size_t)d.num_levels, s);
+    dbg_h.assign(32 * d.num_levels, 0);
   }
   for (int l = 0; l < d.num_levels; l++) {
     const LevelSchedule& L = h.sched[l];
@@ -1825,7 +1851,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     }
     if (trace) cudaEventRecord(ev[3 * l + 1], s);
     if (L.nbig) {
-      int* dbg_l = dbg ? dbg + 8 * l : nullptr;
+      int* dbg_l = dbg ? dbg + 32 * l : nullptr;
       const int* nodes = d.sched_nodes + L.big_begin;
       const int B = L.nbig;
       const long long fm = L.big_max_f;
@@ -1873,6 +1899,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       for (;;) {
         budget += panels;
         for (int it = 0; it < panels; it++) {
+          if (trace) cudaEventRecord(te[0], s);
           if (use_sw)
             k_big_panel_sw<T, kSwThreads, kSwRows><<<B, kSwThreads, sw_smem, s>>>(
                 d, nodes, h.ustab, h.pivot_tol, sw_smem, dbg_l);
@@ -1883,6 +1910,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
             k_big_panel<T, kPanelThreads><<<B, kPanelThreads, panel_cache, s>>>(
                 d, nodes, h.ustab, h.pivot_tol, panel_cache);
           ab::count_launch();
+          if (trace) cudaEventRecord(te[1], s);
           if (use_tc) {
             { k_big_update_tc<<<dim3(B, gtc), tc::kThreads, tc::kSmemBytes, s>>>(
                 d, nodes); ab::count_launch(); }
@@ -1890,6 +1918,15 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
             { k_big_update<T><<<dim3(B, std::max(gu, 1)), NT,
                                 (sizeof(T) == 8 ? kTileSmemD : kTileSmem) * sizeof(T), s>>>(
                 d, nodes); ab::count_launch(); }
+          }
+          if (trace) {
+            cudaEventRecord(te[2], s);
+            cudaEventSynchronize(te[2]);
+            float a = 0.f, b = 0.f;
+            cudaEventElapsedTime(&a, te[0], te[1]);
+            cudaEventElapsedTime(&b, te[1], te[2]);
+            tpan[l] += a;
+            tupd[l] += b;
           }
         }
         // Delayed pivots received from the children can make a front need
@@ -1912,7 +1949,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
   }
   if (trace) {
     cudaStreamSynchronize(s);
-    cudaMemcpy(dbg_h.data(), dbg, 8 * sizeof(int) * (size_t)d.num_levels,
+    cudaMemcpy(dbg_h.data(), dbg, 32 * sizeof(int) * (size_t)d.num_levels,
                cudaMemcpyDeviceToHost);
     cudaFree(dbg);
     float tot_s = 0.f, tot_b = 0.f;
@@ -1927,11 +1964,16 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                    "(fmax %5d) %8.3f ms\n",
                    l, h.sched[l].nsmall, h.sched[l].small_max_f, a,
                    h.sched[l].nbig, h.sched[l].big_max_f, b);
-      const int* q = dbg_h.data() + 8 * l;
+      const int* q = dbg_h.data() + 32 * l;
+      const unsigned long long* cy = reinterpret_cast<const unsigned long long*>(q + 8);
       if (q[5])
         std::fprintf(stderr, "           panel steps: fast %d imax %d 2x2 %d "
-                             "2x2-swap %d delay %d panels %d\n",
-                     q[0], q[1], q[2], q[3], q[4], q[5]);
+                             "2x2-swap %d delay %d panels %d | kcyc: build %llu "
+                             "reduce %llu decide %llu post %llu wb %llu kernel %llu "
+                             "| panel launches %.3f ms update launches %.3f ms\n",
+                     q[0], q[1], q[2], q[3], q[4], q[5], cy[0] / 1000, cy[1] / 1000,
+                     cy[2] / 1000, cy[3] / 1000, cy[4] / 1000, cy[5] / 1000,
+                     tpan[l], tupd[l]);
     }
     std::fprintf(stderr, "total: small %.3f ms, large %.3f ms\n", tot_s, tot_b);
     for (auto& e : ev) cudaEventDestroy(e);

@@ -116,7 +116,10 @@ struct LdlHandle {
   // solved one per CTA ("narrow") and the wide fronts solved by the
   // cooperative multi-CTA kernels, concatenated level by level
   long long factor_epoch = 0, solve_epoch = -1;
-  long long wide_entries = 1 << 18;   // f * npiv from which a front is wide
+  // f * npiv from which a front is solved by a cluster of CTAs, and from
+  // which by the cooperative grid
+  long long cluster_entries = 1 << 14;
+  long long wide_entries = 1 << 22;
   // front storage / arithmetic of the next factorization (64: FP64, 32:
   // FP32 fronts for mixed precision) and of the last one
   int precision = 64, factor_precision = 64;
@@ -126,7 +129,7 @@ struct LdlHandle {
   int panel_cache_bytes = 0;
   int* sv_nodes = nullptr;        // device, nn entries
   int* sv_state = nullptr;        // device, 2 ints per wide front of a level
-  std::vector<int> sv_narrow_ptr, sv_wide_ptr, sv_narrow_smem;
+  std::vector<int> sv_narrow_ptr, sv_clu_ptr, sv_wide_ptr, sv_narrow_smem, sv_clu_smem;
   std::vector<int> sv_host, sv_f, sv_npiv;   // schedule and the sizes it is for
   int sv_max_wide = 0, sv_state_cap = 0;
   long long sv_wide_entries = 0;

@@ -243,6 +243,234 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
 
 
 // ---------------------------------------------------------------------------
+// Mid-size fronts: one thread-block cluster of CS CTAs per front.  CTA 0
+// solves the pivot block (the blocked triangular solve of the narrow
+// kernel, over the pivot rows only, with the front vector's pivot part in
+// its shared memory); the contribution rows' product with the pivot block
+// (the update vector passed to the parent, forward; the pivots' right-hand
+// side correction, backward) is spread over all CS CTAs, which read the
+// front's L21 once.  The cluster barrier orders CTA 0's results before the
+// other CTAs read them from HBM (cluster-scope release / acquire).
+constexpr int CS = 8;
+
+// dst[0:n] = src[0:n] from L2 (src may have been written by another CTA).
+__device__ __forceinline__ void copy_cg(double* dst, const double* src, int n) {
+  for (int t = threadIdx.x; t < n; t += NT) dst[t] = __ldcg(src + t);
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT)
+k_clu_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
+              int nrhs, int ldx, double* ubuf, const long long* uoff) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ double sm[];
+  __shared__ double sL[(SB + 1) * (SB + 1)];
+  __shared__ int sK[SB + 1];
+  __shared__ int s_choff;
+  const int cr = (int)cluster.block_rank();
+  const int node = nodes[blockIdx.x / CS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NWARP = NT / 32;
+  const int f = d.f[node], npiv = d.npiv[node];
+  const int* fvars = d.ipool + d.ioff[node];
+  const int* kind = fvars + 3 * f;
+  const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
+  double* sv = sm;                 // CTA 0: pivot values; others: y1 copy
+  double* part = sm + npiv;        // NWARP x 32 partial sums
+  for (int rhs = 0; rhs < nrhs; rhs++) {
+    double* G = ubuf + uoff[node] + (long long)rhs * f;
+    double* xr = x + (long long)rhs * ldx;
+    if (cr == 0) {
+      assemble_front_vector(d, node, G, xr, ubuf, uoff, rhs, &s_choff);
+      __syncthreads();
+      for (int t = tid; t < npiv; t += NT) sv[t] = G[t];
+      __syncthreads();
+      for (int jb = 0; jb < npiv;) {
+        const int je = block_end(kind, jb, npiv);
+        const int bw = je - jb;
+        for (int t = tid; t < bw * bw; t += NT) {
+          const int i = t % bw, j = t / bw;
+          sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
+        }
+        for (int t = tid; t < bw; t += NT) sK[t] = kind[jb + t];
+        __syncthreads();
+        if (warp == 0) {
+          for (int j = jb; j < je;) {
+            const bool two = sK[j - jb] == 1;
+            const double v0 = sv[j];
+            const double v1 = two ? sv[j + 1] : 0.0;
+            const int i0 = j + (two ? 2 : 1);
+            for (int i = i0 + lane; i < je; i += 32) {
+              double t = sL[(i - jb) + (j - jb) * (SB + 1)] * v0;
+              if (two) t += sL[(i - jb) + (j + 1 - jb) * (SB + 1)] * v1;
+              sv[i] -= t;
+            }
+            __syncwarp();
+            j = i0;
+          }
+        }
+        __syncthreads();
+        // the pivot rows below the block
+        for (int i = je + tid; i < npiv; i += NT) {
+          double acc = 0.0;
+          for (int j = jb; j < je; j++) acc += L[i + (size_t)j * f] * sv[j];
+          sv[i] -= acc;
+        }
+        __syncthreads();
+        jb = je;
+      }
+      for (int t = tid; t < npiv; t += NT) G[t] = sv[t];
+    }
+    cluster.sync();
+    // contribution rows: G[i] -= L21[i, :] y1, 32-row strips over the
+    // cluster's CTAs, the pivot columns split over the CTA's warps and the
+    // warps' partial sums added in a fixed order
+    if (cr != 0) copy_cg(sv, G, npiv);
+    __syncthreads();
+    const int ncr = f - npiv;
+    const int nstrip = (ncr + 31) / 32;
+    const int jc = (npiv + NWARP - 1) / NWARP;
+    const int j0 = warp * jc, j1 = min(npiv, j0 + jc);
+    for (int st = cr; st < nstrip; st += CS) {
+      const int i = npiv + st * 32 + lane;
+      double acc = 0.0;
+      if (i < f) {
+        const T* Li = L + i;
+        int j = j0;
+        for (; j + 4 <= j1; j += 4) {
+          const double a0 = Li[(size_t)j * f], a1 = Li[(size_t)(j + 1) * f];
+          const double a2 = Li[(size_t)(j + 2) * f], a3 = Li[(size_t)(j + 3) * f];
+          acc += a0 * sv[j];
+          acc += a1 * sv[j + 1];
+          acc += a2 * sv[j + 2];
+          acc += a3 * sv[j + 3];
+        }
+        for (; j < j1; j++) acc += Li[(size_t)j * f] * sv[j];
+      }
+      part[warp * 32 + lane] = acc;
+      __syncthreads();
+      if (warp == 0 && i < f) {
+        double s = 0.0;
+        for (int w = 0; w < NWARP; w++) s += part[w * 32 + lane];
+        G[i] = __ldcg(G + i) - s;
+      }
+      __syncthreads();
+    }
+    // D^{-1} and the pivots' values (CTA 0, from its shared copy)
+    if (cr == 0) {
+      for (int j = tid; j < npiv; j += NT) {
+        const int kd = kind[j];
+        double v = sv[j];
+        if (kd == 0) {
+          v = sv[j] / (double)L[j + (size_t)j * f];
+        } else if (kd == 1) {
+          const double d11 = L[j + (size_t)j * f];
+          const double d21 = L[j + 1 + (size_t)j * f];
+          const double d22 = L[j + 1 + (size_t)(j + 1) * f];
+          const double inv = 1.0 / (d11 * d22 - d21 * d21);
+          v = inv * (d22 * sv[j] - d21 * sv[j + 1]);
+        } else {
+          const double d11 = L[j - 1 + (size_t)(j - 1) * f];
+          const double d21 = L[j + (size_t)(j - 1) * f];
+          const double d22 = L[j + (size_t)j * f];
+          const double inv = 1.0 / (d11 * d22 - d21 * d21);
+          v = inv * (d11 * sv[j] - d21 * sv[j - 1]);
+        }
+        xr[decode_var(fvars[j])] = v;
+      }
+    }
+    cluster.sync();
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT)
+k_clu_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
+               int nrhs, int ldx, double* ubuf, const long long* uoff) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ double sm[];
+  __shared__ double sL[(SB + 1) * (SB + 1)];
+  __shared__ int sK[SB + 1];
+  const int cr = (int)cluster.block_rank();
+  const int node = nodes[blockIdx.x / CS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NWARP = NT / 32;
+  const int f = d.f[node], npiv = d.npiv[node];
+  const int* fvars = d.ipool + d.ioff[node];
+  const int* kind = fvars + 3 * f;
+  const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
+  const int ncr = f - npiv;
+  double* sx = sm;            // contribution rows' final values
+  double* sv = sm + ncr;      // CTA 0: pivot values
+  for (int rhs = 0; rhs < nrhs; rhs++) {
+    double* G = ubuf + uoff[node] + (long long)rhs * f;
+    double* xr = x + (long long)rhs * ldx;
+    for (int r = tid; r < ncr; r += NT) sx[r] = xr[fvars[npiv + r]];
+    __syncthreads();
+    // t[j] = z[j] - L21[:, j]^T x2 for every pivot column, one warp per
+    // column over the cluster's warps
+    for (int j = cr * NWARP + warp; j < npiv; j += CS * NWARP) {
+      const T* Lj = L + (size_t)j * f + npiv;
+      double acc = 0.0;
+      for (int i = lane; i < ncr; i += 32) acc += Lj[i] * sx[i];
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+      if (lane == 0) G[j] = xr[decode_var(fvars[j])] - acc;
+    }
+    cluster.sync();
+    if (cr == 0) {
+      for (int t = tid; t < npiv; t += NT) sv[t] = __ldcg(G + t);
+      __syncthreads();
+      int je = npiv;
+      while (je > 0) {
+        int jb = je - SB > 0 ? je - SB : 0;
+        if (jb > 0 && kind[jb] == 2) jb--;  // keep 2x2 pairs together
+        // t[j] -= sum_{je <= i < npiv} L[i, j] t[i] for j in [jb, je)
+        for (int j = jb + warp; j < je; j += NWARP) {
+          double acc = 0.0;
+          for (int i = je + lane; i < npiv; i += 32) acc += L[i + (size_t)j * f] * sv[i];
+          for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+          if (lane == 0) sv[j] -= acc;
+        }
+        const int bw = je - jb;
+        for (int t = tid; t < bw * bw; t += NT) {
+          const int i = t % bw, j = t / bw;
+          sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
+        }
+        for (int t = tid; t < bw; t += NT) sK[t] = kind[jb + t];
+        __syncthreads();
+        if (warp == 0) {
+          for (int j = je - 1; j >= jb;) {
+            const bool two = sK[j - jb] == 2;
+            const int jl = two ? j - 1 : j;
+            double a0 = 0.0, a1 = 0.0;
+            for (int i = j + 1 + lane; i < je; i += 32) {
+              a0 += sL[(i - jb) + (jl - jb) * (SB + 1)] * sv[i];
+              if (two) a1 += sL[(i - jb) + (j - jb) * (SB + 1)] * sv[i];
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+              a0 += __shfl_down_sync(0xffffffffu, a0, o);
+              a1 += __shfl_down_sync(0xffffffffu, a1, o);
+            }
+            if (lane == 0) {
+              sv[jl] -= a0;
+              if (two) sv[j] -= a1;
+            }
+            __syncwarp();
+            j = jl - 1;
+          }
+        }
+        __syncthreads();
+        je = jb;
+      }
+      for (int j = tid; j < npiv; j += NT) xr[decode_var(fvars[j])] = sv[j];
+    }
+    cluster.sync();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Wide fronts (f * npiv large): one cooperative launch per level solves all
 // of the level's wide fronts with every CTA of the GPU.  The front vectors
 // live in ubuf (global memory).  Each column block of WB pivots alternates
@@ -566,8 +794,31 @@ k_wide_backward(DevicePlan d, const int* __restrict__ nodes, int count,
     }                                                                     \
   } while (0)
 
-// Per level: narrow fronts (one CTA each) and wide fronts, from the sizes
-// of the last factorization.
+// One cluster of CS CTAs per front (cudaLaunchKernelEx with a cluster
+// dimension).
+template <class K>
+static int launch_cluster(K kernel, int fronts, int smem, cudaStream_t s,
+                          const DevicePlan& d, const int* nodes, double* x,
+                          int nrhs, int ldx, double* ubuf, const long long* uoff) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(fronts * CS);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CS;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  SCUDA(cudaLaunchKernelEx(&cfg, kernel, d, nodes, x, nrhs, ldx, ubuf, uoff));
+  ab::count_launch();
+  return 0;
+}
+
+// Per level: narrow fronts (one CTA each), cluster fronts (CS CTAs each)
+// and wide fronts, from the sizes of the last factorization.
 static int build_solve_schedule(LdlHandle& h, cudaStream_t s) {
   const int L = h.d.num_levels, nn = h.d.nn;
   // unchanged front sizes (the usual case between IPM iterations): keep it
@@ -580,30 +831,51 @@ static int build_solve_schedule(LdlHandle& h, cudaStream_t s) {
   nodes.clear();
   nodes.reserve(nn);
   h.sv_narrow_ptr.assign(L + 1, 0);
+  h.sv_clu_ptr.assign(L + 1, 0);
   h.sv_wide_ptr.assign(L + 1, 0);
   h.sv_narrow_smem.assign(L, 0);
+  h.sv_clu_smem.assign(L, 0);
   h.sv_max_wide = 0;
+  // a front's class: narrow (one CTA), cluster (CS CTAs) or wide (the
+  // cooperative grid), from f * npiv and, for clusters, the front vector
+  // fitting in shared memory
+  auto cls = [&](int k) {
+    const long long e = (long long)h.h_f[k] * h.h_npiv[k];
+    if (e >= h.wide_entries) return 2;
+    if (e >= h.cluster_entries && ((long long)h.h_f[k] + NT) * 8 <= kMaxDynSmem) return 1;
+    return 0;
+  };
   for (int l = 0; l < L; l++) {
     h.sv_narrow_ptr[l] = (int)nodes.size();
     int fm = 0;
     for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++) {
       const int k = h.level_nodes[q];
-      if ((long long)h.h_f[k] * h.h_npiv[k] < h.wide_entries) {
+      if (cls(k) == 0) {
         nodes.push_back(k);
         fm = std::max(fm, h.h_f[k]);
       }
     }
     h.sv_narrow_smem[l] =
         (int)std::min<long long>((long long)fm * 8, kMaxDynSmem);
+    h.sv_clu_ptr[l] = (int)nodes.size();
+    int cm = 0;
+    for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++) {
+      const int k = h.level_nodes[q];
+      if (cls(k) == 1) {
+        nodes.push_back(k);
+        cm = std::max(cm, h.h_f[k]);
+      }
+    }
+    h.sv_clu_smem[l] = (int)std::min<long long>(((long long)cm + NT) * 8, kMaxDynSmem);
     h.sv_wide_ptr[l] = (int)nodes.size();
     for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++) {
       const int k = h.level_nodes[q];
-      if ((long long)h.h_f[k] * h.h_npiv[k] >= h.wide_entries) nodes.push_back(k);
+      if (cls(k) == 2) nodes.push_back(k);
     }
     h.sv_max_wide = std::max(h.sv_max_wide,
                              (int)nodes.size() - h.sv_wide_ptr[l]);
   }
-  h.sv_narrow_ptr[L] = h.sv_wide_ptr[L] = (int)nodes.size();
+  h.sv_narrow_ptr[L] = h.sv_clu_ptr[L] = h.sv_wide_ptr[L] = (int)nodes.size();
   if (!h.sv_nodes) SCUDA(cudaMalloc((void**)&h.sv_nodes, std::max(nn, 1) * sizeof(int)));
   if (h.sv_max_wide > h.sv_state_cap) {
     if (h.sv_state) SCUDA(cudaFree(h.sv_state));
@@ -634,6 +906,12 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kMaxDynSmem));
     SCUDA(cudaFuncSetAttribute(k_solve_backward<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kMaxDynSmem));
+    SCUDA(cudaFuncSetAttribute(k_clu_forward<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kMaxDynSmem));
+    SCUDA(cudaFuncSetAttribute(k_clu_backward<T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kMaxDynSmem));
     SCUDA(cudaFuncSetAttribute(k_wide_forward<T>,
@@ -684,10 +962,16 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
   }
   for (int l = 0; l < d.num_levels; l++) {
     if (trace) cudaEventRecord(ev[l], s);
-    const int b = h.sv_narrow_ptr[l], cnt = h.sv_wide_ptr[l] - b;
+    const int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
     if (cnt)
       { k_solve_forward<T><<<cnt, NT, h.sv_narrow_smem[l], s>>>(d, h.sv_nodes + b, d_x, nrhs,
                                                ldx, h.ubuf, h.uoff, h.sv_narrow_smem[l] / 8); ab::count_launch(); }
+    const int cb = h.sv_clu_ptr[l], ccnt = h.sv_wide_ptr[l] - cb;
+    if (ccnt) {
+      int rc = launch_cluster(k_clu_forward<T>, ccnt, h.sv_clu_smem[l], s, d,
+                              h.sv_nodes + cb, d_x, nrhs, ldx, h.ubuf, h.uoff);
+      if (rc) return rc;
+    }
     const int wb = h.sv_wide_ptr[l], wc = h.sv_narrow_ptr[l + 1] - wb;
     if (wc) {
       const int* wn = h.sv_nodes + wb;
@@ -705,11 +989,17 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
   if (trace) cudaEventRecord(ev[d.num_levels], s);
   for (int l = d.num_levels - 1; l >= 0; l--) {
     if (trace) cudaEventRecord(ev[d.num_levels + 1 + (d.num_levels - 1 - l)], s);
-    const int b = h.sv_narrow_ptr[l], cnt = h.sv_wide_ptr[l] - b;
+    const int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
     if (cnt)
       { k_solve_backward<T><<<cnt, NT, h.sv_narrow_smem[l], s>>>(d, h.sv_nodes + b, d_x,
                                                 nrhs, ldx, h.ubuf, h.uoff,
                                                 h.sv_narrow_smem[l] / 8); ab::count_launch(); }
+    const int cb = h.sv_clu_ptr[l], ccnt = h.sv_wide_ptr[l] - cb;
+    if (ccnt) {
+      int rc = launch_cluster(k_clu_backward<T>, ccnt, h.sv_clu_smem[l], s, d,
+                              h.sv_nodes + cb, d_x, nrhs, ldx, h.ubuf, h.uoff);
+      if (rc) return rc;
+    }
     const int wb = h.sv_wide_ptr[l], wc = h.sv_narrow_ptr[l + 1] - wb;
     if (wc) {
       const int* wn = h.sv_nodes + wb;
@@ -740,9 +1030,9 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
       for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++)
         fm = std::max(fm, h.h_f[h.level_nodes[q]]);
       std::fprintf(stderr,
-                   "solve level %d: narrow %d wide %d max f %d  fwd %.3f ms  "
+                   "solve level %d: narrow %d cluster %d wide %d max f %d  fwd %.3f ms  "
                    "bwd %.3f ms\n",
-                   l, h.sv_wide_ptr[l] - h.sv_narrow_ptr[l],
+                   l, h.sv_clu_ptr[l] - h.sv_narrow_ptr[l], h.sv_wide_ptr[l] - h.sv_clu_ptr[l],
                    h.sv_narrow_ptr[l + 1] - h.sv_wide_ptr[l], fm, a, b);
     }
     std::fprintf(stderr, "solve total: fwd %.3f ms, bwd %.3f ms\n", tf, tb);

@@ -252,6 +252,11 @@ class SparseLDL:
         HBM)."""
         _lib.call("ab_ldl_set_panel_cache", self._h, int(nbytes))
 
+    def set_cluster_threshold(self, entries):
+        """Fronts with f * npiv >= entries (below the wide threshold) are
+        solved by a thread-block cluster of 8 CTAs each."""
+        _lib.call("ab_ldl_set_cluster_threshold", self._h, int(entries))
+
     def set_wide_threshold(self, entries):
         """Fronts with f * npiv >= entries are solved by the multi-CTA
         kernels (default 2^18)."""

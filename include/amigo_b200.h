@@ -125,11 +125,15 @@ int ab_ldl_set_tensor_cores(ab_ldl_t h, int on);
  * No reference counterpart. */
 int ab_ldl_set_panel_cache(ab_ldl_t h, int bytes);
 
-/* Solve schedule knob: fronts with f * npiv >= entries (default 2^18) are
- * solved by the cooperative multi-CTA kernels, smaller ones one CTA per
- * front.  Both give the same result to rounding.  No reference
- * counterpart (the reference solves every front on one thread). */
+/* Solve schedule knobs: fronts with f * npiv >= the wide threshold
+ * (default 2^22) are solved by the cooperative grid-wide kernels; fronts
+ * from the cluster threshold (default 2^14) up to it by one thread-block
+ * cluster of 8 CTAs each (when the front vector fits in shared memory);
+ * smaller ones by one CTA per front.  All give the same result to
+ * rounding.  No reference counterpart (the reference solves every front on
+ * one thread). */
 int ab_ldl_set_wide_threshold(ab_ldl_t h, long long entries);
+int ab_ldl_set_cluster_threshold(ab_ldl_t h, long long entries);
 
 /* The tensor-core Schur update on plain device arrays (column-major, FP32):
  * lower(C) -= A B^T for n x kw panels A, B (kw <= 31), as 3xTF32 tcgen05

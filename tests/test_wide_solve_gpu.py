@@ -1,7 +1,8 @@
-"""The multi-CTA (cooperative) solve of wide fronts against the one-CTA-per-
-front solve: every golden fixture and a 2D SIMP KKT are solved with all
-fronts on the wide path (threshold 1), with none (threshold 2^62) and with
-the default split.  Each meets the FP64 residual bar 1e-10; the solutions
+"""The multi-CTA solves against the one-CTA-per-front solve: every golden
+fixture and a 2D SIMP KKT are solved with all fronts on the cooperative
+wide path (wide threshold 1), with every front on one CTA (both thresholds
+2^62), with every front on the cluster path (cluster threshold 1, wide
+2^62), and with the default split.  Each meets the FP64 residual bar 1e-10; the solutions
 differ only by summation order (1e-9 relative on the fixtures, 1e-6 on the
 ill-conditioned SIMP KKT).  Also several right-hand sides at once."""
 import os
@@ -32,8 +33,9 @@ def solve_three_ways(M, order, ustab=0.01, nrhs=1):
     assert ldl.factor() == 0
     B = (M @ np.random.RandomState(7).randn(n, nrhs)).T.copy()   # nrhs x n
     out = []
-    for thr in (1, 1 << 62, 1 << 18):
-        ldl.set_wide_threshold(thr)
+    for clu, wide in ((1 << 62, 1), (1 << 62, 1 << 62), (1, 1 << 62), (1 << 14, 1 << 22)):
+        ldl.set_cluster_threshold(clu)
+        ldl.set_wide_threshold(wide)
         xd = torch.from_numpy(B.copy()).cuda()
         ldl.solve_device(xd if nrhs > 1 else xd[0])
         out.append(xd.cpu().numpy())
@@ -47,12 +49,13 @@ def test_golden_cases_wide_equals_narrow():
         rp, ci, v = z[name + "/rowp"], z[name + "/cols"], z[name + "/vals"]
         n = len(rp) - 1
         M = sp.csr_matrix((v, ci, rp), shape=(n, n))
-        B, (xw, xn, xd) = solve_three_ways(M, int(z[name + "/order"]),
-                                           float(z[name + "/ustab"]))
+        B, (xw, xn, xc, xd) = solve_three_ways(M, int(z[name + "/order"]),
+                                               float(z[name + "/ustab"]))
         scale = np.abs(xn).max()
         assert np.abs(xw - xn).max() <= 1e-9 * scale, name
+        assert np.abs(xc - xn).max() <= 1e-9 * scale, name
         assert np.abs(xd - xn).max() <= 1e-9 * scale, name
-        for x in (xw, xn, xd):
+        for x in (xw, xn, xc, xd):
             assert rel_residual(M, x[0], B[0]) <= 1e-10, name
 
 
@@ -68,12 +71,13 @@ def test_simp2d_kkt_wide_fronts_multi_rhs():
     vals[m.diag_pos] += d
     vals[m.fixed_diag_pos] = 1.0
     M = sp.csr_matrix((vals, m.cols, m.rowp), shape=(m.n, m.n))
-    B, (xw, xn, xd) = solve_three_ways(M, linalg.OrderingType.AMD, nrhs=3)
-    for x in (xw, xn, xd):
+    B, (xw, xn, xc, xd) = solve_three_ways(M, linalg.OrderingType.AMD, nrhs=3)
+    for x in (xw, xn, xc, xd):
         for k in range(3):
             assert rel_residual(M, x[k], B[k]) <= 1e-10
     # Emin = 1e-9 makes this KKT ill-conditioned: solutions of equal
     # residual differ at the 1e-8 level
     scale = np.abs(xn).max()
     assert np.abs(xw - xn).max() <= 1e-6 * scale
+    assert np.abs(xc - xn).max() <= 1e-6 * scale
     assert np.abs(xd - xn).max() <= 1e-6 * scale
