@@ -1251,7 +1251,8 @@ struct SwCtl {
   int red_i[4][PT / 32];
   double red_v2[4][PT / 32];
   double wkk[2], wii;
-  double cA[NB], cB[NB];   // L[r, j] = W[r, j] cA[j] + W[r, partner] cB[j]
+  double cA[NB], cB[NB];   // L[r, j] = W[r, j] cA[j] + W[r, cP[j]] cB[j]
+  int cP[NB];              // the column's partner (itself for a 1x1 pivot)
   int kind[NB];            // 0: 1x1, 1 / 2: first / second column of a 2x2
   // row interchanges of the panel's pivots not yet applied to the columns
   // left of the panel, and their composition (rows[t] <- src[t])
@@ -1369,35 +1370,43 @@ __device__ __forceinline__ void sw_reduce(SwCtl<PT>& c, int set, double& v,
 
 // acc[i] -= sum_j L[r_i, j] * y[j] over the panel's columns j < kw, with
 // L recomputed from the shared W columns; y[j] = W[yrow, j] of the column
-// being built.
+// being built.  Every column is L[r, j] = W[r, j] cA[j] + W[r, cP[j]] cB[j]
+// (cB = 0 and cP = j for a 1x1 pivot: the product W[r, j] cA[j] exactly),
+// so the loop has no branch and is unrolled by two.
+template <class T>
+__device__ __forceinline__ T sw_l(T w, T wp, T a, T b) {
+  return fma(wp, b, w * a);
+}
+
 template <class T, int PT, int RPT>
 __device__ __forceinline__ void sw_apply_panel(const T* __restrict__ Ws, int cld,
                                                int kw, int yrow, const SwCtl<PT>& c,
                                                const int (&rr)[RPT],
                                                const bool (&on)[RPT], T (&acc)[RPT]) {
-  for (int j = 0; j < kw;) {
+  int j = 0;
+  for (; j + 2 <= kw; j += 2) {
     const T* w0 = Ws + (size_t)j * cld;
-    if (c.kind[j] == 0) {
-      const T a = T(c.cA[j]), y = w0[yrow];
+    const T* w1 = w0 + cld;
+    const T* p0 = Ws + (size_t)c.cP[j] * cld;
+    const T* p1 = Ws + (size_t)c.cP[j + 1] * cld;
+    const T a0 = T(c.cA[j]), b0 = T(c.cB[j]), y0 = w0[yrow];
+    const T a1 = T(c.cA[j + 1]), b1 = T(c.cB[j + 1]), y1 = w1[yrow];
 #pragma unroll
-      for (int i = 0; i < RPT; i++)
-        if (on[i]) acc[i] -= (w0[rr[i]] * a) * y;
-      j += 1;
-    } else {
-      const T* w1 = w0 + cld;
-      const T i00 = T(c.cA[j]), i10 = T(c.cB[j]);
-      const T i11 = T(c.cA[j + 1]), i01 = T(c.cB[j + 1]);
-      const T y0 = w0[yrow], y1 = w1[yrow];
+    for (int i = 0; i < RPT; i++)
+      if (on[i]) {
+        const T l0 = sw_l(w0[rr[i]], p0[rr[i]], a0, b0);
+        const T l1 = sw_l(w1[rr[i]], p1[rr[i]], a1, b1);
+        acc[i] -= l0 * y0;
+        acc[i] -= l1 * y1;
+      }
+  }
+  if (j < kw) {
+    const T* w0 = Ws + (size_t)j * cld;
+    const T* p0 = Ws + (size_t)c.cP[j] * cld;
+    const T a0 = T(c.cA[j]), b0 = T(c.cB[j]), y0 = w0[yrow];
 #pragma unroll
-      for (int i = 0; i < RPT; i++)
-        if (on[i]) {
-          const T a0 = w0[rr[i]], a1 = w1[rr[i]];
-          const T l0 = a0 * i00 + a1 * i10, l1 = a0 * i01 + a1 * i11;
-          acc[i] -= l0 * y0;
-          acc[i] -= l1 * y1;
-        }
-      j += 2;
-    }
+    for (int i = 0; i < RPT; i++)
+      if (on[i]) acc[i] -= sw_l(w0[rr[i]], p0[rr[i]], a0, b0) * y0;
   }
 }
 
@@ -1560,6 +1569,7 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
       c.kind[kw] = 0;
       c.cA[kw] = pc.zero ? 0.0 : (double)(T(1) / d);
       c.cB[kw] = 0.0;
+      c.cP[kw] = kw;
       if (tid == 0) vars[3 * ld + k] = 0;
     } else if (tid == 0) {
       if (step == 1) {
@@ -1568,6 +1578,7 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
         c.kind[kw] = 0;
         c.cA[kw] = pc.zero ? 0.0 : (double)(T(1) / d);
         c.cB[kw] = 0.0;
+        c.cP[kw] = kw;
         vars[3 * ld + k] = 0;
       } else {
         const T d11 = Ws[(size_t)kw * cld + krow];
@@ -1577,10 +1588,13 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
         if (!isfinite((double)detinv)) atomicOr(status, ST_NAN);
         c.kind[kw] = 1;
         c.kind[kw + 1] = 2;
+        // l0 = w0 i00 + w1 i10, l1 = w1 i11 + w0 i01
         c.cA[kw] = (double)(d22 * detinv);       // i00
         c.cB[kw] = (double)(-d21 * detinv);      // i10
         c.cA[kw + 1] = (double)(d11 * detinv);   // i11
         c.cB[kw + 1] = (double)(-d21 * detinv);  // i01
+        c.cP[kw] = kw + 1;
+        c.cP[kw + 1] = kw;
         vars[k] = -(vars[k] + 1);
         vars[k + 1] = -(vars[k + 1] + 1);
         vars[3 * ld + k] = 1;
@@ -1607,16 +1621,16 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
     const int kd = c.kind[j];
     const T* w0 = Ws + (size_t)j * cld;
     T* Fc = F + (size_t)col * ld;
+    const T* wp = Ws + (size_t)c.cP[j] * cld;
+    const T a = T(c.cA[j]), b = T(c.cB[j]);
     if (kd == 0) {
-      const T a = T(c.cA[j]);
       if (tid == 0) Fc[col] = w0[j];
-      for (int r = col + 1 + tid; r < n; r += PT) Fc[r] = w0[r - kstart] * a;
+      for (int r = col + 1 + tid; r < n; r += PT)
+        Fc[r] = sw_l(w0[r - kstart], wp[r - kstart], a, b);
     } else {
       const int j0 = kd == 1 ? j : j - 1;
       const T* wa = Ws + (size_t)j0 * cld;
       const T* wb = wa + cld;
-      const T i00 = T(c.cA[j0]), i10 = T(c.cB[j0]);
-      const T i11 = T(c.cA[j0 + 1]), i01 = T(c.cB[j0 + 1]);
       const int c0 = kstart + j0;
       if (tid == 0) {
         if (kd == 1) {
@@ -1626,10 +1640,8 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
           Fc[col] = wb[j0 + 1];
         }
       }
-      for (int r = c0 + 2 + tid; r < n; r += PT) {
-        const T a0 = wa[r - kstart], a1 = wb[r - kstart];
-        Fc[r] = kd == 1 ? a0 * i00 + a1 * i10 : a0 * i01 + a1 * i11;
-      }
+      for (int r = c0 + 2 + tid; r < n; r += PT)
+        Fc[r] = sw_l(w0[r - kstart], wp[r - kstart], a, b);
     }
     for (int r = k + tid; r < n; r += PT) Wg[r + (size_t)j * ld] = w0[r - kstart];
   }
