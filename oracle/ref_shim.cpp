@@ -297,4 +297,44 @@ double ref_ipm_compute_constraint_violation_1norm(REF_IPM_ARGS,
   return amigo::ipm::compute_constraint_violation_1norm(P, S, grad);
 }
 
+
+// The remaining backend functions the reference's InteriorPointOptimizer
+// calls (include/interior_point_backend.h:82-201, 539-611).
+void ref_ipm_relax_bounds(int np, int nc, const int* pidx, const int* cidx,
+                          const double* lbx, const double* ubx,
+                          const double* lbh, double* lb_out, double* ub_out,
+                          double factor, double tol) {
+  auto P = make_info(np, nc, pidx, cidx, lbx, ubx, lbh);
+  amigo::ipm::relax_bounds(P, lb_out, ub_out, factor, tol);
+}
+
+void ref_ipm_initialize(int np, int nc, const int* pidx, const int* cidx,
+                        const double* lbx, const double* ubx, const double* lbh,
+                        double mu, double* xlam, double* zl, double* zu,
+                        double* sl, double* su) {
+  auto P = make_info(np, nc, pidx, cidx, lbx, ubx, lbh);
+  amigo::ipm::project_primals_into_interior(P, xlam);
+  amigo::ipm::initialize_bound_duals(mu, P, xlam, zl, zu);
+  amigo::ipm::initialize_slacks(P, xlam, sl, su);
+}
+
+void ref_ipm_compute_kkt_error_sq(REF_IPM_ARGS, const double* grad, double* d,
+                                  double* p, double* c) {
+  REF_IPM_SETUP
+  amigo::ipm::compute_kkt_error_sq(P, S, grad, *d, *p, *c);
+}
+
+double ref_ipm_compute_barrier_dphi_from_kkt(REF_IPM_ARGS, const double* res,
+                                             const double* px,
+                                             const double* diag) {
+  REF_IPM_SETUP
+  return amigo::ipm::compute_barrier_dphi_from_kkt(P, S, res, px, diag);
+}
+
+void ref_ipm_compute_dual_residual_vector(REF_IPM_ARGS, const double* grad,
+                                          double* out, int size) {
+  REF_IPM_SETUP
+  amigo::ipm::compute_dual_residual_vector(P, S, grad, out, size);
+}
+
 }  // extern "C"
