@@ -150,6 +150,7 @@ _SIGS = {
     "ab_launch_count": (ctypes.c_longlong, []),
     "ab_ldl_set_wide_threshold": (_i, [_vp, ctypes.c_longlong]),
     "ab_ldl_set_cluster_threshold": (_i, [_vp, ctypes.c_longlong]),
+    "ab_ldl_set_panel_mode": (_i, [_vp, _i, _i]),
     "ab_ldl_set_precision": (_i, [_vp, _i]),
     "ab_ldl_set_tensor_cores": (_i, [_vp, _i]),
     "ab_ldl_set_panel_cache": (_i, [_vp, _i]),

@@ -166,6 +166,65 @@ class GeneratedModel:
         self.fixed_zero_pos = np.nonzero(zero)[0].astype(np.int32)
         self.fixed_diag_pos = self.diag_pos[self.fixed].astype(np.int32)
 
+    # -- wire format ------------------------------------------------------------
+    # A request carries its problem as JSON: the flattened model -- every
+    # group's component (its expression DAG, component.serialize), index
+    # layout and data, the multiplier indicator, the bounds and the fixed
+    # variables -- which is what amigo's Model.initialize produces from the
+    # linked, named components that Model.serialize writes
+    # (amigo/model.py:1624-1740).  Vectors travel as serialize_vectors
+    # writes them: {name: {"kind": ..., "values": [...]}}.
+    FORMAT = "amigo_b200.model/1"
+
+    def serialize(self):
+        b = lambda a: [None if not np.isfinite(v) else float(v) for v in a]
+        d = {"format": self.FORMAT, "n": self.n,
+             "groups": [{"name": gr.name, "component": gr.comp.serialize(),
+                         "idx": gr.idx.tolist(), "data": gr.data.tolist()}
+                        for gr in self.groups],
+             "mult": np.nonzero(self.mult)[0].tolist(),
+             "lower": b(self.lower), "upper": b(self.upper),
+             "fixed": self.fixed.tolist()}
+        if hasattr(self, "x0"):
+            d["x0"] = [float(v) for v in self.x0]
+        return d
+
+    @classmethod
+    def deserialize(cls, d):
+        from .component import Component
+        if d.get("format") != cls.FORMAT:
+            raise ValueError("not a serialized model")
+        n = int(d["n"])
+        groups = [Group(Component.deserialize(g["component"]), np.asarray(g["idx"], np.int32),
+                        np.asarray(g["data"], np.float64), name=g["name"])
+                  for g in d["groups"]]
+        mult = np.zeros(n, bool)
+        mult[np.asarray(d["mult"], np.int64)] = True
+        lb = lambda a, inf: np.array([inf if v is None else v for v in a], np.float64)
+        return cls(n, groups, mult, lb(d["lower"], -np.inf), lb(d["upper"], np.inf),
+                   fixed=d.get("fixed", ()), x0=d.get("x0"))
+
+    @staticmethod
+    def serialize_vectors(vecs):
+        """{name: (kind, array)} -> JSON-compatible dict; kind is "state"
+        (n: variables and multipliers), "data" or "output"."""
+        out = {}
+        for name, (kind, a) in vecs.items():
+            if kind not in ("state", "data", "output"):
+                raise ValueError("unrecognized vector kind %s" % kind)
+            a = a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)
+            out[name] = {"kind": kind, "values": [float(v) for v in a.ravel()]}
+        return out
+
+    @staticmethod
+    def deserialize_vectors(d):
+        out = {}
+        for name, v in d.items():
+            if v.get("kind") not in ("state", "data", "output"):
+                raise ValueError("unrecognized vector kind %s" % v.get("kind"))
+            out[name] = (v["kind"], np.asarray(v["values"], np.float64))
+        return out
+
     def host_derivatives(self, x, alpha=1.0):
         """Gradient and KKT values assembled on the host from the host build
         of the generated evaluators (test use: no GPU needed)."""

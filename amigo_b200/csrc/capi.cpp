@@ -440,6 +440,13 @@ int ab_ldl_set_cluster_threshold(ab_ldl_t h, long long entries) {
   return AB_OK;
 }
 
+int ab_ldl_set_panel_mode(ab_ldl_t h, int mode, int min_rows) {
+  if (!h || mode < 0 || mode > 2) return AB_ERR_ARG;
+  h->h.panel_mode = mode;
+  if (min_rows > 0) h->h.cl_min_rows = min_rows;
+  return AB_OK;
+}
+
 int ab_ldl_stats(ab_ldl_t H, void* stream, double* flops,
                  double* factor_entries, int* max_front, int* num_delayed,
                  int* levels) {

@@ -16,6 +16,7 @@
 //      the reference's LAPACK dsytrf does (include/sparse_ldl.h:1208-1230);
 //   4. applies the trailing update after every panel and counts the inertia
 //      of its D blocks with the reference's rule (sparse_ldl.h:1917-1969).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -87,31 +88,39 @@ __device__ __forceinline__ void argmax_merge(double& v, int& i, double v2,
 // Symmetric interchange of rows/columns a < b of the lower triangle of F,
 // of the variable list and of the fully-summed permutation record
 // (reference: symm_swap, include/sparse_ldl.h:1252-1274).
-template <class T, int BT>
+template <class T, bool CG>
+__device__ __forceinline__ T ldf(const T* p) {
+  if constexpr (CG) return __ldcg(p);
+  else return *p;
+}
+
+// (CG: loads from L2, for entries another CTA of a cluster may have
+// written in the same launch.)
+template <class T, int BT, bool CG = false>
 __device__ void symm_swap(T* F, int ld, int n, int* vars, int* fsperm,
                           int a, int b) {
   const int tid = threadIdx.x;
   // rows a and b over columns [0, a)
   for (int j = tid; j < a; j += BT) {
-    T t = F[a + (size_t)j * ld];
-    F[a + (size_t)j * ld] = F[b + (size_t)j * ld];
+    T t = ldf<T, CG>(F + a + (size_t)j * ld);
+    F[a + (size_t)j * ld] = ldf<T, CG>(F + b + (size_t)j * ld);
     F[b + (size_t)j * ld] = t;
   }
   // F[j, a] <-> F[b, j] for a < j < b
   for (int j = a + 1 + tid; j < b; j += BT) {
-    T t = F[j + (size_t)a * ld];
-    F[j + (size_t)a * ld] = F[b + (size_t)j * ld];
+    T t = ldf<T, CG>(F + j + (size_t)a * ld);
+    F[j + (size_t)a * ld] = ldf<T, CG>(F + b + (size_t)j * ld);
     F[b + (size_t)j * ld] = t;
   }
   // F[j, a] <-> F[j, b] for j > b
   for (int j = b + 1 + tid; j < n; j += BT) {
-    T t = F[j + (size_t)a * ld];
-    F[j + (size_t)a * ld] = F[j + (size_t)b * ld];
+    T t = ldf<T, CG>(F + j + (size_t)a * ld);
+    F[j + (size_t)a * ld] = ldf<T, CG>(F + j + (size_t)b * ld);
     F[j + (size_t)b * ld] = t;
   }
   if (tid == 0) {
-    T t = F[a + (size_t)a * ld];
-    F[a + (size_t)a * ld] = F[b + (size_t)b * ld];
+    T t = ldf<T, CG>(F + a + (size_t)a * ld);
+    F[a + (size_t)a * ld] = ldf<T, CG>(F + b + (size_t)b * ld);
     F[b + (size_t)b * ld] = t;
     int tv = vars[a];
     vars[a] = vars[b];
@@ -1260,46 +1269,80 @@ struct SwCtl {
   int rows[2 * NB], src[2 * NB], nrows;
 };
 
+// The pending interchanges of a panel composed into one row map (rows[t]
+// takes the value of row src[t]); run by one thread, resets the list.
+template <class C>
+__device__ void compose_swaps(C& c) {
+  int nr = 0;
+  for (int s = 0; s < c.nsw; s++) {
+    const int pr[2] = {c.swa[s], c.swb[s]};
+    int at[2];
+    for (int u = 0; u < 2; u++) {
+      at[u] = -1;
+      for (int t = 0; t < nr; t++)
+        if (c.rows[t] == pr[u]) at[u] = t;
+      if (at[u] < 0) {
+        c.rows[nr] = pr[u];
+        c.src[nr] = pr[u];
+        at[u] = nr++;
+      }
+    }
+    const int tmp = c.src[at[0]];
+    c.src[at[0]] = c.src[at[1]];
+    c.src[at[1]] = tmp;
+  }
+  c.nrows = nr;
+  c.nsw = 0;
+}
+
+// Row map applied to the columns [0, kstart) of F by warps gw, gw + gws,
+// ...: a warp takes 8 columns at a time, its lanes load the mapped rows of
+// all 8 before storing any (nr <= 64 rows).  L2 loads (CG) where another
+// CTA may have written the entries in the same launch.
+template <class T, bool CG>
+__device__ void apply_row_map(T* F, int ld, int kstart, const int* rows,
+                              const int* src, int nr, int gw, int gws) {
+  const int lane = threadIdx.x & 31;
+  const bool h0 = lane < nr, h1 = lane + 32 < nr;
+  const int s0 = h0 ? src[lane] : 0, s1 = h1 ? src[lane + 32] : 0;
+  const int d0 = h0 ? rows[lane] : 0, d1 = h1 ? rows[lane + 32] : 0;
+  constexpr int CB = 8;
+  for (int j0 = gw * CB; j0 < kstart; j0 += gws * CB) {
+    T v0[CB], v1[CB];
+#pragma unroll
+    for (int u = 0; u < CB; u++) {
+      const T* Fj = F + (size_t)(j0 + u) * ld;
+      const bool in = j0 + u < kstart;
+      if constexpr (CG) {
+        v0[u] = in && h0 ? __ldcg(Fj + s0) : T(0);
+        v1[u] = in && h1 ? __ldcg(Fj + s1) : T(0);
+      } else {
+        v0[u] = in && h0 ? Fj[s0] : T(0);
+        v1[u] = in && h1 ? Fj[s1] : T(0);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < CB; u++) {
+      if (j0 + u >= kstart) break;
+      T* Fj = F + (size_t)(j0 + u) * ld;
+      if (h0) Fj[d0] = v0[u];
+      if (h1) Fj[d1] = v1[u];
+    }
+  }
+}
+
 // Apply the pending interchanges to the columns [0, kstart) left of the
-// panel: thread 0 composes them into one row map, then each warp takes
-// columns and its lanes move the rows of the map (loads before stores).
+// panel: thread 0 composes them into one row map, then the CTA's warps
+// move the rows of the map.
 template <class T, int PT>
 __device__ void sw_flush_left(T* F, int ld, int kstart, SwCtl<PT>& c) {
   __syncthreads();
   if (c.nsw == 0) return;
-  if (threadIdx.x == 0) {
-    int nr = 0;
-    for (int s = 0; s < c.nsw; s++) {
-      const int pr[2] = {c.swa[s], c.swb[s]};
-      int at[2];
-      for (int u = 0; u < 2; u++) {
-        at[u] = -1;
-        for (int t = 0; t < nr; t++)
-          if (c.rows[t] == pr[u]) at[u] = t;
-        if (at[u] < 0) {
-          c.rows[nr] = pr[u];
-          c.src[nr] = pr[u];
-          at[u] = nr++;
-        }
-      }
-      const int tmp = c.src[at[0]];
-      c.src[at[0]] = c.src[at[1]];
-      c.src[at[1]] = tmp;
-    }
-    c.nrows = nr;
-    c.nsw = 0;
-  }
+  if (threadIdx.x == 0) compose_swaps(c);
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nr = c.nrows;
-  for (int j = warp; j < kstart; j += PT / 32) {
-    T* Fj = F + (size_t)j * ld;
-    const T v0 = lane < nr ? Fj[c.src[lane]] : T(0);
-    const T v1 = lane + 32 < nr ? Fj[c.src[lane + 32]] : T(0);
-    __syncwarp();
-    if (lane < nr) Fj[c.rows[lane]] = v0;
-    if (lane + 32 < nr) Fj[c.rows[lane + 32]] = v1;
-  }
+  apply_row_map<T, false>(F, ld, kstart, c.rows, c.src, c.nrows, threadIdx.x >> 5,
+                          PT / 32);
   __syncthreads();
 }
 
@@ -1366,6 +1409,21 @@ __device__ __forceinline__ void sw_reduce(SwCtl<PT>& c, int set, double& v,
     argmax_merge(v, i, ov, oi);
     v2 = fmax(v2, ov2);
   }
+}
+
+// The D^-1 of a 2x2 pivot block [d11 d21; d21 d22] as the coefficients of
+// its two L columns in terms of their W columns: l0 = w0 i00 + w1 i10,
+// l1 = w1 i11 + w0 i01.
+struct Coef2 {
+  double i00, i10, i11, i01;
+  bool finite;
+};
+template <class T>
+__device__ __forceinline__ Coef2 pivot2_coeffs(T d11, T d21, T d22) {
+  const T detinv = T(1) / (d11 * d22 - d21 * d21);
+  return Coef2{(double)(d22 * detinv), (double)(-d21 * detinv),
+               (double)(d11 * detinv), (double)(-d21 * detinv),
+               (bool)isfinite((double)detinv)};
 }
 
 // acc[i] -= sum_j L[r_i, j] * y[j] over the panel's columns j < kw, with
@@ -1581,18 +1639,16 @@ __device__ void panel_factor_sw(T* F, int ld, T* Wg, int n, bool root,
         c.cP[kw] = kw;
         vars[3 * ld + k] = 0;
       } else {
-        const T d11 = Ws[(size_t)kw * cld + krow];
-        const T d21 = Ws[(size_t)kw * cld + krow + 1];
-        const T d22 = Ws[(size_t)(kw + 1) * cld + krow + 1];
-        const T detinv = T(1) / (d11 * d22 - d21 * d21);
-        if (!isfinite((double)detinv)) atomicOr(status, ST_NAN);
+        const Coef2 q = pivot2_coeffs<T>(Ws[(size_t)kw * cld + krow],
+                                         Ws[(size_t)kw * cld + krow + 1],
+                                         Ws[(size_t)(kw + 1) * cld + krow + 1]);
+        if (!q.finite) atomicOr(status, ST_NAN);
         c.kind[kw] = 1;
         c.kind[kw + 1] = 2;
-        // l0 = w0 i00 + w1 i10, l1 = w1 i11 + w0 i01
-        c.cA[kw] = (double)(d22 * detinv);       // i00
-        c.cB[kw] = (double)(-d21 * detinv);      // i10
-        c.cA[kw + 1] = (double)(d11 * detinv);   // i11
-        c.cB[kw + 1] = (double)(-d21 * detinv);  // i01
+        c.cA[kw] = q.i00;
+        c.cB[kw] = q.i10;
+        c.cA[kw + 1] = q.i11;
+        c.cB[kw + 1] = q.i01;
         c.cP[kw] = kw + 1;
         c.cP[kw + 1] = kw;
         vars[k] = -(vars[k] + 1);
@@ -1705,6 +1761,533 @@ k_big_panel_sw(DevicePlan d, const int* __restrict__ nodes, double ustab,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Cluster panel: the shared-W panel with the front's rows spread over a
+// thread-block cluster of CS CTAs, for levels of a few large fronts (the
+// top-of-tree chain of a 2D KKT is a sequence of single ~1,100-row fronts,
+// which the one-CTA panel leaves to one SM).  The pivot rule, candidate
+// order, interchanges and the arithmetic of every row are those of
+// panel_factor_sw; what changes is where the rows live:
+//   * rows are dealt to the CTAs in groups of 32 (relative row group g to
+//     CTA g mod CS), so that every warp's global accesses stay coalesced
+//     and the rows still live as k advances stay balanced over the CTAs;
+//   * each CTA keeps the W entries of its own rows in its shared memory,
+//     so a column build reads local shared memory only, plus the W row of
+//     the column being built, which each warp reads once from the owning
+//     CTA (distributed shared memory) and broadcasts by shuffles;
+//   * a reduction stores each warp's partial into every CTA's copy of the
+//     slots and one cluster barrier publishes them, so that every CTA takes
+//     the same decision from the same values -- and so passes the same
+//     sequence of cluster barriers;
+//   * an interchange moves W rows between CTAs through distributed shared
+//     memory; F entries another CTA may have written in the same launch are
+//     read from L2.
+// With the one-CTA panel's widths (width_rule 1) the results are the one-
+// CTA panel's bit for bit; by default every panel takes NB columns.
+constexpr int kClThreads = 128;
+constexpr int kClRows = 4;
+constexpr int kClCS = 8;
+constexpr int kClMaxRows = kClThreads * kClRows * kClCS;
+constexpr int kClSlack = 64;
+constexpr int kClSmemMax = NB * 32 * (kClMaxRows / 32 / kClCS) * 8;
+
+template <int PT, int CS>
+struct ClCtl {
+  static constexpr int NS = CS * (PT / 32);  // warps of the cluster
+  double rv[4][NS];   // reduction slots by step parity and kind, as SwCtl
+  int ri[4][NS];
+  double rv2[4][NS];
+  double wkk[2], wii[2], wik[2];  // from the owners of rows k and imax
+  double cA[NB], cB[NB];
+  int cP[NB], kind[NB];
+  int swa[NB], swb[NB], nsw;
+  int rows[2 * NB], src[2 * NB], nrows;
+  double xrow[2][NB];  // a W row received in an interchange (for a, for b)
+  int u[4];            // launch-uniform values published by CTA 0
+};
+
+template <int CS>
+__device__ __forceinline__ int cl_owner(int q) { return (q >> 5) % CS; }
+template <int CS>
+__device__ __forceinline__ int cl_lrow(int q) { return (((q >> 5) / CS) << 5) | (q & 31); }
+
+// Block-wide reductions of sw_reduce over the whole cluster.
+// (ts: trace only, the clock after the warp fold, the barrier and the
+// final fold.)
+template <int PT, int CS, class Cl>
+__device__ __forceinline__ void cl_reduce(ClCtl<PT, CS>& c, Cl& cluster, int set,
+                                          double& v, int& i, double& v2,
+                                          long long* ts = nullptr) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    const double ov2 = __shfl_xor_sync(0xffffffffu, v2, o);
+    argmax_merge(v, i, ov, oi);
+    v2 = fmax(v2, ov2);
+  }
+  if (ts) ts[0] = clock64() + (v != v ? 1 : 0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int slot = (int)cluster.block_rank() * (PT / 32) + warp;
+  if (lane < CS) {
+    ClCtl<PT, CS>* dst = cluster.map_shared_rank(&c, lane);
+    dst->rv[set][slot] = v;
+    dst->ri[set][slot] = i;
+    dst->rv2[set][slot] = v2;
+  }
+  cluster.sync();
+  if (ts) ts[1] = clock64();
+  constexpr int NS = ClCtl<PT, CS>::NS;
+  static_assert(NS <= 64, "cluster warps");
+  v = lane < NS ? c.rv[set][lane] : -1.0;
+  i = lane < NS ? c.ri[set][lane] : 0x7fffffff;
+  v2 = lane < NS ? c.rv2[set][lane] : 0.0;
+  if (NS > 32 && lane + 32 < NS) {
+    argmax_merge(v, i, c.rv[set][lane + 32], c.ri[set][lane + 32]);
+    v2 = fmax(v2, c.rv2[set][lane + 32]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+    const double ov2 = __shfl_xor_sync(0xffffffffu, v2, o);
+    argmax_merge(v, i, ov, oi);
+    v2 = fmax(v2, ov2);
+  }
+  if (ts) ts[2] = clock64() + (v != v ? 1 : 0);
+}
+
+// *slot = v in every CTA of the cluster (one thread).
+template <int CS, class Cl>
+__device__ __forceinline__ void cl_bcast(Cl& cluster, double* slot, double v) {
+#pragma unroll
+  for (int r = 0; r < CS; r++) *cluster.map_shared_rank(slot, r) = v;
+}
+
+// W rows a and b (relative) interchanged over the columns [0, ncol): the
+// thread owning each row sends its entries to the other row's owner, a
+// cluster barrier, each owner stores what it received, and a second
+// barrier before any CTA reads either row again (the barriers also
+// publish the caller's F writes made before this call).
+template <class T, int PT, int RPT, int CS, class Cl>
+__device__ void cl_swap_wrows(T* Wl, int lld, int ncol, int a, int b,
+                              const int (&rel)[RPT], const int (&lr)[RPT],
+                              ClCtl<PT, CS>& c, Cl& cluster) {
+  const int cr = (int)cluster.block_rank();
+  const int oa = cl_owner<CS>(a), ob = cl_owner<CS>(b);
+#pragma unroll
+  for (int i = 0; i < RPT; i++) {
+    if (cr == oa && rel[i] == a) {
+      double* dst = cluster.map_shared_rank(&c.xrow[1][0], ob);
+      for (int j = 0; j < ncol; j++) dst[j] = (double)Wl[(size_t)j * lld + lr[i]];
+    }
+    if (cr == ob && rel[i] == b) {
+      double* dst = cluster.map_shared_rank(&c.xrow[0][0], oa);
+      for (int j = 0; j < ncol; j++) dst[j] = (double)Wl[(size_t)j * lld + lr[i]];
+    }
+  }
+  cluster.sync();
+#pragma unroll
+  for (int i = 0; i < RPT; i++) {
+    if (cr == oa && rel[i] == a)
+      for (int j = 0; j < ncol; j++) Wl[(size_t)j * lld + lr[i]] = T(c.xrow[0][j]);
+    if (cr == ob && rel[i] == b)
+      for (int j = 0; j < ncol; j++) Wl[(size_t)j * lld + lr[i]] = T(c.xrow[1][j]);
+  }
+  cluster.sync();
+}
+
+template <class T, int PT, int RPT, int CS, class Cl>
+__device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
+                                int* vars, int* fsperm, double ustab,
+                                double pivot_tol, int* status, ClCtl<PT, CS>& c,
+                                T* Wl, int lld, int nbe, int& k_, int& nc_,
+                                int& kw_, int* dbg, Cl& cluster) {
+  constexpr int NW = PT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int cr = (int)cluster.block_rank();
+  const bool lead = cr == 0 && tid == 0;
+  if (tid == 0) c.nsw = 0;
+  int k = k_, nc = nc_, kw = 0;
+  const int kstart = k;
+  int rel[RPT], lr[RPT];  // owned rows: relative to kstart, and local
+  bool on[RPT];
+  T cur[RPT];
+#pragma unroll
+  for (int i = 0; i < RPT; i++) {
+    lr[i] = 32 * (warp + NW * i) + lane;
+    rel[i] = 32 * (CS * (warp + NW * i) + cr) + lane;
+  }
+  auto load_col = [&](int col, T (&dst)[RPT]) {
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+      const int r = kstart + rel[i];
+      dst[i] = (r >= col && r < n) ? __ldcg(F + r + (size_t)col * ld) : T(0);
+    }
+  };
+  // acc[i] -= sum_{j < kw} L[r_i, j] W[y, j] in sw_apply_panel's order; the
+  // warp reads W row y (relative) from its owner once, lane j holding
+  // column j (kw <= NB - 2 < 32)
+  long long ts[10];  // trace only: clocks of the phases of a step (lead)
+  const bool tr = dbg != nullptr && lead;
+  auto apply = [&](int y, T (&acc)[RPT]) {
+    const T* yrow = cluster.map_shared_rank(Wl + cl_lrow<CS>(y), cl_owner<CS>(y));
+    const T yv = lane < kw ? yrow[(size_t)lane * lld] : T(0);
+    if (tr) ts[1] = clock64() + (yv != yv ? 1 : 0);
+    int j = 0;
+    for (; j + 2 <= kw; j += 2) {
+      const T* w0 = Wl + (size_t)j * lld;
+      const T* w1 = w0 + lld;
+      const T* p0 = Wl + (size_t)c.cP[j] * lld;
+      const T* p1 = Wl + (size_t)c.cP[j + 1] * lld;
+      const T a0 = T(c.cA[j]), b0 = T(c.cB[j]);
+      const T a1 = T(c.cA[j + 1]), b1 = T(c.cB[j + 1]);
+      const T y0 = __shfl_sync(0xffffffffu, yv, j);
+      const T y1 = __shfl_sync(0xffffffffu, yv, j + 1);
+#pragma unroll
+      for (int i = 0; i < RPT; i++)
+        if (on[i]) {
+          const T l0 = sw_l(w0[lr[i]], p0[lr[i]], a0, b0);
+          const T l1 = sw_l(w1[lr[i]], p1[lr[i]], a1, b1);
+          acc[i] -= l0 * y0;
+          acc[i] -= l1 * y1;
+        }
+    }
+    if (j < kw) {
+      const T* w0 = Wl + (size_t)j * lld;
+      const T* p0 = Wl + (size_t)c.cP[j] * lld;
+      const T a0 = T(c.cA[j]), b0 = T(c.cB[j]);
+      const T y0 = __shfl_sync(0xffffffffu, yv, j);
+#pragma unroll
+      for (int i = 0; i < RPT; i++)
+        if (on[i]) acc[i] -= sw_l(w0[lr[i]], p0[lr[i]], a0, b0) * y0;
+    }
+    if (tr) ts[2] = clock64() + (acc[0] != acc[0] ? 1 : 0);
+  };
+  load_col(k, cur);
+  int par = 0;
+  unsigned long long* cyc =
+      dbg ? reinterpret_cast<unsigned long long*>(dbg + 8) : nullptr;
+  long long tc0 = 0, tc1 = 0, tc2 = 0, tc3 = 0;
+  while (kw < nbe - 1 && k < nc) {
+    if (cyc && lead) tc0 = clock64();
+    if (tr) ts[0] = tc0;
+    par ^= 1;
+    T nxt[RPT];
+    load_col(k + 1, nxt);
+    T acc[RPT];
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+      const int r = kstart + rel[i];
+      acc[i] = cur[i];
+      on[i] = r >= k && r < n;
+    }
+    apply(k - kstart, acc);
+    long long tb[3];
+    double bv = -1.0, tv = 0.0;
+    int bi = 0x7fffffff;
+    T* wcol = Wl + (size_t)kw * lld;
+#pragma unroll
+    for (int i = 0; i < RPT; i++)
+      if (on[i]) {
+        const int r = kstart + rel[i];
+        wcol[lr[i]] = acc[i];
+        const double a = fabs((double)acc[i]);
+        if (r == k) cl_bcast<CS>(cluster, &c.wkk[par], (double)acc[i]);
+        else if (r < nc) argmax_merge(bv, bi, a, r);
+        else tv = fmax(tv, a);
+      }
+    if (cyc && lead) tc1 = clock64();
+    if (tr) ts[3] = tc1;
+    cl_reduce<PT, CS>(c, cluster, 2 * par, bv, bi, tv, tr ? tb : nullptr);
+    if (cyc && lead) tc2 = clock64();
+    int imax = bi;
+    if (imax >= nc || imax <= k) {
+      if (k + 1 < nc && lead) atomicOr(status, ST_NAN);
+      imax = (k + 1 < n) ? k + 1 : k;
+    }
+    const double wkk = c.wkk[par];
+    const PivotChoice pc = choose_pivot(
+        root, k, nc, wkk, imax, bv < 0.0 ? 0.0 : bv, tv, ustab, pivot_tol, [&]() {
+          // column imax into W[:, kw + 1]; its owner publishes its diagonal
+          // and the candidate column's entry in row imax
+          T a2[RPT];
+#pragma unroll
+          for (int i = 0; i < RPT; i++) {
+            const int r = kstart + rel[i];
+            a2[i] = !on[i] ? T(0)
+                           : (r < imax ? __ldcg(F + imax + (size_t)r * ld)
+                                       : __ldcg(F + r + (size_t)imax * ld));
+          }
+          apply(imax - kstart, a2);
+          double rv = -1.0, rt = 0.0;
+          int ri = 0x7fffffff;
+          T* w2 = Wl + (size_t)(kw + 1) * lld;
+#pragma unroll
+          for (int i = 0; i < RPT; i++)
+            if (on[i]) {
+              const int r = kstart + rel[i];
+              w2[lr[i]] = a2[i];
+              if (r == imax) {
+                cl_bcast<CS>(cluster, &c.wii[par], (double)a2[i]);
+                cl_bcast<CS>(cluster, &c.wik[par], (double)wcol[lr[i]]);
+              } else {
+                rt = fmax(rt, fabs((double)a2[i]));
+              }
+            }
+          cl_reduce<PT, CS>(c, cluster, 2 * par + 1, rv, ri, rt);
+          return ImaxColumn{rt, c.wii[par], c.wik[par]};
+        });
+    if (cyc && lead) {
+      tc3 = clock64();
+      atomicAdd(cyc + 0, (unsigned long long)(tc1 - tc0));
+      atomicAdd(cyc + 1, (unsigned long long)(tc2 - tc1));
+      atomicAdd(cyc + 2, (unsigned long long)(tc3 - tc2));
+      ts[4] = tb[0];
+      ts[5] = tb[1];
+      ts[6] = tb[2];
+      ts[7] = tc3;
+    }
+    if (pc.step == 0) {
+      if (dbg && lead) atomicAdd(dbg + 4, 1);
+      // delay candidate k (the full interchange with nc - 1 after the
+      // pending ones, by CTA 0; the W rows by their owners)
+      if (k < nc - 1) {
+        if (cr == 0) {
+          __syncthreads();
+          if (c.nsw > 0) {
+            if (tid == 0) compose_swaps(c);
+            __syncthreads();
+            apply_row_map<T, true>(F, ld, kstart, c.rows, c.src, c.nrows, warp, NW);
+          }
+          __syncthreads();
+          symm_swap<T, PT, true>(F, ld, n, vars, fsperm, k, nc - 1);
+        } else if (tid == 0) {
+          c.nsw = 0;
+        }
+        cl_swap_wrows<T, PT, RPT, CS>(Wl, lld, kw, k - kstart, nc - 1 - kstart, rel, lr,
+                                      c, cluster);
+      }
+      nc -= 1;
+      load_col(k, cur);
+      continue;
+    }
+    const int step = pc.step, kpiv = pc.kpiv;
+    const int ksrc = k + step - 1;
+    const bool swapped = kpiv != ksrc;
+    if (dbg && lead)
+      atomicAdd(dbg + (step == 1 ? (pc.imax_1x1 ? 1 : 0) : (swapped ? 3 : 2)), 1);
+    if (pc.imax_1x1) {
+      // column imax is the pivot column (own rows)
+      T* w2 = Wl + (size_t)(kw + 1) * lld;
+#pragma unroll
+      for (int i = 0; i < RPT; i++)
+        if (on[i]) wcol[lr[i]] = w2[lr[i]];
+    }
+    if (swapped) {
+      // the entries of the interchange that stay live, from the registers
+      // of column ksrc (own rows); the record for the columns left of the
+      // panel; the W rows by their owners
+      const int a = ksrc, b = kpiv;
+#pragma unroll
+      for (int i = 0; i < RPT; i++) {
+        if (!on[i]) continue;
+        const int r = kstart + rel[i];
+        const T v = step == 1 ? cur[i] : nxt[i];
+        if (r > a && r < b) F[b + (size_t)r * ld] = v;
+        else if (r > b) F[r + (size_t)b * ld] = v;
+        else if (r == a) F[b + (size_t)b * ld] = v;
+      }
+      if (tid == 0) {
+        c.swa[c.nsw] = a;
+        c.swb[c.nsw] = b;
+        c.nsw++;
+      }
+      if (lead) {
+        int tv2 = vars[a];
+        vars[a] = vars[b];
+        vars[b] = tv2;
+        tv2 = fsperm[a];
+        fsperm[a] = fsperm[b];
+        fsperm[b] = tv2;
+      }
+      cl_swap_wrows<T, PT, RPT, CS>(Wl, lld, kw + step, a - kstart, b - kstart, rel, lr,
+                                    c, cluster);
+    }
+    // the pivot block after the interchange: W[k, kw] is the candidate's
+    // diagonal (column imax's for an imax 1x1 pivot); for a 2x2 pivot
+    // W[k + 1, kw] and W[k + 1, kw + 1] are the entry of row imax and the
+    // diagonal of column imax
+    if (step == 1) {
+      const T d = pc.imax_1x1 ? T(c.wii[par]) : T(wkk);
+      if (!isfinite((double)d) && lead) atomicOr(status, ST_NAN);
+      c.kind[kw] = 0;
+      c.cA[kw] = pc.zero ? 0.0 : (double)(T(1) / d);
+      c.cB[kw] = 0.0;
+      c.cP[kw] = kw;
+      if (lead) vars[3 * ld + k] = 0;
+    } else {
+      const Coef2 q = pivot2_coeffs<T>(T(wkk), T(c.wik[par]), T(c.wii[par]));
+      if (!q.finite && lead) atomicOr(status, ST_NAN);
+      c.kind[kw] = 1;
+      c.kind[kw + 1] = 2;
+      c.cA[kw] = q.i00;
+      c.cB[kw] = q.i10;
+      c.cA[kw + 1] = q.i11;
+      c.cB[kw + 1] = q.i01;
+      c.cP[kw] = kw + 1;
+      c.cP[kw + 1] = kw;
+      if (lead) {
+        vars[k] = -(vars[k] + 1);
+        vars[k + 1] = -(vars[k + 1] + 1);
+        vars[3 * ld + k] = 1;
+        vars[3 * ld + k + 1] = 2;
+      }
+    }
+    k += step;
+    kw += step;
+    if (!swapped && step == 1) {
+#pragma unroll
+      for (int i = 0; i < RPT; i++) cur[i] = nxt[i];
+    } else {
+      load_col(k, cur);
+    }
+    if (cyc && lead) atomicAdd(cyc + 3, (unsigned long long)(clock64() - tc3));
+    if (tr) {
+      // fine phases of the steps without an interchange or a second column
+      // (dbg + 32: y row, column build, W stores, warp fold, barrier, final
+      // fold, decision, rest; then all other steps' cycles and count)
+      ts[8] = clock64() + (cur[0] != cur[0] ? 1 : 0);
+      unsigned long long* fine = reinterpret_cast<unsigned long long*>(dbg + 32);
+      if (step == 1 && !swapped && !pc.imax_1x1) {
+        for (int q = 0; q < 8; q++) atomicAdd(fine + q, (unsigned long long)(ts[q + 1] - ts[q]));
+      } else {
+        atomicAdd(fine + 8, (unsigned long long)(ts[8] - ts[0]));
+        atomicAdd(fine + 9, 1ull);
+      }
+    }
+  }
+  // --- the pending interchanges left of the panel (every CTA composes the
+  // same map; the cluster's warps share the columns); the panel's L columns
+  // to F and its W rows below k to HBM, each CTA for its own rows
+  if (cyc && lead) tc0 = clock64();
+  __syncthreads();
+  if (c.nsw > 0) {
+    if (tid == 0) compose_swaps(c);
+    __syncthreads();
+    apply_row_map<T, true>(F, ld, kstart, c.rows, c.src, c.nrows, cr * NW + warp, CS * NW);
+  }
+  for (int j = 0; j < kw; j++) {
+    const int col = kstart + j;
+    const int kd = c.kind[j];
+    const T* w0 = Wl + (size_t)j * lld;
+    const T* wp = Wl + (size_t)c.cP[j] * lld;
+    const T a = T(c.cA[j]), b = T(c.cB[j]);
+    T* Fc = F + (size_t)col * ld;
+    T* Wc = Wg + (size_t)j * ld;
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+      const int r = kstart + rel[i];
+      if (r < col || r >= n) continue;
+      const T w = w0[lr[i]];
+      // the pivot block's own entries are D; below it, L
+      if (r == col || (kd == 1 && r == col + 1)) Fc[r] = w;
+      else Fc[r] = sw_l(w, wp[lr[i]], a, b);
+      if (r >= k) Wc[r] = w;
+    }
+  }
+  if (cyc && lead) atomicAdd(cyc + 4, (unsigned long long)(clock64() - tc0));
+  k_ = k;
+  nc_ = nc;
+  kw_ = kw;
+}
+
+// W local rows of a CTA for a panel starting at relative row 0 of cld
+// rows: the CTA's share of the 32-row groups.
+template <int CS>
+__host__ __device__ __forceinline__ int cl_local_rows(int cld) {
+  return 32 * (((cld + 31) / 32 + CS - 1) / CS);
+}
+
+template <class T, int PT, int RPT, int CS>
+__global__ void __launch_bounds__(PT, 1)
+k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
+               double pivot_tol, int smem_bytes, int width_rule, int* dbg) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  __shared__ ClCtl<PT, CS> c;
+  __shared__ CtlT<PT> ctl;
+  extern __shared__ double cl_raw[];
+  const int cr = (int)cluster.block_rank();
+  const int node = nodes[blockIdx.x / CS];
+  int* st = d.pstate + 4 * node;
+  // every CTA of the cluster has started before any distributed shared
+  // memory access; CTA 0 then publishes the values that steer the launch
+  cluster.sync();
+  if (cr == 0 && threadIdx.x == 0) {
+    const int u0 = big_skip(d) ? 1 : 0, u1 = st[0], u2 = st[1];
+    for (int r = 0; r < CS; r++) {
+      ClCtl<PT, CS>* dst = cluster.map_shared_rank(&c, r);
+      dst->u[0] = u0;
+      dst->u[1] = u1;
+      dst->u[2] = u2;
+    }
+  }
+  cluster.sync();
+  if (c.u[0]) return;
+  int k = c.u[1], nc = c.u[2];
+  if (k >= nc) {
+    if (cr == 0 && threadIdx.x == 0) st[3] = 0;
+    return;
+  }
+  const int f = d.f[node];
+  const int fs = d.ns[node] + d.ndin[node];
+  T* F = reinterpret_cast<T*>(d.fpool) + d.foff[node];
+  T* W = F + (size_t)f * f;
+  int* fvars = d.ipool + d.ioff[node];
+  const int kstart = k;
+  int kw = 0;
+  const int cld = f - kstart;
+  const int lld = cl_local_rows<CS>(cld);
+  // the panel width depends on the front alone: NB, or the one-CTA
+  // panel's (width_rule 1)
+  int nbe = NB;
+  int max_rows = CS * PT * RPT;
+  if (width_rule == 1) {
+    // the one-CTA panel's widths and its row limit (beyond which it takes
+    // the HBM-panel form, as below)
+    const long long fit = (long long)kSwSmemBytes / ((long long)cld * (long long)sizeof(T));
+    nbe = (int)(fit < NB ? fit : NB);
+    max_rows = kSwThreads * kSwRows;
+  }
+  if (nbe >= 4 && cld <= max_rows &&
+      (long long)nbe * lld * (long long)sizeof(T) <= smem_bytes) {
+    long long tk0 = 0;
+    if (dbg && cr == 0 && threadIdx.x == 0) {
+      atomicAdd(dbg + 5, 1);
+      tk0 = clock64();
+    }
+    panel_factor_cl<T, PT, RPT, CS>(F, f, W, f, fs == f, fvars, fvars + f, ustab,
+                                    pivot_tol, d.status, c, reinterpret_cast<T*>(cl_raw),
+                                    lld, nbe, k, nc, kw, dbg, cluster);
+    if (dbg && cr == 0 && threadIdx.x == 0)
+      atomicAdd(reinterpret_cast<unsigned long long*>(dbg + 8) + 5,
+                (unsigned long long)(clock64() - tk0));
+    // no CTA leaves while another may still read its shared memory
+    cluster.sync();
+  } else {
+    // a front grown past the launch's shared memory (delayed pivots): the
+    // HBM-panel form on CTA 0 (no distributed shared memory is used)
+    if (cr != 0) return;
+    panel_factor<T, PT>(F, f, W, f, f, fs == f, fvars, fvars + f, ustab,
+                        pivot_tol, d.status, ctl, k, nc, kw);
+  }
+  if (cr == 0 && threadIdx.x == 0) {
+    st[0] = k;
+    st[1] = nc;
+    st[2] = kstart;
+    st[3] = kw;
+  }
+}
+
 template <class T>
 __global__ void __launch_bounds__(NT)
 k_big_update(DevicePlan d, const int* __restrict__ nodes) {
@@ -1800,6 +2383,30 @@ __global__ void k_big_remaining(DevicePlan d, const int* __restrict__ nodes,
     }                                                                     \
   } while (0)
 
+// One cluster of kClCS CTAs per front (cudaLaunchKernelEx with a cluster
+// dimension).
+template <class T>
+static int launch_panel_cl(int fronts, int smem, cudaStream_t s, const DevicePlan& d,
+                           const int* nodes, double ustab, double pivot_tol,
+                           int width_rule, int* dbg) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(fronts * kClCS);
+  cfg.blockDim = dim3(kClThreads);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kClCS;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  FCUDA(cudaLaunchKernelEx(&cfg, k_big_panel_cl<T, kClThreads, kClRows, kClCS>, d,
+                           nodes, ustab, pivot_tol, smem, width_rule, dbg));
+  ab::count_launch();
+  return 0;
+}
+
 template <class T>
 static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
   DevicePlan& d = h.d;
@@ -1823,6 +2430,9 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     FCUDA(cudaFuncSetAttribute(k_big_update_tc,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::kSmemBytes));
+    FCUDA(cudaFuncSetAttribute(k_big_panel_cl<T, kClThreads, kClRows, kClCS>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kClSmemMax));
     attr_set = true;
   }
   FCUDA(cudaMemsetAsync(d.counters, 0, 2 * sizeof(unsigned long long), s));
@@ -1843,9 +2453,9 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
   if (trace) {
     ev.resize(3 * d.num_levels);
     for (auto& e : ev) cudaEventCreate(&e);
-    cudaMalloc((void**)&dbg, 32 * sizeof(int) * (size_t)d.num_levels);
-    cudaMemsetAsync(dbg, 0, 32 * sizeof(int) * (size_t)d.num_levels, s);
-    dbg_h.assign(32 * d.num_levels, 0);
+    cudaMalloc((void**)&dbg, 64 * sizeof(int) * (size_t)d.num_levels);
+    cudaMemsetAsync(dbg, 0, 64 * sizeof(int) * (size_t)d.num_levels, s);
+    dbg_h.assign(64 * d.num_levels, 0);
   }
   for (int l = 0; l < d.num_levels; l++) {
     const LevelSchedule& L = h.sched[l];
@@ -1863,7 +2473,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     }
     if (trace) cudaEventRecord(ev[3 * l + 1], s);
     if (L.nbig) {
-      int* dbg_l = dbg ? dbg + 32 * l : nullptr;
+      int* dbg_l = dbg ? dbg + 64 * l : nullptr;
       const int* nodes = d.sched_nodes + L.big_begin;
       const int B = L.nbig;
       const long long fm = L.big_max_f;
@@ -1888,12 +2498,21 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       // shared-W panel for levels whose fronts fit its rows; its shared
       // memory holds up to NB columns of W for the largest static front
       // (fronts grown by delayed pivots get fewer columns)
-      const bool use_sw = fm <= (long long)kSwThreads * kSwRows;
+      // cluster panel for levels of large fronts (mode 0: full-width
+      // panels; mode 2: the one-CTA panel's widths); its shared memory
+      // holds NB columns of W for kClSlack rows more than the largest
+      // static front
+      const bool use_cl = h.panel_mode != 1 && fm >= h.cl_min_rows &&
+                          fm + kClSlack <= kClMaxRows;
+      const int cl_rule = h.panel_mode == 2 ? 1 : 0;
+      const int cl_smem =
+          use_cl ? NB * cl_local_rows<kClCS>((int)fm + kClSlack) * (int)sizeof(T) : 0;
+      const bool use_sw = !use_cl && fm <= (long long)kSwThreads * kSwRows;
       const int sw_smem = kSwSmemBytes;
       // panels a front of big_max_fs candidates needs without delays: each
       // takes nbe - 1 pivots, nbe growing as the remaining rows shrink
       int panels = 0;
-      if (use_sw) {
+      if (use_sw || (use_cl && cl_rule == 1)) {
         for (long long kk = 0; kk < L.big_max_fs; panels++) {
           const long long rows = std::max<long long>(fm - kk, 1);
           const long long nbe = std::min<long long>(
@@ -1912,7 +2531,11 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
         budget += panels;
         for (int it = 0; it < panels; it++) {
           if (trace) cudaEventRecord(te[0], s);
-          if (use_sw)
+          if (use_cl) {
+            const int rc = launch_panel_cl<T>(B, cl_smem, s, d, nodes, h.ustab,
+                                              h.pivot_tol, cl_rule, dbg_l);
+            if (rc) return rc;
+          } else if (use_sw)
             k_big_panel_sw<T, kSwThreads, kSwRows><<<B, kSwThreads, sw_smem, s>>>(
                 d, nodes, h.ustab, h.pivot_tol, sw_smem, dbg_l);
           else if (fm > kPanelWideRows)
@@ -1961,7 +2584,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
   }
   if (trace) {
     cudaStreamSynchronize(s);
-    cudaMemcpy(dbg_h.data(), dbg, 32 * sizeof(int) * (size_t)d.num_levels,
+    cudaMemcpy(dbg_h.data(), dbg, 64 * sizeof(int) * (size_t)d.num_levels,
                cudaMemcpyDeviceToHost);
     cudaFree(dbg);
     float tot_s = 0.f, tot_b = 0.f;
@@ -1976,8 +2599,9 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                    "(fmax %5d) %8.3f ms\n",
                    l, h.sched[l].nsmall, h.sched[l].small_max_f, a,
                    h.sched[l].nbig, h.sched[l].big_max_f, b);
-      const int* q = dbg_h.data() + 32 * l;
+      const int* q = dbg_h.data() + 64 * l;
       const unsigned long long* cy = reinterpret_cast<const unsigned long long*>(q + 8);
+      const unsigned long long* fi = reinterpret_cast<const unsigned long long*>(q + 32);
       if (q[5])
         std::fprintf(stderr, "           panel steps: fast %d imax %d 2x2 %d "
                              "2x2-swap %d delay %d panels %d | kcyc: build %llu "
@@ -1986,6 +2610,13 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                      q[0], q[1], q[2], q[3], q[4], q[5], cy[0] / 1000, cy[1] / 1000,
                      cy[2] / 1000, cy[3] / 1000, cy[4] / 1000, cy[5] / 1000,
                      tpan[l], tupd[l]);
+      const unsigned long long nf = (unsigned long long)q[0];
+      if (fi[0] && nf)
+        std::fprintf(stderr, "           plain-step cycles: yrow %llu build %llu stores %llu "
+                             "fold %llu barrier %llu fold2 %llu decide %llu rest %llu | "
+                             "other steps %llu cycles each (%llu)\n",
+                     fi[0] / nf, fi[1] / nf, fi[2] / nf, fi[3] / nf, fi[4] / nf, fi[5] / nf,
+                     fi[6] / nf, fi[7] / nf, fi[9] ? fi[8] / fi[9] : 0ull, fi[9]);
     }
     std::fprintf(stderr, "total: small %.3f ms, large %.3f ms\n", tot_s, tot_b);
     for (auto& e : ev) cudaEventDestroy(e);

@@ -119,6 +119,11 @@ struct LdlHandle {
   // f * npiv from which a front is solved by a cluster of CTAs, and from
   // which by the cooperative grid
   long long cluster_entries = 1 << 14;
+  // large-front panels: 0 cluster panels for levels whose largest front has
+  // at least cl_min_rows rows, 1 one-CTA panels only, 2 cluster panels
+  // with the one-CTA panel's widths
+  int panel_mode = 0;
+  int cl_min_rows = 384;
   long long wide_entries = 1 << 22;
   // front storage / arithmetic of the next factorization (64: FP64, 32:
   // FP32 fronts for mixed precision) and of the last one

@@ -39,6 +39,137 @@ __device__ __forceinline__ int block_end(const int* kind, int jb, int npiv) {
   return je;
 }
 
+// sum_{j < n} col[j * ld] * v(j), accumulated in the order of j, with the
+// loads issued 16 at a time so that they overlap (the factor streams from
+// HBM / L2 with hundreds of cycles of latency per load).
+template <class T, class VF>
+__device__ __forceinline__ double dot_strided(const T* __restrict__ col, size_t ld,
+                                              int n, VF v) {
+  double acc = 0.0;
+  int j = 0;
+  for (; j + 16 <= n; j += 16) {
+    T a[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) a[u] = col[(size_t)(j + u) * ld];
+#pragma unroll
+    for (int u = 0; u < 16; u++) acc += (double)a[u] * v(j + u);
+  }
+  for (; j < n; j++) acc += (double)col[(size_t)j * ld] * v(j);
+  return acc;
+}
+
+// One lane's share of sum_{i0 <= i < i1} col[i] v(i): rows i0 + lane + 32 t
+// in the order of t, with the loads issued 8 at a time.
+template <class T, class VF>
+__device__ __forceinline__ double lane_dot(const T* __restrict__ col, int i0, int i1,
+                                           int lane, VF v) {
+  double acc = 0.0;
+  int i = i0 + lane;
+  for (; i + 7 * 32 < i1; i += 8 * 32) {
+    T a[8];
+    double b[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      a[u] = col[i + 32 * u];
+      b[u] = v(i + 32 * u);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) acc += (double)a[u] * b[u];
+  }
+  for (; i < i1; i += 32) acc += (double)col[i] * v(i);
+  return acc;
+}
+
+__device__ __forceinline__ double warp_sum_down(double a) {
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+  return a;
+}
+
+// The value of row j of a block held R rows per lane (row lane + 32 r in
+// v[r]), broadcast to the warp.
+template <int R>
+__device__ __forceinline__ double warp_row(const double (&v)[R], int j) {
+  double s = v[0];
+#pragma unroll
+  for (int r = 1; r < R; r++)
+    if ((j >> 5) == r) s = v[r];
+  return __shfl_sync(0xffffffffu, s, j & 31);
+}
+
+// One warp solves the unit lower triangle of a diagonal block (bw <= 32 R
+// rows, column-major in sL with leading dimension lds, pivot kinds in sK)
+// in place on V[0:bw], with the block's values in registers: each step is
+// one broadcast and one multiply-add per row.  A 2x2 pair (kind 1, 2)
+// eliminates both columns at once; its off-diagonal entry belongs to D.
+template <int R>
+__device__ __forceinline__ void warp_lower_solve(const double* sL, int lds,
+                                                 const int* sK, int bw, double* V,
+                                                 int lane) {
+  double v[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = lane + 32 * r;
+    v[r] = i < bw ? V[i] : 0.0;
+  }
+  for (int j = 0; j < bw;) {
+    const bool two = sK[j] == 1;
+    const double v0 = warp_row<R>(v, j);
+    const double v1 = two ? warp_row<R>(v, j + 1) : 0.0;
+    const int i0 = j + (two ? 2 : 1);
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int i = lane + 32 * r;
+      if (i >= i0 && i < bw) {
+        double t = sL[i + j * lds] * v0;
+        if (two) t += sL[i + (j + 1) * lds] * v1;
+        v[r] -= t;
+      }
+    }
+    j = i0;
+  }
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = lane + 32 * r;
+    if (i < bw) V[i] = v[r];
+  }
+}
+
+// One warp solves the unit upper triangle L^T of a diagonal block in place
+// on V[0:bw], from the last pivot backwards: once a pivot's value is final
+// it is broadcast and every earlier row subtracts its term.
+template <int R>
+__device__ __forceinline__ void warp_upper_solve(const double* sL, int lds,
+                                                 const int* sK, int bw, double* V,
+                                                 int lane) {
+  double v[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = lane + 32 * r;
+    v[r] = i < bw ? V[i] : 0.0;
+  }
+  for (int j = bw - 1; j >= 0;) {
+    const bool two = sK[j] == 2;
+    const int jl = two ? j - 1 : j;
+    const double xj = warp_row<R>(v, j);
+    const double xl = two ? warp_row<R>(v, jl) : 0.0;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int i = lane + 32 * r;
+      if (i < jl) {
+        double t = sL[j + i * lds] * xj;
+        if (two) t += sL[jl + i * lds] * xl;
+        v[r] -= t;
+      }
+    }
+    j = jl - 1;
+  }
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = lane + 32 * r;
+    if (i < bw) V[i] = v[r];
+  }
+}
+
 // Front vector of `node` for one right-hand side: the node's own entries
 // of the right-hand side plus the update vectors of its children, placed
 // by the same row map as the factorization's extend-add.  Called by a
@@ -120,27 +251,11 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
       }
       for (int t = tid; t < bw; t += NT) sK[t] = kind[jb + t];
       __syncthreads();
-      if (warp == 0) {
-        for (int j = jb; j < je;) {
-          const bool two = sK[j - jb] == 1;
-          const double v0 = V[j];
-          const double v1 = two ? V[j + 1] : 0.0;
-          const int i0 = j + (two ? 2 : 1);
-          for (int i = i0 + lane; i < je; i += 32) {
-            double t = sL[(i - jb) + (j - jb) * (SB + 1)] * v0;
-            if (two) t += sL[(i - jb) + (j + 1 - jb) * (SB + 1)] * v1;
-            V[i] -= t;
-          }
-          __syncwarp();
-          j = i0;
-        }
-      }
+      if (warp == 0) warp_lower_solve<2>(sL, SB + 1, sK, bw, V + jb, lane);
       __syncthreads();
-      for (int i = je + tid; i < f; i += NT) {
-        double acc = 0.0;
-        for (int j = jb; j < je; j++) acc += L[i + (size_t)j * f] * V[j];
-        V[i] -= acc;
-      }
+      for (int i = je + tid; i < f; i += NT)
+        V[i] -= dot_strided(L + i + (size_t)jb * f, (size_t)f, bw,
+                            [&](int j) { return V[jb + j]; });
       __syncthreads();
       jb = je;
     }
@@ -198,9 +313,8 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
       // t[j] -= sum_{i >= je} L[i, j] t[i] for j in [jb, je): one warp per
       // column, lanes over rows.
       for (int j = jb + warp; j < je; j += NWARP) {
-        double acc = 0.0;
-        for (int i = je + lane; i < f; i += 32) acc += L[i + (size_t)j * f] * V[i];
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        const double acc = warp_sum_down(
+            lane_dot(L + (size_t)j * f, je, f, lane, [&](int i) { return V[i]; }));
         if (lane == 0) V[j] -= acc;
       }
       const int bw = je - jb;
@@ -210,29 +324,8 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
       }
       for (int t = tid; t < bw; t += NT) sK[t] = kind[jb + t];
       __syncthreads();
-      if (warp == 0) {
-        // within the block, backwards: column j (or pair j-1, j)
-        for (int j = je - 1; j >= jb;) {
-          const bool two = sK[j - jb] == 2;
-          const int jl = two ? j - 1 : j;
-          // rows strictly inside the block below this pivot
-          double a0 = 0.0, a1 = 0.0;
-          for (int i = j + 1 + lane; i < je; i += 32) {
-            a0 += sL[(i - jb) + (jl - jb) * (SB + 1)] * V[i];
-            if (two) a1 += sL[(i - jb) + (j - jb) * (SB + 1)] * V[i];
-          }
-          for (int o = 16; o > 0; o >>= 1) {
-            a0 += __shfl_down_sync(0xffffffffu, a0, o);
-            a1 += __shfl_down_sync(0xffffffffu, a1, o);
-          }
-          if (lane == 0) {
-            V[jl] -= a0;
-            if (two) V[j] -= a1;
-          }
-          __syncwarp();
-          j = jl - 1;
-        }
-      }
+      // within the block, backwards: column j (or pair j-1, j)
+      if (warp == 0) warp_upper_solve<2>(sL, SB + 1, sK, bw, V + jb, lane);
       __syncthreads();
       je = jb;
     }
@@ -259,7 +352,7 @@ __device__ __forceinline__ void copy_cg(double* dst, const double* src, int n) {
 }
 
 template <class T>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 1)
 k_clu_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
               int nrhs, int ldx, double* ubuf, const long long* uoff) {
   namespace cg = cooperative_groups;
@@ -295,28 +388,12 @@ k_clu_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
         }
         for (int t = tid; t < bw; t += NT) sK[t] = kind[jb + t];
         __syncthreads();
-        if (warp == 0) {
-          for (int j = jb; j < je;) {
-            const bool two = sK[j - jb] == 1;
-            const double v0 = sv[j];
-            const double v1 = two ? sv[j + 1] : 0.0;
-            const int i0 = j + (two ? 2 : 1);
-            for (int i = i0 + lane; i < je; i += 32) {
-              double t = sL[(i - jb) + (j - jb) * (SB + 1)] * v0;
-              if (two) t += sL[(i - jb) + (j + 1 - jb) * (SB + 1)] * v1;
-              sv[i] -= t;
-            }
-            __syncwarp();
-            j = i0;
-          }
-        }
+        if (warp == 0) warp_lower_solve<2>(sL, SB + 1, sK, bw, sv + jb, lane);
         __syncthreads();
         // the pivot rows below the block
-        for (int i = je + tid; i < npiv; i += NT) {
-          double acc = 0.0;
-          for (int j = jb; j < je; j++) acc += L[i + (size_t)j * f] * sv[j];
-          sv[i] -= acc;
-        }
+        for (int i = je + tid; i < npiv; i += NT)
+          sv[i] -= dot_strided(L + i + (size_t)jb * f, (size_t)f, bw,
+                               [&](int j) { return sv[jb + j]; });
         __syncthreads();
         jb = je;
       }
@@ -335,19 +412,9 @@ k_clu_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
     for (int st = cr; st < nstrip; st += CS) {
       const int i = npiv + st * 32 + lane;
       double acc = 0.0;
-      if (i < f) {
-        const T* Li = L + i;
-        int j = j0;
-        for (; j + 4 <= j1; j += 4) {
-          const double a0 = Li[(size_t)j * f], a1 = Li[(size_t)(j + 1) * f];
-          const double a2 = Li[(size_t)(j + 2) * f], a3 = Li[(size_t)(j + 3) * f];
-          acc += a0 * sv[j];
-          acc += a1 * sv[j + 1];
-          acc += a2 * sv[j + 2];
-          acc += a3 * sv[j + 3];
-        }
-        for (; j < j1; j++) acc += Li[(size_t)j * f] * sv[j];
-      }
+      if (i < f && j1 > j0)
+        acc = dot_strided(L + i + (size_t)j0 * f, (size_t)f, j1 - j0,
+                          [&](int j) { return sv[j0 + j]; });
       part[warp * 32 + lane] = acc;
       __syncthreads();
       if (warp == 0 && i < f) {
@@ -385,7 +452,7 @@ k_clu_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
 }
 
 template <class T>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 1)
 k_clu_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
                int nrhs, int ldx, double* ubuf, const long long* uoff) {
   namespace cg = cooperative_groups;
@@ -412,10 +479,8 @@ k_clu_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
     // t[j] = z[j] - L21[:, j]^T x2 for every pivot column, one warp per
     // column over the cluster's warps
     for (int j = cr * NWARP + warp; j < npiv; j += CS * NWARP) {
-      const T* Lj = L + (size_t)j * f + npiv;
-      double acc = 0.0;
-      for (int i = lane; i < ncr; i += 32) acc += Lj[i] * sx[i];
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+      const double acc = warp_sum_down(lane_dot(L + (size_t)j * f + npiv, 0, ncr, lane,
+                                                [&](int i) { return sx[i]; }));
       if (lane == 0) G[j] = xr[decode_var(fvars[j])] - acc;
     }
     cluster.sync();
@@ -428,9 +493,8 @@ k_clu_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
         if (jb > 0 && kind[jb] == 2) jb--;  // keep 2x2 pairs together
         // t[j] -= sum_{je <= i < npiv} L[i, j] t[i] for j in [jb, je)
         for (int j = jb + warp; j < je; j += NWARP) {
-          double acc = 0.0;
-          for (int i = je + lane; i < npiv; i += 32) acc += L[i + (size_t)j * f] * sv[i];
-          for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+          const double acc = warp_sum_down(lane_dot(L + (size_t)j * f, je, npiv, lane,
+                                                    [&](int i) { return sv[i]; }));
           if (lane == 0) sv[j] -= acc;
         }
         const int bw = je - jb;
@@ -440,27 +504,7 @@ k_clu_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
         }
         for (int t = tid; t < bw; t += NT) sK[t] = kind[jb + t];
         __syncthreads();
-        if (warp == 0) {
-          for (int j = je - 1; j >= jb;) {
-            const bool two = sK[j - jb] == 2;
-            const int jl = two ? j - 1 : j;
-            double a0 = 0.0, a1 = 0.0;
-            for (int i = j + 1 + lane; i < je; i += 32) {
-              a0 += sL[(i - jb) + (jl - jb) * (SB + 1)] * sv[i];
-              if (two) a1 += sL[(i - jb) + (j - jb) * (SB + 1)] * sv[i];
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-              a0 += __shfl_down_sync(0xffffffffu, a0, o);
-              a1 += __shfl_down_sync(0xffffffffu, a1, o);
-            }
-            if (lane == 0) {
-              sv[jl] -= a0;
-              if (two) sv[j] -= a1;
-            }
-            __syncwarp();
-            j = jl - 1;
-          }
-        }
+        if (warp == 0) warp_upper_solve<2>(sL, SB + 1, sK, bw, sv + jb, lane);
         __syncthreads();
         je = jb;
       }
@@ -566,21 +610,7 @@ k_wide_forward(DevicePlan d, const int* __restrict__ nodes, int count,
           sK[t] = w.kind[jb + t];
         }
         __syncthreads();
-        if (warp == 0) {
-          for (int j = 0; j < bw;) {
-            const bool two = sK[j] == 1;
-            const double v0 = sv[j];
-            const double v1 = two ? sv[j + 1] : 0.0;
-            const int i0 = j + (two ? 2 : 1);
-            for (int i = i0 + lane; i < bw; i += 32) {
-              double t = sL[i + j * (WB + 1)] * v0;
-              if (two) t += sL[i + (j + 1) * (WB + 1)] * v1;
-              sv[i] -= t;
-            }
-            __syncwarp();
-            j = i0;
-          }
-        }
+        if (warp == 0) warp_lower_solve<(WB + 32) / 32>(sL, WB + 1, sK, bw, sv, lane);
         __syncthreads();
         for (int t = tid; t < bw; t += NT) w.G[jb + t] = sv[t];
         if (tid == 0) {
@@ -612,9 +642,8 @@ k_wide_forward(DevicePlan d, const int* __restrict__ nodes, int count,
           }
           const int i = je + (int)it * NT + tid;
           if (i < w.f) {
-            const T* Li = w.L + i + (size_t)jb * w.f;
-            double acc = 0.0;
-            for (int j = 0; j < bw; j++) acc += Li[(size_t)j * w.f] * sv[j];
+            const double acc = dot_strided(w.L + i + (size_t)jb * w.f, (size_t)w.f, bw,
+                                           [&](int j) { return sv[j]; });
             w.G[i] = __ldcg(w.G + i) - acc;
           }
         }
@@ -684,12 +713,9 @@ k_wide_backward(DevicePlan d, const int* __restrict__ nodes, int count,
         long long r = (gw - base) % gwarps;
         if (r < 0) r += gwarps;
         for (long long j = r; j < w.npiv; j += gwarps) {
-          const T* Lj = w.L + (size_t)j * w.f;
-          double acc = 0.0;
-          for (int i = w.npiv + lane; i < w.f; i += 32)
-            acc += Lj[i] * __ldcg(w.G + i);
-          for (int o = 16; o > 0; o >>= 1)
-            acc += __shfl_down_sync(0xffffffffu, acc, o);
+          const double acc = warp_sum_down(lane_dot(w.L + (size_t)j * w.f, w.npiv, w.f,
+                                                    lane,
+                                                    [&](int i) { return __ldcg(w.G + i); }));
           if (lane == 0) w.G[j] = __ldcg(w.G + j) - acc;
         }
         base += w.npiv;
@@ -717,27 +743,7 @@ k_wide_backward(DevicePlan d, const int* __restrict__ nodes, int count,
           sK[t] = w.kind[jb + t];
         }
         __syncthreads();
-        if (warp == 0) {
-          for (int j = bw - 1; j >= 0;) {
-            const bool two = sK[j] == 2;
-            const int jl = two ? j - 1 : j;
-            double a0 = 0.0, a1 = 0.0;
-            for (int i = j + 1 + lane; i < bw; i += 32) {
-              a0 += sL[i + jl * (WB + 1)] * sv[i];
-              if (two) a1 += sL[i + j * (WB + 1)] * sv[i];
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-              a0 += __shfl_down_sync(0xffffffffu, a0, o);
-              a1 += __shfl_down_sync(0xffffffffu, a1, o);
-            }
-            if (lane == 0) {
-              sv[jl] -= a0;
-              if (two) sv[j] -= a1;
-            }
-            __syncwarp();
-            j = jl - 1;
-          }
-        }
+        if (warp == 0) warp_upper_solve<(WB + 32) / 32>(sL, WB + 1, sK, bw, sv, lane);
         __syncthreads();
         for (int t = tid; t < bw; t += NT) w.G[jb + t] = sv[t];
         if (tid == 0) {
@@ -762,11 +768,8 @@ k_wide_backward(DevicePlan d, const int* __restrict__ nodes, int count,
         long long r = (gw - base) % gwarps;
         if (r < 0) r += gwarps;
         for (long long j = r; j < jb; j += gwarps) {
-          const T* Lj = w.L + (size_t)j * w.f;
-          double acc = 0.0;
-          for (int i = jb + lane; i < je; i += 32) acc += Lj[i] * __ldcg(w.G + i);
-          for (int o = 16; o > 0; o >>= 1)
-            acc += __shfl_down_sync(0xffffffffu, acc, o);
+          const double acc = warp_sum_down(lane_dot(w.L + (size_t)j * w.f, jb, je, lane,
+                                                    [&](int i) { return __ldcg(w.G + i); }));
           if (lane == 0) w.G[j] = __ldcg(w.G + j) - acc;
         }
         base += jb;

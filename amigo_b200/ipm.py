@@ -124,6 +124,7 @@ class InteriorPointOptimizer:
         # self.lbx / self.ubx, which the kernels use
         self.lbx0, self.ubx0 = self.lbx.clone(), self.ubx.clone()
         self._relaxed = False
+        self._host_bounds = {}
         self._nslack = 0
         self._obj_scale = 1.0
         self._scaling = False
@@ -164,25 +165,35 @@ class InteriorPointOptimizer:
     def get_num_inequalities(self):
         return 0
 
+    def _host_bound(self, name):
+        """Host copy of a bound vector (numpy, n_primal), as the reference's
+        bindings return them (amigo/amigo.cpp:853-880); cached until
+        relax_bounds changes the relaxed ones."""
+        c = self._host_bounds.get(name)
+        if c is None:
+            c = getattr(self, name).cpu().numpy()
+            c.setflags(write=False)
+            self._host_bounds[name] = c
+        return c
+
     def get_lbx(self):
-        """Primal lower bounds as given (device tensor, n_primal)."""
-        return self.lbx0
+        """Primal lower bounds as given."""
+        return self._host_bound("lbx0")
 
     def get_ubx(self):
-        return self.ubx0
+        return self._host_bound("ubx0")
 
     def get_lbx_relaxed(self):
         """The bounds the IPM kernels use: relaxed once relax_bounds ran."""
-        return self.lbx if self._relaxed else self.lbx0
+        return self._host_bound("lbx" if self._relaxed else "lbx0")
 
     def get_ubx_relaxed(self):
-        return self.ubx if self._relaxed else self.ubx0
+        return self._host_bound("ubx" if self._relaxed else "ubx0")
 
     def get_kkt_element_counts(self):
         """(n_d, n_p, n_c): dual-stationarity rows, primal-feasibility rows
         and finite bounds (interior_point_optimizer.h:441-449)."""
-        n_c = int(torch.isfinite(self.lbx0).sum().item() +
-                  torch.isfinite(self.ubx0).sum().item())
+        n_c = int(np.isfinite(self.get_lbx()).sum() + np.isfinite(self.get_ubx()).sum())
         return self.np_, self.nc_, n_c
 
     # -- setup -----------------------------------------------------------
@@ -194,6 +205,8 @@ class InteriorPointOptimizer:
                   self.ubx.data_ptr(), float(factor), float(constr_viol_tol),
                   self._s())
         self._relaxed = True
+        self._host_bounds.pop("lbx", None)
+        self._host_bounds.pop("ubx", None)
 
     # -- slacks (interior_point_optimizer.h:462-494) ----------------------
     def set_slack_mapping(self, slack_indices, constr_indices):

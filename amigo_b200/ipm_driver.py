@@ -206,6 +206,27 @@ class CartPoleProblem:
         self.dm.objective(x, self._obj)
         return float(self._obj.item())
 
+    def create_vector(self):
+        return torch.zeros(self.model.n, dtype=torch.float64, device=self.device)
+
+    def lagrangian(self, alpha, x):
+        """alpha f(x) + lambda^T c(x) (include/optimization_problem.h
+        lagrangian): the multiplier rows of the gradient are c(x)."""
+        return alpha * self.objective(x) + _multiplier_term(self, x)
+
+    def update(self, x):
+        pass
+
+
+def _multiplier_term(p, x):
+    if not hasattr(p, "_g_tmp"):
+        p._g_tmp = torch.zeros(p.model.n, dtype=torch.float64, device=p.device)
+        p._mult_idx = torch.from_numpy(
+            np.nonzero(np.asarray(p.model.mult, bool))[0]).to(p.device)
+    p.gradient(1.0, x, p._g_tmp)
+    i = p._mult_idx
+    return float(torch.dot(x[i], p._g_tmp[i]).item())
+
 
 GeneratedProblem = CartPoleProblem
 
@@ -241,6 +262,16 @@ class SimpProblem:
 
     def objective(self, x):
         return float(torch.dot(self._f, x).item())
+
+    def create_vector(self):
+        return torch.zeros(self.model.n, dtype=torch.float64, device=self.device)
+
+    def lagrangian(self, alpha, x):
+        """alpha f(x) + lambda^T c(x), as CartPoleProblem.lagrangian."""
+        return alpha * self.objective(x) + _multiplier_term(self, x)
+
+    def update(self, x):
+        pass
 
 
 class DeviceBackend:

@@ -257,9 +257,16 @@ class SparseLDL:
         solved by a thread-block cluster of 8 CTAs each."""
         _lib.call("ab_ldl_set_cluster_threshold", self._h, int(entries))
 
+    def set_panel_mode(self, mode, min_rows=0):
+        """Large-front panels: 0 (default) a thread-block cluster of 8 CTAs
+        per front on levels whose largest front has >= min_rows rows, 1 one
+        CTA per front, 2 cluster panels with the one-CTA widths (identical
+        results to mode 1)."""
+        _lib.call("ab_ldl_set_panel_mode", self._h, int(mode), int(min_rows))
+
     def set_wide_threshold(self, entries):
         """Fronts with f * npiv >= entries are solved by the multi-CTA
-        kernels (default 2^18)."""
+        kernels (default 2^22)."""
         _lib.call("ab_ldl_set_wide_threshold", self._h, int(entries))
 
     def stats(self):

@@ -297,13 +297,15 @@ class InertiaCorrection:
 
     @classmethod
     def _mask(cls, m, like):
+        """The boolean mask m as an index for `like` (its device copy for a
+        tensor, cached; the cache holds m itself, so its id stays unique)."""
         if torch is not None and isinstance(like, torch.Tensor):
             key = (id(m), str(like.device))
-            t = cls._masks.get(key)
-            if t is None:
-                t = torch.from_numpy(np.ascontiguousarray(m)).to(like.device)
-                cls._masks[key] = t
-            return t
+            hit = cls._masks.get(key)
+            if hit is None or hit[0] is not m:
+                hit = (m, torch.from_numpy(np.ascontiguousarray(m)).to(like.device))
+                cls._masks[key] = hit
+            return hit[1]
         return m
 
 

@@ -85,13 +85,19 @@ class B200Solver:
 
     # -- refinement -------------------------------------------------------
     def _ir_setup(self, mult_ind, lbx, ubx):
-        key = (id(mult_ind), id(lbx), id(ubx))
-        if self._ir is not None and self._ir["key"] == key:
-            return self._ir
+        # device copies of the index sets and bounds, rebuilt when any of
+        # them changes (compared by value)
         mult_ind = np.asarray(mult_ind, dtype=bool)
+        lbx = np.asarray(lbx, dtype=np.float64)
+        ubx = np.asarray(ubx, dtype=np.float64)
+        ir = self._ir
+        if ir is not None and np.array_equal(ir["key"][0], mult_ind) and \
+                np.array_equal(ir["key"][1], lbx) and np.array_equal(ir["key"][2], ubx):
+            return ir
+        key = (mult_ind.copy(), lbx.copy(), ubx.copy())
         pidx = np.nonzero(~mult_ind)[0].astype(np.int32)
         cidx = np.nonzero(mult_ind)[0].astype(np.int32)
-        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+        t = lambda a: torch.from_numpy(np.array(a, copy=True)).to(self.device)
         ir = dict(key=key, pidx=t(pidx), cidx=t(cidx),
                   lbx=t(np.asarray(lbx, dtype=np.float64)),
                   ubx=t(np.asarray(ubx, dtype=np.float64)),

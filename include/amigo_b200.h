@@ -135,6 +135,15 @@ int ab_ldl_set_panel_cache(ab_ldl_t h, int bytes);
 int ab_ldl_set_wide_threshold(ab_ldl_t h, long long entries);
 int ab_ldl_set_cluster_threshold(ab_ldl_t h, long long entries);
 
+/* Large-front panel knob.  mode 0 (default): levels whose largest front
+ * has at least min_rows rows (default 384) factor their panels on one
+ * thread-block cluster of 8 CTAs per front, NB = 32 columns a panel;
+ * mode 1: one CTA per front for every level; mode 2: cluster panels with
+ * the one-CTA panel's widths, whose results are the one-CTA panel's bit
+ * for bit (a test mode).  min_rows <= 0 keeps the current value.  No
+ * reference counterpart (the reference factors each front on one thread). */
+int ab_ldl_set_panel_mode(ab_ldl_t h, int mode, int min_rows);
+
 /* The tensor-core Schur update on plain device arrays (column-major, FP32):
  * lower(C) -= A B^T for n x kw panels A, B (kw <= 31), as 3xTF32 tcgen05
  * products accumulated in FP32 in tensor memory -- the update the

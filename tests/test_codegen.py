@@ -126,3 +126,27 @@ def test_declaration_errors():
         Bad().build()
     with pytest.raises(ValueError):
         cg.Group(C.BoundaryState(), np.zeros((3, 5), np.int32))
+
+
+def test_model_wire_format_round_trip():
+    """A whole problem as a request carries it: GeneratedModel.serialize ->
+    JSON -> deserialize gives the same KKT pattern, multiplier indicator,
+    bounds, fixed rows and start point, and derivatives equal to rounding;
+    vectors round-trip through serialize_vectors."""
+    m = CartPole(N=12, seed=3)
+    G = C.cartpole_model(m)
+    s = json.dumps(G.serialize())
+    B = cg.GeneratedModel.deserialize(json.loads(s))
+    assert B.n == G.n and np.array_equal(B.rowp, G.rowp) and np.array_equal(B.cols, G.cols)
+    assert np.array_equal(B.mult, G.mult) and np.array_equal(B.fixed, G.fixed)
+    assert np.array_equal(B.lower, G.lower) and np.array_equal(B.upper, G.upper)
+    x = m.x0 + 0.05 * np.random.RandomState(2).randn(m.n)
+    g1, v1 = G.host_derivatives(x, 0.8)
+    g2, v2 = B.host_derivatives(x, 0.8)
+    assert np.abs(g1 - g2).max() <= 1e-14 * np.abs(g1).max()
+    assert np.abs(v1 - v2).max() <= 1e-14 * np.abs(v1).max()
+    vec = cg.GeneratedModel.serialize_vectors({"x": ("state", x), "p": ("data", np.arange(3.0))})
+    back = cg.GeneratedModel.deserialize_vectors(json.loads(json.dumps(vec)))
+    assert back["x"][0] == "state" and np.array_equal(back["x"][1], x)
+    with pytest.raises(ValueError):
+        cg.GeneratedModel.serialize_vectors({"y": ("bogus", x)})
