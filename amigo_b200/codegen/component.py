@@ -84,6 +84,7 @@ class Component:
         self._data = _Decl()
         self._cons = _Decl()
         self._obj = _Decl()
+        self._outs = _Decl()
         self._built = None
 
     # -- declarations (amigo/component.py:639-706) --------------------------
@@ -102,6 +103,11 @@ class Component:
 
     def add_objective(self, name, **kw):
         self._obj.add(name, None, **kw)
+
+    def add_output(self, name, shape=None, **kw):
+        """A model output computed from the inputs and data (amigo's
+        add_output); outputs do not enter the Lagrangian."""
+        self._outs.add(name, shape, **kw)
 
     def compute(self):
         raise NotImplementedError
@@ -123,6 +129,10 @@ class Component:
     @property
     def num_data(self):
         return self._data.size()
+
+    @property
+    def num_outputs(self):
+        return self._outs.size()
 
     def var_names(self):
         """Flattened names of the variable vector, e.g. q[1], lam_res[2]."""
@@ -171,10 +181,22 @@ class Component:
         self.constants = {k: self._const.meta[k]["value"] for k in self._const}
         self.constraints = _Assign(self._cons)
         self.objective = _Assign(self._obj)
+        self.outputs = _Assign(self._outs)
         self.compute()
         missing = [k for k in self._cons if k not in self.constraints]
+        missing += [k for k in self._outs if k not in self.outputs]
         if missing:
-            raise ValueError("compute() left constraints unset: %s" % missing)
+            raise ValueError("compute() left constraints or outputs unset: %s" % missing)
+        outs = []
+        for k in self._outs:
+            sh = self._outs.shapes[k]
+            vals = self.outputs[k]
+            flat = [vals] if not sh else list(np.asarray(vals, dtype=object).ravel())
+            if len(flat) != _size(sh):
+                raise ValueError("output %s has %d entries, declared %d"
+                                 % (k, len(flat), _size(sh)))
+            outs += [self._node(g, v) for v in flat]
+        self._out_nodes = outs
         ni = self.num_inputs
         lam = [g.var(ni + t) for t in range(self.num_constraints)]
         xs = [g.var(i) for i in range(ni)] + lam
@@ -216,6 +238,8 @@ class Component:
             flat = [vals] if not sh else list(np.asarray(vals, dtype=object).ravel())
             cons.append([self._node(g, v) for v in flat])
             roots += cons[-1]
+        outs = list(self._out_nodes)
+        roots += outs
         order = E._topo(roots)
         ids = {n.id: i for i, n in enumerate(order)}
         nodes = [[n.op, [ids[a.id] for a in n.args], n.val] for n in order]
@@ -223,8 +247,10 @@ class Component:
         return {"format": "amigo_b200.component/1", "name": type(self).__name__,
                 "inputs": decl(self._inputs), "data": decl(self._data),
                 "constraints": decl(self._cons), "objective": decl(self._obj),
+                "outputs": decl(self._outs),
                 "nodes": nodes, "objective_root": ids[obj.id],
-                "constraint_roots": [[ids[n.id] for n in c] for c in cons]}
+                "constraint_roots": [[ids[n.id] for n in c] for c in cons],
+                "output_roots": [ids[n.id] for n in outs]}
 
     @classmethod
     def deserialize(cls, d):
@@ -269,6 +295,8 @@ class _Deserialized(Component):
             self.add_constraint(k, sh or None, **meta)
         for k, sh, meta in d["objective"]:
             self.add_objective(k, **meta)
+        for k, sh, meta in d.get("outputs", []):
+            self.add_output(k, sh or None, **meta)
 
     def compute(self):
         g = self._g
@@ -303,3 +331,9 @@ class _Deserialized(Component):
         for (k, sh, _), roots in zip(self._d["constraints"], self._d["constraint_roots"]):
             vals = [ex(i) for i in roots]
             self.constraints[k] = vals[0] if not sh else vals
+        roots = list(self._d.get("output_roots", []))
+        for k, sh, _ in self._d.get("outputs", []):
+            m = _size(tuple(sh))
+            vals = [ex(i) for i in roots[:m]]
+            roots = roots[m:]
+            self.outputs[k] = vals[0] if not sh else vals

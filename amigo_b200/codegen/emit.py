@@ -138,6 +138,42 @@ def struct_source(comp, sym):
     return "".join(out)
 
 
+def sens_source(comp, sym):
+    """C++ source of `<sym>_sens`: the outputs and the derivatives a
+    post-optimality analysis needs (amigo/algorithm/post_optimization.py),
+    dense per instance: out[NO], dgd[NQ * ND] = d(dL/dq_i)/dd_m,
+    doq[NO * NQ] = d out_o / dq_i, dod[NO * ND] = d out_o / dd_m."""
+    g, xs, lag, obj, grad, hess = derivatives(comp)
+    nq, nd, no = comp.num_vars, comp.num_data, comp.num_outputs
+    ds = [g.data(m) for m in range(nd)]
+    outs = list(comp._out_nodes)
+    dgd = [E.gradient(g, gi, ds) for gi in grad]
+    doq = [E.gradient(g, o, xs) for o in outs]
+    dod = [E.gradient(g, o, ds) for o in outs]
+    roots = list(grad) + outs + [h for r in dgd + doq + dod for h in r]
+    nodes = _closure(roots, set())
+    out = ["struct %s_sens {\n" % sym,
+           "  static constexpr int NO = %d;\n" % no,
+           "  __host__ __device__ static void eval(const double* __restrict__ q,\n"
+           "      const double* __restrict__ d, double alpha, double* out, double* dgd,\n"
+           "      double* doq, double* dod) {\n",
+           "    (void)q; (void)d; (void)alpha; (void)out; (void)dgd; (void)doq; (void)dod;\n",
+           _stmts(nodes, "    ")]
+    for o, n in enumerate(outs):
+        out.append("    out[%d] = %s;\n" % (o, _ref(n)))
+    for i, row in enumerate(dgd):
+        for m, n in enumerate(row):
+            out.append("    dgd[%d] = %s;\n" % (i * nd + m, _ref(n)))
+    for o, row in enumerate(doq):
+        for i, n in enumerate(row):
+            out.append("    doq[%d] = %s;\n" % (o * nq + i, _ref(n)))
+    for o, row in enumerate(dod):
+        for m, n in enumerate(row):
+            out.append("    dod[%d] = %s;\n" % (o * nd + m, _ref(n)))
+    out.append("  }\n};\n")
+    return "".join(out)
+
+
 def module_source(groups, header="codegen_kernels.cuh"):
     """Full CUDA source of a generated module: one evaluator struct and the
     extern "C" launchers (gradient, Hessian, objective) per component
@@ -146,7 +182,9 @@ def module_source(groups, header="codegen_kernels.cuh"):
              "#include \"%s\"\n\n" % header]
     for sym, comp in groups:
         parts.append(struct_source(comp, sym))
-        parts.append("AB_GEN_ENTRY_POINTS(%s)\n\n" % sym)
+        parts.append(sens_source(comp, sym))
+        parts.append("AB_GEN_ENTRY_POINTS(%s)\n" % sym)
+        parts.append("AB_GEN_SENS(%s)\n\n" % sym)
     return "".join(parts)
 
 

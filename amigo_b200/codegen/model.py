@@ -242,6 +242,17 @@ class GeneratedModel:
         vals[self.fixed_diag_pos] = 1.0
         return g, vals
 
+    def host_lagrangian(self, x, alpha=1.0):
+        """alpha f(x) + lambda^T c(x) on the host (test use): the objective
+        from the host evaluators, c(x) from the gradient's multiplier rows."""
+        f = 0.0
+        for sym, gr in zip(self.syms, self.groups):
+            ev = host_evaluator(gr.comp, sym)
+            for e in range(gr.E):
+                f += ev(x[gr.idx[e]], gr.data[e], 1.0)[2]
+        g, _ = self.host_derivatives(x, alpha)
+        return alpha * f + float(x[self.mult] @ g[self.mult])
+
     def source(self):
         return emit.module_source(list(zip(self.syms, [g.comp for g in self.groups])))
 

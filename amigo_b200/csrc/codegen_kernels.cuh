@@ -248,3 +248,29 @@ struct HostOut {
   }
 
 #endif
+
+// Post-optimality sensitivities of every instance of a group, on the host
+// (dense per-instance blocks; see <C>_sens in the generated source):
+// out[E x NO], dgd[E x NQ x ND], doq[E x NO x NQ], dod[E x NO x ND] at the
+// global iterate x gathered through idx[E x NQ].
+#define AB_GEN_SENS(C)                                                         \
+  extern "C" int C##_sens_batch(int ne, const int* idx, const double* x,       \
+                                const double* data, double alpha, double* out, \
+                                double* dgd, double* doq, double* dod) {       \
+    constexpr int NQ = C::NQ, ND = C::ND, NO = C##_sens::NO;                   \
+    double q[NQ > 0 ? NQ : 1];                                                 \
+    for (int e = 0; e < ne; e++) {                                             \
+      for (int i = 0; i < NQ; i++) q[i] = x[idx[(long long)e * NQ + i]];       \
+      C##_sens::eval(q, data + (long long)e * ND, alpha,                       \
+                     out + (long long)e * NO, dgd + (long long)e * NQ * ND,    \
+                     doq + (long long)e * NO * NQ, dod + (long long)e * NO * ND); \
+    }                                                                          \
+    return 0;                                                                  \
+  }                                                                            \
+  extern "C" int C##_sens_sizes(int* nq, int* nd, int* no) {                   \
+    *nq = C::NQ;                                                               \
+    *nd = C::ND;                                                               \
+    *no = C##_sens::NO;                                                        \
+    return 0;                                                                  \
+  }
+

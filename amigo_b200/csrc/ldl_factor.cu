@@ -1784,12 +1784,15 @@ k_big_panel_sw(DevicePlan d, const int* __restrict__ nodes, double ustab,
 //     read from L2.
 // With the one-CTA panel's widths (width_rule 1) the results are the one-
 // CTA panel's bit for bit; by default every panel takes NB columns.
-constexpr int kClThreads = 128;
-constexpr int kClRows = 4;
+constexpr int kClThreads = 256;
+constexpr int kClRows = 2;
 constexpr int kClCS = 8;
-constexpr int kClMaxRows = kClThreads * kClRows * kClCS;
+// Rows a cluster panel takes: up to its threads' rows, capped so that W
+// and L of NB columns fit in a CTA's shared memory.
+constexpr int kClMaxRows = 3072;
 constexpr int kClSlack = 64;
-constexpr int kClSmemMax = NB * 32 * (kClMaxRows / 32 / kClCS) * 8;
+constexpr int kClSmemMax = 2 * NB * (kClMaxRows / kClCS) * 8;
+static_assert(kClMaxRows <= kClThreads * kClRows * kClCS, "cluster panel rows");
 
 template <int PT, int CS>
 struct ClCtl {
@@ -1802,8 +1805,8 @@ struct ClCtl {
   int cP[NB], kind[NB];
   int swa[NB], swb[NB], nsw;
   int rows[2 * NB], src[2 * NB], nrows;
-  double xrow[2][NB];  // a W row received in an interchange (for a, for b)
-  int u[4];            // launch-uniform values published by CTA 0
+  double xw[2][NB], xl[2][NB];  // W and L rows received in an interchange
+  int u[4];                     // launch-uniform values published by CTA 0
 };
 
 template <int CS>
@@ -1811,20 +1814,41 @@ __device__ __forceinline__ int cl_owner(int q) { return (q >> 5) % CS; }
 template <int CS>
 __device__ __forceinline__ int cl_lrow(int q) { return (((q >> 5) / CS) << 5) | (q & 31); }
 
-// Block-wide reductions of sw_reduce over the whole cluster.
-// (ts: trace only, the clock after the warp fold, the barrier and the
-// final fold.)
+// Warp fold of (v, i) -- the first argmax of v >= 0 (v < 0: no entry, index
+// 0x7fffffff) -- and of the maximum of v2 >= 0, with warp reductions on the
+// doubles' bit patterns (for non-negative doubles their order): high word,
+// then low word among the lanes holding the maximal high word, then the
+// smallest index among the maximal keys.  argmax_merge's result, exactly,
+// and the same in every lane.
+__device__ __forceinline__ void warp_fold_redux(double& v, int& i, double& v2) {
+  const unsigned FULL = 0xffffffffu;
+  const unsigned long long kv =
+      v < 0.0 ? 0ull : (unsigned long long)__double_as_longlong(v);
+  const unsigned hi = (unsigned)(kv >> 32), lo = (unsigned)kv;
+  const unsigned mh = __reduce_max_sync(FULL, hi);
+  const unsigned ml = __reduce_max_sync(FULL, hi == mh ? lo : 0u);
+  const unsigned mi =
+      __reduce_min_sync(FULL, (hi == mh && lo == ml) ? (unsigned)i : 0xffffffffu);
+  i = (int)mi;
+  v = mi == 0x7fffffffu
+          ? -1.0
+          : __longlong_as_double((long long)(((unsigned long long)mh << 32) | ml));
+  const unsigned long long k2 = (unsigned long long)__double_as_longlong(v2);
+  const unsigned h2 = (unsigned)(k2 >> 32), l2 = (unsigned)k2;
+  const unsigned m2h = __reduce_max_sync(FULL, h2);
+  const unsigned m2l = __reduce_max_sync(FULL, h2 == m2h ? l2 : 0u);
+  v2 = __longlong_as_double((long long)(((unsigned long long)m2h << 32) | m2l));
+}
+
+// Block-wide reductions of sw_reduce over the whole cluster: every warp's
+// fold goes into every CTA's copy of the slots (distributed shared memory
+// stores), one cluster barrier, every warp folds the slots.  (ts: trace
+// only, the clock after the warp fold, the barrier and the final fold.)
 template <int PT, int CS, class Cl>
 __device__ __forceinline__ void cl_reduce(ClCtl<PT, CS>& c, Cl& cluster, int set,
                                           double& v, int& i, double& v2,
                                           long long* ts = nullptr) {
-  for (int o = 16; o > 0; o >>= 1) {
-    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-    const double ov2 = __shfl_xor_sync(0xffffffffu, v2, o);
-    argmax_merge(v, i, ov, oi);
-    v2 = fmax(v2, ov2);
-  }
+  warp_fold_redux(v, i, v2);
   if (ts) ts[0] = clock64() + (v != v ? 1 : 0);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int slot = (int)cluster.block_rank() * (PT / 32) + warp;
@@ -1845,13 +1869,7 @@ __device__ __forceinline__ void cl_reduce(ClCtl<PT, CS>& c, Cl& cluster, int set
     argmax_merge(v, i, c.rv[set][lane + 32], c.ri[set][lane + 32]);
     v2 = fmax(v2, c.rv2[set][lane + 32]);
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-    const double ov2 = __shfl_xor_sync(0xffffffffu, v2, o);
-    argmax_merge(v, i, ov, oi);
-    v2 = fmax(v2, ov2);
-  }
+  warp_fold_redux(v, i, v2);
   if (ts) ts[2] = clock64() + (v != v ? 1 : 0);
 }
 
@@ -1862,35 +1880,41 @@ __device__ __forceinline__ void cl_bcast(Cl& cluster, double* slot, double v) {
   for (int r = 0; r < CS; r++) *cluster.map_shared_rank(slot, r) = v;
 }
 
-// W rows a and b (relative) interchanged over the columns [0, ncol): the
-// thread owning each row sends its entries to the other row's owner, a
-// cluster barrier, each owner stores what it received, and a second
-// barrier before any CTA reads either row again (the barriers also
-// publish the caller's F writes made before this call).
-template <class T, int PT, int RPT, int CS, class Cl>
-__device__ void cl_swap_wrows(T* Wl, int lld, int ncol, int a, int b,
-                              const int (&rel)[RPT], const int (&lr)[RPT],
-                              ClCtl<PT, CS>& c, Cl& cluster) {
+// W rows a and b (relative) interchanged over the columns [0, nw) and L
+// rows over [0, nl): warp 0 of each row's CTA sends the row (a lane per
+// column) to the other row's CTA, a cluster barrier, warp 0 stores what it
+// received, a second barrier before any thread reads either row again
+// (the barriers also publish the caller's F writes made before the call).
+template <class T, int PT, int CS, class Cl>
+__device__ void cl_swap_rows(T* Wl, T* Ll, int lld, int nw, int nl, int a, int b,
+                             ClCtl<PT, CS>& c, Cl& cluster) {
   const int cr = (int)cluster.block_rank();
+  const int lane = threadIdx.x & 31;
   const int oa = cl_owner<CS>(a), ob = cl_owner<CS>(b);
-#pragma unroll
-  for (int i = 0; i < RPT; i++) {
-    if (cr == oa && rel[i] == a) {
-      double* dst = cluster.map_shared_rank(&c.xrow[1][0], ob);
-      for (int j = 0; j < ncol; j++) dst[j] = (double)Wl[(size_t)j * lld + lr[i]];
+  const int la = cl_lrow<CS>(a), lb = cl_lrow<CS>(b);
+  __syncthreads();  // this CTA's writes to rows a and b, before warp 0 reads
+  if (threadIdx.x < 32) {
+    if (cr == oa) {
+      ClCtl<PT, CS>* dst = cluster.map_shared_rank(&c, ob);
+      if (lane < nw) dst->xw[1][lane] = (double)Wl[(size_t)lane * lld + la];
+      if (lane < nl) dst->xl[1][lane] = (double)Ll[(size_t)lane * lld + la];
     }
-    if (cr == ob && rel[i] == b) {
-      double* dst = cluster.map_shared_rank(&c.xrow[0][0], oa);
-      for (int j = 0; j < ncol; j++) dst[j] = (double)Wl[(size_t)j * lld + lr[i]];
+    if (cr == ob) {
+      ClCtl<PT, CS>* dst = cluster.map_shared_rank(&c, oa);
+      if (lane < nw) dst->xw[0][lane] = (double)Wl[(size_t)lane * lld + lb];
+      if (lane < nl) dst->xl[0][lane] = (double)Ll[(size_t)lane * lld + lb];
     }
   }
   cluster.sync();
-#pragma unroll
-  for (int i = 0; i < RPT; i++) {
-    if (cr == oa && rel[i] == a)
-      for (int j = 0; j < ncol; j++) Wl[(size_t)j * lld + lr[i]] = T(c.xrow[0][j]);
-    if (cr == ob && rel[i] == b)
-      for (int j = 0; j < ncol; j++) Wl[(size_t)j * lld + lr[i]] = T(c.xrow[1][j]);
+  if (threadIdx.x < 32) {
+    if (cr == oa) {
+      if (lane < nw) Wl[(size_t)lane * lld + la] = T(c.xw[0][lane]);
+      if (lane < nl) Ll[(size_t)lane * lld + la] = T(c.xl[0][lane]);
+    }
+    if (cr == ob) {
+      if (lane < nw) Wl[(size_t)lane * lld + lb] = T(c.xw[1][lane]);
+      if (lane < nl) Ll[(size_t)lane * lld + lb] = T(c.xl[1][lane]);
+    }
   }
   cluster.sync();
 }
@@ -1899,9 +1923,10 @@ template <class T, int PT, int RPT, int CS, class Cl>
 __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
                                 int* vars, int* fsperm, double ustab,
                                 double pivot_tol, int* status, ClCtl<PT, CS>& c,
-                                T* Wl, int lld, int nbe, int& k_, int& nc_,
+                                T* Wl, T* Ll, int lld, int nbe, int& k_, int& nc_,
                                 int& kw_, int* dbg, Cl& cluster) {
   constexpr int NW = PT / 32;
+  const unsigned FULL = 0xffffffffu;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int cr = (int)cluster.block_rank();
   const bool lead = cr == 0 && tid == 0;
@@ -1923,53 +1948,43 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
       dst[i] = (r >= col && r < n) ? __ldcg(F + r + (size_t)col * ld) : T(0);
     }
   };
-  // acc[i] -= sum_{j < kw} L[r_i, j] W[y, j] in sw_apply_panel's order; the
-  // warp reads W row y (relative) from its owner once, lane j holding
-  // column j (kw <= NB - 2 < 32)
+  // lanes j < ncol: W[q, j] (q relative), from the row's CTA
+  auto wrow = [&](int q, int ncol) -> T {
+    const T* p = cluster.map_shared_rank(Wl + cl_lrow<CS>(q), cl_owner<CS>(q));
+    return lane < ncol ? p[(size_t)lane * lld] : T(0);
+  };
   long long ts[10];  // trace only: clocks of the phases of a step (lead)
+  unsigned long long acc_t[16] = {};
   const bool tr = dbg != nullptr && lead;
-  auto apply = [&](int y, T (&acc)[RPT]) {
-    const T* yrow = cluster.map_shared_rank(Wl + cl_lrow<CS>(y), cl_owner<CS>(y));
-    const T yv = lane < kw ? yrow[(size_t)lane * lld] : T(0);
-    if (tr) ts[1] = clock64() + (yv != yv ? 1 : 0);
-    int j = 0;
-    for (; j + 2 <= kw; j += 2) {
-      const T* w0 = Wl + (size_t)j * lld;
-      const T* w1 = w0 + lld;
-      const T* p0 = Wl + (size_t)c.cP[j] * lld;
-      const T* p1 = Wl + (size_t)c.cP[j + 1] * lld;
-      const T a0 = T(c.cA[j]), b0 = T(c.cB[j]);
-      const T a1 = T(c.cA[j + 1]), b1 = T(c.cB[j + 1]);
-      const T y0 = __shfl_sync(0xffffffffu, yv, j);
-      const T y1 = __shfl_sync(0xffffffffu, yv, j + 1);
+  // acc[i] -= sum_{j < kw} L[r_i, j] y_j (the order of sw_apply_panel), y_j
+  // in lane j of yv; the L entries of 8 columns are loaded before their
+  // multiply-adds
+  auto apply = [&](T yv, T (&acc)[RPT]) {
+    for (int j0 = 0; j0 < kw; j0 += 8) {
+      T lv[RPT][8];
 #pragma unroll
-      for (int i = 0; i < RPT; i++)
-        if (on[i]) {
-          const T l0 = sw_l(w0[lr[i]], p0[lr[i]], a0, b0);
-          const T l1 = sw_l(w1[lr[i]], p1[lr[i]], a1, b1);
-          acc[i] -= l0 * y0;
-          acc[i] -= l1 * y1;
+      for (int u = 0; u < 8; u++)
+#pragma unroll
+        for (int i = 0; i < RPT; i++)
+          lv[i][u] = (on[i] && j0 + u < kw) ? Ll[(size_t)(j0 + u) * lld + lr[i]] : T(0);
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const T yj = __shfl_sync(FULL, yv, (j0 + u) & 31);
+        if (j0 + u < kw) {
+#pragma unroll
+          for (int i = 0; i < RPT; i++)
+            if (on[i]) acc[i] -= lv[i][u] * yj;
         }
-    }
-    if (j < kw) {
-      const T* w0 = Wl + (size_t)j * lld;
-      const T* p0 = Wl + (size_t)c.cP[j] * lld;
-      const T a0 = T(c.cA[j]), b0 = T(c.cB[j]);
-      const T y0 = __shfl_sync(0xffffffffu, yv, j);
-#pragma unroll
-      for (int i = 0; i < RPT; i++)
-        if (on[i]) acc[i] -= sw_l(w0[lr[i]], p0[lr[i]], a0, b0) * y0;
+      }
     }
     if (tr) ts[2] = clock64() + (acc[0] != acc[0] ? 1 : 0);
   };
   load_col(k, cur);
   int par = 0;
-  unsigned long long* cyc =
-      dbg ? reinterpret_cast<unsigned long long*>(dbg + 8) : nullptr;
-  long long tc0 = 0, tc1 = 0, tc2 = 0, tc3 = 0;
+  bool have_y = false;  // ynext holds the next candidate's W row
+  T ynext = T(0);
   while (kw < nbe - 1 && k < nc) {
-    if (cyc && lead) tc0 = clock64();
-    if (tr) ts[0] = tc0;
+    if (tr) ts[0] = clock64();
     par ^= 1;
     T nxt[RPT];
     load_col(k + 1, nxt);
@@ -1980,8 +1995,9 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
       acc[i] = cur[i];
       on[i] = r >= k && r < n;
     }
-    apply(k - kstart, acc);
-    long long tb[3];
+    const T yv = have_y ? ynext : wrow(k - kstart, kw);
+    if (tr) ts[1] = clock64() + (yv != yv ? 1 : 0);
+    apply(yv, acc);
     double bv = -1.0, tv = 0.0;
     int bi = 0x7fffffff;
     T* wcol = Wl + (size_t)kw * lld;
@@ -1995,16 +2011,20 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
         else if (r < nc) argmax_merge(bv, bi, a, r);
         else tv = fmax(tv, a);
       }
-    if (cyc && lead) tc1 = clock64();
-    if (tr) ts[3] = tc1;
+    if (tr) ts[3] = clock64();
+    long long tb[3];
     cl_reduce<PT, CS>(c, cluster, 2 * par, bv, bi, tv, tr ? tb : nullptr);
-    if (cyc && lead) tc2 = clock64();
+    // the next candidate's W row, in case this step takes a 1x1 pivot
+    // without an interchange (its entry in column kw is published now)
+    have_y = false;
+    if (k + 1 < n) ynext = wrow(k + 1 - kstart, kw + 1);
     int imax = bi;
     if (imax >= nc || imax <= k) {
       if (k + 1 < nc && lead) atomicOr(status, ST_NAN);
       imax = (k + 1 < n) ? k + 1 : k;
     }
     const double wkk = c.wkk[par];
+    const T dinv = T(1) / T(wkk);  // the 1x1 pivot's, ahead of the decision
     const PivotChoice pc = choose_pivot(
         root, k, nc, wkk, imax, bv < 0.0 ? 0.0 : bv, tv, ustab, pivot_tol, [&]() {
           // column imax into W[:, kw + 1]; its owner publishes its diagonal
@@ -2017,7 +2037,7 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
                            : (r < imax ? __ldcg(F + imax + (size_t)r * ld)
                                        : __ldcg(F + r + (size_t)imax * ld));
           }
-          apply(imax - kstart, a2);
+          apply(wrow(imax - kstart, kw), a2);
           double rv = -1.0, rt = 0.0;
           int ri = 0x7fffffff;
           T* w2 = Wl + (size_t)(kw + 1) * lld;
@@ -2036,20 +2056,16 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
           cl_reduce<PT, CS>(c, cluster, 2 * par + 1, rv, ri, rt);
           return ImaxColumn{rt, c.wii[par], c.wik[par]};
         });
-    if (cyc && lead) {
-      tc3 = clock64();
-      atomicAdd(cyc + 0, (unsigned long long)(tc1 - tc0));
-      atomicAdd(cyc + 1, (unsigned long long)(tc2 - tc1));
-      atomicAdd(cyc + 2, (unsigned long long)(tc3 - tc2));
+    if (tr) {
       ts[4] = tb[0];
       ts[5] = tb[1];
       ts[6] = tb[2];
-      ts[7] = tc3;
+      ts[7] = clock64();
     }
     if (pc.step == 0) {
       if (dbg && lead) atomicAdd(dbg + 4, 1);
       // delay candidate k (the full interchange with nc - 1 after the
-      // pending ones, by CTA 0; the W rows by their owners)
+      // pending ones, by CTA 0; the W and L rows by their CTAs)
       if (k < nc - 1) {
         if (cr == 0) {
           __syncthreads();
@@ -2063,8 +2079,8 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
         } else if (tid == 0) {
           c.nsw = 0;
         }
-        cl_swap_wrows<T, PT, RPT, CS>(Wl, lld, kw, k - kstart, nc - 1 - kstart, rel, lr,
-                                      c, cluster);
+        cl_swap_rows<T, PT, CS>(Wl, Ll, lld, kw, kw, k - kstart, nc - 1 - kstart, c,
+                                cluster);
       }
       nc -= 1;
       load_col(k, cur);
@@ -2085,7 +2101,7 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
     if (swapped) {
       // the entries of the interchange that stay live, from the registers
       // of column ksrc (own rows); the record for the columns left of the
-      // panel; the W rows by their owners
+      // panel; the W and L rows by their CTAs
       const int a = ksrc, b = kpiv;
 #pragma unroll
       for (int i = 0; i < RPT; i++) {
@@ -2109,21 +2125,27 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
         fsperm[a] = fsperm[b];
         fsperm[b] = tv2;
       }
-      cl_swap_wrows<T, PT, RPT, CS>(Wl, lld, kw + step, a - kstart, b - kstart, rel, lr,
-                                    c, cluster);
+      cl_swap_rows<T, PT, CS>(Wl, Ll, lld, kw + step, kw, a - kstart, b - kstart, c,
+                              cluster);
     }
     // the pivot block after the interchange: W[k, kw] is the candidate's
     // diagonal (column imax's for an imax 1x1 pivot); for a 2x2 pivot
     // W[k + 1, kw] and W[k + 1, kw + 1] are the entry of row imax and the
-    // diagonal of column imax
+    // diagonal of column imax.  The L columns of the pivot (own rows) from
+    // their W columns, with the expression that writes them to F.
     if (step == 1) {
       const T d = pc.imax_1x1 ? T(c.wii[par]) : T(wkk);
       if (!isfinite((double)d) && lead) atomicOr(status, ST_NAN);
+      const T ainv = pc.zero ? T(0) : (pc.imax_1x1 ? T(1) / d : dinv);
       c.kind[kw] = 0;
-      c.cA[kw] = pc.zero ? 0.0 : (double)(T(1) / d);
+      c.cA[kw] = (double)ainv;
       c.cB[kw] = 0.0;
       c.cP[kw] = kw;
       if (lead) vars[3 * ld + k] = 0;
+      T* lc = Ll + (size_t)kw * lld;
+#pragma unroll
+      for (int i = 0; i < RPT; i++)
+        if (on[i]) lc[lr[i]] = sw_l(wcol[lr[i]], wcol[lr[i]], ainv, T(0));
     } else {
       const Coef2 q = pivot2_coeffs<T>(T(wkk), T(c.wik[par]), T(c.wii[par]));
       if (!q.finite && lead) atomicOr(status, ST_NAN);
@@ -2141,34 +2163,45 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
         vars[3 * ld + k] = 1;
         vars[3 * ld + k + 1] = 2;
       }
+      const T* w0 = wcol;
+      const T* w1 = wcol + lld;
+      T* l0 = Ll + (size_t)kw * lld;
+      T* l1 = l0 + lld;
+#pragma unroll
+      for (int i = 0; i < RPT; i++)
+        if (on[i]) {
+          l0[lr[i]] = sw_l(w0[lr[i]], w1[lr[i]], T(q.i00), T(q.i10));
+          l1[lr[i]] = sw_l(w1[lr[i]], w0[lr[i]], T(q.i11), T(q.i01));
+        }
     }
+    const bool plain = step == 1 && !swapped;
     k += step;
     kw += step;
-    if (!swapped && step == 1) {
+    if (plain) {
 #pragma unroll
       for (int i = 0; i < RPT; i++) cur[i] = nxt[i];
+      have_y = true;
     } else {
       load_col(k, cur);
     }
-    if (cyc && lead) atomicAdd(cyc + 3, (unsigned long long)(clock64() - tc3));
     if (tr) {
       // fine phases of the steps without an interchange or a second column
-      // (dbg + 32: y row, column build, W stores, warp fold, barrier, final
-      // fold, decision, rest; then all other steps' cycles and count)
+      // (y row, column build, W stores, warp fold, barrier, final fold,
+      // decision, rest); then all other steps' cycles and count
       ts[8] = clock64() + (cur[0] != cur[0] ? 1 : 0);
-      unsigned long long* fine = reinterpret_cast<unsigned long long*>(dbg + 32);
-      if (step == 1 && !swapped && !pc.imax_1x1) {
-        for (int q = 0; q < 8; q++) atomicAdd(fine + q, (unsigned long long)(ts[q + 1] - ts[q]));
+      if (plain && !pc.imax_1x1) {
+        for (int q = 0; q < 8; q++) acc_t[q] += (unsigned long long)(ts[q + 1] - ts[q]);
+        acc_t[10] += 1;
       } else {
-        atomicAdd(fine + 8, (unsigned long long)(ts[8] - ts[0]));
-        atomicAdd(fine + 9, 1ull);
+        acc_t[8] += (unsigned long long)(ts[8] - ts[0]);
+        acc_t[9] += 1;
       }
     }
   }
   // --- the pending interchanges left of the panel (every CTA composes the
   // same map; the cluster's warps share the columns); the panel's L columns
   // to F and its W rows below k to HBM, each CTA for its own rows
-  if (cyc && lead) tc0 = clock64();
+  long long tw = tr ? clock64() : 0;
   __syncthreads();
   if (c.nsw > 0) {
     if (tid == 0) compose_swaps(c);
@@ -2179,8 +2212,7 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
     const int col = kstart + j;
     const int kd = c.kind[j];
     const T* w0 = Wl + (size_t)j * lld;
-    const T* wp = Wl + (size_t)c.cP[j] * lld;
-    const T a = T(c.cA[j]), b = T(c.cB[j]);
+    const T* l0 = Ll + (size_t)j * lld;
     T* Fc = F + (size_t)col * ld;
     T* Wc = Wg + (size_t)j * ld;
 #pragma unroll
@@ -2190,18 +2222,23 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
       const T w = w0[lr[i]];
       // the pivot block's own entries are D; below it, L
       if (r == col || (kd == 1 && r == col + 1)) Fc[r] = w;
-      else Fc[r] = sw_l(w, wp[lr[i]], a, b);
+      else Fc[r] = l0[lr[i]];
       if (r >= k) Wc[r] = w;
     }
   }
-  if (cyc && lead) atomicAdd(cyc + 4, (unsigned long long)(clock64() - tc0));
+  if (tr) {
+    unsigned long long* fine = reinterpret_cast<unsigned long long*>(dbg + 32);
+    for (int q = 0; q < 11; q++) atomicAdd(fine + q, acc_t[q]);
+    atomicAdd(reinterpret_cast<unsigned long long*>(dbg + 8) + 4,
+              (unsigned long long)(clock64() - tw));
+  }
   k_ = k;
   nc_ = nc;
   kw_ = kw;
 }
 
-// W local rows of a CTA for a panel starting at relative row 0 of cld
-// rows: the CTA's share of the 32-row groups.
+// W local rows of a CTA for a panel of cld rows: the CTA's share of the
+// 32-row groups.
 template <int CS>
 __host__ __device__ __forceinline__ int cl_local_rows(int cld) {
   return 32 * (((cld + 31) / 32 + CS - 1) / CS);
@@ -2250,7 +2287,7 @@ k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
   // the panel width depends on the front alone: NB, or the one-CTA
   // panel's (width_rule 1)
   int nbe = NB;
-  int max_rows = CS * PT * RPT;
+  int max_rows = kClMaxRows;
   if (width_rule == 1) {
     // the one-CTA panel's widths and its row limit (beyond which it takes
     // the HBM-panel form, as below)
@@ -2259,14 +2296,15 @@ k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
     max_rows = kSwThreads * kSwRows;
   }
   if (nbe >= 4 && cld <= max_rows &&
-      (long long)nbe * lld * (long long)sizeof(T) <= smem_bytes) {
+      2ll * nbe * lld * (long long)sizeof(T) <= smem_bytes) {
     long long tk0 = 0;
     if (dbg && cr == 0 && threadIdx.x == 0) {
       atomicAdd(dbg + 5, 1);
       tk0 = clock64();
     }
+    T* Wl = reinterpret_cast<T*>(cl_raw);
     panel_factor_cl<T, PT, RPT, CS>(F, f, W, f, fs == f, fvars, fvars + f, ustab,
-                                    pivot_tol, d.status, c, reinterpret_cast<T*>(cl_raw),
+                                    pivot_tol, d.status, c, Wl, Wl + (size_t)nbe * lld,
                                     lld, nbe, k, nc, kw, dbg, cluster);
     if (dbg && cr == 0 && threadIdx.x == 0)
       atomicAdd(reinterpret_cast<unsigned long long*>(dbg + 8) + 5,
@@ -2506,7 +2544,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                           fm + kClSlack <= kClMaxRows;
       const int cl_rule = h.panel_mode == 2 ? 1 : 0;
       const int cl_smem =
-          use_cl ? NB * cl_local_rows<kClCS>((int)fm + kClSlack) * (int)sizeof(T) : 0;
+          use_cl ? 2 * NB * cl_local_rows<kClCS>((int)fm + kClSlack) * (int)sizeof(T) : 0;
       const bool use_sw = !use_cl && fm <= (long long)kSwThreads * kSwRows;
       const int sw_smem = kSwSmemBytes;
       // panels a front of big_max_fs candidates needs without delays: each
@@ -2610,7 +2648,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                      q[0], q[1], q[2], q[3], q[4], q[5], cy[0] / 1000, cy[1] / 1000,
                      cy[2] / 1000, cy[3] / 1000, cy[4] / 1000, cy[5] / 1000,
                      tpan[l], tupd[l]);
-      const unsigned long long nf = (unsigned long long)q[0];
+      const unsigned long long nf = fi[10];
       if (fi[0] && nf)
         std::fprintf(stderr, "           plain-step cycles: yrow %llu build %llu stores %llu "
                              "fold %llu barrier %llu fold2 %llu decide %llu rest %llu | "

@@ -29,7 +29,8 @@ class TrapezoidInterval(Component):
     """One collocation interval: node states and controls at both ends, the
     trapezoidal defects q1 - q0 - h/2 (f(q0, u0) + f(q1, u1)) = 0 and the
     trapezoidal objective h/2 (u0^2 + u1^2).  Data: the interval length and
-    the pole mass (per instance, so batched instances can differ)."""
+    the pole mass (per instance, so batched instances can differ).  Outputs:
+    the interval's control effort and its end state's cart position."""
 
     def __init__(self):
         super().__init__()
@@ -41,6 +42,8 @@ class TrapezoidInterval(Component):
         self.add_input("u1")
         self.add_constraint("defect", shape=4)
         self.add_objective("effort")
+        self.add_output("effort")
+        self.add_output("x_end")
 
     def compute(self):
         h, m = self.data["h"], self.data["m_pole"]
@@ -51,6 +54,8 @@ class TrapezoidInterval(Component):
         self.constraints["defect"] = [q1[j] - q0[j] - 0.5 * h * (f0[j] + f1[j])
                                       for j in range(4)]
         self.objective["effort"] = 0.5 * h * (u0 * u0 + u1 * u1)
+        self.outputs["effort"] = 0.5 * h * (u0 * u0 + u1 * u1)
+        self.outputs["x_end"] = q1[0]
 
 
 class BoundaryState(Component):
