@@ -1270,7 +1270,9 @@ struct SwCtl {
 };
 
 // The pending interchanges of a panel composed into one row map (rows[t]
-// takes the value of row src[t]); run by one thread, resets the list.
+// takes the value of row src[t]); run by one thread.  The count c.nsw is
+// left for the caller to reset after a barrier: every thread reads it to
+// decide whether to join the barriers of the flush.
 template <class C>
 __device__ void compose_swaps(C& c) {
   int nr = 0;
@@ -1292,7 +1294,6 @@ __device__ void compose_swaps(C& c) {
     c.src[at[1]] = tmp;
   }
   c.nrows = nr;
-  c.nsw = 0;
 }
 
 // Row map applied to the columns [0, kstart) of F by warps gw, gw + gws,
@@ -1338,12 +1339,14 @@ __device__ void apply_row_map(T* F, int ld, int kstart, const int* rows,
 template <class T, int PT>
 __device__ void sw_flush_left(T* F, int ld, int kstart, SwCtl<PT>& c) {
   __syncthreads();
+  // every thread takes the count before any thread changes it
   if (c.nsw == 0) return;
   if (threadIdx.x == 0) compose_swaps(c);
   __syncthreads();
   apply_row_map<T, false>(F, ld, kstart, c.rows, c.src, c.nrows, threadIdx.x >> 5,
                           PT / 32);
   __syncthreads();
+  if (threadIdx.x == 0) c.nsw = 0;
 }
 
 // Interchange a < b for a pivot taken at position a (an imax 1x1 pivot,
@@ -2023,21 +2026,26 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
       if (k + 1 < nc && lead) atomicOr(status, ST_NAN);
       imax = (k + 1 < n) ? k + 1 : k;
     }
+    // column imax (F[imax, r] left of it, F[r, imax] below), loaded before
+    // the decision on whether the pivot test needs it
+    T a2[RPT];
+#pragma unroll
+    for (int i = 0; i < RPT; i++) {
+      const int r = kstart + rel[i];
+      a2[i] = !on[i] ? T(0)
+                     : (r < imax ? __ldcg(F + imax + (size_t)r * ld)
+                                 : __ldcg(F + r + (size_t)imax * ld));
+    }
     const double wkk = c.wkk[par];
     const T dinv = T(1) / T(wkk);  // the 1x1 pivot's, ahead of the decision
+    long long tl[7];  // trace only: phases of the column-imax evaluation
     const PivotChoice pc = choose_pivot(
         root, k, nc, wkk, imax, bv < 0.0 ? 0.0 : bv, tv, ustab, pivot_tol, [&]() {
           // column imax into W[:, kw + 1]; its owner publishes its diagonal
           // and the candidate column's entry in row imax
-          T a2[RPT];
-#pragma unroll
-          for (int i = 0; i < RPT; i++) {
-            const int r = kstart + rel[i];
-            a2[i] = !on[i] ? T(0)
-                           : (r < imax ? __ldcg(F + imax + (size_t)r * ld)
-                                       : __ldcg(F + r + (size_t)imax * ld));
-          }
+          if (tr) tl[0] = clock64() + (a2[0] != a2[0] || a2[RPT - 1] != a2[RPT - 1] ? 1 : 0);
           apply(wrow(imax - kstart, kw), a2);
+          if (tr) tl[1] = ts[2];
           double rv = -1.0, rt = 0.0;
           int ri = 0x7fffffff;
           T* w2 = Wl + (size_t)(kw + 1) * lld;
@@ -2053,9 +2061,11 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
                 rt = fmax(rt, fabs((double)a2[i]));
               }
             }
-          cl_reduce<PT, CS>(c, cluster, 2 * par + 1, rv, ri, rt);
+          if (tr) tl[2] = clock64();
+          cl_reduce<PT, CS>(c, cluster, 2 * par + 1, rv, ri, rt, tr ? tl + 3 : nullptr);
           return ImaxColumn{rt, c.wii[par], c.wik[par]};
         });
+    if (tr) tl[6] = clock64();
     if (tr) {
       ts[4] = tb[0];
       ts[5] = tb[1];
@@ -2069,12 +2079,15 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
       if (k < nc - 1) {
         if (cr == 0) {
           __syncthreads();
-          if (c.nsw > 0) {
+          // every thread takes the count before thread 0 changes it
+          const int nsw = c.nsw;
+          if (nsw > 0) {
             if (tid == 0) compose_swaps(c);
             __syncthreads();
             apply_row_map<T, true>(F, ld, kstart, c.rows, c.src, c.nrows, warp, NW);
           }
           __syncthreads();
+          if (tid == 0) c.nsw = 0;
           symm_swap<T, PT, true>(F, ld, n, vars, fsperm, k, nc - 1);
         } else if (tid == 0) {
           c.nsw = 0;
@@ -2125,8 +2138,10 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
         fsperm[a] = fsperm[b];
         fsperm[b] = tv2;
       }
+      if (tr) ts[9] = clock64();
       cl_swap_rows<T, PT, CS>(Wl, Ll, lld, kw + step, kw, a - kstart, b - kstart, c,
                               cluster);
+      if (tr) acc_t[14] += (unsigned long long)(clock64() - ts[9]);
     }
     // the pivot block after the interchange: W[k, kw] is the candidate's
     // diagonal (column imax's for an imax 1x1 pivot); for a 2x2 pivot
@@ -2195,6 +2210,15 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
       } else {
         acc_t[8] += (unsigned long long)(ts[8] - ts[0]);
         acc_t[9] += 1;
+        if (step == 2) {
+          // 2x2 steps: to the end of the first reduction, column imax's
+          // loads, build, stores, reduction, and the rest (the interchange
+          // separately in acc_t[14])
+          acc_t[11] += (unsigned long long)(ts[6] - ts[0]);
+          acc_t[12] += (unsigned long long)(tl[0] - ts[6]);
+          acc_t[13] += (unsigned long long)(tl[1] - tl[0]);
+          acc_t[15] += (unsigned long long)(tl[5] - tl[1]);
+        }
       }
     }
   }
@@ -2203,7 +2227,9 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
   // to F and its W rows below k to HBM, each CTA for its own rows
   long long tw = tr ? clock64() : 0;
   __syncthreads();
-  if (c.nsw > 0) {
+  // every thread takes the count before thread 0 composes the map
+  const int nsw = c.nsw;
+  if (nsw > 0) {
     if (tid == 0) compose_swaps(c);
     __syncthreads();
     apply_row_map<T, true>(F, ld, kstart, c.rows, c.src, c.nrows, cr * NW + warp, CS * NW);
@@ -2228,7 +2254,7 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
   }
   if (tr) {
     unsigned long long* fine = reinterpret_cast<unsigned long long*>(dbg + 32);
-    for (int q = 0; q < 11; q++) atomicAdd(fine + q, acc_t[q]);
+    for (int q = 0; q < 16; q++) atomicAdd(fine + q, acc_t[q]);
     atomicAdd(reinterpret_cast<unsigned long long*>(dbg + 8) + 4,
               (unsigned long long)(clock64() - tw));
   }
@@ -2655,6 +2681,14 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                              "other steps %llu cycles each (%llu)\n",
                      fi[0] / nf, fi[1] / nf, fi[2] / nf, fi[3] / nf, fi[4] / nf, fi[5] / nf,
                      fi[6] / nf, fi[7] / nf, fi[9] ? fi[8] / fi[9] : 0ull, fi[9]);
+      const unsigned long long n2 = (unsigned long long)(q[2] + q[3]);
+      const unsigned long long nsw = (unsigned long long)(q[1] + q[3]);
+      if (fi[0] && n2)
+        std::fprintf(stderr, "           2x2-step cycles: to first reduction %llu "
+                             "imax loads %llu imax build %llu imax stores+reduce %llu | "
+                             "interchange %llu per swap\n",
+                     fi[11] / n2, fi[12] / n2, fi[13] / n2, fi[15] / n2,
+                     nsw ? fi[14] / nsw : 0ull);
     }
     std::fprintf(stderr, "total: small %.3f ms, large %.3f ms\n", tot_s, tot_b);
     for (auto& e : ev) cudaEventDestroy(e);

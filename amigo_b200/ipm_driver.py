@@ -135,7 +135,7 @@ def solve(backend, options=None, verbose=False):
 
 
 def solve_batch(model, device="cuda", options=None, verbose=False,
-                precision="fp64"):
+                precision="fp64", rescue=True):
     """`solve` for every instance of a batch (problems.cartpole.CartPoleBatch)
     at once, on batch_engine.BatchEngine: each phase is one launch over all
     instances (the KKT matrices are factored together by the block-diagonal
@@ -148,7 +148,10 @@ def solve_batch(model, device="cuda", options=None, verbose=False,
     analysis, uploads), fallbacks (FP64 refactorizations of the
     mixed-precision form) and x (host, concatenated).  precision "fp32"
     factors with FP32 fronts and refines every direction against the FP64
-    KKT."""
+    KKT.  With `rescue`, an instance the batched driver leaves unconverged is
+    solved again, alone, by optimizer.Optimizer (amigo's default algorithm:
+    heuristic barrier, filter line search, restoration) on the same GPU
+    core; `rescued` marks them (their time is part of time_s)."""
     from .batch_engine import BatchEngine
     dev = torch.device(device)
     t0 = time.perf_counter()
@@ -164,12 +167,35 @@ def solve_batch(model, device="cuda", options=None, verbose=False,
         if verbose:
             print("live %d" % (model.k - len(results)))
     R = [results[k] for k in range(model.k)]
+    rescued = np.zeros(model.k, bool)
+    if rescue:
+        for k, r in enumerate(R):
+            if not r["converged"]:
+                R[k] = _solve_reference_algorithm(model.inst[k], dev)
+                rescued[k] = True
     col = lambda key, dt: np.array([r[key] for r in R], dtype=dt)
     return dict(converged=col("converged", bool), iterations=col("iterations", np.int64),
                 objective=col("objective", float), kkt_error=col("kkt_error", float),
                 inertia_corrections=col("inertia_corrections", np.int64),
-                time_s=time.perf_counter() - t0, setup_s=t_setup,
+                time_s=time.perf_counter() - t0, setup_s=t_setup, rescued=rescued,
                 fallbacks=eng.fallbacks, x=np.concatenate([r["x"] for r in R]))
+
+
+def _solve_reference_algorithm(m, dev):
+    """One cart-pole instance by optimizer.Optimizer on the GPU core."""
+    from .optimizer import Optimizer
+    P = CartPoleProblem(m, dev)
+    x = torch.from_numpy(np.asarray(m.x0, dtype=np.float64)).to(dev)
+    opt = Optimizer(P, x, np.asarray(m.lower, np.float64), np.asarray(m.upper, np.float64),
+                    B200Solver(P), device=dev)
+    r = opt.optimize()
+    xf = opt.vars.get_solution()
+    last = r["iterations"][-1]
+    return dict(converged=bool(r["converged"]), iterations=len(r["iterations"]) - 1,
+                objective=P.objective(xf), kkt_error=float(last["nlp_error"]),
+                inertia_corrections=int(sum(1 for it in r["iterations"]
+                                            if it.get("inertia_delta", 0.0) > 0.0)),
+                x=xf.cpu().numpy())
 
 
 class CartPoleProblem:
