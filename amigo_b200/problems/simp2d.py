@@ -113,6 +113,12 @@ class Simp2D:
         fixed = np.concatenate([self.u0 + 2 * left, self.u0 + 2 * left + 1,
                                 self.lam0 + 2 * left, self.lam0 + 2 * left + 1])
         self.fixed = np.sort(fixed).astype(np.int32)
+        # a fixed row is an identity row, not a constraint: the fixed
+        # multipliers leave the multiplier set (they are neither bounded
+        # nor counted among the constraints an inertia check expects)
+        self.mult[self.fixed] = False
+        self.lower[self.fixed] = -np.inf
+        self.upper[self.fixed] = np.inf
 
         # element variable tables
         c = self.conn

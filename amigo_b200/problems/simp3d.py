@@ -146,6 +146,12 @@ class Simp3D:
         fixed = np.concatenate([self.u0 + 3 * face + d for d in range(3)] +
                                [self.lam0 + 3 * face + d for d in range(3)])
         self.fixed = np.sort(fixed).astype(np.int32)
+        # a fixed row is an identity row, not a constraint: the fixed
+        # multipliers leave the multiplier set (they are neither bounded
+        # nor counted among the constraints an inertia check expects)
+        self.mult[self.fixed] = False
+        self.lower[self.fixed] = -np.inf
+        self.upper[self.fixed] = np.inf
 
         c = self.conn
         udofs = np.stack([3 * c[:, a] + d for a in range(8) for d in range(3)], axis=1)
