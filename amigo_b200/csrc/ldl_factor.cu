@@ -1432,11 +1432,19 @@ __device__ __forceinline__ Coef2 pivot2_coeffs(T d11, T d21, T d22) {
 // acc[i] -= sum_j L[r_i, j] * y[j] over the panel's columns j < kw, with
 // L recomputed from the shared W columns; y[j] = W[yrow, j] of the column
 // being built.  Every column is L[r, j] = W[r, j] cA[j] + W[r, cP[j]] cB[j]
-// (cB = 0 and cP = j for a 1x1 pivot: the product W[r, j] cA[j] exactly),
-// so the loop has no branch and is unrolled by two.
+// (cB = 0 and cP = j for a 1x1 pivot: the product W[r, j] cA[j] exactly).
+// The sum runs in four partial sums, column j into partial j mod 4 in the
+// order of j, added as (s0 + s1) + (s2 + s3): four independent chains of
+// multiply-adds instead of one (the cluster panel sums in the same order).
 template <class T>
 __device__ __forceinline__ T sw_l(T w, T wp, T a, T b) {
   return fma(wp, b, w * a);
+}
+
+template <class T, int RPT>
+__device__ __forceinline__ void sum4_apply(T (&acc)[RPT], const T (&s)[RPT][4]) {
+#pragma unroll
+  for (int i = 0; i < RPT; i++) acc[i] -= (s[i][0] + s[i][1]) + (s[i][2] + s[i][3]);
 }
 
 template <class T, int PT, int RPT>
@@ -1444,31 +1452,39 @@ __device__ __forceinline__ void sw_apply_panel(const T* __restrict__ Ws, int cld
                                                int kw, int yrow, const SwCtl<PT>& c,
                                                const int (&rr)[RPT],
                                                const bool (&on)[RPT], T (&acc)[RPT]) {
+  T s[RPT][4];
+#pragma unroll
+  for (int i = 0; i < RPT; i++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) s[i][q] = T(0);
   int j = 0;
-  for (; j + 2 <= kw; j += 2) {
-    const T* w0 = Ws + (size_t)j * cld;
-    const T* w1 = w0 + cld;
-    const T* p0 = Ws + (size_t)c.cP[j] * cld;
-    const T* p1 = Ws + (size_t)c.cP[j + 1] * cld;
-    const T a0 = T(c.cA[j]), b0 = T(c.cB[j]), y0 = w0[yrow];
-    const T a1 = T(c.cA[j + 1]), b1 = T(c.cB[j + 1]), y1 = w1[yrow];
+  for (; j + 4 <= kw; j += 4) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const T* w0 = Ws + (size_t)(j + q) * cld;
+      const T* p0 = Ws + (size_t)c.cP[j + q] * cld;
+      const T a0 = T(c.cA[j + q]), b0 = T(c.cB[j + q]), y0 = w0[yrow];
+#pragma unroll
+      for (int i = 0; i < RPT; i++)
+        if (on[i]) s[i][q] += sw_l(w0[rr[i]], p0[rr[i]], a0, b0) * y0;
+    }
+  }
+  // the last kw mod 4 columns (j is a multiple of 4 here: column j + q goes
+  // to partial q)
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    if (j + q >= kw) break;
+    const T* w0 = Ws + (size_t)(j + q) * cld;
+    const T* p0 = Ws + (size_t)c.cP[j + q] * cld;
+    const T a0 = T(c.cA[j + q]), b0 = T(c.cB[j + q]), y0 = w0[yrow];
 #pragma unroll
     for (int i = 0; i < RPT; i++)
-      if (on[i]) {
-        const T l0 = sw_l(w0[rr[i]], p0[rr[i]], a0, b0);
-        const T l1 = sw_l(w1[rr[i]], p1[rr[i]], a1, b1);
-        acc[i] -= l0 * y0;
-        acc[i] -= l1 * y1;
-      }
+      if (on[i]) s[i][q] += sw_l(w0[rr[i]], p0[rr[i]], a0, b0) * y0;
   }
-  if (j < kw) {
-    const T* w0 = Ws + (size_t)j * cld;
-    const T* p0 = Ws + (size_t)c.cP[j] * cld;
-    const T a0 = T(c.cA[j]), b0 = T(c.cB[j]), y0 = w0[yrow];
 #pragma unroll
-    for (int i = 0; i < RPT; i++)
-      if (on[i]) acc[i] -= sw_l(w0[rr[i]], p0[rr[i]], a0, b0) * y0;
-  }
+  for (int i = 0; i < RPT; i++)
+    if (!on[i]) s[i][0] = s[i][1] = s[i][2] = s[i][3] = T(0);
+  sum4_apply<T, RPT>(acc, s);
 }
 
 // Rows a and b interchanged in the shared W columns [0, ncol).
@@ -1922,7 +1938,33 @@ __device__ void cl_swap_rows(T* Wl, T* Ll, int lld, int nw, int nl, int a, int b
   cluster.sync();
 }
 
-template <class T, int PT, int RPT, int CS, class Cl>
+// The composed row map (rows[t] <- src[t], nr <= 64) applied to the
+// variable list and the fully-summed permutation by one warp: loads before
+// stores.
+__device__ __forceinline__ void cl_map_vars(int* vars, int* fsperm, const int* rows,
+                                            const int* src, int nr) {
+  const int lane = threadIdx.x & 31;
+  int v0 = 0, v1 = 0, p0 = 0, p1 = 0;
+  if (lane < nr) {
+    v0 = vars[src[lane]];
+    p0 = fsperm[src[lane]];
+  }
+  if (lane + 32 < nr) {
+    v1 = vars[src[lane + 32]];
+    p1 = fsperm[src[lane + 32]];
+  }
+  __syncwarp();
+  if (lane < nr) {
+    vars[rows[lane]] = v0;
+    fsperm[rows[lane]] = p0;
+  }
+  if (lane + 32 < nr) {
+    vars[rows[lane + 32]] = v1;
+    fsperm[rows[lane + 32]] = p1;
+  }
+}
+
+template <class T, int PT, int RPT, int CS, bool TR, class Cl>
 __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
                                 int* vars, int* fsperm, double ustab,
                                 double pivot_tol, int* status, ClCtl<PT, CS>& c,
@@ -1958,11 +2000,17 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
   };
   long long ts[10];  // trace only: clocks of the phases of a step (lead)
   unsigned long long acc_t[16] = {};
-  const bool tr = dbg != nullptr && lead;
+  // (TR: the trace build, with the step counters and phase clocks)
+  const bool tr = TR && dbg != nullptr && lead;
   // acc[i] -= sum_{j < kw} L[r_i, j] y_j (the order of sw_apply_panel), y_j
   // in lane j of yv; the L entries of 8 columns are loaded before their
   // multiply-adds
   auto apply = [&](T yv, T (&acc)[RPT]) {
+    T sm4[RPT][4];
+#pragma unroll
+    for (int i = 0; i < RPT; i++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) sm4[i][q] = T(0);
     for (int j0 = 0; j0 < kw; j0 += 8) {
       T lv[RPT][8];
 #pragma unroll
@@ -1976,10 +2024,14 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
         if (j0 + u < kw) {
 #pragma unroll
           for (int i = 0; i < RPT; i++)
-            if (on[i]) acc[i] -= lv[i][u] * yj;
+            if (on[i]) sm4[i][u & 3] += lv[i][u] * yj;
         }
       }
     }
+#pragma unroll
+    for (int i = 0; i < RPT; i++)
+      if (!on[i]) sm4[i][0] = sm4[i][1] = sm4[i][2] = sm4[i][3] = T(0);
+    sum4_apply<T, RPT>(acc, sm4);
     if (tr) ts[2] = clock64() + (acc[0] != acc[0] ? 1 : 0);
   };
   load_col(k, cur);
@@ -2073,7 +2125,7 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
       ts[7] = clock64();
     }
     if (pc.step == 0) {
-      if (dbg && lead) atomicAdd(dbg + 4, 1);
+      if (tr) atomicAdd(dbg + 4, 1);
       // delay candidate k (the full interchange with nc - 1 after the
       // pending ones, by CTA 0; the W and L rows by their CTAs)
       if (k < nc - 1) {
@@ -2085,6 +2137,7 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
             if (tid == 0) compose_swaps(c);
             __syncthreads();
             apply_row_map<T, true>(F, ld, kstart, c.rows, c.src, c.nrows, warp, NW);
+            if (warp == 0) cl_map_vars(vars, fsperm, c.rows, c.src, c.nrows);
           }
           __syncthreads();
           if (tid == 0) c.nsw = 0;
@@ -2102,7 +2155,7 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
     const int step = pc.step, kpiv = pc.kpiv;
     const int ksrc = k + step - 1;
     const bool swapped = kpiv != ksrc;
-    if (dbg && lead)
+    if (tr)
       atomicAdd(dbg + (step == 1 ? (pc.imax_1x1 ? 1 : 0) : (swapped ? 3 : 2)), 1);
     if (pc.imax_1x1) {
       // column imax is the pivot column (own rows)
@@ -2130,14 +2183,8 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
         c.swb[c.nsw] = b;
         c.nsw++;
       }
-      if (lead) {
-        int tv2 = vars[a];
-        vars[a] = vars[b];
-        vars[b] = tv2;
-        tv2 = fsperm[a];
-        fsperm[a] = fsperm[b];
-        fsperm[b] = tv2;
-      }
+      // (the variable list and the fully-summed permutation follow the
+      // recorded interchanges at the end of the panel)
       if (tr) ts[9] = clock64();
       cl_swap_rows<T, PT, CS>(Wl, Ll, lld, kw + step, kw, a - kstart, b - kstart, c,
                               cluster);
@@ -2156,7 +2203,6 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
       c.cA[kw] = (double)ainv;
       c.cB[kw] = 0.0;
       c.cP[kw] = kw;
-      if (lead) vars[3 * ld + k] = 0;
       T* lc = Ll + (size_t)kw * lld;
 #pragma unroll
       for (int i = 0; i < RPT; i++)
@@ -2172,12 +2218,6 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
       c.cB[kw + 1] = q.i01;
       c.cP[kw] = kw + 1;
       c.cP[kw + 1] = kw;
-      if (lead) {
-        vars[k] = -(vars[k] + 1);
-        vars[k + 1] = -(vars[k + 1] + 1);
-        vars[3 * ld + k] = 1;
-        vars[3 * ld + k + 1] = 2;
-      }
       const T* w0 = wcol;
       const T* w1 = wcol + lld;
       T* l0 = Ll + (size_t)kw * lld;
@@ -2234,6 +2274,18 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
     __syncthreads();
     apply_row_map<T, true>(F, ld, kstart, c.rows, c.src, c.nrows, cr * NW + warp, CS * NW);
   }
+  // the panel's interchanges of the variable list and the fully-summed
+  // permutation, then its pivot kinds (2x2 pivots' variables encoded
+  // -(v + 1)), by warp 0 of CTA 0
+  if (cr == 0 && warp == 0) {
+    if (nsw > 0) cl_map_vars(vars, fsperm, c.rows, c.src, c.nrows);
+    __syncwarp();
+    if (lane < kw) {
+      const int col = kstart + lane, kd = c.kind[lane];
+      vars[3 * ld + col] = kd;
+      if (kd != 0) vars[col] = -(vars[col] + 1);
+    }
+  }
   for (int j = 0; j < kw; j++) {
     const int col = kstart + j;
     const int kd = c.kind[j];
@@ -2270,7 +2322,7 @@ __host__ __device__ __forceinline__ int cl_local_rows(int cld) {
   return 32 * (((cld + 31) / 32 + CS - 1) / CS);
 }
 
-template <class T, int PT, int RPT, int CS>
+template <class T, int PT, int RPT, int CS, bool TR>
 __global__ void __launch_bounds__(PT, 1)
 k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
                double pivot_tol, int smem_bytes, int width_rule, int* dbg) {
@@ -2324,15 +2376,15 @@ k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
   if (nbe >= 4 && cld <= max_rows &&
       2ll * nbe * lld * (long long)sizeof(T) <= smem_bytes) {
     long long tk0 = 0;
-    if (dbg && cr == 0 && threadIdx.x == 0) {
+    if (TR && dbg && cr == 0 && threadIdx.x == 0) {
       atomicAdd(dbg + 5, 1);
       tk0 = clock64();
     }
     T* Wl = reinterpret_cast<T*>(cl_raw);
-    panel_factor_cl<T, PT, RPT, CS>(F, f, W, f, fs == f, fvars, fvars + f, ustab,
+    panel_factor_cl<T, PT, RPT, CS, TR>(F, f, W, f, fs == f, fvars, fvars + f, ustab,
                                     pivot_tol, d.status, c, Wl, Wl + (size_t)nbe * lld,
                                     lld, nbe, k, nc, kw, dbg, cluster);
-    if (dbg && cr == 0 && threadIdx.x == 0)
+    if (TR && dbg && cr == 0 && threadIdx.x == 0)
       atomicAdd(reinterpret_cast<unsigned long long*>(dbg + 8) + 5,
                 (unsigned long long)(clock64() - tk0));
     // no CTA leaves while another may still read its shared memory
@@ -2465,8 +2517,12 @@ static int launch_panel_cl(int fronts, int smem, cudaStream_t s, const DevicePla
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  FCUDA(cudaLaunchKernelEx(&cfg, k_big_panel_cl<T, kClThreads, kClRows, kClCS>, d,
-                           nodes, ustab, pivot_tol, smem, width_rule, dbg));
+  if (dbg)
+    FCUDA(cudaLaunchKernelEx(&cfg, k_big_panel_cl<T, kClThreads, kClRows, kClCS, true>, d,
+                             nodes, ustab, pivot_tol, smem, width_rule, dbg));
+  else
+    FCUDA(cudaLaunchKernelEx(&cfg, k_big_panel_cl<T, kClThreads, kClRows, kClCS, false>, d,
+                             nodes, ustab, pivot_tol, smem, width_rule, nullptr));
   ab::count_launch();
   return 0;
 }
@@ -2494,7 +2550,10 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     FCUDA(cudaFuncSetAttribute(k_big_update_tc,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::kSmemBytes));
-    FCUDA(cudaFuncSetAttribute(k_big_panel_cl<T, kClThreads, kClRows, kClCS>,
+    FCUDA(cudaFuncSetAttribute(k_big_panel_cl<T, kClThreads, kClRows, kClCS, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kClSmemMax));
+    FCUDA(cudaFuncSetAttribute(k_big_panel_cl<T, kClThreads, kClRows, kClCS, true>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kClSmemMax));
     attr_set = true;

@@ -123,7 +123,7 @@ struct LdlHandle {
   // at least cl_min_rows rows, 1 one-CTA panels only, 2 cluster panels
   // with the one-CTA panel's widths
   int panel_mode = 0;
-  int cl_min_rows = 384;
+  int cl_min_rows = 768;
   long long wide_entries = 1 << 22;
   // front storage / arithmetic of the next factorization (64: FP64, 32:
   // FP32 fronts for mixed precision) and of the last one

@@ -136,7 +136,7 @@ int ab_ldl_set_wide_threshold(ab_ldl_t h, long long entries);
 int ab_ldl_set_cluster_threshold(ab_ldl_t h, long long entries);
 
 /* Large-front panel knob.  mode 0 (default): levels whose largest front
- * has at least min_rows rows (default 384) factor their panels on one
+ * has at least min_rows rows (default 768) factor their panels on one
  * thread-block cluster of 8 CTAs per front, NB = 32 columns a panel;
  * mode 1: one CTA per front for every level; mode 2: cluster panels with
  * the one-CTA panel's widths, whose results are the one-CTA panel's bit
