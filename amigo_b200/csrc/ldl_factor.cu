@@ -85,6 +85,16 @@ __device__ __forceinline__ void argmax_merge(double& v, int& i, double v2,
   }
 }
 
+// Programmatic dependent launch: the large-front panel and update kernels
+// are launched so that the next one may be scheduled while the previous one
+// drains; each waits here for its predecessor's completion and memory
+// before touching the front, then lets its own successor be scheduled.
+// (Both are no-ops for a kernel launched without the attribute.)
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Symmetric interchange of rows/columns a < b of the lower triangle of F,
 // of the variable list and of the fully-summed permutation record
 // (reference: symm_swap, include/sparse_ldl.h:1252-1274).
@@ -1202,6 +1212,7 @@ template <class T, int PT>
 __global__ void __launch_bounds__(PT)
 k_big_panel(DevicePlan d, const int* __restrict__ nodes, double ustab,
             double pivot_tol, int cache_bytes) {
+  pdl_enter();
   __shared__ CtlT<PT> ctl;
   extern __shared__ double cache_raw[];
   if (big_skip(d)) return;
@@ -1730,6 +1741,7 @@ template <class T, int PT, int RPT>
 __global__ void __launch_bounds__(PT)
 k_big_panel_sw(DevicePlan d, const int* __restrict__ nodes, double ustab,
                double pivot_tol, int smem_bytes, int* dbg) {
+  pdl_enter();
   __shared__ SwCtl<PT> c;
   __shared__ CtlT<PT> ctl;
   extern __shared__ double sw_raw[];
@@ -2326,6 +2338,7 @@ template <class T, int PT, int RPT, int CS, bool TR>
 __global__ void __launch_bounds__(PT, 1)
 k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
                double pivot_tol, int smem_bytes, int width_rule, int* dbg) {
+  pdl_enter();
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   __shared__ ClCtl<PT, CS> c;
@@ -2407,6 +2420,7 @@ k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
 template <class T>
 __global__ void __launch_bounds__(NT)
 k_big_update(DevicePlan d, const int* __restrict__ nodes) {
+  pdl_enter();
   extern __shared__ double tiles_raw[];
   T* tiles = reinterpret_cast<T*>(tiles_raw);
   if (big_skip(d)) return;
@@ -2499,6 +2513,24 @@ __global__ void k_big_remaining(DevicePlan d, const int* __restrict__ nodes,
     }                                                                     \
   } while (0)
 
+// A launch that may start while the previous kernel of the stream drains
+// (programmatic stream serialization; the kernel waits in pdl_enter).
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block,
+                              size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // One cluster of kClCS CTAs per front (cudaLaunchKernelEx with a cluster
 // dimension).
 template <class T>
@@ -2510,20 +2542,21 @@ static int launch_panel_cl(int fronts, int smem, cudaStream_t s, const DevicePla
   cfg.blockDim = dim3(kClThreads);
   cfg.dynamicSmemBytes = (size_t)smem;
   cfg.stream = s;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = kClCS;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = 2;
   if (dbg)
     FCUDA(cudaLaunchKernelEx(&cfg, k_big_panel_cl<T, kClThreads, kClRows, kClCS, true>, d,
                              nodes, ustab, pivot_tol, smem, width_rule, dbg));
   else
     FCUDA(cudaLaunchKernelEx(&cfg, k_big_panel_cl<T, kClThreads, kClRows, kClCS, false>, d,
                              nodes, ustab, pivot_tol, smem, width_rule, nullptr));
-  ab::count_launch();
   return 0;
 }
 
@@ -2658,24 +2691,29 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
             const int rc = launch_panel_cl<T>(B, cl_smem, s, d, nodes, h.ustab,
                                               h.pivot_tol, cl_rule, dbg_l);
             if (rc) return rc;
-          } else if (use_sw)
-            k_big_panel_sw<T, kSwThreads, kSwRows><<<B, kSwThreads, sw_smem, s>>>(
-                d, nodes, h.ustab, h.pivot_tol, sw_smem, dbg_l);
-          else if (fm > kPanelWideRows)
-            k_big_panel<T, kPanelThreadsWide><<<B, kPanelThreadsWide, panel_cache, s>>>(
-                d, nodes, h.ustab, h.pivot_tol, panel_cache);
-          else
-            k_big_panel<T, kPanelThreads><<<B, kPanelThreads, panel_cache, s>>>(
-                d, nodes, h.ustab, h.pivot_tol, panel_cache);
+          } else if (use_sw) {
+            FCUDA(launch_pdl(k_big_panel_sw<T, kSwThreads, kSwRows>, dim3(B),
+                             dim3(kSwThreads), (size_t)sw_smem, s, d, nodes, h.ustab,
+                             h.pivot_tol, sw_smem, dbg_l));
+          } else if (fm > kPanelWideRows) {
+            FCUDA(launch_pdl(k_big_panel<T, kPanelThreadsWide>, dim3(B),
+                             dim3(kPanelThreadsWide), (size_t)panel_cache, s, d, nodes,
+                             h.ustab, h.pivot_tol, panel_cache));
+          } else {
+            FCUDA(launch_pdl(k_big_panel<T, kPanelThreads>, dim3(B), dim3(kPanelThreads),
+                             (size_t)panel_cache, s, d, nodes, h.ustab, h.pivot_tol,
+                             panel_cache));
+          }
           ab::count_launch();
           if (trace) cudaEventRecord(te[1], s);
           if (use_tc) {
             { k_big_update_tc<<<dim3(B, gtc), tc::kThreads, tc::kSmemBytes, s>>>(
                 d, nodes); ab::count_launch(); }
           } else {
-            { k_big_update<T><<<dim3(B, std::max(gu, 1)), NT,
-                                (sizeof(T) == 8 ? kTileSmemD : kTileSmem) * sizeof(T), s>>>(
-                d, nodes); ab::count_launch(); }
+            FCUDA(launch_pdl(k_big_update<T>, dim3(B, std::max(gu, 1)), dim3(NT),
+                             (size_t)((sizeof(T) == 8 ? kTileSmemD : kTileSmem) * sizeof(T)),
+                             s, d, nodes));
+            ab::count_launch();
           }
           if (trace) {
             cudaEventRecord(te[2], s);

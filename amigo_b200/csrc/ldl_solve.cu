@@ -170,6 +170,13 @@ __device__ __forceinline__ void warp_upper_solve(const double* sL, int lds,
   }
 }
 
+// Programmatic dependent launch (see the factorization's pdl_enter): wait
+// for the previous kernel of the stream, then let the next be scheduled.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Front vector of `node` for one right-hand side: the node's own entries
 // of the right-hand side plus the update vectors of its children, placed
 // by the same row map as the factorization's extend-add.  Called by a
@@ -219,6 +226,7 @@ __global__ void __launch_bounds__(NT)
 k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
                 int nrhs, int ldx, double* ubuf, const long long* uoff,
                 int smem_doubles) {
+  pdl_enter();
   extern __shared__ double sV[];
   const int node = nodes[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -287,6 +295,7 @@ __global__ void __launch_bounds__(NT)
 k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
                  int nrhs, int ldx, double* ubuf, const long long* uoff,
                  int smem_doubles) {
+  pdl_enter();
   extern __shared__ double sV[];
   const int node = nodes[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -355,6 +364,7 @@ template <class T>
 __global__ void __launch_bounds__(NT, 1)
 k_clu_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
               int nrhs, int ldx, double* ubuf, const long long* uoff) {
+  pdl_enter();
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ double sm[];
@@ -455,6 +465,7 @@ template <class T>
 __global__ void __launch_bounds__(NT, 1)
 k_clu_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
                int nrhs, int ldx, double* ubuf, const long long* uoff) {
+  pdl_enter();
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ double sm[];
@@ -797,6 +808,24 @@ k_wide_backward(DevicePlan d, const int* __restrict__ nodes, int count,
     }                                                                     \
   } while (0)
 
+// A launch that may start while the previous kernel of the stream drains
+// (programmatic stream serialization; the kernel waits in pdl_enter).
+template <class... KArgs, class... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block,
+                              size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // One cluster of CS CTAs per front (cudaLaunchKernelEx with a cluster
 // dimension).
 template <class K>
@@ -808,13 +837,15 @@ static int launch_cluster(K kernel, int fronts, int smem, cudaStream_t s,
   cfg.blockDim = dim3(NT);
   cfg.dynamicSmemBytes = (size_t)smem;
   cfg.stream = s;
-  cudaLaunchAttribute attr[1];
+  cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = CS;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
+  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = 2;
   SCUDA(cudaLaunchKernelEx(&cfg, kernel, d, nodes, x, nrhs, ldx, ubuf, uoff));
   ab::count_launch();
   return 0;
@@ -966,9 +997,12 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
   for (int l = 0; l < d.num_levels; l++) {
     if (trace) cudaEventRecord(ev[l], s);
     const int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
-    if (cnt)
-      { k_solve_forward<T><<<cnt, NT, h.sv_narrow_smem[l], s>>>(d, h.sv_nodes + b, d_x, nrhs,
-                                               ldx, h.ubuf, h.uoff, h.sv_narrow_smem[l] / 8); ab::count_launch(); }
+    if (cnt) {
+      SCUDA(launch_pdl(k_solve_forward<T>, dim3(cnt), dim3(NT), (size_t)h.sv_narrow_smem[l],
+                       s, d, h.sv_nodes + b, d_x, nrhs, ldx, h.ubuf, h.uoff,
+                       h.sv_narrow_smem[l] / 8));
+      ab::count_launch();
+    }
     const int cb = h.sv_clu_ptr[l], ccnt = h.sv_wide_ptr[l] - cb;
     if (ccnt) {
       int rc = launch_cluster(k_clu_forward<T>, ccnt, h.sv_clu_smem[l], s, d,
@@ -993,10 +1027,12 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
   for (int l = d.num_levels - 1; l >= 0; l--) {
     if (trace) cudaEventRecord(ev[d.num_levels + 1 + (d.num_levels - 1 - l)], s);
     const int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
-    if (cnt)
-      { k_solve_backward<T><<<cnt, NT, h.sv_narrow_smem[l], s>>>(d, h.sv_nodes + b, d_x,
-                                                nrhs, ldx, h.ubuf, h.uoff,
-                                                h.sv_narrow_smem[l] / 8); ab::count_launch(); }
+    if (cnt) {
+      SCUDA(launch_pdl(k_solve_backward<T>, dim3(cnt), dim3(NT), (size_t)h.sv_narrow_smem[l],
+                       s, d, h.sv_nodes + b, d_x, nrhs, ldx, h.ubuf, h.uoff,
+                       h.sv_narrow_smem[l] / 8));
+      ab::count_launch();
+    }
     const int cb = h.sv_clu_ptr[l], ccnt = h.sv_wide_ptr[l] - cb;
     if (ccnt) {
       int rc = launch_cluster(k_clu_backward<T>, ccnt, h.sv_clu_smem[l], s, d,
