@@ -2763,6 +2763,9 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       const int* q = dbg_h.data() + 64 * l;
       const unsigned long long* cy = reinterpret_cast<const unsigned long long*>(q + 8);
       const unsigned long long* fi = reinterpret_cast<const unsigned long long*>(q + 32);
+      if (!q[5] && (tpan[l] > 0.f || tupd[l] > 0.f))
+        std::fprintf(stderr, "           panel launches %.3f ms update launches %.3f ms\n",
+                     tpan[l], tupd[l]);
       if (q[5])
         std::fprintf(stderr, "           panel steps: fast %d imax %d 2x2 %d "
                              "2x2-swap %d delay %d panels %d | kcyc: build %llu "

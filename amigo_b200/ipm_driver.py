@@ -162,7 +162,9 @@ def solve_batch(model, device="cuda", options=None, verbose=False,
     t_setup = time.perf_counter() - t0
     results = {}
     while len(results) < model.k:
-        for r in eng.step(rebuild=False):
+        # compact the layout once half of it has retired, so the last
+        # instances' iterations factor only the live ones
+        for r in eng.step(rebuild=eng.live() > 0 and eng.dead_fraction() >= 0.5):
             results[r["id"]] = r
         if verbose:
             print("live %d" % (model.k - len(results)))
