@@ -184,8 +184,18 @@ int ab_ldl_mem_estimate(ab_ldl_t H, int precision, double delay_growth,
   }
   plan += 12LL * amap;
   const long long solve = 8LL * fsum * (nrhs > 0 ? nrhs : 1);
+  // global scratch of the cluster panel for fronts past shared memory: W
+  // and L rows of NB columns for every CTA of a cluster of up to 16, with
+  // each CTA's rows rounded up to whole 32-row groups (bounded by the sum
+  // over those fronts)
+  long long clg = 0;
+  for (int k = 0; k < T.num_nodes; k++) {
+    const long long f = (T.node_ptr[k + 1] - T.node_ptr[k]) +
+                        (T.contrib_ptr[k + 1] - T.contrib_ptr[k]);
+    if (f + 64 > 3072) clg += 2LL * ab::kPanel * (f + 64 + 16 * 32) * el;
+  }
   *bytes = (long long)(g * (double)(fronts * el)) + (long long)(g * (double)(ints * 4)) +
-           plan + solve;
+           plan + solve + clg;
   return AB_OK;
 }
 
@@ -441,7 +451,7 @@ int ab_ldl_set_cluster_threshold(ab_ldl_t h, long long entries) {
 }
 
 int ab_ldl_set_panel_mode(ab_ldl_t h, int mode, int min_rows) {
-  if (!h || mode < 0 || mode > 2) return AB_ERR_ARG;
+  if (!h || mode < 0 || mode > 3) return AB_ERR_ARG;
   h->h.panel_mode = mode;
   if (min_rows > 0) h->h.cl_min_rows = min_rows;
   return AB_OK;

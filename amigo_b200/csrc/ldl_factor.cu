@@ -1822,6 +1822,11 @@ constexpr int kClCS = 8;
 // and L of NB columns fit in a CTA's shared memory.
 constexpr int kClMaxRows = 3072;
 constexpr int kClSlack = 64;
+// Global-scratch cluster panel (GL): rows per thread; clusters of 8 take
+// fronts to 8 x 256 x 8 rows, of 16 to twice that.
+constexpr int kClRowsG = 8;
+constexpr int kClMaxRowsG8 = kClThreads * kClRowsG * 8;
+constexpr int kClMaxRowsG16 = kClThreads * kClRowsG * 16;
 constexpr int kClSmemMax = 2 * NB * (kClMaxRows / kClCS) * 8;
 static_assert(kClMaxRows <= kClThreads * kClRows * kClCS, "cluster panel rows");
 
@@ -1837,6 +1842,7 @@ struct ClCtl {
   int swa[NB], swb[NB], nsw;
   int rows[2 * NB], src[2 * NB], nrows;
   double xw[2][NB], xl[2][NB];  // W and L rows received in an interchange
+  double ys[PT / 32][32];       // each warp's copy of the W row being applied
   int u[4];                     // launch-uniform values published by CTA 0
 };
 
@@ -1892,13 +1898,14 @@ __device__ __forceinline__ void cl_reduce(ClCtl<PT, CS>& c, Cl& cluster, int set
   cluster.sync();
   if (ts) ts[1] = clock64();
   constexpr int NS = ClCtl<PT, CS>::NS;
-  static_assert(NS <= 64, "cluster warps");
+  static_assert(NS <= 128, "cluster warps");
   v = lane < NS ? c.rv[set][lane] : -1.0;
   i = lane < NS ? c.ri[set][lane] : 0x7fffffff;
   v2 = lane < NS ? c.rv2[set][lane] : 0.0;
-  if (NS > 32 && lane + 32 < NS) {
-    argmax_merge(v, i, c.rv[set][lane + 32], c.ri[set][lane + 32]);
-    v2 = fmax(v2, c.rv2[set][lane + 32]);
+#pragma unroll
+  for (int q = lane + 32; q < NS; q += 32) {
+    argmax_merge(v, i, c.rv[set][q], c.ri[set][q]);
+    v2 = fmax(v2, c.rv2[set][q]);
   }
   warp_fold_redux(v, i, v2);
   if (ts) ts[2] = clock64() + (v != v ? 1 : 0);
@@ -1976,12 +1983,16 @@ __device__ __forceinline__ void cl_map_vars(int* vars, int* fsperm, const int* r
   }
 }
 
-template <class T, int PT, int RPT, int CS, bool TR, class Cl>
+// (GL: the panel's W and L rows of each CTA in a global scratch region --
+// CTA r's at Wcl + r * stride -- instead of its shared memory, for fronts
+// past what shared memory holds; rows of other CTAs are read from L2.)
+template <class T, int PT, int RPT, int CS, bool TR, bool GL, class Cl>
 __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
                                 int* vars, int* fsperm, double ustab,
                                 double pivot_tol, int* status, ClCtl<PT, CS>& c,
                                 T* Wl, T* Ll, int lld, int nbe, int& k_, int& nc_,
-                                int& kw_, int* dbg, Cl& cluster) {
+                                int& kw_, int* dbg, Cl& cluster, const T* Wcl,
+                                size_t stride) {
   constexpr int NW = PT / 32;
   const unsigned FULL = 0xffffffffu;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -2007,8 +2018,13 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
   };
   // lanes j < ncol: W[q, j] (q relative), from the row's CTA
   auto wrow = [&](int q, int ncol) -> T {
-    const T* p = cluster.map_shared_rank(Wl + cl_lrow<CS>(q), cl_owner<CS>(q));
-    return lane < ncol ? p[(size_t)lane * lld] : T(0);
+    if constexpr (GL) {
+      const T* p = Wcl + (size_t)cl_owner<CS>(q) * stride + cl_lrow<CS>(q);
+      return lane < ncol ? __ldcg(p + (size_t)lane * lld) : T(0);
+    } else {
+      const T* p = cluster.map_shared_rank(Wl + cl_lrow<CS>(q), cl_owner<CS>(q));
+      return lane < ncol ? p[(size_t)lane * lld] : T(0);
+    }
   };
   long long ts[10];  // trace only: clocks of the phases of a step (lead)
   unsigned long long acc_t[16] = {};
@@ -2017,33 +2033,48 @@ __device__ void panel_factor_cl(T* F, int ld, T* Wg, int n, bool root,
   // acc[i] -= sum_{j < kw} L[r_i, j] y_j (the order of sw_apply_panel), y_j
   // in lane j of yv; the L entries of 8 columns are loaded before their
   // multiply-adds
+  // the rows in chunks of RC (the partial sums and the loaded L entries of
+  // one chunk in registers); y from the warp's shared copy
+  constexpr int RC = RPT < 2 ? RPT : 2;
+  double* ys = c.ys[warp];
   auto apply = [&](T yv, T (&acc)[RPT]) {
-    T sm4[RPT][4];
+    ys[lane] = (double)yv;
+    __syncwarp();
 #pragma unroll
-    for (int i = 0; i < RPT; i++)
+    for (int i0 = 0; i0 < RPT; i0 += RC) {
+      T sm4[RC][4];
 #pragma unroll
-      for (int q = 0; q < 4; q++) sm4[i][q] = T(0);
-    for (int j0 = 0; j0 < kw; j0 += 8) {
-      T lv[RPT][8];
+      for (int i = 0; i < RC; i++)
 #pragma unroll
-      for (int u = 0; u < 8; u++)
+        for (int q = 0; q < 4; q++) sm4[i][q] = T(0);
+      bool any = false;
 #pragma unroll
-        for (int i = 0; i < RPT; i++)
-          lv[i][u] = (on[i] && j0 + u < kw) ? Ll[(size_t)(j0 + u) * lld + lr[i]] : T(0);
+      for (int i = 0; i < RC; i++) any |= on[i0 + i];
+      if (__any_sync(FULL, any)) {
+        for (int j0 = 0; j0 < kw; j0 += 8) {
+          T lv[RC][8];
 #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const T yj = __shfl_sync(FULL, yv, (j0 + u) & 31);
-        if (j0 + u < kw) {
+          for (int u = 0; u < 8; u++)
 #pragma unroll
-          for (int i = 0; i < RPT; i++)
-            if (on[i]) sm4[i][u & 3] += lv[i][u] * yj;
+            for (int i = 0; i < RC; i++)
+              lv[i][u] = (on[i0 + i] && j0 + u < kw)
+                             ? Ll[(size_t)(j0 + u) * lld + lr[i0 + i]] : T(0);
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            const T yj = T(ys[(j0 + u) & 31]);
+            if (j0 + u < kw) {
+#pragma unroll
+              for (int i = 0; i < RC; i++)
+                if (on[i0 + i]) sm4[i][u & 3] += lv[i][u] * yj;
+            }
+          }
         }
       }
-    }
 #pragma unroll
-    for (int i = 0; i < RPT; i++)
-      if (!on[i]) sm4[i][0] = sm4[i][1] = sm4[i][2] = sm4[i][3] = T(0);
-    sum4_apply<T, RPT>(acc, sm4);
+      for (int i = 0; i < RC; i++)
+        if (on[i0 + i]) acc[i0 + i] -= (sm4[i][0] + sm4[i][1]) + (sm4[i][2] + sm4[i][3]);
+    }
+    __syncwarp();
     if (tr) ts[2] = clock64() + (acc[0] != acc[0] ? 1 : 0);
   };
   load_col(k, cur);
@@ -2334,10 +2365,11 @@ __host__ __device__ __forceinline__ int cl_local_rows(int cld) {
   return 32 * (((cld + 31) / 32 + CS - 1) / CS);
 }
 
-template <class T, int PT, int RPT, int CS, bool TR>
+template <class T, int PT, int RPT, int CS, bool TR, bool GL>
 __global__ void __launch_bounds__(PT, 1)
 k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
-               double pivot_tol, int smem_bytes, int width_rule, int* dbg) {
+               double pivot_tol, int smem_bytes, int width_rule, int fit_rows,
+               int* dbg, T* scratch, long long stride) {
   pdl_enter();
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
@@ -2378,7 +2410,7 @@ k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
   // the panel width depends on the front alone: NB, or the one-CTA
   // panel's (width_rule 1)
   int nbe = NB;
-  int max_rows = kClMaxRows;
+  int max_rows = GL ? CS * PT * RPT : kClMaxRows;
   if (width_rule == 1) {
     // the one-CTA panel's widths and its row limit (beyond which it takes
     // the HBM-panel form, as below)
@@ -2386,17 +2418,24 @@ k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
     nbe = (int)(fit < NB ? fit : NB);
     max_rows = kSwThreads * kSwRows;
   }
-  if (nbe >= 4 && cld <= max_rows &&
-      2ll * nbe * lld * (long long)sizeof(T) <= smem_bytes) {
+  // full-width panels: fronts of up to fit_rows rows (the level's largest
+  // static front plus the slack its W and L rows were sized for, whatever
+  // the cluster size); the one-CTA widths: as long as W and L fit
+  const bool fits = width_rule == 0
+                        ? cld <= fit_rows
+                        : 2ll * nbe * lld * (long long)sizeof(T) <= smem_bytes;
+  if (nbe >= 4 && cld <= max_rows && fits) {
     long long tk0 = 0;
     if (TR && dbg && cr == 0 && threadIdx.x == 0) {
       atomicAdd(dbg + 5, 1);
       tk0 = clock64();
     }
-    T* Wl = reinterpret_cast<T*>(cl_raw);
-    panel_factor_cl<T, PT, RPT, CS, TR>(F, f, W, f, fs == f, fvars, fvars + f, ustab,
-                                    pivot_tol, d.status, c, Wl, Wl + (size_t)nbe * lld,
-                                    lld, nbe, k, nc, kw, dbg, cluster);
+    T* Wcl = GL ? scratch + (size_t)(blockIdx.x / CS) * CS * (size_t)stride : nullptr;
+    T* Wl = GL ? Wcl + (size_t)cr * (size_t)stride : reinterpret_cast<T*>(cl_raw);
+    panel_factor_cl<T, PT, RPT, CS, TR, GL>(F, f, W, f, fs == f, fvars, fvars + f, ustab,
+                                            pivot_tol, d.status, c, Wl,
+                                            Wl + (size_t)nbe * lld, lld, nbe, k, nc, kw,
+                                            dbg, cluster, Wcl, (size_t)stride);
     if (TR && dbg && cr == 0 && threadIdx.x == 0)
       atomicAdd(reinterpret_cast<unsigned long long*>(dbg + 8) + 5,
                 (unsigned long long)(clock64() - tk0));
@@ -2531,20 +2570,29 @@ static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block,
   return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-// One cluster of kClCS CTAs per front (cudaLaunchKernelEx with a cluster
-// dimension).
+// Whether clusters of 16 CTAs of the global-scratch panel can be scheduled
+// on this device (set once, with the kernels' attributes).
 template <class T>
+static bool& cl16_ok() {
+  static bool ok = false;
+  return ok;
+}
+
+// One cluster of CS CTAs per front (cudaLaunchKernelEx with a cluster
+// dimension).
+template <class T, int RPT = kClRows, int CS = kClCS, bool GL = false>
 static int launch_panel_cl(int fronts, int smem, cudaStream_t s, const DevicePlan& d,
                            const int* nodes, double ustab, double pivot_tol,
-                           int width_rule, int* dbg) {
+                           int width_rule, int fit_rows, int* dbg, T* scratch = nullptr,
+                           long long stride = 0) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(fronts * kClCS);
+  cfg.gridDim = dim3(fronts * CS);
   cfg.blockDim = dim3(kClThreads);
   cfg.dynamicSmemBytes = (size_t)smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[2];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = kClCS;
+  attr[0].val.clusterDim.x = CS;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -2552,11 +2600,13 @@ static int launch_panel_cl(int fronts, int smem, cudaStream_t s, const DevicePla
   cfg.attrs = attr;
   cfg.numAttrs = 2;
   if (dbg)
-    FCUDA(cudaLaunchKernelEx(&cfg, k_big_panel_cl<T, kClThreads, kClRows, kClCS, true>, d,
-                             nodes, ustab, pivot_tol, smem, width_rule, dbg));
+    FCUDA(cudaLaunchKernelEx(&cfg, k_big_panel_cl<T, kClThreads, RPT, CS, true, GL>, d,
+                             nodes, ustab, pivot_tol, smem, width_rule, fit_rows, dbg,
+                             scratch, stride));
   else
-    FCUDA(cudaLaunchKernelEx(&cfg, k_big_panel_cl<T, kClThreads, kClRows, kClCS, false>, d,
-                             nodes, ustab, pivot_tol, smem, width_rule, nullptr));
+    FCUDA(cudaLaunchKernelEx(&cfg, k_big_panel_cl<T, kClThreads, RPT, CS, false, GL>, d,
+                             nodes, ustab, pivot_tol, smem, width_rule, fit_rows,
+                             (int*)nullptr, scratch, stride));
   return 0;
 }
 
@@ -2583,12 +2633,38 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     FCUDA(cudaFuncSetAttribute(k_big_update_tc,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                tc::kSmemBytes));
-    FCUDA(cudaFuncSetAttribute(k_big_panel_cl<T, kClThreads, kClRows, kClCS, false>,
+    FCUDA(cudaFuncSetAttribute(k_big_panel_cl<T, kClThreads, kClRows, kClCS, false, false>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kClSmemMax));
-    FCUDA(cudaFuncSetAttribute(k_big_panel_cl<T, kClThreads, kClRows, kClCS, true>,
+    FCUDA(cudaFuncSetAttribute(k_big_panel_cl<T, kClThreads, kClRows, kClCS, true, false>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kClSmemMax));
+    // the global-scratch cluster panel for the largest fronts: clusters of
+    // 16 CTAs (a non-portable size) where the device schedules them
+    FCUDA(cudaFuncSetAttribute(k_big_panel_cl<T, kClThreads, kClRowsG, 16, false, true>,
+                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    FCUDA(cudaFuncSetAttribute(k_big_panel_cl<T, kClThreads, kClRowsG, 16, true, true>,
+                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    {
+      cudaLaunchConfig_t q = {};
+      q.gridDim = dim3(16);
+      q.blockDim = dim3(kClThreads);
+      q.dynamicSmemBytes = 0;
+      cudaLaunchAttribute a[1];
+      a[0].id = cudaLaunchAttributeClusterDimension;
+      a[0].val.clusterDim.x = 16;
+      a[0].val.clusterDim.y = 1;
+      a[0].val.clusterDim.z = 1;
+      q.attrs = a;
+      q.numAttrs = 1;
+      int nclu = 0;
+      if (cudaOccupancyMaxActiveClusters(
+              &nclu, k_big_panel_cl<T, kClThreads, kClRowsG, 16, false, true>, &q) !=
+          cudaSuccess)
+        nclu = 0;
+      cudaGetLastError();
+      cl16_ok<T>() = nclu > 0;
+    }
     attr_set = true;
   }
   FCUDA(cudaMemsetAsync(d.counters, 0, 2 * sizeof(unsigned long long), s));
@@ -2658,12 +2734,37 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
       // panels; mode 2: the one-CTA panel's widths); its shared memory
       // holds NB columns of W for kClSlack rows more than the largest
       // static front
-      const bool use_cl = h.panel_mode != 1 && fm >= h.cl_min_rows &&
+      const bool use_cl = (h.panel_mode == 0 || h.panel_mode == 2) && fm >= h.cl_min_rows &&
                           fm + kClSlack <= kClMaxRows;
       const int cl_rule = h.panel_mode == 2 ? 1 : 0;
       const int cl_smem =
           use_cl ? 2 * NB * cl_local_rows<kClCS>((int)fm + kClSlack) * (int)sizeof(T) : 0;
-      const bool use_sw = !use_cl && fm <= (long long)kSwThreads * kSwRows;
+      // past shared memory: the cluster panel with its W and L rows in a
+      // global scratch region (clusters of 8, or 16 for the largest fronts;
+      // mode 3, a test mode: clusters of 16 on every level they can take,
+      // bit-identical to mode 0)
+      const long long gmax = cl16_ok<T>() ? kClMaxRowsG16 : kClMaxRowsG8;
+      const bool force16 = h.panel_mode == 3 && cl16_ok<T>();
+      const bool use_clg = ((h.panel_mode == 0 && !use_cl && fm + kClSlack > kClMaxRows) ||
+                            force16) &&
+                           fm >= h.cl_min_rows && fm + kClSlack <= gmax;
+      const bool g16 = use_clg && (force16 || fm + kClSlack > kClMaxRowsG8);
+      long long g_stride = 0;
+      if (use_clg) {
+        const int gcs = g16 ? 16 : 8;
+        const long long glld = g16 ? cl_local_rows<16>((int)fm + kClSlack)
+                                   : cl_local_rows<8>((int)fm + kClSlack);
+        g_stride = 2ll * NB * glld;
+        const size_t need = (size_t)B * gcs * (size_t)g_stride * sizeof(T);
+        if (need > h.cl_scratch_bytes) {
+          if (h.cl_scratch) FCUDA(cudaFree(h.cl_scratch));
+          h.cl_scratch = nullptr;
+          h.cl_scratch_bytes = 0;
+          FCUDA(cudaMalloc(&h.cl_scratch, need));
+          h.cl_scratch_bytes = need;
+        }
+      }
+      const bool use_sw = !use_cl && !use_clg && fm <= (long long)kSwThreads * kSwRows;
       const int sw_smem = kSwSmemBytes;
       // panels a front of big_max_fs candidates needs without delays: each
       // takes nbe - 1 pivots, nbe growing as the remaining rows shrink
@@ -2689,7 +2790,19 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
           if (trace) cudaEventRecord(te[0], s);
           if (use_cl) {
             const int rc = launch_panel_cl<T>(B, cl_smem, s, d, nodes, h.ustab,
-                                              h.pivot_tol, cl_rule, dbg_l);
+                                              h.pivot_tol, cl_rule, (int)fm + kClSlack,
+                                              dbg_l);
+            if (rc) return rc;
+          } else if (use_clg) {
+            T* scr = reinterpret_cast<T*>(h.cl_scratch);
+            const int fr = (int)fm + kClSlack;
+            const int rc =
+                g16 ? launch_panel_cl<T, kClRowsG, 16, true>(B, 0, s, d, nodes, h.ustab,
+                                                             h.pivot_tol, 0, fr, dbg_l, scr,
+                                                             g_stride)
+                    : launch_panel_cl<T, kClRowsG, 8, true>(B, 0, s, d, nodes, h.ustab,
+                                                            h.pivot_tol, 0, fr, dbg_l, scr,
+                                                            g_stride);
             if (rc) return rc;
           } else if (use_sw) {
             FCUDA(launch_pdl(k_big_panel_sw<T, kSwThreads, kSwRows>, dim3(B),

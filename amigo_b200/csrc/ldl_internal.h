@@ -124,6 +124,9 @@ struct LdlHandle {
   // with the one-CTA panel's widths
   int panel_mode = 0;
   int cl_min_rows = 768;
+  // global scratch of the cluster panel for fronts past shared memory
+  void* cl_scratch = nullptr;
+  size_t cl_scratch_bytes = 0;
   long long wide_entries = 1 << 22;
   // front storage / arithmetic of the next factorization (64: FP64, 32:
   // FP32 fronts for mixed precision) and of the last one

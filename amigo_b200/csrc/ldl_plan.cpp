@@ -248,10 +248,12 @@ void free_plan(LdlHandle& h) {
                   d.scratch_int, d.f, d.npiv, d.ndel, d.ndin,
                   d.foff, d.ioff, d.inertia, d.node_prob, d.status,
                   d.counters, d.fpool,
-                  d.ipool, h.ubuf, h.uoff, h.sv_nodes, h.sv_state};
+                  d.ipool, h.ubuf, h.uoff, h.sv_nodes, h.sv_state, h.cl_scratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   d = DevicePlan();
+  h.cl_scratch = nullptr;
+  h.cl_scratch_bytes = 0;
   h.ubuf = nullptr;
   h.uoff = nullptr;
   h.sv_nodes = nullptr;

@@ -259,9 +259,11 @@ class SparseLDL:
 
     def set_panel_mode(self, mode, min_rows=0):
         """Large-front panels: 0 (default) a thread-block cluster of 8 CTAs
-        per front on levels whose largest front has >= min_rows rows, 1 one
-        CTA per front, 2 cluster panels with the one-CTA widths (identical
-        results to mode 1)."""
+        per front on levels whose largest front has >= min_rows rows (fronts
+        past shared memory with W and L in global scratch, on clusters of 8
+        or 16), 1 one CTA per front, 2 cluster panels with the one-CTA
+        widths (identical results to mode 1), 3 the global-scratch form on
+        clusters of 16 wherever it applies (identical results to mode 0)."""
         _lib.call("ab_ldl_set_panel_mode", self._h, int(mode), int(min_rows))
 
     def set_wide_threshold(self, entries):

@@ -138,10 +138,15 @@ int ab_ldl_set_cluster_threshold(ab_ldl_t h, long long entries);
 /* Large-front panel knob.  mode 0 (default): levels whose largest front
  * has at least min_rows rows (default 768) factor their panels on one
  * thread-block cluster of 8 CTAs per front, NB = 32 columns a panel;
+ * fronts past what shared memory holds (> 3,008 rows) keep W and L in a
+ * global scratch region, on clusters of 8 CTAs to 16,320 rows and of 16
+ * (where the device schedules them) to 32,704;
  * mode 1: one CTA per front for every level; mode 2: cluster panels with
  * the one-CTA panel's widths, whose results are the one-CTA panel's bit
- * for bit (a test mode).  min_rows <= 0 keeps the current value.  No
- * reference counterpart (the reference factors each front on one thread). */
+ * for bit (a test mode); mode 3: the global-scratch form on clusters of 16
+ * for every level from min_rows, bit-identical to mode 0 (a test mode).
+ * min_rows <= 0 keeps the current value.  No reference counterpart (the
+ * reference factors each front on one thread). */
 int ab_ldl_set_panel_mode(ab_ldl_t h, int mode, int min_rows);
 
 /* The tensor-core Schur update on plain device arrays (column-major, FP32):

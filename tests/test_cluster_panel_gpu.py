@@ -5,7 +5,10 @@ per-node pivot and delay counts and the solution of a solve -- since every
 row's arithmetic, the reductions and the pivot decisions are the same.
 With full-width panels (mode 0, the default) the factor is a different
 rounding of the same algorithm: identical inertia, per-node pivot counts
-equal on >= 90% of the nodes, relative residual <= 1e-10."""
+equal on >= 90% of the nodes, relative residual <= 1e-10.  The
+global-scratch form (W and L in HBM/L2, clusters of 16 CTAs; panel mode 3)
+reproduces mode 0 bit for bit, and on 3D fronts past shared memory (mode 0
+switches to it by itself) it agrees with the one-CTA panel to rounding."""
 import os
 
 import numpy as np
@@ -93,3 +96,48 @@ def test_simp2d_64x32_fp32():
 
 def test_simp2d_128x64_default_threshold():
     check(simp_kkt(128, 64), 0)
+
+
+def check_global_form(K, min_rows, precision=64):
+    i0, p0, d0, x0, b = factor_solve(K, 0, min_rows, precision)
+    i3, p3, d3, x3, _ = factor_solve(K, 3, min_rows, precision)
+    assert i3 == i0
+    assert np.array_equal(p3, p0) and np.array_equal(d3, d0)
+    assert np.array_equal(x3, x0), np.abs(x3 - x0).max()
+
+
+def test_global_scratch_form_simp2d_128x64():
+    check_global_form(simp_kkt(128, 64), 1)
+
+
+def test_global_scratch_form_with_delays():
+    check_global_form(kkt_matrix(2500, 1200, 11), 1)
+
+
+def test_global_scratch_form_fp32():
+    check_global_form(simp_kkt(64, 32), 1, precision=32)
+
+
+def simp3d_kkt(nx, ny, nz, seed=3):
+    from amigo_b200.problems.simp3d import Simp3D
+    m = Simp3D(nx, ny, nz, seed=seed)
+    rp, ci = m.rowp, m.cols
+    rng = np.random.RandomState(seed)
+    n = m.n
+    # a quasi-definite KKT on the pattern: SPD primal block, negative
+    # diagonal on the multiplier rows
+    A = sp.csr_matrix((rng.randn(len(ci)) * 0.1, ci, rp), shape=(n, n))
+    A = (A + A.T) * 0.5
+    d = np.where(m.mult, -1.0, 1.0) * (1.0 + abs(A).sum(axis=1).A1)
+    K = sp.csr_matrix(A + sp.diags(d))
+    K.sort_indices()
+    return K
+
+
+def test_simp3d_large_fronts_global_form():
+    K = simp3d_kkt(20, 10, 10)
+    i1, p1, d1, x1, b = factor_solve(K, 1, 1)
+    i0, p0, d0, x0, _ = factor_solve(K, 0, 0)
+    assert i0 == i1
+    assert rel_residual(K, x0, b) <= 1e-10
+    assert rel_residual(K, x1, b) <= 1e-10
