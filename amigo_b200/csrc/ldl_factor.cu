@@ -165,13 +165,36 @@ __device__ void update_tile(T* F, int ld, const T* W, int ldw,
                             T* As, T* Bs) {
   const int tid = threadIdx.x;
   const int r0 = k + ti * kTile, c0 = k + tj * kTile;
-  for (int idx = tid; idx < kTile * kw; idx += NT) {
+  const int tr = tid % 16, tc = tid / 16;  // 16 x 16 threads, 4 x 4 outputs each
+  // C first, then A and B with all loads in flight before the shared stores
+  T cv[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int r = r0 + tr + 16 * a, c = c0 + tc + 16 * b;
+      cv[a][b] = (r < n && c < n && r >= c) ? F[r + (size_t)c * ld] : T(0);
+    }
+  constexpr int kSt = kTile * NB / NT;
+  T av[kSt], bv[kSt];
+#pragma unroll
+  for (int u = 0; u < kSt; u++) {
+    const int idx = tid + u * NT;
     const int rr = idx % kTile, jj = idx / kTile;
-    As[rr * TP + jj] = (r0 + rr < n) ? F[r0 + rr + (size_t)(kstart + jj) * ld] : T(0);
-    Bs[rr * TP + jj] = (c0 + rr < n) ? W[c0 + rr + (size_t)jj * ldw] : T(0);
+    const bool in = jj < kw;
+    av[u] = (in && r0 + rr < n) ? F[r0 + rr + (size_t)(kstart + jj) * ld] : T(0);
+    bv[u] = (in && c0 + rr < n) ? W[c0 + rr + (size_t)jj * ldw] : T(0);
+  }
+#pragma unroll
+  for (int u = 0; u < kSt; u++) {
+    const int idx = tid + u * NT;
+    const int rr = idx % kTile, jj = idx / kTile;
+    if (jj < kw) {
+      As[rr * TP + jj] = av[u];
+      Bs[rr * TP + jj] = bv[u];
+    }
   }
   __syncthreads();
-  const int tr = tid % 16, tc = tid / 16;  // 16 x 16 threads, 4 x 4 outputs each
   T acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; a++)
@@ -194,7 +217,7 @@ __device__ void update_tile(T* F, int ld, const T* W, int ldw,
 #pragma unroll
     for (int b = 0; b < 4; b++) {
       const int c = c0 + tc + 16 * b;
-      if (r < n && c < n && r >= c) F[r + (size_t)c * ld] -= acc[a][b];
+      if (r < n && c < n && r >= c) F[r + (size_t)c * ld] = cv[a][b] - acc[a][b];
     }
   }
   __syncthreads();
@@ -209,7 +232,6 @@ __device__ void update_tile(T* F, int ld, const T* W, int ldw,
 // mma.m8n8k4 .f64): a0 at (lane / 4, lane % 4), b0 at (k = lane % 4,
 // n = lane / 4), c0 / c1 at (lane / 4, 2 (lane % 4) + 0 / 1).
 constexpr int TPD = 36;
-constexpr int kTileSmemD = 2 * kTile * TPD;  // doubles
 
 __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a,
                                            double b) {
@@ -220,52 +242,6 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a,
       : "d"(a), "d"(b));
 }
 
-__device__ void update_tile_dmma(double* F, int ld, const double* W, int ldw,
-                                 int n, int k, int kstart, int kw, int ti,
-                                 int tj, double* As, double* Bs) {
-  const int tid = threadIdx.x;
-  const int r0 = k + ti * kTile, c0 = k + tj * kTile;
-  const int kp = (kw + 3) & ~3;
-  for (int idx = tid; idx < kTile * kp; idx += NT) {
-    const int rr = idx % kTile, jj = idx / kTile;
-    const bool in = jj < kw;
-    As[rr * TPD + jj] = (in && r0 + rr < n) ? F[r0 + rr + (size_t)(kstart + jj) * ld] : 0.0;
-    Bs[rr * TPD + jj] = (in && c0 + rr < n) ? W[c0 + rr + (size_t)jj * ldw] : 0.0;
-  }
-  __syncthreads();
-  const int lane = tid & 31, warp = tid >> 5;
-  const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;
-  const int g = lane >> 2, q = lane & 3;
-  double acc[4][2][2];
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-#pragma unroll
-    for (int b = 0; b < 2; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
-  for (int kk = 0; kk < kp; kk += 4) {
-    double af[4], bf[2];
-#pragma unroll
-    for (int a = 0; a < 4; a++) af[a] = As[(wr + 8 * a + g) * TPD + kk + q];
-#pragma unroll
-    for (int b = 0; b < 2; b++) bf[b] = Bs[(wc + 8 * b + g) * TPD + kk + q];
-#pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-      for (int b = 0; b < 2; b++) dmma_8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
-  }
-#pragma unroll
-  for (int a = 0; a < 4; a++) {
-    const int r = r0 + wr + 8 * a + g;
-#pragma unroll
-    for (int b = 0; b < 2; b++)
-#pragma unroll
-      for (int e = 0; e < 2; e++) {
-        const int c = c0 + wc + 8 * b + 2 * q + e;
-        if (r < n && c < n && r >= c) F[r + (size_t)c * ld] -= acc[a][b][e];
-      }
-  }
-  __syncthreads();
-}
-
 // Lower-triangle tile index t -> (ti, tj), ti >= tj.
 __device__ __forceinline__ void tile_coords(int t, int& ti, int& tj) {
   int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
@@ -273,6 +249,210 @@ __device__ __forceinline__ void tile_coords(int t, int& ti, int& tj) {
   while (i * (i + 1) / 2 > t) i--;
   ti = i;
   tj = t - i * (i + 1) / 2;
+}
+
+// 8-byte asynchronous global -> shared copy; a false predicate writes zeros
+// (source size 0, nothing read).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool pred) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+               "r"(pred ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Shared A and B tiles of the FP64 update, column-major (k-major) with a
+// column stride of APD = 68 doubles: the staging stores (consecutive rows
+// in consecutive lanes) and the fragment loads ((row g, k q) for lane
+// 4 g + q) both fall on distinct bank pairs within each half-warp.
+constexpr int APD = 68;
+constexpr int kUpdSmemD = 3 * NB * APD;  // doubles: B and two A buffers
+constexpr int kStD = kTile * NB / NT;    // staged entries of A (and of B) per thread
+static_assert(kTile * NB % NT == 0 && NT % kTile == 0, "staging split");
+
+// Tiles [tbeg, tend) of the trailing update C -= A * B^T, in column-major
+// order of the lower triangle of nt x nt tiles (column tj holds tiles
+// ti = tj .. nt - 1), on the FP64 tensor path (DMMA m8n8k4); A =
+// F[r0:r0+64, kstart:kstart+kw], B = W[c0:c0+64, 0:kw].  8 warps as 2 x 4,
+// each a 32 x 16 block of the 64 x 64 tile.  B is staged once per column;
+// the next tile's A is in flight to the other shared buffer (cp.async) and
+// its C entries to registers while the current tile's products run.  The
+// products accumulate from zero in k order and C - A B^T goes back (lower
+// triangle).  Offsets inside a tile are 32-bit and computed once; interior
+// tiles skip the bounds tests.
+__device__ void update_tiles_dmma(double* F, int ld, const double* W, int ldw,
+                                  int n, int k, int kstart, int kw, int nt, int tbeg,
+                                  int tend, double* smem) {
+  if (tbeg >= tend) return;
+  double* Bs = smem;
+  double* As = smem + NB * APD;
+  const int tid = threadIdx.x;
+  const int kp = (kw + 3) & ~3;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;
+  const int g = lane >> 2, q = lane & 3;
+  // accumulator (a, b, e) sits at row wr + 8 a + g, column wc + 8 b + 2 q + e
+  int coff[2][2];
+#pragma unroll
+  for (int b = 0; b < 2; b++)
+#pragma unroll
+    for (int e = 0; e < 2; e++) coff[b][e] = (wc + 8 * b + 2 * q + e) * ld;
+  const int rrow = wr + g;
+  // staging: this thread's row rr and columns jj0 + kJs u of A and B
+  constexpr int kJs = NT / kTile;
+  const int rr = tid % kTile, jj0 = tid / kTile;
+  const int aoff = rr + (kstart + jj0) * ld, boff = rr + jj0 * ldw;
+  auto load_c = [&](double (&cv)[4][2][2], int ti, int tj) {
+    const int r0 = k + ti * kTile, c0 = k + tj * kTile;
+    const double* Ct = F + r0 + (size_t)c0 * ld;
+    if (ti != tj && r0 + kTile <= n) {
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+          for (int e = 0; e < 2; e++) cv[a][b][e] = Ct[rrow + 8 * a + coff[b][e]];
+    } else {
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int r = r0 + rrow + 8 * a;
+#pragma unroll
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            const int c = c0 + wc + 8 * b + 2 * q + e;
+            cv[a][b][e] = (r < n && c < n && r >= c) ? Ct[rrow + 8 * a + coff[b][e]] : 0.0;
+          }
+      }
+    }
+  };
+  auto stage_a = [&](double* dst, int ti) {
+    const int r0 = k + ti * kTile;
+    const bool ra = r0 + rr < n;
+    const double* Fa = F + r0;
+#pragma unroll
+    for (int u = 0; u < kStD; u++) {
+      const int jj = jj0 + kJs * u;
+      if (jj < kp) {
+        const bool p = ra && jj < kw;
+        cp_async8(dst + jj * APD + rr, p ? Fa + aoff + kJs * u * ld : F, p);
+      }
+    }
+    cp_async_commit();
+  };
+  auto stage_b = [&](int tj) {
+    const int c0 = k + tj * kTile;
+    const bool rb = c0 + rr < n;
+    const double* Wb = W + c0;
+    double bv[kStD];
+#pragma unroll
+    for (int u = 0; u < kStD; u++)
+      bv[u] = (rb && jj0 + kJs * u < kw) ? Wb[boff + kJs * u * ldw] : 0.0;
+#pragma unroll
+    for (int u = 0; u < kStD; u++)
+      if (jj0 + kJs * u < kp) Bs[(jj0 + kJs * u) * APD + rr] = bv[u];
+  };
+  // (tj, ti) of tile tbeg: the largest tj whose column starts at or before it
+  int tj, ti;
+  {
+    const double b2 = 2.0 * nt + 1.0;
+    int c = (int)((b2 - sqrt(b2 * b2 - 8.0 * tbeg)) * 0.5);
+    auto start = [&](int cc) { return cc * nt - cc * (cc - 1) / 2; };
+    while (c > 0 && start(c) > tbeg) c--;
+    while (c + 1 < nt && start(c + 1) <= tbeg) c++;
+    tj = c;
+    ti = tj + (tbeg - start(c));
+  }
+  stage_b(tj);
+  stage_a(As, ti);
+  double cv[4][2][2];
+  load_c(cv, ti, tj);
+  int buf = 0;
+  for (int t = tbeg;; t++) {
+    cp_async_wait_all();
+    __syncthreads();  // A[buf] and B are in place; nobody reads A[buf ^ 1]
+    const bool more = t + 1 < tend;
+    int tin = ti + 1, tjn = tj;
+    if (tin == nt) {
+      tjn = tj + 1;
+      tin = tjn;
+    }
+    double cvn[4][2][2];
+    if (more) {
+      if (tjn == tj) stage_a(As + (buf ^ 1) * NB * APD, tin);
+      load_c(cvn, tin, tjn);
+    }
+    const double* A = As + buf * NB * APD;
+    double acc[4][2][2];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 2; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < NB; kk += 4) {
+      if (kk < kp) {
+        double af[4], bf[2];
+#pragma unroll
+        for (int a = 0; a < 4; a++) af[a] = A[(kk + q) * APD + rrow + 8 * a];
+#pragma unroll
+        for (int b = 0; b < 2; b++) bf[b] = Bs[(kk + q) * APD + wc + 8 * b + g];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int b = 0; b < 2; b++) dmma_8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+      }
+    }
+    {
+      const int r0 = k + ti * kTile, c0 = k + tj * kTile;
+      double* Ct = F + r0 + (size_t)c0 * ld;
+      if (ti != tj && r0 + kTile <= n) {
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int e = 0; e < 2; e++)
+              Ct[rrow + 8 * a + coff[b][e]] = cv[a][b][e] - acc[a][b][e];
+      } else {
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+          const int r = r0 + rrow + 8 * a;
+#pragma unroll
+          for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+              const int c = c0 + wc + 8 * b + 2 * q + e;
+              if (r < n && c < n && r >= c)
+                Ct[rrow + 8 * a + coff[b][e]] = cv[a][b][e] - acc[a][b][e];
+            }
+        }
+      }
+    }
+    if (!more) break;
+    if (tjn != tj) {
+      // a new column: its B, and the next A, after every warp is done
+      // with the current ones
+      __syncthreads();
+      stage_b(tjn);
+      stage_a(As + (buf ^ 1) * NB * APD, tin);
+    }
+    ti = tin;
+    tj = tjn;
+    buf ^= 1;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 2; b++) {
+        cv[a][b][0] = cvn[a][b][0];
+        cv[a][b][1] = cvn[a][b][1];
+      }
+  }
+  cp_async_wait_all();
 }
 
 // Column imax as the pivot search sees it: the largest |entry| off its
@@ -2457,7 +2637,7 @@ k_big_panel_cl(DevicePlan d, const int* __restrict__ nodes, double ustab,
 }
 
 template <class T>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 2)
 k_big_update(DevicePlan d, const int* __restrict__ nodes) {
   pdl_enter();
   extern __shared__ double tiles_raw[];
@@ -2474,15 +2654,18 @@ k_big_update(DevicePlan d, const int* __restrict__ nodes) {
   const T* W = F + (size_t)f * f;
   const int nt = (m + kTile - 1) / kTile;
   const int ntiles = nt * (nt + 1) / 2;
-  for (int t = blockIdx.y; t < ntiles; t += gridDim.y) {
-    int ti, tj;
-    tile_coords(t, ti, tj);
-    if constexpr (sizeof(T) == 8)
-      update_tile_dmma(F, f, W, f, f, k, kstart, kw, ti, tj, tiles,
-                       tiles + kTile * TPD);
-    else
-      update_tile(F, f, W, f, f, k, kstart, kw, ti, tj, tiles,
-                  tiles + kTile * TP);
+  if constexpr (sizeof(T) == 8) {
+    // a contiguous run of tiles per CTA (column-major), so that B is
+    // staged once per column
+    const int per = (ntiles + (int)gridDim.y - 1) / (int)gridDim.y;
+    const int tb = (int)blockIdx.y * per;
+    update_tiles_dmma(F, f, W, f, f, k, kstart, kw, nt, tb, min(ntiles, tb + per), tiles);
+  } else {
+    for (int t = blockIdx.y; t < ntiles; t += gridDim.y) {
+      int ti, tj;
+      tile_coords(t, ti, tj);
+      update_tile(F, f, W, f, f, k, kstart, kw, ti, tj, tiles, tiles + kTile * TP);
+    }
   }
 }
 
@@ -2570,6 +2753,19 @@ static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block,
   return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
+// Streaming multiprocessors of the current device.
+static int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    n = v;
+  }
+  return n;
+}
+
 // Whether clusters of 16 CTAs of the global-scratch panel can be scheduled
 // on this device (set once, with the kernels' attributes).
 template <class T>
@@ -2620,7 +2816,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                                kMaxDynSmem));
     FCUDA(cudaFuncSetAttribute(k_big_update<T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (sizeof(T) == 8 ? kTileSmemD : kTileSmem) * sizeof(T)));
+                               (sizeof(T) == 8 ? kUpdSmemD : kTileSmem) * sizeof(T)));
     FCUDA(cudaFuncSetAttribute(k_big_panel<T, kPanelThreads>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kPanelCacheBytes));
@@ -2824,7 +3020,7 @@ static int launch_factor(LdlHandle& h, const double* d_vals, cudaStream_t s) {
                 d, nodes); ab::count_launch(); }
           } else {
             FCUDA(launch_pdl(k_big_update<T>, dim3(B, std::max(gu, 1)), dim3(NT),
-                             (size_t)((sizeof(T) == 8 ? kTileSmemD : kTileSmem) * sizeof(T)),
+                             (size_t)((sizeof(T) == 8 ? kUpdSmemD : kTileSmem) * sizeof(T)),
                              s, d, nodes));
             ab::count_launch();
           }

@@ -66,6 +66,9 @@ def parse():
                     help="folder for the nvidia-smi clock samples of the timed region")
     ap.add_argument("--no-3d", action="store_true",
                     help="skip the 3D SIMP 48x24x24 factorization")
+    ap.add_argument("--simp3d", default="48,24,24",
+                    help="mesh of the 3D SIMP factorization, NX,NY,NZ (a smaller "
+                         "mesh for profiling)")
     return ap.parse_args()
 
 
@@ -345,7 +348,8 @@ def run_ours(args, rank, world, local):
         # one factorization per GPU: every replica runs it on its own device
         del core, flush
         torch.cuda.empty_cache()
-        out["simp3d_factor"] = simp3d_bench(device)
+        out["simp3d_factor"] = simp3d_bench(
+            device, dims=tuple(int(v) for v in args.simp3d.split(",")))
         torch.cuda.empty_cache()
     if not args.no_ipm_solve:
         out["ipm_solve"] = ipm_solve_bench(device, args.solves)
@@ -400,7 +404,7 @@ def serve_bench(device, n_requests, batch_capacity, rank=0, world=1):
     return summ
 
 
-def simp3d_bench(device, reps=2):
+def simp3d_bench(device, reps=2, dims=(48, 24, 24)):
     """The 3D SIMP cantilever 48x24x24 KKT (n = 272,650, nnz = 4.1e7; AMD;
     largest front ~25k): one FP64 factorization and one solve per rep,
     CUDA events, after one warm-up factorization.  Diagonal: 1e-2 + U(0, 1)
@@ -410,7 +414,7 @@ def simp3d_bench(device, reps=2):
     from amigo_b200 import linalg
     from amigo_b200.problems.simp3d import Simp3D
     t0 = time.perf_counter()
-    m = Simp3D(48, 24, 24)
+    m = Simp3D(*dims)
     dm = m.device_model(device)
     K = linalg.CSRMat(m.n, m.n, m.rowp, m.cols, device=device)
     ldl = linalg.SparseLDL(K, order=linalg.OrderingType.AMD)
@@ -497,8 +501,8 @@ def simp3d_bench(device, reps=2):
                      "precision IPM drivers refactor in FP64 when the inertia "
                      "differs from the expected one or refinement stalls "
                      "above 1e-10"}
-    return {"workload": "3D SIMP cantilever 48x24x24 full-space KKT, FP64 "
-                        "factor + solve",
+    return {"workload": "3D SIMP cantilever %dx%dx%d full-space KKT, FP64 "
+                        "factor + solve" % tuple(dims),
             "n": int(m.n), "nnz": int(m.nnz), "flops": st["flops"],
             "factor_s": round(fac_s, 4), "solve_s": round(float(np.median(sol)) * 1e-3, 4),
             "tflops": round(st["flops"] / fac_s / 1e12, 3),
