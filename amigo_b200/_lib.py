@@ -75,8 +75,47 @@ class CartPoleStruct(ctypes.Structure):
                 + [("nbc", _i), ("ninst", _i), ("inst_iv", _vp)])
 
 
+class BctlStruct(ctypes.Structure):
+    """Mirror of ab_bctl (include/amigo_b200.h): device arrays of ninst."""
+    DOUBLES = ("mu", "nu", "dw", "dc", "dwf", "dcf", "dw_last", "alpha", "az",
+               "phi0", "dphi", "ratio", "ratio_old", "nrm", "e0")
+    INTS = ("live", "pending", "search", "on", "its", "n_ic", "retire",
+            "np_each", "nc_each", "n_each")
+    _fields_ = ([("ninst", _i)] + [(k, _vp) for k in DOUBLES]
+                + [(k, _vp) for k in INTS] + [("flags", _vp)])
+
+
+class BctlOpts(ctypes.Structure):
+    """Mirror of ab_bctl_opts."""
+    NAMES = ("tol", "mu_min", "kappa_eps", "kappa_mu", "theta_mu", "dw_first",
+             "dw_min", "dw_max", "kw_plus_first", "kw_plus", "kw_minus", "dc",
+             "kappa_c", "armijo")
+    _fields_ = [(k, _d) for k in NAMES] + [("max_iter", _i)]
+
+
+BCTL_RETIRED, BCTL_LIVE, BCTL_IC_PENDING, BCTL_REFINING, BCTL_STALLED, \
+    BCTL_SEARCHING = range(6)
+BCTL_NFLAGS = 8
+
+_BC = ctypes.POINTER(BctlStruct)
+_BO = ctypes.POINTER(BctlOpts)
+
 # name -> (restype, argtypes)
 _SIGS = {
+    "ab_bctl_clear_flags": (_i, [_BC, _vp]),
+    "ab_bctl_converge_barrier": (_i, [_BC, _BO, _vp, _vp]),
+    "ab_bctl_ic_begin": (_i, [_BC, _vp]),
+    "ab_bctl_shift_diag": (_i, [_BC, _i, _vp, _vp, _vp, _vp, _vp]),
+    "ab_bctl_ic_step": (_i, [_BC, _BO, _vp, _vp]),
+    "ab_bctl_ic_end": (_i, [_BC, _vp]),
+    "ab_bctl_refine_init": (_i, [_BC, _vp, _vp]),
+    "ab_bctl_refine_step": (_i, [_BC, _vp, _i, _vp]),
+    "ab_bctl_refine_stalled": (_i, [_BC, _vp]),
+    "ab_bctl_mask_update": (_i, [_BC, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "ab_bctl_ls_begin": (_i, [_BC, _vp, _vp, _vp]),
+    "ab_bctl_ls_test": (_i, [_BC, _BO, _vp, _vp, _vp]),
+    "ab_bctl_end": (_i, [_BC, _vp]),
+    "ab_ldl_inertia_device": (_i, [_vp, ctypes.POINTER(_vp)]),
     "ab_ldl_create": (_i, [_i, _ip, _ip, _i, _i, _d, _d, _d, ctypes.POINTER(_vp)]),
     "ab_ldl_analyze": (_i, [_i, _ip, _ip, _i, ctypes.POINTER(_vp)]),
     "ab_ldl_destroy": (_i, [_vp]),

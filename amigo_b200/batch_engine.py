@@ -8,8 +8,13 @@ instances -- the block-diagonal multifrontal LDL^T of
 `linalg.BatchedSparseLDL`, the per-instance IPM kernels of
 `ipm.BatchedInteriorPointOptimizer` -- while every decision (barrier
 parameter, inertia correction, refinement stopping, step lengths, line
-search) is taken per instance.  Because no computation mixes instances, an
-instance's iterates do not depend on which other instances share its batch.
+search) is taken per instance, on the device: the decision kernels of
+csrc/batch_ctrl.cu (ab_bctl_*) read the per-instance reductions, inertia
+and objectives where the other kernels left them, so an iteration moves no
+per-instance array to the host; the host reads one flags word at the end of
+each loop (inertia correction, refinement, line search) and the retired
+instances' results.  Because no computation mixes instances, an instance's
+iterates do not depend on which other instances share its batch.
 
 Instances are admitted (`admit`) and retired (converged or out of
 iterations) at iteration boundaries.  Admission rebuilds the batch: the
@@ -25,6 +30,9 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._lib import (BCTL_IC_PENDING, BCTL_LIVE, BCTL_NFLAGS, BCTL_REFINING,
+                   BCTL_RETIRED, BCTL_SEARCHING, BCTL_STALLED, BctlOpts,
+                   BctlStruct)
 from .linalg import OrderingType, _stream_ptr
 
 
@@ -79,6 +87,9 @@ class BatchEngine:
         if not self._built:
             return
         st, B, poff = self.st, self.B, self.poff
+        mu, nu = self.cd["mu"].cpu().numpy(), self.cd["nu"].cpu().numpy()
+        dw_last = self.cd["dw_last"].cpu().numpy()
+        n_ic = self.ci["n_ic"].cpu().numpy()
         for k, r in enumerate(self.insts):
             if r.done:
                 continue
@@ -87,8 +98,8 @@ class BatchEngine:
             r.state = (st.x[a:b].clone(), st.zl[p0:p1].clone(),
                        st.zu[p0:p1].clone(), st.sl[p0:p1].clone(),
                        st.su[p0:p1].clone())
-            r.mu, r.nu = float(self.mu[k]), float(self.nu[k])
-            r.dw_last, r.n_ic = float(self.dw_last[k]), int(self.n_ic[k])
+            r.mu, r.nu = float(mu[k]), float(nu[k])
+            r.dw_last, r.n_ic = float(dw_last[k]), int(n_ic[k])
 
     def _build(self):
         from .ipm import BatchedInteriorPointOptimizer
@@ -154,40 +165,67 @@ class BatchEngine:
             st.su[p0:p1].copy_(r.state[4])
             r.state = None
         self.st = st
-        self.mu = np.array([r.mu for r in self.insts])
-        self.nu = np.array([r.nu for r in self.insts])
-        self.dw_last = np.array([r.dw_last for r in self.insts])
-        self.n_ic = np.array([r.n_ic for r in self.insts], np.int64)
-        opt.set_barrier_params(self.mu)
+        opt.set_barrier_params(np.array([r.mu for r in self.insts]))
+        # the per-instance decision state on the device (ab_bctl); its mu is
+        # the barrier array the batched IPM kernels read
+        t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt).to(dev)
+        self.cd = {k: torch.zeros(K, **f64) for k in BctlStruct.DOUBLES}
+        self.cd["mu"] = opt.mu
+        self.cd["nu"] = t([r.nu for r in self.insts], torch.float64)
+        self.cd["dw_last"] = t([r.dw_last for r in self.insts], torch.float64)
+        i32 = dict(dtype=torch.int32, device=dev)
+        self.ci = {k: torch.zeros(K, **i32) for k in BctlStruct.INTS}
+        self.ci["live"].fill_(1)
+        self.ci["its"] = t([r.it for r in self.insts], torch.int32)
+        self.ci["n_ic"] = t([r.n_ic for r in self.insts], torch.int32)
+        self.ci["np_each"] = t(opt.np_each, torch.int32)
+        self.ci["nc_each"] = t(opt.nc_each, torch.int32)
+        self.ci["n_each"] = t(self.ldl.n_each, torch.int32)
+        self.flags_d = torch.zeros(BCTL_NFLAGS, **i32)
+        self.flags_h = torch.zeros(BCTL_NFLAGS, dtype=torch.int32).pin_memory()
+        self.ctl = BctlStruct(K, *([self.cd[k].data_ptr() for k in BctlStruct.DOUBLES]
+                                   + [self.ci[k].data_ptr() for k in BctlStruct.INTS]
+                                   + [self.flags_d.data_ptr()]))
+        o = self.o
+        self.copts = BctlOpts(*([float(o[k]) for k in BctlOpts.NAMES]
+                                + [int(o["max_iter"])]))
+        self.obj_t = torch.zeros(K, **f64)
+        self.vinst32 = opt.vinst
+        self.pinst32 = opt.pinst
         self.stream = _stream_ptr(dev)
         self._built = True
 
     # -- helpers -----------------------------------------------------------
-    def _dev_vec(self, a, dtype=torch.float64):
-        return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).to(self.dev)
+    def _objective(self, v, out=None):
+        out = self.obj if out is None else out
+        self.dm.objective(v.x, out)
+        return out
 
-    def _objective(self, v):
-        self.dm.objective(v.x, self.obj)
-        return self.obj.cpu().numpy()
+    def _ctl(self, name, *args):
+        _lib.call("ab_bctl_" + name, ctypes.byref(self.ctl), *args, self.stream)
 
-    def _direction(self, st, steps, live):
-        """px = K^-1 res with per-instance 8-block refinement; returns each
-        instance's last residual ratio."""
-        opt, K = self.opt, self.K
+    def _flags(self):
+        """The decision flags (one small copy and a stream synchronisation)."""
+        self.flags_h.copy_(self.flags_d, non_blocking=True)
+        torch.cuda.current_stream(self.dev).synchronize()
+        return self.flags_h.tolist()
+
+    def _direction(self, st, steps):
+        """px = K^-1 res with per-instance 8-block refinement; the stopping
+        rule runs on the device (ab_bctl_refine_step), the host only learns
+        whether any instance still refines."""
+        opt = self.opt
         P = ctypes.byref(opt._p)
         opt.residual(st, self.g, self.res)
         self.px.copy_(self.res)
         self.ldl.solve_device(self.px)
-        ratio = np.zeros(K)
         if not steps:
-            return ratio
+            return
         S = ctypes.byref(opt._state(st))
         _lib.call("ab_ipm_refine_init_seg", P, S, self.g.data_ptr(),
                   self.res.data_ptr(), self.px.data_ptr(), self.izl.data_ptr(),
                   self.izu.data_ptr(), self.seg.data_ptr(), self.stream)
-        nrm_rhs = self.seg[:K].cpu().numpy()
-        ratio_old = np.full(K, 1e30)
-        on = live.copy()
+        self._ctl("refine_init", self.seg.data_ptr())
         for step in range(steps + 1):
             self.H.mult(self.px, self.kpx)
             _lib.call("ab_ipm_refine_residual_seg", P, S, self.g.data_ptr(),
@@ -195,34 +233,39 @@ class BatchEngine:
                       self.izl.data_ptr(), self.izu.data_ptr(), self.ecnd.data_ptr(),
                       self.ezl.data_ptr(), self.ezu.data_ptr(), self.seg.data_ptr(),
                       self.stream)
-            ns = self.seg.view(K, 2).cpu().numpy()
-            r = ns[:, 0] / (np.minimum(ns[:, 1], 1e6 * nrm_rhs) + nrm_rhs)
-            ratio = np.where(on, r, ratio)
-            if step >= 1:
-                on &= ~((r < 1e-10) | (r > 0.999999999 * ratio_old))
-            if not on.any():
+            self._ctl("clear_flags")
+            self._ctl("refine_step", self.seg.data_ptr(), step)
+            # at step 0 every live instance refines (the rule stops from
+            # step 1), so only later steps need the flags
+            if step >= 1 and not self._flags()[BCTL_REFINING]:
                 break
-            ratio_old = np.where(on, r, ratio_old)
             self.corr.copy_(self.ecnd)
             self.ldl.solve_device(self.corr)
-            self.act.copy_(self._dev_vec(on.astype(np.int32), torch.int32))
-            _lib.call("ab_ipm_refine_update_seg", P, S, self.act.data_ptr(),
+            _lib.call("ab_ipm_refine_update_seg", P, S, self.ci["on"].data_ptr(),
                       self.corr.data_ptr(), self.ezl.data_ptr(), self.ezu.data_ptr(),
                       self.px.data_ptr(), self.izl.data_ptr(), self.izu.data_ptr(),
                       self.stream)
-        return ratio
 
-    def _retire(self, k, converged, kkt, objective):
-        r = self.insts[k]
+    def _retire_marked(self):
+        """Results of the instances ab_bctl_converge_barrier retired."""
+        retire = self.ci["retire"].cpu().numpy()
+        e0 = self.cd["e0"].cpu().numpy()
+        n_ic = self.ci["n_ic"].cpu().numpy()
+        objv = self._objective(self.st).cpu().numpy()
         B = self.B
-        a, b = int(B.var_off[k]), int(B.var_off[k + 1])
-        r.done = True
-        r.result = dict(id=r.id, converged=bool(converged), iterations=int(r.it),
-                        objective=float(objective), kkt_error=float(kkt),
-                        inertia_corrections=int(self.n_ic[k]),
-                        x=self.st.x[a:b].cpu().numpy(),
-                        t_done=time.perf_counter())
-        return r.result
+        out = []
+        for k in np.nonzero(retire)[0]:
+            r = self.insts[k]
+            a, b = int(B.var_off[k]), int(B.var_off[k + 1])
+            r.done = True
+            r.n_ic = int(n_ic[k])
+            r.result = dict(id=r.id, converged=bool(retire[k] == 1), iterations=int(r.it),
+                            objective=float(objv[k]), kkt_error=float(e0[k]),
+                            inertia_corrections=int(n_ic[k]),
+                            x=self.st.x[a:b].cpu().numpy(),
+                            t_done=time.perf_counter())
+            out.append(r.result)
+        return out
 
     # -- one iteration -------------------------------------------------------
     def step(self, rebuild=None):
@@ -239,110 +282,75 @@ class BatchEngine:
         opt, dm, H, ldl = self.opt, self.dm, self.H, self.ldl
         st, upd, trial = self.st, self.upd, self.trial
         g, diag, dtot, primal = self.g, self.diag, self.dtot, self.primal
-        mu, nu, dw_last, n_ic = self.mu, self.nu, self.dw_last, self.n_ic
-        dev_vec = self._dev_vec
-        live = np.array([not r.done for r in self.insts])
-        its = np.array([r.it for r in self.insts])
-        finished = []
-        # convergence test (E_0 <= tol) or iteration limit, per instance
+        copts = ctypes.byref(self.copts)
+        # convergence test (E_0 <= tol) or iteration limit, then the
+        # monotone barrier update, per instance on the device
         dm.gradient(st.x, 1.0, g)
-        q = opt.seg_reduce(st, grad=g, zero_mu=True)
-        E0 = q[:, :3].max(axis=1)
-        conv = live & (E0 <= o["tol"])
-        out = live & ~conv & (its >= o["max_iter"])
-        if conv.any() or out.any():
-            objv = self._objective(st)
-            for k in np.nonzero(conv | out)[0]:
-                finished.append(self._retire(k, conv[k], E0[k], objv[k]))
-        live &= ~(conv | out)
-        if not live.any():
+        opt.seg_reduce_device(st, grad=g)
+        self._ctl("clear_flags")
+        self._ctl("converge_barrier", copts, opt._seg.data_ptr())
+        f = self._flags()
+        finished = self._retire_marked() if f[BCTL_RETIRED] else []
+        if not f[BCTL_LIVE]:
             return finished
-        # monotone barrier update
-        while True:
-            q = opt.seg_reduce(st, grad=g)
-            Emu = q[:, :3].max(axis=1)
-            dec = live & (Emu <= o["kappa_eps"] * mu) & (mu > o["mu_min"])
-            if not dec.any():
-                break
-            mu[dec] = np.maximum(o["mu_min"], np.minimum(o["kappa_mu"] * mu[dec],
-                                                         mu[dec] ** o["theta_mu"]))
-            opt.set_barrier_params(mu)
         # inertia-corrected factorization
         opt.compute_diagonal(st, diag)
-        dw, dc = np.zeros(K), np.zeros(K)
-        dwf, dcf = dw.copy(), dc.copy()     # values the factor was made with
-        pending = live.copy()
+        self._ctl("ic_begin")
         for attempt in range(41):
-            dwv, dcv = dev_vec(dwf)[self.vinst], dev_vec(dcf)[self.vinst]
-            torch.addcmul(diag, dwv, primal, out=dtot)
-            dtot.sub_(dcv * (1.0 - primal))
+            self._ctl("shift_diag", n, self.vinst32.data_ptr(), primal.data_ptr(),
+                      diag.data_ptr(), dtot.data_ptr())
             dm.hessian(st.x, 1.0, H.vals)
             H.add_diagonal(dtot)
             ldl.factor(H.vals)
-            inertia = np.array(ldl.get_inertia())
-            ok = (inertia[:, 0] == opt.np_each) & (inertia[:, 1] == opt.nc_each)
-            bad = pending & ~ok
-            if not bad.any():
+            self._ctl("clear_flags")
+            self._ctl("ic_step", copts, ldl.inertia_device())
+            if not self._flags()[BCTL_IC_PENDING]:
                 break
-            n_ic[bad] += 1
-            sing = bad & (inertia.sum(axis=1) < ldl.n_each) & (dc == 0.0)
-            dc[sing] = o["dc"] * mu[sing] ** o["kappa_c"]
-            first = bad & (dw == 0.0)
-            dw[first] = np.where(dw_last[first] == 0.0, o["dw_first"],
-                                 np.maximum(o["dw_min"], o["kw_minus"] * dw_last[first]))
-            grow = bad & ~first
-            dw[grow] *= np.where(dw_last[grow] == 0.0, o["kw_plus_first"], o["kw_plus"])
-            pending = bad & (dw <= o["dw_max"])
-            dwf[pending], dcf[pending] = dw[pending], dc[pending]
-            if not pending.any():
-                break
-        self.dw_last = np.where(live & (dw > 0.0), dw, dw_last)
+        self._ctl("ic_end")
         # Newton direction; a stalled refinement on FP32 fronts is redone on
         # an FP64 refactorization of the same matrices
         from .ipm_driver import DeviceBackend
         steps = o["refine_steps"]
         if self.precision == "fp32":
             steps = max(steps, DeviceBackend.mixed_refine_steps)
-        ratio = self._direction(st, steps, live)
-        if self.precision == "fp32" and np.any(live & (ratio > 1e-10)):
-            self.fallbacks += 1
-            ldl.set_precision("fp64")
-            dm.hessian(st.x, 1.0, H.vals)
-            H.add_diagonal(dtot)
-            ldl.factor(H.vals)
-            self._direction(st, steps, live)
-            ldl.set_precision("fp32")
+        self._direction(st, steps)
+        if self.precision == "fp32":
+            self._ctl("clear_flags")
+            self._ctl("refine_stalled")
+            if self._flags()[BCTL_STALLED]:
+                self.fallbacks += 1
+                ldl.set_precision("fp64")
+                dm.hessian(st.x, 1.0, H.vals)
+                H.add_diagonal(dtot)
+                ldl.factor(H.vals)
+                self._direction(st, steps)
+                ldl.set_precision("fp32")
         opt.compute_update(0.0, st, self.px, upd)
         # instances that have retired take no step
-        lv = dev_vec(live, torch.bool)
-        upd.x.copy_(torch.where(lv[self.vinst], upd.x, 0.0))
-        upd.duals.view(2, -1).copy_(torch.where(lv[self.pinst], upd.duals.view(2, -1), 0.0))
+        self._ctl("mask_update", n, opt.np_, self.vinst32.data_ptr(),
+                  self.pinst32.data_ptr(), upd.x.data_ptr(), upd.zl.data_ptr(),
+                  upd.zu.data_ptr())
         # fraction to the boundary, merit, line search
         self.xtmp.copy_(st.x)
         self.xtmp[self.mult_idx] = 0.0
         dm.gradient(self.xtmp, 1.0, self.gf)
-        q = opt.seg_reduce(st, grad=g, upd=upd, gf=self.gf, tau=-o["tau_min"])
-        ax, az = q[:, 5].copy(), q[:, 6].copy()
-        self.nu = nu = np.where(live, np.maximum(nu, 1.1 * q[:, 8]), nu)
-        theta0 = q[:, 3]
-        phi0 = self._objective(st) + q[:, 4] + nu * theta0
-        dphi = q[:, 7] - nu * theta0
-        alpha = np.where(live, ax, 0.0)
-        az_d = dev_vec(np.where(live, az, 0.0))
-        search = live.copy()
+        opt.seg_reduce_device(st, grad=g, upd=upd, gf=self.gf, tau=-o["tau_min"])
+        self._ctl("ls_begin", opt._seg.data_ptr(), self._objective(st).data_ptr())
         trial.copy(st)
+        alpha, az = self.cd["alpha"], self.cd["az"]
         for ls in range(o["max_ls"]):
-            opt.apply_step_seg(dev_vec(alpha), az_d, st, upd, trial)
+            opt.apply_step_seg(alpha, az, st, upd, trial)
             dm.gradient(trial.x, 1.0, self.gt)
-            qt = opt.seg_reduce(trial, grad=self.gt)
-            phi = self._objective(trial) + qt[:, 4] + nu * qt[:, 3]
-            accept = (phi <= phi0 + o["armijo"] * alpha * dphi) | ~np.isfinite(dphi)
-            search &= ~accept
-            if not search.any():
+            opt.seg_reduce_device(trial, grad=self.gt)
+            self._objective(trial, self.obj_t)
+            self._ctl("clear_flags")
+            self._ctl("ls_test", copts, opt._seg.data_ptr(), self.obj_t.data_ptr())
+            if not self._flags()[BCTL_SEARCHING]:
                 break
-            alpha = np.where(search, 0.5 * alpha, alpha)
         self.st, self.trial = trial, st
         opt.reset_bound_multipliers(0.0, o["kappa_sigma"], self.st)
-        for k in np.nonzero(live)[0]:
-            self.insts[k].it += 1
+        self._ctl("end")
+        for r in self.insts:
+            if not r.done:
+                r.it += 1
         return finished

@@ -28,11 +28,13 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 # Per-file extra flags.  The IPM vector kernels must not contract a*b+c
 # into fused multiply-adds, so their elementwise results match the CPU
 # reference bit for bit.
-EXTRA = {"ipm_kernels.cu": ["--fmad=false"], "ipm_scaling.cu": ["--fmad=false"]}
+EXTRA = {"ipm_kernels.cu": ["--fmad=false"], "ipm_scaling.cu": ["--fmad=false"],
+         "batch_ctrl.cu": ["--fmad=false"]}
 
 SOURCES = ["symbolic.cpp", "ldl_plan.cpp", "ldl_factor.cu", "ldl_solve.cu",
            "capi.cpp", "ipm_kernels.cu", "capi_ipm.cpp", "csr_kernels.cu",
-           "fem_simp.cu", "cartpole.cu", "tc_kernels.cu", "ipm_scaling.cu"]
+           "fem_simp.cu", "cartpole.cu", "tc_kernels.cu", "ipm_scaling.cu",
+           "batch_ctrl.cu"]
 
 
 def nvcc():

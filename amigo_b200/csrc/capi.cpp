@@ -249,6 +249,14 @@ int ab_ldl_factor(ab_ldl_t H, const double* d_vals, void* stream) {
   return ab::factor_numeric(H->h, d_vals, (cudaStream_t)stream);
 }
 
+int ab_ldl_inertia_device(ab_ldl_t H, const int** out) {
+  if (!H || !out) return AB_ERR_ARG;
+  if (!H->h.factored) return AB_ERR_NOT_FACTORED;
+  if (!H->h.has_plan) return AB_ERR_UNSUPPORTED;
+  *out = H->h.d.inertia;
+  return AB_OK;
+}
+
 int ab_ldl_batch_inertia(ab_ldl_t H, void* stream, int* npos, int* nneg) {
   if (!H || !npos || !nneg) return AB_ERR_ARG;
   if (!H->h.factored) return AB_ERR_NOT_FACTORED;

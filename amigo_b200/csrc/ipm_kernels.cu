@@ -610,8 +610,12 @@ __global__ void k_max2_final(int nblocks, const double* partial, double* out) {
 //   0 dual inf-norm, 1 primal inf-norm, 2 complementarity inf-norm
 //   (|gap z - mu_k|), 3 constraint violation 1-norm, 4 barrier log-sum,
 //   5 max primal step, 6 max dual step (fraction to the boundary, seeded
-//   at 1), 7 barrier directional derivative, 8 max |lam + dlam|.
-constexpr int kSegQ = 10;
+//   at 1), 7 barrier directional derivative, 8 max |lam + dlam|, 9 / 10 the
+//   largest / smallest gap product s z over the bounded entries (-/+inf
+//   when there are none): the complementarity inf-norm for any barrier
+//   parameter m is then max(0, q9 - m, m - q10), the same value the
+//   element-wise max of |s z - m| gives, because rounding is monotone.
+constexpr int kSegQ = 12;
 __global__ void k_seg_reduce(P p, S s, double tau, const double* grad,
                              const double* px, const double* dzl,
                              const double* dzu, const double* gf,
@@ -622,17 +626,23 @@ __global__ void k_seg_reduce(P p, S s, double tau, const double* grad,
   const double tk = tau < 0.0 ? fmax(-tau, 1.0 - mu) : tau;
   const int p0 = p.poff[k], p1 = p.poff[k + 1];
   const int c0 = p.coff[k], c1 = p.coff[k + 1];
-  double q[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, 0.0};
+  double q[11] = {0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, 0.0, -INFINITY, INFINITY};
   for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
     const int idx = p.pidx[i];
     const bool hl = finite_bound(p.lbx[i]), hu = finite_bound(p.ubx[i]);
     if (grad) q[0] = fmax(q[0], fabs(grad[idx] - s.zl[i] + s.zu[i]));
     if (hl) {
-      q[2] = fmax(q[2], fabs(s.sl[i] * s.zl[i] - mu));
+      const double g = s.sl[i] * s.zl[i];
+      q[2] = fmax(q[2], fabs(g - mu));
+      q[9] = fmax(q[9], g);
+      q[10] = fmin(q[10], g);
       if (s.sl[i] > 0) q[4] -= mu * log(s.sl[i]);
     }
     if (hu) {
-      q[2] = fmax(q[2], fabs(s.su[i] * s.zu[i] - mu));
+      const double g = s.su[i] * s.zu[i];
+      q[2] = fmax(q[2], fabs(g - mu));
+      q[9] = fmax(q[9], g);
+      q[10] = fmin(q[10], g);
       if (s.su[i] > 0) q[4] -= mu * log(s.su[i]);
     }
     if (px && dzl) {
@@ -662,26 +672,26 @@ __global__ void k_seg_reduce(P p, S s, double tau, const double* grad,
     }
     if (px && s.xlam) q[8] = fmax(q[8], fabs(s.xlam[idx] + px[idx]));
   }
-  __shared__ double sh[9][RT / 32];
+  __shared__ double sh[11][RT / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int t = 0; t < 9; t++) {
+  for (int t = 0; t < 11; t++) {
     double v = q[t];
     for (int o = 16; o > 0; o >>= 1) {
       const double w = __shfl_down_sync(0xffffffffu, v, o);
-      if (t == 5 || t == 6) v = fmin(v, w);
+      if (t == 5 || t == 6 || t == 10) v = fmin(v, w);
       else if (t == 3 || t == 4 || t == 7) v += w;
       else v = fmax(v, w);
     }
     if (lane == 0) sh[t][warp] = v;
   }
   __syncthreads();
-  if (threadIdx.x < 9) {
+  if (threadIdx.x < 11) {
     const int t = threadIdx.x;
     double v = sh[t][0];
     for (int w = 1; w < RT / 32; w++) {
       const double x = sh[t][w];
-      if (t == 5 || t == 6) v = fmin(v, x);
+      if (t == 5 || t == 6 || t == 10) v = fmin(v, x);
       else if (t == 3 || t == 4 || t == 7) v += x;
       else v = fmax(v, x);
     }

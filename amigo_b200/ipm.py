@@ -447,7 +447,7 @@ class BatchedInteriorPointOptimizer(InteriorPointOptimizer):
         f64 = dict(dtype=torch.float64, device=self.device)
         self.mu = torch.zeros(self.ninst, **f64)
         self.mu0 = torch.zeros(self.ninst, **f64)
-        self._seg = torch.zeros(self.ninst * 10, **f64)
+        self._seg = torch.zeros(self.ninst * 12, **f64)
         self._ir = torch.zeros(self.ninst * 2, **f64)
         self._p = self._mk(self.mu)
         self._pz = self._mk(self.mu0)
@@ -471,12 +471,10 @@ class BatchedInteriorPointOptimizer(InteriorPointOptimizer):
         self._c("ab_ipm_residual", ctypes.byref(self._state(vars)), 0.0,
                 _dev(grad).data_ptr(), r.data_ptr(), None, self._s())
 
-    def seg_reduce(self, vars, grad=None, upd=None, gf=None, tau=0.0,
-                   zero_mu=False):
-        """Per-instance quantities as a (ninst, 10) host array (see
-        ab_ipm_seg_reduce): 0 dual, 1 primal, 2 comp inf-norms, 3 constraint
-        violation 1-norm, 4 barrier log-sum, 5/6 primal/dual step,
-        7 barrier directional derivative, 8 max |lam + dlam|."""
+    def seg_reduce_device(self, vars, grad=None, upd=None, gf=None, tau=0.0,
+                          zero_mu=False):
+        """seg_reduce into the device array `_seg` ((ninst, 12) doubles),
+        with no copy to the host."""
         p = self._pz if zero_mu else self._p
         ptr = lambda a: None if a is None else a.data_ptr()
         _lib.call("ab_ipm_seg_reduce", ctypes.byref(p),
@@ -487,7 +485,17 @@ class BatchedInteriorPointOptimizer(InteriorPointOptimizer):
                   ptr(None if upd is None else upd.zu),
                   ptr(None if gf is None else _dev(gf)),
                   self._seg.data_ptr(), self._s())
-        return self._seg.view(self.ninst, 10).cpu().numpy()
+        return self._seg
+
+    def seg_reduce(self, vars, grad=None, upd=None, gf=None, tau=0.0,
+                   zero_mu=False):
+        """Per-instance quantities as a (ninst, 12) host array (see
+        ab_ipm_seg_reduce): 0 dual, 1 primal, 2 comp inf-norms, 3 constraint
+        violation 1-norm, 4 barrier log-sum, 5/6 primal/dual step,
+        7 barrier directional derivative, 8 max |lam + dlam|, 9/10 largest
+        and smallest gap product."""
+        self.seg_reduce_device(vars, grad, upd, gf, tau, zero_mu)
+        return self._seg.view(self.ninst, 12).cpu().numpy()
 
     def apply_step_seg(self, ax, az, vars, upd, tmp):
         """tmp = vars + (ax[k], az[k]) * upd per instance; ax, az device."""

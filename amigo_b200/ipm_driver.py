@@ -38,6 +38,19 @@ DEFAULTS = dict(tol=1e-8, max_iter=200, mu0=0.1, mu_min=1e-11,
                 refine_steps=1)
 
 
+def _pw(m, e):
+    """m ** e as the device decision kernels evaluate it (csrc/batch_ctrl.cu):
+    m * sqrt(m) for 1.5 and sqrt(sqrt(m)) for 0.25, correctly rounded
+    square roots on both sides, so host and device decisions agree."""
+    if e == 1.5:
+        return m * math.sqrt(m)
+    if e == 0.25:
+        return math.sqrt(math.sqrt(m))
+    if e == 1.0:
+        return m
+    return m ** e
+
+
 def solve(backend, options=None, verbose=False):
     """Run the interior-point loop; returns a dict with converged,
     iterations, objective, kkt_error, time_s, inertia_corrections."""
@@ -64,7 +77,7 @@ def solve(backend, options=None, verbose=False):
         while True:
             Emu = max(B.kkt_error(mu, st, g))
             if Emu <= o["kappa_eps"] * mu and mu > o["mu_min"]:
-                mu = max(o["mu_min"], min(o["kappa_mu"] * mu, mu ** o["theta_mu"]))
+                mu = max(o["mu_min"], min(o["kappa_mu"] * mu, _pw(mu, o["theta_mu"])))
                 continue
             break
         # inertia-corrected factorization
@@ -80,7 +93,7 @@ def solve(backend, options=None, verbose=False):
                     break
                 n += 1
                 if inertia[0] + inertia[1] < B.n and dc == 0.0:
-                    dc = o["dc"] * mu ** o["kappa_c"]
+                    dc = o["dc"] * _pw(mu, o["kappa_c"])
                 if dw == 0.0:
                     dw = o["dw_first"] if dw_last == 0.0 else max(o["dw_min"],
                                                                   o["kw_minus"] * dw_last)

@@ -451,6 +451,13 @@ class BatchedSparseLDL:
                   _iptr(a), _iptr(b))
         return list(zip(a.tolist(), b.tolist()))
 
+    def inertia_device(self):
+        """Device pointer of the per-problem [npos, nneg] of the last
+        factorization (ab_ldl_inertia_device)."""
+        p = ctypes.c_void_p()
+        _lib.call("ab_ldl_inertia_device", self._h, ctypes.byref(p))
+        return p.value
+
     def solve_device(self, xd):
         nrhs = 1 if xd.dim() == 1 else xd.shape[0]
         with torch.cuda.device(self.device):

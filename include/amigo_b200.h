@@ -348,14 +348,17 @@ int ab_ipm_refine_update_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
                              double* px, double* dzl, double* dzu,
                              void* stream);
 /* Batched problems: per-instance reductions, one block per instance
- * (deterministic).  out[k * 10 + q] for instance k: 0 dual, 1 primal,
+ * (deterministic).  out[k * 12 + q] for instance k: 0 dual, 1 primal,
  * 2 complementarity inf-norms of compute_kkt_error (:450-466, with
  * mu_inst[k]); 3 constraint violation 1-norm (:565-573); 4 barrier log-sum
  * (:471-484); 5, 6 primal / dual fraction-to-boundary steps
  * (compute_max_step :329-369, seeded at 1); 7 barrier directional
  * derivative (:491-502, with gf); 8 max |lam + dlam| over the
- * constraints.  Null inputs skip the quantities that need them.  tau < 0
- * selects the per-instance fraction max(-tau, 1 - mu_inst[k]). */
+ * constraints; 9 / 10 the largest / smallest gap product s z over the
+ * bounded entries (-/+inf without any), from which the complementarity
+ * norm for any barrier parameter m is max(0, q9 - m, m - q10) exactly.
+ * Null inputs skip the quantities that need them.  tau < 0 selects the
+ * per-instance fraction max(-tau, 1 - mu_inst[k]). */
 int ab_ipm_seg_reduce(const ab_ipm_problem* p, const ab_ipm_state* s,
                       double tau, const double* grad, const double* px,
                       const double* dzl, const double* dzu, const double* gf,
@@ -535,6 +538,89 @@ int ab_cartpole_hessian(const ab_cartpole* m, const double* x, double alpha,
  * instance of a batch */
 int ab_cartpole_objective(const ab_cartpole* m, const double* x, double* out,
                           void* stream);
+
+/* ----------------------------------------------------------------------
+ * Device-side decisions of the batched interior-point loop (one thread per
+ * instance).  The loop is ipm_driver's (amigo_b200/ipm_driver.py): the
+ * convergence test E_0 <= tol and the monotone barrier update (the
+ * reference's monotone strategy, amigo/algorithm/barrier_strategy/:
+ * mu <- max(mu_min, min(kappa_mu mu, mu^theta_mu)) while
+ * E_mu <= kappa_eps mu), inertia correction (Algorithm IC,
+ * amigo/algorithm/inertia_correction.py:261-402: delta_w from dw_first,
+ * dw_last kw_minus, growth kw_plus_first / kw_plus; delta_c = dc mu^kappa_c
+ * on singular matrices), the 8-block refinement stopping rule (ratio below
+ * 1e-10 or no longer decreasing), and the l1-merit backtracking line
+ * search (Armijo on phi = f + barrier + nu theta, alpha halved).  All
+ * arrays are device arrays of ninst entries; mu is the barrier array the
+ * batched IPM kernels read (ab_ipm_problem.mu_inst).  Each call sets bits
+ * of flags[] (cleared by ab_bctl_clear_flags) that the host reads to end
+ * its loops; no other per-instance data needs to leave the device inside
+ * an iteration.  No single reference counterpart: the reference takes
+ * these decisions in Python for one problem at a time. */
+enum {
+  AB_BCTL_RETIRED = 0,     /* an instance converged or ran out of iterations */
+  AB_BCTL_LIVE = 1,        /* an instance continues this iteration */
+  AB_BCTL_IC_PENDING = 2,  /* an instance needs another factorization */
+  AB_BCTL_REFINING = 3,    /* an instance takes another refinement step */
+  AB_BCTL_STALLED = 4,     /* an instance's refinement ended above 1e-10 */
+  AB_BCTL_SEARCHING = 5,   /* an instance's line search continues */
+  AB_BCTL_NFLAGS = 8
+};
+
+typedef struct ab_bctl {
+  int ninst;
+  double *mu, *nu, *dw, *dc, *dwf, *dcf, *dw_last, *alpha, *az, *phi0, *dphi;
+  double *ratio, *ratio_old, *nrm, *e0;
+  int *live, *pending, *search, *on, *its, *n_ic, *retire;
+  const int *np_each, *nc_each, *n_each; /* wanted inertia and sizes */
+  int* flags;                            /* AB_BCTL_NFLAGS ints */
+} ab_bctl;
+
+typedef struct ab_bctl_opts {
+  double tol, mu_min, kappa_eps, kappa_mu, theta_mu, dw_first, dw_min, dw_max;
+  double kw_plus_first, kw_plus, kw_minus, dc, kappa_c, armijo;
+  int max_iter;
+} ab_bctl_opts;
+
+int ab_bctl_clear_flags(const ab_bctl* c, void* stream);
+/* q: ab_ipm_seg_reduce output (grad given, current mu).  Retires converged
+ * (retire = 1) and exhausted (retire = 2) instances, e0 = E_0; updates mu
+ * of the others by the monotone rule, with E_mu from the gap-product
+ * extremes (q slots 9, 10). */
+int ab_bctl_converge_barrier(const ab_bctl* c, const ab_bctl_opts* o, const double* q,
+                             void* stream);
+/* delta_w = delta_c = 0, pending = live */
+int ab_bctl_ic_begin(const ab_bctl* c, void* stream);
+/* dtot = diag + dwf[inst] primal - dcf[inst] (1 - primal) */
+int ab_bctl_shift_diag(const ab_bctl* c, int n, const int* vinst, const double* primal,
+                       const double* diag, double* dtot, void* stream);
+/* inertia: the batched factorization's [npos, nneg] per instance (device,
+ * ab_ldl_inertia_device) */
+int ab_bctl_ic_step(const ab_bctl* c, const ab_bctl_opts* o, const int* inertia,
+                    void* stream);
+/* dw_last = dw where an instance is live and dw > 0 */
+int ab_bctl_ic_end(const ab_bctl* c, void* stream);
+/* seg: ab_ipm_refine_init_seg's right-hand-side norms */
+int ab_bctl_refine_init(const ab_bctl* c, const double* seg, void* stream);
+/* seg: ab_ipm_refine_residual_seg's per-instance pairs; `on` is the active
+ * mask ab_ipm_refine_update_seg takes */
+int ab_bctl_refine_step(const ab_bctl* c, const double* seg, int step, void* stream);
+int ab_bctl_refine_stalled(const ab_bctl* c, void* stream);
+/* zero the update of instances that are not live */
+int ab_bctl_mask_update(const ab_bctl* c, int n, int np, const int* vinst, const int* pinst,
+                        double* dx, double* dzl, double* dzu, void* stream);
+/* q: seg_reduce with the update, gf and tau < 0; obj: objective per
+ * instance.  Sets nu, phi0, dphi, alpha (primal step), az, search. */
+int ab_bctl_ls_begin(const ab_bctl* c, const double* q, const double* obj, void* stream);
+/* q, obj at the trial point: accept, or halve alpha and keep searching */
+int ab_bctl_ls_test(const ab_bctl* c, const ab_bctl_opts* o, const double* q,
+                    const double* obj, void* stream);
+/* its += 1 for live instances */
+int ab_bctl_end(const ab_bctl* c, void* stream);
+
+/* Device pointer of a factorization's per-problem inertia, [npos, nneg]
+ * per problem (valid after ab_ldl_factor, until the next one). */
+int ab_ldl_inertia_device(ab_ldl_t h, const int** out);
 
 #ifdef __cplusplus
 }
