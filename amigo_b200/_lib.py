@@ -116,6 +116,8 @@ _SIGS = {
     "ab_bctl_ls_test": (_i, [_BC, _BO, _vp, _vp, _vp]),
     "ab_bctl_end": (_i, [_BC, _vp]),
     "ab_ldl_inertia_device": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "ab_ldl_set_solve_queue": (_i, [_vp, _i]),
+    "ab_ldl_solve_status": (_i, [_vp, _vp]),
     "ab_ldl_create": (_i, [_i, _ip, _ip, _i, _i, _d, _d, _d, ctypes.POINTER(_vp)]),
     "ab_ldl_analyze": (_i, [_i, _ip, _ip, _i, ctypes.POINTER(_vp)]),
     "ab_ldl_destroy": (_i, [_vp]),

@@ -249,6 +249,28 @@ int ab_ldl_factor(ab_ldl_t H, const double* d_vals, void* stream) {
   return ab::factor_numeric(H->h, d_vals, (cudaStream_t)stream);
 }
 
+int ab_ldl_set_solve_queue(ab_ldl_t H, int on) {
+  if (!H) return AB_ERR_ARG;
+  H->h.solve_queue = on != 0;
+  return AB_OK;
+}
+
+int ab_ldl_solve_status(ab_ldl_t H, void* stream) {
+  if (!H) return AB_ERR_ARG;
+  if (!H->h.sv_err) return AB_OK;
+  int e = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(&e, H->h.sv_err, sizeof(int), cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return AB_ERR_CUDA;
+  if (e) {
+    cudaMemsetAsync(H->h.sv_err, 0, sizeof(int), s);
+    return AB_ERR_CUDA;
+  }
+  return AB_OK;
+}
+
 int ab_ldl_inertia_device(ab_ldl_t H, const int** out) {
   if (!H || !out) return AB_ERR_ARG;
   if (!H->h.factored) return AB_ERR_NOT_FACTORED;

@@ -3112,11 +3112,20 @@ int factor_numeric(LdlHandle& h, const double* d_vals, cudaStream_t s) {
     int rc = h.precision == 32 ? launch_factor<float>(h, d_vals, s)
                                : launch_factor<double>(h, d_vals, s);
     if (rc) return rc;
-    int status = 0;
+    int status = 0, solve_err = 0;
     FCUDA(cudaMemcpyAsync(&status, d.status, sizeof(int),
                           cudaMemcpyDeviceToHost, s));
+    if (h.sv_err)
+      FCUDA(cudaMemcpyAsync(&solve_err, h.sv_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     FCUDA(cudaStreamSynchronize(s));
     h.last_status = status;
+    if (solve_err) {
+      // a work-queue solve sweep since the last factorization gave up
+      // waiting for a front (its result was wrong)
+      std::fprintf(stderr, "amigo_b200: a solve sweep's dependency wait ran out\n");
+      FCUDA(cudaMemsetAsync(h.sv_err, 0, sizeof(int), s));
+      return AB_ERR_CUDA;
+    }
     if (status & tc::kStatusTimeout) {
       std::fprintf(stderr, "amigo_b200: tensor-core update wait ran out\n");
       return AB_ERR_CUDA;

@@ -143,6 +143,19 @@ struct LdlHandle {
   long long sv_wide_entries = 0;
   std::vector<int> sv_fwd_grid, sv_bwd_grid;   // cooperative grid per level
   int sv_grid_cap = 0;
+  // work-queue sweeps over the all-narrow levels [0, sv_qlevels): the
+  // backward queue and its dependencies (parent in the queue, or -1), done
+  // flags per node with an epoch per sweep, the queue counters and the
+  // wait-ran-out word
+  bool solve_queue = true;
+  int sv_qlevels = 0, sv_qcount = 0, sv_qsmem = 0, sv_qgrid = 0;
+  std::vector<int> sv_bq_host, sv_dep_host;
+  int* sv_bq = nullptr;
+  int* sv_dep = nullptr;
+  unsigned* sv_done = nullptr;   // 2 x nn: forward, backward
+  unsigned* sv_ctr = nullptr;    // 2
+  int* sv_err = nullptr;
+  unsigned sv_epoch = 0;
 };
 
 int build_plan(LdlHandle& h, const int* rowp, const int* cols);

@@ -248,12 +248,16 @@ void free_plan(LdlHandle& h) {
                   d.scratch_int, d.f, d.npiv, d.ndel, d.ndin,
                   d.foff, d.ioff, d.inertia, d.node_prob, d.status,
                   d.counters, d.fpool,
-                  d.ipool, h.ubuf, h.uoff, h.sv_nodes, h.sv_state, h.cl_scratch};
+                  d.ipool, h.ubuf, h.uoff, h.sv_nodes, h.sv_state, h.cl_scratch,
+                  h.sv_bq, h.sv_dep, h.sv_done, h.sv_ctr, h.sv_err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   d = DevicePlan();
   h.cl_scratch = nullptr;
   h.cl_scratch_bytes = 0;
+  h.sv_bq = h.sv_dep = h.sv_err = nullptr;
+  h.sv_done = h.sv_ctr = nullptr;
+  h.sv_qlevels = h.sv_qcount = 0;
   h.ubuf = nullptr;
   h.uoff = nullptr;
   h.sv_nodes = nullptr;

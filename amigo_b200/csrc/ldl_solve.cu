@@ -213,7 +213,7 @@ __device__ void assemble_front_vector(const DevicePlan& d, int node, double* V,
         pos = r0 < ns ? r0 : r0 + ndin;
       }
       if (pos < fs) pos = fsinv[pos];
-      V[pos] += uc[a];
+      V[pos] += __ldcg(uc + a);  // written by another CTA (queue sweeps)
     }
     __syncthreads();
     if (tid == 0) *s_choff = choff + ndc;
@@ -221,22 +221,27 @@ __device__ void assemble_front_vector(const DevicePlan& d, int node, double* V,
   }
 }
 
+// Shared scratch of the one-CTA front solves.
+struct NarrowSmem {
+  int choff;
+  double L[(SB + 1) * (SB + 1)];
+  int K[SB + 1];  // the block's pivot kinds
+};
+
+// Forward solve of one front by the whole CTA (sV: dynamic shared memory
+// of smem_doubles).
 template <class T>
-__global__ void __launch_bounds__(NT)
-k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
-                int nrhs, int ldx, double* ubuf, const long long* uoff,
-                int smem_doubles) {
-  pdl_enter();
-  extern __shared__ double sV[];
-  const int node = nodes[blockIdx.x];
+__device__ void forward_front(const DevicePlan& d, int node, double* x, int nrhs,
+                              int ldx, double* ubuf, const long long* uoff,
+                              int smem_doubles, double* sV, NarrowSmem& sm) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int f = d.f[node], npiv = d.npiv[node];
   const int* fvars = d.ipool + d.ioff[node];
   const int* kind = fvars + 3 * f;
   const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
-  __shared__ int s_choff;
-  __shared__ double sL[(SB + 1) * (SB + 1)];
-  __shared__ int sK[SB + 1];  // the block's pivot kinds
+  int& s_choff = sm.choff;
+  double* sL = sm.L;
+  int* sK = sm.K;
 
   for (int rhs = 0; rhs < nrhs; rhs++) {
     // The front vector is worked on in shared memory when it fits (every
@@ -292,27 +297,36 @@ k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
 
 template <class T>
 __global__ void __launch_bounds__(NT)
-k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
-                 int nrhs, int ldx, double* ubuf, const long long* uoff,
-                 int smem_doubles) {
+k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
+                int nrhs, int ldx, double* ubuf, const long long* uoff,
+                int smem_doubles) {
   pdl_enter();
   extern __shared__ double sV[];
-  const int node = nodes[blockIdx.x];
+  __shared__ NarrowSmem sm;
+  forward_front<T>(d, nodes[blockIdx.x], x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
+}
+
+// Backward solve of one front by the whole CTA.
+template <class T>
+__device__ void backward_front(const DevicePlan& d, int node, double* x, int nrhs,
+                               int ldx, double* ubuf, const long long* uoff,
+                               int smem_doubles, double* sV, NarrowSmem& sm) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NWARP = NT / 32;
   const int f = d.f[node], npiv = d.npiv[node];
   const int* fvars = d.ipool + d.ioff[node];
   const int* kind = fvars + 3 * f;
   const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
-  __shared__ double sL[(SB + 1) * (SB + 1)];
-  __shared__ int sK[SB + 1];  // the block's pivot kinds
+  double* sL = sm.L;
+  int* sK = sm.K;
   for (int rhs = 0; rhs < nrhs; rhs++) {
     double* V = f <= smem_doubles ? sV : ubuf + uoff[node] + (long long)rhs * f;
     double* xr = x + (long long)rhs * ldx;
     // pivots: their forward values (written to x by the forward sweep);
-    // delayed and contribution rows: final values of the ancestors
+    // delayed and contribution rows: final values of the ancestors (from
+    // L2: another CTA of the same sweep may have written them)
     for (int r = tid; r < npiv; r += NT) V[r] = xr[decode_var(fvars[r])];
-    for (int r = npiv + tid; r < f; r += NT) V[r] = xr[fvars[r]];
+    for (int r = npiv + tid; r < f; r += NT) V[r] = __ldcg(xr + fvars[r]);
     __syncthreads();
     // Column blocks from the last one backwards.
     int je = npiv;
@@ -340,6 +354,107 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
     }
     for (int j = tid; j < npiv; j += NT) xr[decode_var(fvars[j])] = V[j];
     __syncthreads();
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT)
+k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
+                 int nrhs, int ldx, double* ubuf, const long long* uoff,
+                 int smem_doubles) {
+  pdl_enter();
+  extern __shared__ double sV[];
+  __shared__ NarrowSmem sm;
+  backward_front<T>(d, nodes[blockIdx.x], x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
+}
+
+// ---------------------------------------------------------------------------
+// Work-queue sweeps over the levels whose fronts are all narrow: one launch
+// per sweep instead of one per level.  `nodes` lists the fronts in the
+// order of a sweep (forward: level by level from the leaves; backward: the
+// reverse); each CTA takes the next front from an atomic counter, waits
+// until the fronts it depends on are done (forward: its children;
+// backward: its parent, when the parent is in the queue), solves it and
+// marks it done with this sweep's epoch.  Fronts are handed out in
+// dependency order and a CTA takes a front only while it runs, so the
+// earliest unfinished front always has its dependencies done: the waits
+// end.  Each wait is still bounded; when one runs out the kernel records
+// it in *err (the host reports it) and goes on.
+constexpr long long kQueuePolls = 1ll << 22;
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void wait_done(const unsigned* flag, unsigned epoch, int* err) {
+  for (long long it = 0; it < kQueuePolls; it++) {
+    if (ld_acquire(flag) == epoch) return;
+    __nanosleep(64);
+  }
+  atomicOr(err, 1);
+}
+
+// Take the next queue entry (-1 when the queue is exhausted).
+__device__ __forceinline__ int queue_next(unsigned* ctr, int count, int* s_idx) {
+  __syncthreads();
+  if (threadIdx.x == 0) *s_idx = (int)atomicAdd(ctr, 1u);
+  __syncthreads();
+  const int idx = *s_idx;
+  return idx < count ? idx : -1;
+}
+
+// This front's results are visible GPU-wide before its done flag.
+__device__ __forceinline__ void mark_done(unsigned* flag, unsigned epoch) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) st_release(flag, epoch);
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT)
+k_solve_forward_q(DevicePlan d, const int* __restrict__ nodes, int count, double* x,
+                  int nrhs, int ldx, double* ubuf, const long long* uoff,
+                  int smem_doubles, unsigned* ctr, unsigned* done, unsigned epoch,
+                  int* err) {
+  pdl_enter();
+  extern __shared__ double sV[];
+  __shared__ NarrowSmem sm;
+  __shared__ int s_idx;
+  for (;;) {
+    const int idx = queue_next(ctr, count, &s_idx);
+    if (idx < 0) break;
+    const int node = nodes[idx];
+    for (int q = d.kid_ptr[node] + threadIdx.x; q < d.kid_ptr[node + 1]; q += NT)
+      wait_done(done + d.kids[q], epoch, err);
+    __syncthreads();
+    forward_front<T>(d, node, x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
+    mark_done(done + node, epoch);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(NT)
+k_solve_backward_q(DevicePlan d, const int* __restrict__ nodes,
+                   const int* __restrict__ dep, int count, double* x, int nrhs,
+                   int ldx, double* ubuf, const long long* uoff, int smem_doubles,
+                   unsigned* ctr, unsigned* done, unsigned epoch, int* err) {
+  pdl_enter();
+  extern __shared__ double sV[];
+  __shared__ NarrowSmem sm;
+  __shared__ int s_idx;
+  for (;;) {
+    const int idx = queue_next(ctr, count, &s_idx);
+    if (idx < 0) break;
+    const int node = nodes[idx];
+    if (threadIdx.x == 0 && dep[idx] >= 0) wait_done(done + dep[idx], epoch, err);
+    __syncthreads();
+    backward_front<T>(d, node, x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
+    mark_done(done + node, epoch);
   }
 }
 
@@ -920,6 +1035,44 @@ static int build_solve_schedule(LdlHandle& h, cudaStream_t s) {
   // nodes is a member: it outlives the asynchronous copy
   SCUDA(cudaMemcpyAsync(h.sv_nodes, nodes.data(), nodes.size() * sizeof(int),
                         cudaMemcpyHostToDevice, s));
+  // the all-narrow levels from the leaves, swept by one work-queue launch
+  // each way (worth it from two levels)
+  int ql = 0;
+  while (ql < L && h.sv_clu_ptr[ql] == h.sv_narrow_ptr[ql + 1]) ql++;
+  h.sv_qlevels = ql >= 2 ? ql : 0;
+  h.sv_qcount = h.sv_qlevels ? h.sv_narrow_ptr[h.sv_qlevels] : 0;
+  if (h.sv_qcount) {
+    const int qc = h.sv_qcount;
+    // position of each queued node in the forward order
+    std::vector<int> pos(nn, -1);
+    for (int i = 0; i < qc; i++) pos[nodes[i]] = i;
+    std::vector<int>& bq = h.sv_bq_host;
+    std::vector<int>& dep = h.sv_dep_host;
+    bq.resize(qc);
+    dep.resize(qc);
+    int sm = 0;
+    for (int l = 0; l < h.sv_qlevels; l++) sm = std::max(sm, h.sv_narrow_smem[l]);
+    h.sv_qsmem = sm;
+    for (int i = 0; i < qc; i++) {
+      const int k = nodes[qc - 1 - i];
+      const int par = h.sym.node_parent[k];
+      bq[i] = k;
+      dep[i] = (par >= 0 && pos[par] >= 0) ? par : -1;
+    }
+    if (!h.sv_bq) {
+      SCUDA(cudaMalloc((void**)&h.sv_bq, std::max(nn, 1) * sizeof(int)));
+      SCUDA(cudaMalloc((void**)&h.sv_dep, std::max(nn, 1) * sizeof(int)));
+      SCUDA(cudaMalloc((void**)&h.sv_done, 2 * (size_t)std::max(nn, 1) * sizeof(unsigned)));
+      SCUDA(cudaMalloc((void**)&h.sv_ctr, 2 * sizeof(unsigned)));
+      SCUDA(cudaMalloc((void**)&h.sv_err, sizeof(int)));
+      SCUDA(cudaMemsetAsync(h.sv_done, 0, 2 * (size_t)std::max(nn, 1) * sizeof(unsigned), s));
+      SCUDA(cudaMemsetAsync(h.sv_err, 0, sizeof(int), s));
+      h.sv_epoch = 0;
+    }
+    SCUDA(cudaMemcpyAsync(h.sv_bq, bq.data(), qc * sizeof(int), cudaMemcpyHostToDevice, s));
+    SCUDA(cudaMemcpyAsync(h.sv_dep, dep.data(), qc * sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  h.sv_qgrid = 0;
   h.sv_f = h.h_f;
   h.sv_npiv = h.h_npiv;
   h.sv_fwd_grid.clear();
@@ -940,6 +1093,12 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kMaxDynSmem));
     SCUDA(cudaFuncSetAttribute(k_solve_backward<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kMaxDynSmem));
+    SCUDA(cudaFuncSetAttribute(k_solve_forward_q<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kMaxDynSmem));
+    SCUDA(cudaFuncSetAttribute(k_solve_backward_q<T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                kMaxDynSmem));
     SCUDA(cudaFuncSetAttribute(k_clu_forward<T>,
@@ -994,7 +1153,27 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
     ev.resize(2 * d.num_levels + 2);
     for (auto& e : ev) cudaEventCreate(&e);
   }
-  for (int l = 0; l < d.num_levels; l++) {
+  const bool queue = h.solve_queue && h.sv_qcount > 0;
+  const unsigned ep = h.sv_epoch + 1;
+  if (queue) {
+    if (h.sv_qgrid == 0) {
+      // CTAs resident at once, at most one per queued front
+      int dev = 0, sms = 0, per = 0;
+      SCUDA(cudaGetDevice(&dev));
+      SCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_forward_q<T>, NT,
+                                                          (size_t)h.sv_qsmem));
+      h.sv_qgrid = std::max(1, std::min(h.sv_qcount, sms * std::max(per, 1)));
+    }
+    h.sv_epoch = ep;
+    SCUDA(cudaMemsetAsync(h.sv_ctr, 0, 2 * sizeof(unsigned), s));
+    SCUDA(launch_pdl(k_solve_forward_q<T>, dim3(h.sv_qgrid), dim3(NT), (size_t)h.sv_qsmem, s,
+                     d, (const int*)h.sv_nodes, h.sv_qcount, d_x, nrhs, ldx, h.ubuf,
+                     (const long long*)h.uoff, h.sv_qsmem / 8, h.sv_ctr, h.sv_done, ep,
+                     h.sv_err));
+    ab::count_launch();
+  }
+  for (int l = queue ? h.sv_qlevels : 0; l < d.num_levels; l++) {
     if (trace) cudaEventRecord(ev[l], s);
     const int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
     if (cnt) {
@@ -1024,7 +1203,7 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
     }
   }
   if (trace) cudaEventRecord(ev[d.num_levels], s);
-  for (int l = d.num_levels - 1; l >= 0; l--) {
+  for (int l = d.num_levels - 1; l >= (queue ? h.sv_qlevels : 0); l--) {
     if (trace) cudaEventRecord(ev[d.num_levels + 1 + (d.num_levels - 1 - l)], s);
     const int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
     if (cnt) {
@@ -1051,6 +1230,20 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
                                         dim3(h.sv_bwd_grid[l]), dim3(NT), args,
                                         wide_smem, s));
       ab::count_launch();
+    }
+  }
+  if (queue) {
+    SCUDA(launch_pdl(k_solve_backward_q<T>, dim3(h.sv_qgrid), dim3(NT), (size_t)h.sv_qsmem,
+                     s, d, (const int*)h.sv_bq, (const int*)h.sv_dep, h.sv_qcount, d_x,
+                     nrhs, ldx, h.ubuf, (const long long*)h.uoff, h.sv_qsmem / 8,
+                     h.sv_ctr + 1, h.sv_done + d.nn, ep, h.sv_err));
+    ab::count_launch();
+  }
+  if (trace && queue) {
+    // the queued levels ran as one launch each way: no per-level times
+    for (int l = 0; l < h.sv_qlevels; l++) {
+      cudaEventRecord(ev[l], s);
+      cudaEventRecord(ev[d.num_levels + 1 + (d.num_levels - 1 - l)], s);
     }
   }
   if (trace) {

@@ -257,6 +257,16 @@ class SparseLDL:
         solved by a thread-block cluster of 8 CTAs each."""
         _lib.call("ab_ldl_set_cluster_threshold", self._h, int(entries))
 
+    def set_solve_queue(self, on):
+        """Solve sweeps over the all-narrow levels as one work-queue launch
+        each way (default) or one launch per level (identical results)."""
+        _lib.call("ab_ldl_set_solve_queue", self._h, int(bool(on)))
+
+    def solve_status(self):
+        """Raise if a work-queue solve sweep's wait ran out since the last
+        check (ab_ldl_solve_status)."""
+        _lib.call("ab_ldl_solve_status", self._h, _stream_ptr(self.device))
+
     def set_panel_mode(self, mode, min_rows=0):
         """Large-front panels: 0 (default) a thread-block cluster of 8 CTAs
         per front on levels whose largest front has >= min_rows rows (fronts
@@ -450,6 +460,13 @@ class BatchedSparseLDL:
         _lib.call("ab_ldl_batch_inertia", self._h, _stream_ptr(self.device),
                   _iptr(a), _iptr(b))
         return list(zip(a.tolist(), b.tolist()))
+
+    def set_solve_queue(self, on):
+        """See SparseLDL.set_solve_queue."""
+        _lib.call("ab_ldl_set_solve_queue", self._h, int(bool(on)))
+
+    def solve_status(self):
+        _lib.call("ab_ldl_solve_status", self._h, _stream_ptr(self.device))
 
     def inertia_device(self):
         """Device pointer of the per-problem [npos, nneg] of the last

@@ -149,6 +149,17 @@ int ab_ldl_set_cluster_threshold(ab_ldl_t h, long long entries);
  * reference factors each front on one thread). */
 int ab_ldl_set_panel_mode(ab_ldl_t h, int mode, int min_rows);
 
+/* Solve sweeps over the elimination-tree levels whose fronts are all
+ * solved one CTA per front (from the leaves): on (default), one
+ * work-queue launch per sweep -- CTAs take fronts in dependency order from
+ * an atomic counter and wait (bounded) for the fronts they depend on;
+ * off, one launch per level.  Both give the same result bit for bit.
+ * ab_ldl_solve_status reports (AB_ERR_CUDA) and clears a wait that ran
+ * out since the last check; ab_ldl_factor also reports it.  No reference
+ * counterpart (the reference solves front by front on the host). */
+int ab_ldl_set_solve_queue(ab_ldl_t h, int on);
+int ab_ldl_solve_status(ab_ldl_t h, void* stream);
+
 /* The tensor-core Schur update on plain device arrays (column-major, FP32):
  * lower(C) -= A B^T for n x kw panels A, B (kw <= 31), as 3xTF32 tcgen05
  * products accumulated in FP32 in tensor memory -- the update the
