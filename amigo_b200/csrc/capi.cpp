@@ -249,9 +249,9 @@ int ab_ldl_factor(ab_ldl_t H, const double* d_vals, void* stream) {
   return ab::factor_numeric(H->h, d_vals, (cudaStream_t)stream);
 }
 
-int ab_ldl_set_solve_queue(ab_ldl_t H, int on) {
-  if (!H) return AB_ERR_ARG;
-  H->h.solve_queue = on != 0;
+int ab_ldl_set_solve_queue(ab_ldl_t H, int mode) {
+  if (!H || mode < 0 || mode > 3) return AB_ERR_ARG;
+  H->h.solve_queue = mode;
   return AB_OK;
 }
 

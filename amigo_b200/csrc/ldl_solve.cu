@@ -52,9 +52,9 @@ __device__ __forceinline__ double dot_strided(const T* __restrict__ col, size_t 
 #pragma unroll
     for (int u = 0; u < 16; u++) a[u] = col[(size_t)(j + u) * ld];
 #pragma unroll
-    for (int u = 0; u < 16; u++) acc += (double)a[u] * v(j + u);
+    for (int u = 0; u < 16; u++) acc = __fma_rn((double)a[u], v(j + u), acc);
   }
-  for (; j < n; j++) acc += (double)col[(size_t)j * ld] * v(j);
+  for (; j < n; j++) acc = __fma_rn((double)col[(size_t)j * ld], v(j), acc);
   return acc;
 }
 
@@ -74,10 +74,25 @@ __device__ __forceinline__ double lane_dot(const T* __restrict__ col, int i0, in
       b[u] = v(i + 32 * u);
     }
 #pragma unroll
-    for (int u = 0; u < 8; u++) acc += (double)a[u] * b[u];
+    for (int u = 0; u < 8; u++) acc = __fma_rn((double)a[u], b[u], acc);
   }
-  for (; i < i1; i += 32) acc += (double)col[i] * v(i);
+  for (; i < i1; i += 32) acc = __fma_rn((double)col[i], v(i), acc);
   return acc;
+}
+
+// The 2x2 block of D applied to (x1, x2): every product and difference
+// rounded on its own (no contraction), so that every kernel that solves
+// with a 2x2 pivot gives the same bits.
+__device__ __forceinline__ double inv2x2(double d11, double d21, double d22) {
+  return __ddiv_rn(1.0, __dsub_rn(__dmul_rn(d11, d22), __dmul_rn(d21, d21)));
+}
+__device__ __forceinline__ double piv2_first(double inv, double d21, double d22,
+                                             double x1, double x2) {
+  return __dmul_rn(inv, __dsub_rn(__dmul_rn(d22, x1), __dmul_rn(d21, x2)));
+}
+__device__ __forceinline__ double piv2_second(double inv, double d11, double d21,
+                                              double x1, double x2) {
+  return __dmul_rn(inv, __dsub_rn(__dmul_rn(d11, x2), __dmul_rn(d21, x1)));
 }
 
 __device__ __forceinline__ double warp_sum_down(double a) {
@@ -120,9 +135,9 @@ __device__ __forceinline__ void warp_lower_solve(const double* sL, int lds,
     for (int r = 0; r < R; r++) {
       const int i = lane + 32 * r;
       if (i >= i0 && i < bw) {
-        double t = sL[i + j * lds] * v0;
-        if (two) t += sL[i + (j + 1) * lds] * v1;
-        v[r] -= t;
+        double t = __dmul_rn(sL[i + j * lds], v0);
+        if (two) t = __fma_rn(sL[i + (j + 1) * lds], v1, t);
+        v[r] = __dsub_rn(v[r], t);
       }
     }
     j = i0;
@@ -156,9 +171,9 @@ __device__ __forceinline__ void warp_upper_solve(const double* sL, int lds,
     for (int r = 0; r < R; r++) {
       const int i = lane + 32 * r;
       if (i < jl) {
-        double t = sL[j + i * lds] * xj;
-        if (two) t += sL[jl + i * lds] * xl;
-        v[r] -= t;
+        double t = __dmul_rn(sL[j + i * lds], xj);
+        if (two) t = __fma_rn(sL[jl + i * lds], xl, t);
+        v[r] = __dsub_rn(v[r], t);
       }
     }
     j = jl - 1;
@@ -281,10 +296,10 @@ __device__ void forward_front(const DevicePlan& d, int node, double* x, int nrhs
         const double d11 = L[j + (size_t)j * f];
         const double d21 = L[j + 1 + (size_t)j * f];
         const double d22 = L[j + 1 + (size_t)(j + 1) * f];
-        const double inv = 1.0 / (d11 * d22 - d21 * d21);
+        const double inv = inv2x2(d11, d21, d22);
         const double x1 = V[j], x2 = V[j + 1];
-        V[j] = inv * (d22 * x1 - d21 * x2);
-        V[j + 1] = inv * (d11 * x2 - d21 * x1);
+        V[j] = piv2_first(inv, d21, d22, x1, x2);
+        V[j + 1] = piv2_second(inv, d11, d21, x1, x2);
       }
     }
     __syncthreads();
@@ -366,6 +381,167 @@ k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
   extern __shared__ double sV[];
   __shared__ NarrowSmem sm;
   backward_front<T>(d, nodes[blockIdx.x], x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
+}
+
+// ---------------------------------------------------------------------------
+// Small fronts (f <= kWarpRows): one warp per front, the same steps in the
+// same order as forward_front / backward_front (the blocked triangular
+// solves, the dot products of the rows below each block, D^{-1}), so the
+// results are the same bit for bit; CTAs of kWarpsPerCta warps, each with
+// its own slice of shared memory for the front vector and the staged
+// diagonal block.  Warps never wait for one another.
+constexpr int kWarpRows = 128;
+constexpr int kWarpsPerCta = 4;
+constexpr int kWarpSlice = kWarpRows + (SB + 1) * (SB + 1) + (SB + 2) / 2;  // doubles
+constexpr int kWarpSmem = kWarpsPerCta * kWarpSlice * (int)sizeof(double);
+
+template <class T>
+__device__ void forward_front_w(const DevicePlan& d, int node, double* x, int nrhs,
+                                int ldx, double* ubuf, const long long* uoff,
+                                double* slice) {
+  const int lane = threadIdx.x & 31;
+  const int f = d.f[node], npiv = d.npiv[node];
+  const int* fvars = d.ipool + d.ioff[node];
+  const int* kind = fvars + 3 * f;
+  const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
+  double* V = slice;
+  double* sL = slice + kWarpRows;
+  int* sK = reinterpret_cast<int*>(sL + (SB + 1) * (SB + 1));
+  const int ns = d.ns[node], ndin = d.ndin[node];
+  const int fs = ns + ndin;
+  const int* fsinv = d.ipool + d.ioff[node] + 2 * f;
+  const int vb = d.var_ptr[node];
+  for (int rhs = 0; rhs < nrhs; rhs++) {
+    double* G = ubuf + uoff[node] + (long long)rhs * f;
+    double* xr = x + (long long)rhs * ldx;
+    // front vector: own entries of the right-hand side, then the children's
+    // update vectors in order (assemble_front_vector, by one warp)
+    for (int r = lane; r < f; r += 32) V[r] = 0.0;
+    __syncwarp();
+    for (int r = lane; r < ns; r += 32) V[fsinv[r]] = xr[d.vars[vb + r]];
+    __syncwarp();
+    int choff = ns;
+    for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
+      const int c = d.kids[q];
+      const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
+      const int cc = fc - npc;
+      const double* uc = ubuf + uoff[c] + (long long)rhs * fc + npc;
+      const int cb = d.cptr[c];
+      for (int a = lane; a < cc; a += 32) {
+        int pos;
+        if (a < ndc) {
+          pos = choff + a;
+        } else {
+          int r0 = d.cmap[cb + a - ndc];
+          pos = r0 < ns ? r0 : r0 + ndin;
+        }
+        if (pos < fs) pos = fsinv[pos];
+        V[pos] += __ldcg(uc + a);
+      }
+      __syncwarp();
+      choff += ndc;
+    }
+    for (int jb = 0; jb < npiv;) {
+      const int je = block_end(kind, jb, npiv);
+      const int bw = je - jb;
+      for (int t = lane; t < bw * bw; t += 32) {
+        const int i = t % bw, j = t / bw;
+        sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
+      }
+      for (int t = lane; t < bw; t += 32) sK[t] = kind[jb + t];
+      __syncwarp();
+      warp_lower_solve<2>(sL, SB + 1, sK, bw, V + jb, lane);
+      __syncwarp();
+      for (int i = je + lane; i < f; i += 32)
+        V[i] -= dot_strided(L + i + (size_t)jb * f, (size_t)f, bw,
+                            [&](int j) { return V[jb + j]; });
+      __syncwarp();
+      jb = je;
+    }
+    for (int j = lane; j < npiv; j += 32) {
+      const int kd = kind[j];
+      if (kd == 0) {
+        V[j] = V[j] / L[j + (size_t)j * f];
+      } else if (kd == 1) {
+        const double d11 = L[j + (size_t)j * f];
+        const double d21 = L[j + 1 + (size_t)j * f];
+        const double d22 = L[j + 1 + (size_t)(j + 1) * f];
+        const double inv = inv2x2(d11, d21, d22);
+        const double x1 = V[j], x2 = V[j + 1];
+        V[j] = piv2_first(inv, d21, d22, x1, x2);
+        V[j + 1] = piv2_second(inv, d11, d21, x1, x2);
+      }
+    }
+    __syncwarp();
+    for (int j = lane; j < npiv; j += 32) xr[decode_var(fvars[j])] = V[j];
+    for (int r = npiv + lane; r < f; r += 32) G[r] = V[r];
+    __syncwarp();
+  }
+}
+
+template <class T>
+__device__ void backward_front_w(const DevicePlan& d, int node, double* x, int nrhs,
+                                 int ldx, double* slice) {
+  const int lane = threadIdx.x & 31;
+  const int f = d.f[node], npiv = d.npiv[node];
+  const int* fvars = d.ipool + d.ioff[node];
+  const int* kind = fvars + 3 * f;
+  const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
+  double* V = slice;
+  double* sL = slice + kWarpRows;
+  int* sK = reinterpret_cast<int*>(sL + (SB + 1) * (SB + 1));
+  for (int rhs = 0; rhs < nrhs; rhs++) {
+    double* xr = x + (long long)rhs * ldx;
+    for (int r = lane; r < npiv; r += 32) V[r] = xr[decode_var(fvars[r])];
+    for (int r = npiv + lane; r < f; r += 32) V[r] = __ldcg(xr + fvars[r]);
+    __syncwarp();
+    int je = npiv;
+    while (je > 0) {
+      int jb = je - SB > 0 ? je - SB : 0;
+      if (jb > 0 && kind[jb] == 2) jb--;
+      for (int j = jb; j < je; j++) {
+        const double acc = warp_sum_down(
+            lane_dot(L + (size_t)j * f, je, f, lane, [&](int i) { return V[i]; }));
+        if (lane == 0) V[j] -= acc;
+      }
+      const int bw = je - jb;
+      for (int t = lane; t < bw * bw; t += 32) {
+        const int i = t % bw, j = t / bw;
+        sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
+      }
+      for (int t = lane; t < bw; t += 32) sK[t] = kind[jb + t];
+      __syncwarp();
+      warp_upper_solve<2>(sL, SB + 1, sK, bw, V + jb, lane);
+      __syncwarp();
+      je = jb;
+    }
+    for (int j = lane; j < npiv; j += 32) xr[decode_var(fvars[j])] = V[j];
+    __syncwarp();
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kWarpsPerCta * 32)
+k_solve_forward_w(DevicePlan d, const int* __restrict__ nodes, int cnt, double* x,
+                  int nrhs, int ldx, double* ubuf, const long long* uoff) {
+  pdl_enter();
+  extern __shared__ double wsm[];
+  const int w = threadIdx.x >> 5;
+  const int i = blockIdx.x * kWarpsPerCta + w;
+  if (i >= cnt) return;
+  forward_front_w<T>(d, nodes[i], x, nrhs, ldx, ubuf, uoff, wsm + w * kWarpSlice);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kWarpsPerCta * 32)
+k_solve_backward_w(DevicePlan d, const int* __restrict__ nodes, int cnt, double* x,
+                   int nrhs, int ldx) {
+  pdl_enter();
+  extern __shared__ double wsm[];
+  const int w = threadIdx.x >> 5;
+  const int i = blockIdx.x * kWarpsPerCta + w;
+  if (i >= cnt) return;
+  backward_front_w<T>(d, nodes[i], x, nrhs, ldx, wsm + w * kWarpSlice);
 }
 
 // ---------------------------------------------------------------------------
@@ -458,6 +634,61 @@ k_solve_backward_q(DevicePlan d, const int* __restrict__ nodes,
   }
 }
 
+
+// The work-queue sweeps with one warp per front (every queued front has at
+// most kWarpRows rows): each warp takes fronts on its own.
+__device__ __forceinline__ int queue_next_w(unsigned* ctr, int count) {
+  unsigned v = 0;
+  if ((threadIdx.x & 31) == 0) v = atomicAdd(ctr, 1u);
+  const int idx = (int)__shfl_sync(0xffffffffu, v, 0);
+  return idx < count ? idx : -1;
+}
+
+__device__ __forceinline__ void mark_done_w(unsigned* flag, unsigned epoch) {
+  __threadfence();
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) st_release(flag, epoch);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kWarpsPerCta * 32)
+k_solve_forward_qw(DevicePlan d, const int* __restrict__ nodes, int count, double* x,
+                   int nrhs, int ldx, double* ubuf, const long long* uoff,
+                   unsigned* ctr, unsigned* done, unsigned epoch, int* err) {
+  pdl_enter();
+  extern __shared__ double wsm[];
+  double* slice = wsm + (threadIdx.x >> 5) * kWarpSlice;
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    const int idx = queue_next_w(ctr, count);
+    if (idx < 0) break;
+    const int node = nodes[idx];
+    for (int q = d.kid_ptr[node] + lane; q < d.kid_ptr[node + 1]; q += 32)
+      wait_done(done + d.kids[q], epoch, err);
+    __syncwarp();
+    forward_front_w<T>(d, node, x, nrhs, ldx, ubuf, uoff, slice);
+    mark_done_w(done + node, epoch);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kWarpsPerCta * 32)
+k_solve_backward_qw(DevicePlan d, const int* __restrict__ nodes,
+                    const int* __restrict__ dep, int count, double* x, int nrhs,
+                    int ldx, unsigned* ctr, unsigned* done, unsigned epoch, int* err) {
+  pdl_enter();
+  extern __shared__ double wsm[];
+  double* slice = wsm + (threadIdx.x >> 5) * kWarpSlice;
+  for (;;) {
+    const int idx = queue_next_w(ctr, count);
+    if (idx < 0) break;
+    const int node = nodes[idx];
+    if ((threadIdx.x & 31) == 0 && dep[idx] >= 0) wait_done(done + dep[idx], epoch, err);
+    __syncwarp();
+    backward_front_w<T>(d, node, x, nrhs, ldx, slice);
+    mark_done_w(done + node, epoch);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Mid-size fronts: one thread-block cluster of CS CTAs per front.  CTA 0
@@ -560,14 +791,14 @@ k_clu_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
           const double d11 = L[j + (size_t)j * f];
           const double d21 = L[j + 1 + (size_t)j * f];
           const double d22 = L[j + 1 + (size_t)(j + 1) * f];
-          const double inv = 1.0 / (d11 * d22 - d21 * d21);
-          v = inv * (d22 * sv[j] - d21 * sv[j + 1]);
+          const double inv = inv2x2(d11, d21, d22);
+          v = piv2_first(inv, d21, d22, sv[j], sv[j + 1]);
         } else {
           const double d11 = L[j - 1 + (size_t)(j - 1) * f];
           const double d21 = L[j + (size_t)(j - 1) * f];
           const double d22 = L[j + (size_t)j * f];
-          const double inv = 1.0 / (d11 * d22 - d21 * d21);
-          v = inv * (d11 * sv[j] - d21 * sv[j - 1]);
+          const double inv = inv2x2(d11, d21, d22);
+          v = piv2_second(inv, d11, d21, sv[j - 1], sv[j]);
         }
         xr[decode_var(fvars[j])] = v;
       }
@@ -790,10 +1021,10 @@ k_wide_forward(DevicePlan d, const int* __restrict__ nodes, int count,
           const double d11 = L[j + j * f];
           const double d21 = L[j + 1 + j * f];
           const double d22 = L[j + 1 + (j + 1) * f];
-          const double inv = 1.0 / (d11 * d22 - d21 * d21);
+          const double inv = inv2x2(d11, d21, d22);
           const double x1 = __ldcg(w.G + j), x2 = __ldcg(w.G + j + 1);
-          w.G[j] = inv * (d22 * x1 - d21 * x2);
-          w.G[j + 1] = inv * (d11 * x2 - d21 * x1);
+          w.G[j] = piv2_first(inv, d21, d22, x1, x2);
+          w.G[j + 1] = piv2_second(inv, d11, d21, x1, x2);
         }
       }
       __syncthreads();
@@ -994,16 +1225,22 @@ static int build_solve_schedule(LdlHandle& h, cudaStream_t s) {
     if (e >= h.cluster_entries && ((long long)h.h_f[k] + NT) * 8 <= kMaxDynSmem) return 1;
     return 0;
   };
+  h.sv_small_cnt.assign(L, 0);
   for (int l = 0; l < L; l++) {
     h.sv_narrow_ptr[l] = (int)nodes.size();
     int fm = 0;
-    for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++) {
-      const int k = h.level_nodes[q];
-      if (cls(k) == 0) {
-        nodes.push_back(k);
-        fm = std::max(fm, h.h_f[k]);
+    // narrow fronts: the small ones (one warp each) first
+    for (int pass = 0; pass < 2; pass++)
+      for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++) {
+        const int k = h.level_nodes[q];
+        if (cls(k) == 0 && (h.h_f[k] <= kWarpRows) == (pass == 0)) {
+          nodes.push_back(k);
+          if (pass == 0)
+            h.sv_small_cnt[l]++;
+          else
+            fm = std::max(fm, h.h_f[k]);
+        }
       }
-    }
     h.sv_narrow_smem[l] =
         (int)std::min<long long>((long long)fm * 8, kMaxDynSmem);
     h.sv_clu_ptr[l] = (int)nodes.size();
@@ -1041,6 +1278,9 @@ static int build_solve_schedule(LdlHandle& h, cudaStream_t s) {
   while (ql < L && h.sv_clu_ptr[ql] == h.sv_narrow_ptr[ql + 1]) ql++;
   h.sv_qlevels = ql >= 2 ? ql : 0;
   h.sv_qcount = h.sv_qlevels ? h.sv_narrow_ptr[h.sv_qlevels] : 0;
+  h.sv_qwarp = true;
+  for (int l = 0; l < h.sv_qlevels; l++)
+    if (h.sv_small_cnt[l] != h.sv_clu_ptr[l] - h.sv_narrow_ptr[l]) h.sv_qwarp = false;
   if (h.sv_qcount) {
     const int qc = h.sv_qcount;
     // position of each queued node in the forward order
@@ -1153,29 +1393,54 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
     ev.resize(2 * d.num_levels + 2);
     for (auto& e : ev) cudaEventCreate(&e);
   }
-  const bool queue = h.solve_queue && h.sv_qcount > 0;
+  const bool queue = (h.solve_queue & 1) && h.sv_qcount > 0;
+  const bool warps = (h.solve_queue & 2) != 0;
+  const bool qwarp = queue && warps && h.sv_qwarp;
   const unsigned ep = h.sv_epoch + 1;
   if (queue) {
-    if (h.sv_qgrid == 0) {
-      // CTAs resident at once, at most one per queued front
+    if (h.sv_qgrid == 0 || h.sv_qgrid_warp != qwarp) {
+      // CTAs resident at once, at most one per queued front (per
+      // kWarpsPerCta fronts with one warp each)
       int dev = 0, sms = 0, per = 0;
       SCUDA(cudaGetDevice(&dev));
       SCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_forward_q<T>, NT,
-                                                          (size_t)h.sv_qsmem));
-      h.sv_qgrid = std::max(1, std::min(h.sv_qcount, sms * std::max(per, 1)));
+      if (qwarp)
+        SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per, k_solve_forward_qw<T>, kWarpsPerCta * 32, (size_t)kWarpSmem));
+      else
+        SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_forward_q<T>, NT,
+                                                            (size_t)h.sv_qsmem));
+      const int need = qwarp ? (h.sv_qcount + kWarpsPerCta - 1) / kWarpsPerCta : h.sv_qcount;
+      h.sv_qgrid = std::max(1, std::min(need, sms * std::max(per, 1)));
+      h.sv_qgrid_warp = qwarp;
     }
     h.sv_epoch = ep;
     SCUDA(cudaMemsetAsync(h.sv_ctr, 0, 2 * sizeof(unsigned), s));
-    SCUDA(launch_pdl(k_solve_forward_q<T>, dim3(h.sv_qgrid), dim3(NT), (size_t)h.sv_qsmem, s,
-                     d, (const int*)h.sv_nodes, h.sv_qcount, d_x, nrhs, ldx, h.ubuf,
-                     (const long long*)h.uoff, h.sv_qsmem / 8, h.sv_ctr, h.sv_done, ep,
-                     h.sv_err));
+    if (qwarp)
+      SCUDA(launch_pdl(k_solve_forward_qw<T>, dim3(h.sv_qgrid), dim3(kWarpsPerCta * 32),
+                       (size_t)kWarpSmem, s, d, (const int*)h.sv_nodes, h.sv_qcount, d_x,
+                       nrhs, ldx, h.ubuf, (const long long*)h.uoff, h.sv_ctr, h.sv_done,
+                       ep, h.sv_err));
+    else
+      SCUDA(launch_pdl(k_solve_forward_q<T>, dim3(h.sv_qgrid), dim3(NT), (size_t)h.sv_qsmem,
+                       s, d, (const int*)h.sv_nodes, h.sv_qcount, d_x, nrhs, ldx, h.ubuf,
+                       (const long long*)h.uoff, h.sv_qsmem / 8, h.sv_ctr, h.sv_done, ep,
+                       h.sv_err));
     ab::count_launch();
   }
   for (int l = queue ? h.sv_qlevels : 0; l < d.num_levels; l++) {
     if (trace) cudaEventRecord(ev[l], s);
-    const int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
+    int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
+    if (warps && h.sv_small_cnt[l]) {
+      const int sc = h.sv_small_cnt[l];
+      SCUDA(launch_pdl(k_solve_forward_w<T>, dim3((sc + kWarpsPerCta - 1) / kWarpsPerCta),
+                       dim3(kWarpsPerCta * 32), (size_t)kWarpSmem, s, d,
+                       (const int*)(h.sv_nodes + b), sc, d_x, nrhs, ldx, h.ubuf,
+                       (const long long*)h.uoff));
+      ab::count_launch();
+      b += sc;
+      cnt -= sc;
+    }
     if (cnt) {
       SCUDA(launch_pdl(k_solve_forward<T>, dim3(cnt), dim3(NT), (size_t)h.sv_narrow_smem[l],
                        s, d, h.sv_nodes + b, d_x, nrhs, ldx, h.ubuf, h.uoff,
@@ -1205,7 +1470,16 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
   if (trace) cudaEventRecord(ev[d.num_levels], s);
   for (int l = d.num_levels - 1; l >= (queue ? h.sv_qlevels : 0); l--) {
     if (trace) cudaEventRecord(ev[d.num_levels + 1 + (d.num_levels - 1 - l)], s);
-    const int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
+    int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
+    if (warps && h.sv_small_cnt[l]) {
+      const int sc = h.sv_small_cnt[l];
+      SCUDA(launch_pdl(k_solve_backward_w<T>, dim3((sc + kWarpsPerCta - 1) / kWarpsPerCta),
+                       dim3(kWarpsPerCta * 32), (size_t)kWarpSmem, s, d,
+                       (const int*)(h.sv_nodes + b), sc, d_x, nrhs, ldx));
+      ab::count_launch();
+      b += sc;
+      cnt -= sc;
+    }
     if (cnt) {
       SCUDA(launch_pdl(k_solve_backward<T>, dim3(cnt), dim3(NT), (size_t)h.sv_narrow_smem[l],
                        s, d, h.sv_nodes + b, d_x, nrhs, ldx, h.ubuf, h.uoff,
@@ -1233,10 +1507,16 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
     }
   }
   if (queue) {
-    SCUDA(launch_pdl(k_solve_backward_q<T>, dim3(h.sv_qgrid), dim3(NT), (size_t)h.sv_qsmem,
-                     s, d, (const int*)h.sv_bq, (const int*)h.sv_dep, h.sv_qcount, d_x,
-                     nrhs, ldx, h.ubuf, (const long long*)h.uoff, h.sv_qsmem / 8,
-                     h.sv_ctr + 1, h.sv_done + d.nn, ep, h.sv_err));
+    if (qwarp)
+      SCUDA(launch_pdl(k_solve_backward_qw<T>, dim3(h.sv_qgrid), dim3(kWarpsPerCta * 32),
+                       (size_t)kWarpSmem, s, d, (const int*)h.sv_bq, (const int*)h.sv_dep,
+                       h.sv_qcount, d_x, nrhs, ldx, h.sv_ctr + 1, h.sv_done + d.nn, ep,
+                       h.sv_err));
+    else
+      SCUDA(launch_pdl(k_solve_backward_q<T>, dim3(h.sv_qgrid), dim3(NT), (size_t)h.sv_qsmem,
+                       s, d, (const int*)h.sv_bq, (const int*)h.sv_dep, h.sv_qcount, d_x,
+                       nrhs, ldx, h.ubuf, (const long long*)h.uoff, h.sv_qsmem / 8,
+                       h.sv_ctr + 1, h.sv_done + d.nn, ep, h.sv_err));
     ab::count_launch();
   }
   if (trace && queue) {

@@ -257,10 +257,12 @@ class SparseLDL:
         solved by a thread-block cluster of 8 CTAs each."""
         _lib.call("ab_ldl_set_cluster_threshold", self._h, int(entries))
 
-    def set_solve_queue(self, on):
-        """Solve sweeps over the all-narrow levels as one work-queue launch
-        each way (default) or one launch per level (identical results)."""
-        _lib.call("ab_ldl_set_solve_queue", self._h, int(bool(on)))
+    def set_solve_queue(self, mode):
+        """Narrow-front solve schedule (ab_ldl_set_solve_queue): bit 0 one
+        work-queue launch per sweep over the all-narrow levels, bit 1 one
+        warp per front of at most 128 rows; default 1; every mode gives the
+        same result bit for bit."""
+        _lib.call("ab_ldl_set_solve_queue", self._h, int(mode))
 
     def solve_status(self):
         """Raise if a work-queue solve sweep's wait ran out since the last
@@ -461,9 +463,9 @@ class BatchedSparseLDL:
                   _iptr(a), _iptr(b))
         return list(zip(a.tolist(), b.tolist()))
 
-    def set_solve_queue(self, on):
+    def set_solve_queue(self, mode):
         """See SparseLDL.set_solve_queue."""
-        _lib.call("ab_ldl_set_solve_queue", self._h, int(bool(on)))
+        _lib.call("ab_ldl_set_solve_queue", self._h, int(mode))
 
     def solve_status(self):
         _lib.call("ab_ldl_solve_status", self._h, _stream_ptr(self.device))

@@ -149,15 +149,22 @@ int ab_ldl_set_cluster_threshold(ab_ldl_t h, long long entries);
  * reference factors each front on one thread). */
 int ab_ldl_set_panel_mode(ab_ldl_t h, int mode, int min_rows);
 
-/* Solve sweeps over the elimination-tree levels whose fronts are all
- * solved one CTA per front (from the leaves): on (default), one
- * work-queue launch per sweep -- CTAs take fronts in dependency order from
- * an atomic counter and wait (bounded) for the fronts they depend on;
- * off, one launch per level.  Both give the same result bit for bit.
- * ab_ldl_solve_status reports (AB_ERR_CUDA) and clears a wait that ran
- * out since the last check; ab_ldl_factor also reports it.  No reference
- * counterpart (the reference solves front by front on the host). */
-int ab_ldl_set_solve_queue(ab_ldl_t h, int on);
+/* Solve schedule of the fronts solved without a cluster or the
+ * cooperative grid ("narrow"), mode bits (default 1):
+ *   bit 0: the sweeps over the levels whose fronts are all narrow (from
+ *          the leaves) are one work-queue launch each -- fronts are taken
+ *          in dependency order from an atomic counter and each waits
+ *          (bounded) for the fronts it depends on; without it, one launch
+ *          per level;
+ *   bit 1: fronts of at most 128 rows are solved by one warp each (four
+ *          per CTA) instead of one CTA each (measured slower on the
+ *          batched cart-pole KKT: the per-front steps are latency chains
+ *          that a whole CTA shortens).
+ * All modes give the same result bit for bit.  ab_ldl_solve_status
+ * reports (AB_ERR_CUDA) and clears a wait that ran out since the last
+ * check; ab_ldl_factor also reports it.  No reference counterpart (the
+ * reference solves front by front on the host). */
+int ab_ldl_set_solve_queue(ab_ldl_t h, int mode);
 int ab_ldl_solve_status(ab_ldl_t h, void* stream);
 
 /* The tensor-core Schur update on plain device arrays (column-major, FP32):

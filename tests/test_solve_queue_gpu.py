@@ -1,9 +1,10 @@
-"""Work-queue solve sweeps (one launch per sweep over the levels whose
-fronts are all solved one CTA per front) against one launch per level: the
-per-front arithmetic and the order of the children's update vectors are the
-same, so the solutions agree bit for bit -- on a batch of cart-pole KKT
-systems (every level narrow), on a 2D SIMP KKT (queue below the first level
-with cluster fronts) and with several right-hand sides."""
+"""Narrow-front solve schedules against one another: one launch per level
+or one work-queue launch per sweep (over the levels whose fronts are all
+narrow), each with one CTA per front or one warp per front of at most 128
+rows.  The per-front arithmetic and the order of the children's update
+vectors are the same in all four, so the solutions agree bit for bit -- on
+seeded KKT systems (one and several right-hand sides) and on a batch of
+cart-pole KKT systems (every level narrow, every front small)."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -15,15 +16,19 @@ pytestmark = pytest.mark.gpu
 
 
 def solve_both(ldl, b, n):
+    """Solutions with schedule modes 0 (per level, CTA fronts) and 3 (queue,
+    warp fronts); modes 1 and 2 must equal them too."""
     out = []
-    for on in (False, True):
-        ldl.set_solve_queue(on)
+    for mode in (0, 1, 2, 3):
+        ldl.set_solve_queue(mode)
         x = b.clone()
         ldl.solve_device(x)
         torch.cuda.synchronize()
         out.append(x.cpu().numpy())
     ldl.solve_status()
-    return out
+    for y in out[1:3]:
+        assert np.array_equal(y, out[0])
+    return out[0], out[3]
 
 
 def test_single_kkt_queue_equals_levels():
