@@ -94,7 +94,7 @@ class BctlOpts(ctypes.Structure):
 
 
 BCTL_RETIRED, BCTL_LIVE, BCTL_IC_PENDING, BCTL_REFINING, BCTL_STALLED, \
-    BCTL_SEARCHING = range(6)
+    BCTL_SEARCHING, BCTL_MISMATCH = range(7)
 BCTL_NFLAGS = 8
 
 _BC = ctypes.POINTER(BctlStruct)
@@ -108,6 +108,7 @@ _SIGS = {
     "ab_bctl_shift_diag": (_i, [_BC, _i, _vp, _vp, _vp, _vp, _vp]),
     "ab_bctl_ic_step": (_i, [_BC, _BO, _vp, _vp]),
     "ab_bctl_ic_end": (_i, [_BC, _vp]),
+    "ab_bctl_ic_check": (_i, [_BC, _vp, _vp]),
     "ab_bctl_refine_init": (_i, [_BC, _vp, _vp]),
     "ab_bctl_refine_step": (_i, [_BC, _vp, _i, _vp]),
     "ab_bctl_refine_stalled": (_i, [_BC, _vp]),

@@ -30,9 +30,9 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import (BCTL_IC_PENDING, BCTL_LIVE, BCTL_NFLAGS, BCTL_REFINING,
-                   BCTL_RETIRED, BCTL_SEARCHING, BCTL_STALLED, BctlOpts,
-                   BctlStruct)
+from ._lib import (BCTL_IC_PENDING, BCTL_LIVE, BCTL_MISMATCH, BCTL_NFLAGS,
+                   BCTL_REFINING, BCTL_RETIRED, BCTL_SEARCHING, BCTL_STALLED,
+                   BctlOpts, BctlStruct)
 from .linalg import OrderingType, _stream_ptr
 
 
@@ -62,7 +62,8 @@ class BatchEngine:
         self.precision = precision
         self.insts = []        # current layout, in batch order
         self.waiting = []      # admitted, not yet in the layout
-        self.fallbacks = 0
+        self.fallbacks = 0          # FP64 re-solves after a stalled refinement
+        self.inertia_fallbacks = 0  # FP64 refactorizations on an FP32 inertia mismatch
         self.rebuilds = 0
         self.rebuild_s = 0.0   # host + device time spent rebuilding layouts
         self._built = False
@@ -246,6 +247,42 @@ class BatchEngine:
                       self.px.data_ptr(), self.izl.data_ptr(), self.izu.data_ptr(),
                       self.stream)
 
+    def _factorize(self, force_fp64=False):
+        """Inertia-corrected factorization of every live instance's KKT
+        (Algorithm IC on the device).  With FP32 fronts, an attempt whose
+        inertia differs from the wanted one for any pending instance is
+        factored again in FP64 and the correction decides on the FP64
+        inertia (the mismatch may be an FP32 artefact); force_fp64 runs the
+        whole loop in FP64."""
+        dm, H, ldl, st = self.dm, self.H, self.ldl, self.st
+        copts = ctypes.byref(self.copts)
+        mixed = self.precision == "fp32"
+        if mixed and force_fp64:
+            ldl.set_precision("fp64")
+        self._ctl("ic_begin")
+        for attempt in range(41):
+            self._ctl("shift_diag", self.n, self.vinst32.data_ptr(),
+                      self.primal.data_ptr(), self.diag.data_ptr(), self.dtot.data_ptr())
+            dm.hessian(st.x, 1.0, H.vals)
+            H.add_diagonal(self.dtot)
+            ldl.factor(H.vals)
+            if mixed and not force_fp64:
+                self._ctl("clear_flags")
+                self._ctl("ic_check", ldl.inertia_device())
+                if self._flags()[BCTL_MISMATCH]:
+                    self.inertia_fallbacks += 1
+                    ldl.set_precision("fp64")
+                    ldl.factor(H.vals)
+                    ldl.set_precision("fp32")
+            self._ctl("clear_flags")
+            self._ctl("ic_step", copts, ldl.inertia_device())
+            if not self._flags()[BCTL_IC_PENDING]:
+                break
+        self._ctl("ic_end")
+        if mixed and force_fp64:
+            # the factor stays FP64 for this iteration's solves
+            ldl.set_precision("fp32")
+
     def _retire_marked(self):
         """Results of the instances ab_bctl_converge_barrier retired."""
         retire = self.ci["retire"].cpu().numpy()
@@ -295,20 +332,10 @@ class BatchEngine:
             return finished
         # inertia-corrected factorization
         opt.compute_diagonal(st, diag)
-        self._ctl("ic_begin")
-        for attempt in range(41):
-            self._ctl("shift_diag", n, self.vinst32.data_ptr(), primal.data_ptr(),
-                      diag.data_ptr(), dtot.data_ptr())
-            dm.hessian(st.x, 1.0, H.vals)
-            H.add_diagonal(dtot)
-            ldl.factor(H.vals)
-            self._ctl("clear_flags")
-            self._ctl("ic_step", copts, ldl.inertia_device())
-            if not self._flags()[BCTL_IC_PENDING]:
-                break
-        self._ctl("ic_end")
-        # Newton direction; a stalled refinement on FP32 fronts is redone on
-        # an FP64 refactorization of the same matrices
+        self._factorize()
+        # Newton direction; a stalled refinement on FP32 fronts is redone
+        # after the whole inertia correction in FP64 (the FP32 factor's
+        # accepted inertia may not be the FP64 factor's)
         from .ipm_driver import DeviceBackend
         steps = o["refine_steps"]
         if self.precision == "fp32":
@@ -319,12 +346,8 @@ class BatchEngine:
             self._ctl("refine_stalled")
             if self._flags()[BCTL_STALLED]:
                 self.fallbacks += 1
-                ldl.set_precision("fp64")
-                dm.hessian(st.x, 1.0, H.vals)
-                H.add_diagonal(dtot)
-                ldl.factor(H.vals)
+                self._factorize(force_fp64=True)
                 self._direction(st, steps)
-                ldl.set_precision("fp32")
         opt.compute_update(0.0, st, self.px, upd)
         # instances that have retired take no step
         self._ctl("mask_update", n, opt.np_, self.vinst32.data_ptr(),

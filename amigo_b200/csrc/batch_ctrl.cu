@@ -114,6 +114,13 @@ __global__ void k_ic_step(ab_bctl c, ab_bctl_opts o, const int* inertia) {
   }
 }
 
+__global__ void k_ic_check(ab_bctl c, const int* inertia) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= c.ninst || !c.pending[k]) return;
+  if (inertia[2 * k] != c.np_each[k] || inertia[2 * k + 1] != c.nc_each[k])
+    flag(c.flags, AB_BCTL_MISMATCH);
+}
+
 __global__ void k_ic_end(ab_bctl c) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= c.ninst) return;
@@ -247,6 +254,14 @@ int ab_bctl_ic_step(const ab_bctl* c, const ab_bctl_opts* o, const int* inertia,
   if (bad(c) || !o || !inertia) return AB_ERR_ARG;
   if (!c->ninst) return AB_OK;
   k_ic_step<<<grid(c->ninst), kT, 0, (cudaStream_t)stream>>>(*c, *o, inertia);
+  ab::count_launch();
+  return done();
+}
+
+int ab_bctl_ic_check(const ab_bctl* c, const int* inertia, void* stream) {
+  if (bad(c) || !inertia) return AB_ERR_ARG;
+  if (!c->ninst) return AB_OK;
+  k_ic_check<<<grid(c->ninst), kT, 0, (cudaStream_t)stream>>>(*c, inertia);
   ab::count_launch();
   return done();
 }

@@ -159,9 +159,10 @@ def solve_batch(model, device="cuda", options=None, verbose=False,
     per-instance arrays: converged, iterations, objective, kkt_error,
     inertia_corrections, plus time_s (all of it), setup_s (symbolic
     analysis, uploads), fallbacks (FP64 refactorizations of the
-    mixed-precision form) and x (host, concatenated).  precision "fp32"
-    factors with FP32 fronts and refines every direction against the FP64
-    KKT.  With `rescue`, an instance the batched driver leaves unconverged is
+    mixed-precision form after a stalled refinement), inertia_fallbacks
+    (FP64 refactorizations on an FP32 inertia mismatch) and x (host,
+    concatenated).  precision "fp32" factors with FP32 fronts and refines
+    every direction against the FP64 KKT.  With `rescue`, an instance the batched driver leaves unconverged is
     solved again, alone, by optimizer.Optimizer (amigo's default algorithm:
     heuristic barrier, filter line search, restoration) on the same GPU
     core; `rescued` marks them (their time is part of time_s)."""
@@ -193,7 +194,8 @@ def solve_batch(model, device="cuda", options=None, verbose=False,
                 objective=col("objective", float), kkt_error=col("kkt_error", float),
                 inertia_corrections=col("inertia_corrections", np.int64),
                 time_s=time.perf_counter() - t0, setup_s=t_setup, rescued=rescued,
-                fallbacks=eng.fallbacks, x=np.concatenate([r["x"] for r in R]))
+                fallbacks=eng.fallbacks, inertia_fallbacks=eng.inertia_fallbacks,
+                x=np.concatenate([r["x"] for r in R]))
 
 
 def _solve_reference_algorithm(m, dev):

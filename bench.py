@@ -546,6 +546,7 @@ def batch_solve_bench(device, k, sequential_sample=8, rank=0, world=1):
     mixed = {"solves_per_s": round(conv_m_all / wall_m, 3),
              "wall_s": round(wall_m, 3), "converged": int(rm["converged"].sum()),
              "fp64_fallbacks": int(rm["fallbacks"]),
+             "fp64_inertia_refactorizations": int(rm["inertia_fallbacks"]),
              "max_rel_objective_diff_vs_fp64": obj_dev,
              "max_kkt_error_converged": (float(rm["kkt_error"][rm["converged"]].max())
                                          if rm["converged"].any() else None)}

@@ -582,6 +582,7 @@ enum {
   AB_BCTL_REFINING = 3,    /* an instance takes another refinement step */
   AB_BCTL_STALLED = 4,     /* an instance's refinement ended above 1e-10 */
   AB_BCTL_SEARCHING = 5,   /* an instance's line search continues */
+  AB_BCTL_MISMATCH = 6,    /* a pending instance's inertia is not the wanted one */
   AB_BCTL_NFLAGS = 8
 };
 
@@ -616,6 +617,10 @@ int ab_bctl_shift_diag(const ab_bctl* c, int n, const int* vinst, const double* 
  * ab_ldl_inertia_device) */
 int ab_bctl_ic_step(const ab_bctl* c, const ab_bctl_opts* o, const int* inertia,
                     void* stream);
+/* sets AB_BCTL_MISMATCH when a pending instance's inertia differs from
+ * (np_each, nc_each); changes nothing else (the mixed-precision loop
+ * refactors in FP64 before deciding) */
+int ab_bctl_ic_check(const ab_bctl* c, const int* inertia, void* stream);
 /* dw_last = dw where an instance is live and dw > 0 */
 int ab_bctl_ic_end(const ab_bctl* c, void* stream);
 /* seg: ab_ipm_refine_init_seg's right-hand-side norms */

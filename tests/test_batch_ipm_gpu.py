@@ -38,3 +38,18 @@ def test_batch_of_one_equals_config_size():
     B = batch_config(k=1, seed=5, nmin=100, nmax=100)
     r = ipm_driver.solve_batch(B, "cuda:0")
     assert r["converged"].all() and r["kkt_error"][0] <= 1e-8
+
+
+def test_batch_mixed_precision_matches_fp64():
+    """FP32 fronts with FP64 refinement: every instance converges to the
+    FP64 batch's optimum (1e-9 relative objective, KKT error <= 1e-8).  An
+    attempt whose FP32 inertia is not the wanted one is refactored in FP64
+    before the inertia correction decides (counted in inertia_fallbacks)."""
+    B = batch_config(k=6, seed=3, nmin=50, nmax=150)
+    r64 = ipm_driver.solve_batch(B, "cuda:0", rescue=False)
+    r32 = ipm_driver.solve_batch(B, "cuda:0", precision="fp32", rescue=False)
+    assert r64["converged"].all() and r32["converged"].all()
+    assert (r32["kkt_error"] <= 1e-8).all()
+    rel = np.abs(r32["objective"] - r64["objective"]) / np.abs(r64["objective"])
+    assert rel.max() <= 1e-9, rel
+    assert r32["inertia_fallbacks"] >= 0 and r32["fallbacks"] >= 0
