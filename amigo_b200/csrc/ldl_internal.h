@@ -147,12 +147,13 @@ struct LdlHandle {
   // backward queue and its dependencies (parent in the queue, or -1), done
   // flags per node with an epoch per sweep, the queue counters and the
   // wait-ran-out word
-  // bit 0: work-queue sweeps (default on); bit 1: one warp per front of
-  // at most 128 rows (off: measured slower than one CTA per front)
+  // bit 0: work-queue sweeps (default on); bit 1: fronts of at most 128
+  // rows on 128-thread CTAs (off: measured slower)
   int solve_queue = 1;
-  int sv_qlevels = 0, sv_qcount = 0, sv_qsmem = 0, sv_qgrid = 0;
-  bool sv_qwarp = false, sv_qgrid_warp = false;
-  std::vector<int> sv_small_cnt;   // per level: narrow fronts solved by a warp
+  int sv_qlevels = 0, sv_qcount = 0, sv_qsmem = 0, sv_qgrid = 0, sv_qsmall_smem = 0;
+  bool sv_qsmall = false, sv_qgrid_small = false;
+  std::vector<int> sv_small_cnt;   // per level: narrow fronts of <= 128 rows
+  std::vector<int> sv_small_smem;  // per level: their front vector bytes
   std::vector<int> sv_bq_host, sv_dep_host;
   int* sv_bq = nullptr;
   int* sv_dep = nullptr;

@@ -196,6 +196,7 @@ __device__ __forceinline__ void pdl_enter() {
 // of the right-hand side plus the update vectors of its children, placed
 // by the same row map as the factorization's extend-add.  Called by a
 // whole CTA; V may be shared or global memory.
+template <int NTH = NT>
 __device__ void assemble_front_vector(const DevicePlan& d, int node, double* V,
                                       const double* xr, const double* ubuf,
                                       const long long* uoff, int rhs,
@@ -205,10 +206,10 @@ __device__ void assemble_front_vector(const DevicePlan& d, int node, double* V,
   const int ns = d.ns[node], ndin = d.ndin[node];
   const int fs = ns + ndin;
   const int* fsinv = d.ipool + d.ioff[node] + 2 * f;
-  for (int r = tid; r < f; r += NT) V[r] = 0.0;
+  for (int r = tid; r < f; r += NTH) V[r] = 0.0;
   __syncthreads();
   const int vb = d.var_ptr[node];
-  for (int r = tid; r < ns; r += NT) V[fsinv[r]] = xr[d.vars[vb + r]];
+  for (int r = tid; r < ns; r += NTH) V[fsinv[r]] = xr[d.vars[vb + r]];
   __syncthreads();
   if (tid == 0) *s_choff = ns;
   __syncthreads();
@@ -219,7 +220,7 @@ __device__ void assemble_front_vector(const DevicePlan& d, int node, double* V,
     const double* uc = ubuf + uoff[c] + (long long)rhs * fc + npc;
     const int cb = d.cptr[c];
     const int choff = *s_choff;
-    for (int a = tid; a < cc; a += NT) {
+    for (int a = tid; a < cc; a += NTH) {
       int pos;
       if (a < ndc) {
         pos = choff + a;
@@ -245,7 +246,7 @@ struct NarrowSmem {
 
 // Forward solve of one front by the whole CTA (sV: dynamic shared memory
 // of smem_doubles).
-template <class T>
+template <class T, int NTH = NT>
 __device__ void forward_front(const DevicePlan& d, int node, double* x, int nrhs,
                               int ldx, double* ubuf, const long long* uoff,
                               int smem_doubles, double* sV, NarrowSmem& sm) {
@@ -265,7 +266,7 @@ __device__ void forward_front(const DevicePlan& d, int node, double* x, int nrhs
     double* G = ubuf + uoff[node] + (long long)rhs * f;
     double* V = f <= smem_doubles ? sV : G;
     double* xr = x + (long long)rhs * ldx;
-    assemble_front_vector(d, node, V, xr, ubuf, uoff, rhs, &s_choff);
+    assemble_front_vector<NTH>(d, node, V, xr, ubuf, uoff, rhs, &s_choff);
 
     // Forward elimination with the unit lower factor.  The diagonal block
     // of each column block is staged in shared memory first, so that the
@@ -273,22 +274,22 @@ __device__ void forward_front(const DevicePlan& d, int node, double* x, int nrhs
     for (int jb = 0; jb < npiv;) {
       const int je = block_end(kind, jb, npiv);
       const int bw = je - jb;
-      for (int t = tid; t < bw * bw; t += NT) {
+      for (int t = tid; t < bw * bw; t += NTH) {
         const int i = t % bw, j = t / bw;
         sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
       }
-      for (int t = tid; t < bw; t += NT) sK[t] = kind[jb + t];
+      for (int t = tid; t < bw; t += NTH) sK[t] = kind[jb + t];
       __syncthreads();
       if (warp == 0) warp_lower_solve<2>(sL, SB + 1, sK, bw, V + jb, lane);
       __syncthreads();
-      for (int i = je + tid; i < f; i += NT)
+      for (int i = je + tid; i < f; i += NTH)
         V[i] -= dot_strided(L + i + (size_t)jb * f, (size_t)f, bw,
                             [&](int j) { return V[jb + j]; });
       __syncthreads();
       jb = je;
     }
     // D^{-1} and the pivots' forward values.
-    for (int j = tid; j < npiv; j += NT) {
+    for (int j = tid; j < npiv; j += NTH) {
       const int kd = kind[j];
       if (kd == 0) {
         V[j] = V[j] / L[j + (size_t)j * f];
@@ -303,31 +304,31 @@ __device__ void forward_front(const DevicePlan& d, int node, double* x, int nrhs
       }
     }
     __syncthreads();
-    for (int j = tid; j < npiv; j += NT) xr[decode_var(fvars[j])] = V[j];
+    for (int j = tid; j < npiv; j += NTH) xr[decode_var(fvars[j])] = V[j];
     if (V != G)
-      for (int r = npiv + tid; r < f; r += NT) G[r] = V[r];
+      for (int r = npiv + tid; r < f; r += NTH) G[r] = V[r];
     __syncthreads();
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(NT)
+template <class T, int NTH = NT>
+__global__ void __launch_bounds__(NTH)
 k_solve_forward(DevicePlan d, const int* __restrict__ nodes, double* x,
                 int nrhs, int ldx, double* ubuf, const long long* uoff,
                 int smem_doubles) {
   pdl_enter();
   extern __shared__ double sV[];
   __shared__ NarrowSmem sm;
-  forward_front<T>(d, nodes[blockIdx.x], x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
+  forward_front<T, NTH>(d, nodes[blockIdx.x], x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
 }
 
 // Backward solve of one front by the whole CTA.
-template <class T>
+template <class T, int NTH = NT>
 __device__ void backward_front(const DevicePlan& d, int node, double* x, int nrhs,
                                int ldx, double* ubuf, const long long* uoff,
                                int smem_doubles, double* sV, NarrowSmem& sm) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  constexpr int NWARP = NT / 32;
+  constexpr int NWARP = NTH / 32;
   const int f = d.f[node], npiv = d.npiv[node];
   const int* fvars = d.ipool + d.ioff[node];
   const int* kind = fvars + 3 * f;
@@ -340,8 +341,8 @@ __device__ void backward_front(const DevicePlan& d, int node, double* x, int nrh
     // pivots: their forward values (written to x by the forward sweep);
     // delayed and contribution rows: final values of the ancestors (from
     // L2: another CTA of the same sweep may have written them)
-    for (int r = tid; r < npiv; r += NT) V[r] = xr[decode_var(fvars[r])];
-    for (int r = npiv + tid; r < f; r += NT) V[r] = __ldcg(xr + fvars[r]);
+    for (int r = tid; r < npiv; r += NTH) V[r] = xr[decode_var(fvars[r])];
+    for (int r = npiv + tid; r < f; r += NTH) V[r] = __ldcg(xr + fvars[r]);
     __syncthreads();
     // Column blocks from the last one backwards.
     int je = npiv;
@@ -356,193 +357,38 @@ __device__ void backward_front(const DevicePlan& d, int node, double* x, int nrh
         if (lane == 0) V[j] -= acc;
       }
       const int bw = je - jb;
-      for (int t = tid; t < bw * bw; t += NT) {
+      for (int t = tid; t < bw * bw; t += NTH) {
         const int i = t % bw, j = t / bw;
         sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
       }
-      for (int t = tid; t < bw; t += NT) sK[t] = kind[jb + t];
+      for (int t = tid; t < bw; t += NTH) sK[t] = kind[jb + t];
       __syncthreads();
       // within the block, backwards: column j (or pair j-1, j)
       if (warp == 0) warp_upper_solve<2>(sL, SB + 1, sK, bw, V + jb, lane);
       __syncthreads();
       je = jb;
     }
-    for (int j = tid; j < npiv; j += NT) xr[decode_var(fvars[j])] = V[j];
+    for (int j = tid; j < npiv; j += NTH) xr[decode_var(fvars[j])] = V[j];
     __syncthreads();
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(NT)
+template <class T, int NTH = NT>
+__global__ void __launch_bounds__(NTH)
 k_solve_backward(DevicePlan d, const int* __restrict__ nodes, double* x,
                  int nrhs, int ldx, double* ubuf, const long long* uoff,
                  int smem_doubles) {
   pdl_enter();
   extern __shared__ double sV[];
   __shared__ NarrowSmem sm;
-  backward_front<T>(d, nodes[blockIdx.x], x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
+  backward_front<T, NTH>(d, nodes[blockIdx.x], x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
 }
 
-// ---------------------------------------------------------------------------
-// Small fronts (f <= kWarpRows): one warp per front, the same steps in the
-// same order as forward_front / backward_front (the blocked triangular
-// solves, the dot products of the rows below each block, D^{-1}), so the
-// results are the same bit for bit; CTAs of kWarpsPerCta warps, each with
-// its own slice of shared memory for the front vector and the staged
-// diagonal block.  Warps never wait for one another.
-constexpr int kWarpRows = 128;
-constexpr int kWarpsPerCta = 4;
-constexpr int kWarpSlice = kWarpRows + (SB + 1) * (SB + 1) + (SB + 2) / 2;  // doubles
-constexpr int kWarpSmem = kWarpsPerCta * kWarpSlice * (int)sizeof(double);
-
-template <class T>
-__device__ void forward_front_w(const DevicePlan& d, int node, double* x, int nrhs,
-                                int ldx, double* ubuf, const long long* uoff,
-                                double* slice) {
-  const int lane = threadIdx.x & 31;
-  const int f = d.f[node], npiv = d.npiv[node];
-  const int* fvars = d.ipool + d.ioff[node];
-  const int* kind = fvars + 3 * f;
-  const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
-  double* V = slice;
-  double* sL = slice + kWarpRows;
-  int* sK = reinterpret_cast<int*>(sL + (SB + 1) * (SB + 1));
-  const int ns = d.ns[node], ndin = d.ndin[node];
-  const int fs = ns + ndin;
-  const int* fsinv = d.ipool + d.ioff[node] + 2 * f;
-  const int vb = d.var_ptr[node];
-  for (int rhs = 0; rhs < nrhs; rhs++) {
-    double* G = ubuf + uoff[node] + (long long)rhs * f;
-    double* xr = x + (long long)rhs * ldx;
-    // front vector: own entries of the right-hand side, then the children's
-    // update vectors in order (assemble_front_vector, by one warp)
-    for (int r = lane; r < f; r += 32) V[r] = 0.0;
-    __syncwarp();
-    for (int r = lane; r < ns; r += 32) V[fsinv[r]] = xr[d.vars[vb + r]];
-    __syncwarp();
-    int choff = ns;
-    for (int q = d.kid_ptr[node]; q < d.kid_ptr[node + 1]; q++) {
-      const int c = d.kids[q];
-      const int fc = d.f[c], npc = d.npiv[c], ndc = d.ndel[c];
-      const int cc = fc - npc;
-      const double* uc = ubuf + uoff[c] + (long long)rhs * fc + npc;
-      const int cb = d.cptr[c];
-      for (int a = lane; a < cc; a += 32) {
-        int pos;
-        if (a < ndc) {
-          pos = choff + a;
-        } else {
-          int r0 = d.cmap[cb + a - ndc];
-          pos = r0 < ns ? r0 : r0 + ndin;
-        }
-        if (pos < fs) pos = fsinv[pos];
-        V[pos] += __ldcg(uc + a);
-      }
-      __syncwarp();
-      choff += ndc;
-    }
-    for (int jb = 0; jb < npiv;) {
-      const int je = block_end(kind, jb, npiv);
-      const int bw = je - jb;
-      for (int t = lane; t < bw * bw; t += 32) {
-        const int i = t % bw, j = t / bw;
-        sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
-      }
-      for (int t = lane; t < bw; t += 32) sK[t] = kind[jb + t];
-      __syncwarp();
-      warp_lower_solve<2>(sL, SB + 1, sK, bw, V + jb, lane);
-      __syncwarp();
-      for (int i = je + lane; i < f; i += 32)
-        V[i] -= dot_strided(L + i + (size_t)jb * f, (size_t)f, bw,
-                            [&](int j) { return V[jb + j]; });
-      __syncwarp();
-      jb = je;
-    }
-    for (int j = lane; j < npiv; j += 32) {
-      const int kd = kind[j];
-      if (kd == 0) {
-        V[j] = V[j] / L[j + (size_t)j * f];
-      } else if (kd == 1) {
-        const double d11 = L[j + (size_t)j * f];
-        const double d21 = L[j + 1 + (size_t)j * f];
-        const double d22 = L[j + 1 + (size_t)(j + 1) * f];
-        const double inv = inv2x2(d11, d21, d22);
-        const double x1 = V[j], x2 = V[j + 1];
-        V[j] = piv2_first(inv, d21, d22, x1, x2);
-        V[j + 1] = piv2_second(inv, d11, d21, x1, x2);
-      }
-    }
-    __syncwarp();
-    for (int j = lane; j < npiv; j += 32) xr[decode_var(fvars[j])] = V[j];
-    for (int r = npiv + lane; r < f; r += 32) G[r] = V[r];
-    __syncwarp();
-  }
-}
-
-template <class T>
-__device__ void backward_front_w(const DevicePlan& d, int node, double* x, int nrhs,
-                                 int ldx, double* slice) {
-  const int lane = threadIdx.x & 31;
-  const int f = d.f[node], npiv = d.npiv[node];
-  const int* fvars = d.ipool + d.ioff[node];
-  const int* kind = fvars + 3 * f;
-  const T* L = reinterpret_cast<const T*>(d.fpool) + d.foff[node];
-  double* V = slice;
-  double* sL = slice + kWarpRows;
-  int* sK = reinterpret_cast<int*>(sL + (SB + 1) * (SB + 1));
-  for (int rhs = 0; rhs < nrhs; rhs++) {
-    double* xr = x + (long long)rhs * ldx;
-    for (int r = lane; r < npiv; r += 32) V[r] = xr[decode_var(fvars[r])];
-    for (int r = npiv + lane; r < f; r += 32) V[r] = __ldcg(xr + fvars[r]);
-    __syncwarp();
-    int je = npiv;
-    while (je > 0) {
-      int jb = je - SB > 0 ? je - SB : 0;
-      if (jb > 0 && kind[jb] == 2) jb--;
-      for (int j = jb; j < je; j++) {
-        const double acc = warp_sum_down(
-            lane_dot(L + (size_t)j * f, je, f, lane, [&](int i) { return V[i]; }));
-        if (lane == 0) V[j] -= acc;
-      }
-      const int bw = je - jb;
-      for (int t = lane; t < bw * bw; t += 32) {
-        const int i = t % bw, j = t / bw;
-        sL[i + j * (SB + 1)] = L[jb + i + (size_t)(jb + j) * f];
-      }
-      for (int t = lane; t < bw; t += 32) sK[t] = kind[jb + t];
-      __syncwarp();
-      warp_upper_solve<2>(sL, SB + 1, sK, bw, V + jb, lane);
-      __syncwarp();
-      je = jb;
-    }
-    for (int j = lane; j < npiv; j += 32) xr[decode_var(fvars[j])] = V[j];
-    __syncwarp();
-  }
-}
-
-template <class T>
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
-k_solve_forward_w(DevicePlan d, const int* __restrict__ nodes, int cnt, double* x,
-                  int nrhs, int ldx, double* ubuf, const long long* uoff) {
-  pdl_enter();
-  extern __shared__ double wsm[];
-  const int w = threadIdx.x >> 5;
-  const int i = blockIdx.x * kWarpsPerCta + w;
-  if (i >= cnt) return;
-  forward_front_w<T>(d, nodes[i], x, nrhs, ldx, ubuf, uoff, wsm + w * kWarpSlice);
-}
-
-template <class T>
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
-k_solve_backward_w(DevicePlan d, const int* __restrict__ nodes, int cnt, double* x,
-                   int nrhs, int ldx) {
-  pdl_enter();
-  extern __shared__ double wsm[];
-  const int w = threadIdx.x >> 5;
-  const int i = blockIdx.x * kWarpsPerCta + w;
-  if (i >= cnt) return;
-  backward_front_w<T>(d, nodes[i], x, nrhs, ldx, wsm + w * kWarpSlice);
-}
+// Narrow fronts of at most kSmallRows rows run on CTAs of kSmallThreads
+// threads (more fronts in flight per SM; the same steps in the same order,
+// so the same bits).
+constexpr int kSmallRows = 128;
+constexpr int kSmallThreads = 128;
 
 // ---------------------------------------------------------------------------
 // Work-queue sweeps over the levels whose fronts are all narrow: one launch
@@ -591,8 +437,8 @@ __device__ __forceinline__ void mark_done(unsigned* flag, unsigned epoch) {
   if (threadIdx.x == 0) st_release(flag, epoch);
 }
 
-template <class T>
-__global__ void __launch_bounds__(NT)
+template <class T, int NTH = NT>
+__global__ void __launch_bounds__(NTH)
 k_solve_forward_q(DevicePlan d, const int* __restrict__ nodes, int count, double* x,
                   int nrhs, int ldx, double* ubuf, const long long* uoff,
                   int smem_doubles, unsigned* ctr, unsigned* done, unsigned epoch,
@@ -605,16 +451,16 @@ k_solve_forward_q(DevicePlan d, const int* __restrict__ nodes, int count, double
     const int idx = queue_next(ctr, count, &s_idx);
     if (idx < 0) break;
     const int node = nodes[idx];
-    for (int q = d.kid_ptr[node] + threadIdx.x; q < d.kid_ptr[node + 1]; q += NT)
+    for (int q = d.kid_ptr[node] + threadIdx.x; q < d.kid_ptr[node + 1]; q += NTH)
       wait_done(done + d.kids[q], epoch, err);
     __syncthreads();
-    forward_front<T>(d, node, x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
+    forward_front<T, NTH>(d, node, x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
     mark_done(done + node, epoch);
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(NT)
+template <class T, int NTH = NT>
+__global__ void __launch_bounds__(NTH)
 k_solve_backward_q(DevicePlan d, const int* __restrict__ nodes,
                    const int* __restrict__ dep, int count, double* x, int nrhs,
                    int ldx, double* ubuf, const long long* uoff, int smem_doubles,
@@ -629,66 +475,11 @@ k_solve_backward_q(DevicePlan d, const int* __restrict__ nodes,
     const int node = nodes[idx];
     if (threadIdx.x == 0 && dep[idx] >= 0) wait_done(done + dep[idx], epoch, err);
     __syncthreads();
-    backward_front<T>(d, node, x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
+    backward_front<T, NTH>(d, node, x, nrhs, ldx, ubuf, uoff, smem_doubles, sV, sm);
     mark_done(done + node, epoch);
   }
 }
 
-
-// The work-queue sweeps with one warp per front (every queued front has at
-// most kWarpRows rows): each warp takes fronts on its own.
-__device__ __forceinline__ int queue_next_w(unsigned* ctr, int count) {
-  unsigned v = 0;
-  if ((threadIdx.x & 31) == 0) v = atomicAdd(ctr, 1u);
-  const int idx = (int)__shfl_sync(0xffffffffu, v, 0);
-  return idx < count ? idx : -1;
-}
-
-__device__ __forceinline__ void mark_done_w(unsigned* flag, unsigned epoch) {
-  __threadfence();
-  __syncwarp();
-  if ((threadIdx.x & 31) == 0) st_release(flag, epoch);
-}
-
-template <class T>
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
-k_solve_forward_qw(DevicePlan d, const int* __restrict__ nodes, int count, double* x,
-                   int nrhs, int ldx, double* ubuf, const long long* uoff,
-                   unsigned* ctr, unsigned* done, unsigned epoch, int* err) {
-  pdl_enter();
-  extern __shared__ double wsm[];
-  double* slice = wsm + (threadIdx.x >> 5) * kWarpSlice;
-  const int lane = threadIdx.x & 31;
-  for (;;) {
-    const int idx = queue_next_w(ctr, count);
-    if (idx < 0) break;
-    const int node = nodes[idx];
-    for (int q = d.kid_ptr[node] + lane; q < d.kid_ptr[node + 1]; q += 32)
-      wait_done(done + d.kids[q], epoch, err);
-    __syncwarp();
-    forward_front_w<T>(d, node, x, nrhs, ldx, ubuf, uoff, slice);
-    mark_done_w(done + node, epoch);
-  }
-}
-
-template <class T>
-__global__ void __launch_bounds__(kWarpsPerCta * 32)
-k_solve_backward_qw(DevicePlan d, const int* __restrict__ nodes,
-                    const int* __restrict__ dep, int count, double* x, int nrhs,
-                    int ldx, unsigned* ctr, unsigned* done, unsigned epoch, int* err) {
-  pdl_enter();
-  extern __shared__ double wsm[];
-  double* slice = wsm + (threadIdx.x >> 5) * kWarpSlice;
-  for (;;) {
-    const int idx = queue_next_w(ctr, count);
-    if (idx < 0) break;
-    const int node = nodes[idx];
-    if ((threadIdx.x & 31) == 0 && dep[idx] >= 0) wait_done(done + dep[idx], epoch, err);
-    __syncwarp();
-    backward_front_w<T>(d, node, x, nrhs, ldx, slice);
-    mark_done_w(done + node, epoch);
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Mid-size fronts: one thread-block cluster of CS CTAs per front.  CTA 0
@@ -1226,21 +1017,25 @@ static int build_solve_schedule(LdlHandle& h, cudaStream_t s) {
     return 0;
   };
   h.sv_small_cnt.assign(L, 0);
+  h.sv_small_smem.assign(L, 0);
   for (int l = 0; l < L; l++) {
     h.sv_narrow_ptr[l] = (int)nodes.size();
-    int fm = 0;
-    // narrow fronts: the small ones (one warp each) first
+    int fm = 0, fsm = 0;
+    // narrow fronts: the small ones (kSmallThreads-thread CTAs) first
     for (int pass = 0; pass < 2; pass++)
       for (int q = h.level_ptr[l]; q < h.level_ptr[l + 1]; q++) {
         const int k = h.level_nodes[q];
-        if (cls(k) == 0 && (h.h_f[k] <= kWarpRows) == (pass == 0)) {
+        if (cls(k) == 0 && (h.h_f[k] <= kSmallRows) == (pass == 0)) {
           nodes.push_back(k);
-          if (pass == 0)
+          if (pass == 0) {
             h.sv_small_cnt[l]++;
-          else
+            fsm = std::max(fsm, h.h_f[k]);
+          } else {
             fm = std::max(fm, h.h_f[k]);
+          }
         }
       }
+    h.sv_small_smem[l] = fsm * 8;
     h.sv_narrow_smem[l] =
         (int)std::min<long long>((long long)fm * 8, kMaxDynSmem);
     h.sv_clu_ptr[l] = (int)nodes.size();
@@ -1278,9 +1073,13 @@ static int build_solve_schedule(LdlHandle& h, cudaStream_t s) {
   while (ql < L && h.sv_clu_ptr[ql] == h.sv_narrow_ptr[ql + 1]) ql++;
   h.sv_qlevels = ql >= 2 ? ql : 0;
   h.sv_qcount = h.sv_qlevels ? h.sv_narrow_ptr[h.sv_qlevels] : 0;
-  h.sv_qwarp = true;
-  for (int l = 0; l < h.sv_qlevels; l++)
-    if (h.sv_small_cnt[l] != h.sv_clu_ptr[l] - h.sv_narrow_ptr[l]) h.sv_qwarp = false;
+  h.sv_qsmall = true;
+  int qsm = 0;
+  for (int l = 0; l < h.sv_qlevels; l++) {
+    if (h.sv_small_cnt[l] != h.sv_clu_ptr[l] - h.sv_narrow_ptr[l]) h.sv_qsmall = false;
+    qsm = std::max(qsm, h.sv_small_smem[l]);
+  }
+  h.sv_qsmall_smem = qsm;
   if (h.sv_qcount) {
     const int qc = h.sv_qcount;
     // position of each queued node in the forward order
@@ -1394,49 +1193,48 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
     for (auto& e : ev) cudaEventCreate(&e);
   }
   const bool queue = (h.solve_queue & 1) && h.sv_qcount > 0;
-  const bool warps = (h.solve_queue & 2) != 0;
-  const bool qwarp = queue && warps && h.sv_qwarp;
+  const bool small = (h.solve_queue & 2) != 0;
+  const bool qsmall = queue && small && h.sv_qsmall;
+  const int qth = qsmall ? kSmallThreads : NT;
+  const int qsm = qsmall ? h.sv_qsmall_smem : h.sv_qsmem;
   const unsigned ep = h.sv_epoch + 1;
   if (queue) {
-    if (h.sv_qgrid == 0 || h.sv_qgrid_warp != qwarp) {
-      // CTAs resident at once, at most one per queued front (per
-      // kWarpsPerCta fronts with one warp each)
+    if (h.sv_qgrid == 0 || h.sv_qgrid_small != qsmall) {
+      // CTAs resident at once, at most one per queued front
       int dev = 0, sms = 0, per = 0;
       SCUDA(cudaGetDevice(&dev));
       SCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      if (qwarp)
+      if (qsmall)
         SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per, k_solve_forward_qw<T>, kWarpsPerCta * 32, (size_t)kWarpSmem));
+            &per, k_solve_forward_q<T, kSmallThreads>, kSmallThreads, (size_t)qsm));
       else
         SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_forward_q<T>, NT,
-                                                            (size_t)h.sv_qsmem));
-      const int need = qwarp ? (h.sv_qcount + kWarpsPerCta - 1) / kWarpsPerCta : h.sv_qcount;
-      h.sv_qgrid = std::max(1, std::min(need, sms * std::max(per, 1)));
-      h.sv_qgrid_warp = qwarp;
+                                                            (size_t)qsm));
+      h.sv_qgrid = std::max(1, std::min(h.sv_qcount, sms * std::max(per, 1)));
+      h.sv_qgrid_small = qsmall;
     }
     h.sv_epoch = ep;
     SCUDA(cudaMemsetAsync(h.sv_ctr, 0, 2 * sizeof(unsigned), s));
-    if (qwarp)
-      SCUDA(launch_pdl(k_solve_forward_qw<T>, dim3(h.sv_qgrid), dim3(kWarpsPerCta * 32),
-                       (size_t)kWarpSmem, s, d, (const int*)h.sv_nodes, h.sv_qcount, d_x,
-                       nrhs, ldx, h.ubuf, (const long long*)h.uoff, h.sv_ctr, h.sv_done,
+    if (qsmall)
+      SCUDA(launch_pdl(k_solve_forward_q<T, kSmallThreads>, dim3(h.sv_qgrid), dim3(qth),
+                       (size_t)qsm, s, d, (const int*)h.sv_nodes, h.sv_qcount, d_x, nrhs,
+                       ldx, h.ubuf, (const long long*)h.uoff, qsm / 8, h.sv_ctr, h.sv_done,
                        ep, h.sv_err));
     else
-      SCUDA(launch_pdl(k_solve_forward_q<T>, dim3(h.sv_qgrid), dim3(NT), (size_t)h.sv_qsmem,
-                       s, d, (const int*)h.sv_nodes, h.sv_qcount, d_x, nrhs, ldx, h.ubuf,
-                       (const long long*)h.uoff, h.sv_qsmem / 8, h.sv_ctr, h.sv_done, ep,
+      SCUDA(launch_pdl(k_solve_forward_q<T>, dim3(h.sv_qgrid), dim3(qth), (size_t)qsm, s, d,
+                       (const int*)h.sv_nodes, h.sv_qcount, d_x, nrhs, ldx, h.ubuf,
+                       (const long long*)h.uoff, qsm / 8, h.sv_ctr, h.sv_done, ep,
                        h.sv_err));
     ab::count_launch();
   }
   for (int l = queue ? h.sv_qlevels : 0; l < d.num_levels; l++) {
     if (trace) cudaEventRecord(ev[l], s);
     int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
-    if (warps && h.sv_small_cnt[l]) {
+    if (small && h.sv_small_cnt[l]) {
       const int sc = h.sv_small_cnt[l];
-      SCUDA(launch_pdl(k_solve_forward_w<T>, dim3((sc + kWarpsPerCta - 1) / kWarpsPerCta),
-                       dim3(kWarpsPerCta * 32), (size_t)kWarpSmem, s, d,
-                       (const int*)(h.sv_nodes + b), sc, d_x, nrhs, ldx, h.ubuf,
-                       (const long long*)h.uoff));
+      SCUDA(launch_pdl(k_solve_forward<T, kSmallThreads>, dim3(sc), dim3(kSmallThreads),
+                       (size_t)h.sv_small_smem[l], s, d, (const int*)(h.sv_nodes + b), d_x,
+                       nrhs, ldx, h.ubuf, (const long long*)h.uoff, h.sv_small_smem[l] / 8));
       ab::count_launch();
       b += sc;
       cnt -= sc;
@@ -1471,11 +1269,11 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
   for (int l = d.num_levels - 1; l >= (queue ? h.sv_qlevels : 0); l--) {
     if (trace) cudaEventRecord(ev[d.num_levels + 1 + (d.num_levels - 1 - l)], s);
     int b = h.sv_narrow_ptr[l], cnt = h.sv_clu_ptr[l] - b;
-    if (warps && h.sv_small_cnt[l]) {
+    if (small && h.sv_small_cnt[l]) {
       const int sc = h.sv_small_cnt[l];
-      SCUDA(launch_pdl(k_solve_backward_w<T>, dim3((sc + kWarpsPerCta - 1) / kWarpsPerCta),
-                       dim3(kWarpsPerCta * 32), (size_t)kWarpSmem, s, d,
-                       (const int*)(h.sv_nodes + b), sc, d_x, nrhs, ldx));
+      SCUDA(launch_pdl(k_solve_backward<T, kSmallThreads>, dim3(sc), dim3(kSmallThreads),
+                       (size_t)h.sv_small_smem[l], s, d, (const int*)(h.sv_nodes + b), d_x,
+                       nrhs, ldx, h.ubuf, (const long long*)h.uoff, h.sv_small_smem[l] / 8));
       ab::count_launch();
       b += sc;
       cnt -= sc;
@@ -1507,16 +1305,16 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
     }
   }
   if (queue) {
-    if (qwarp)
-      SCUDA(launch_pdl(k_solve_backward_qw<T>, dim3(h.sv_qgrid), dim3(kWarpsPerCta * 32),
-                       (size_t)kWarpSmem, s, d, (const int*)h.sv_bq, (const int*)h.sv_dep,
-                       h.sv_qcount, d_x, nrhs, ldx, h.sv_ctr + 1, h.sv_done + d.nn, ep,
-                       h.sv_err));
+    if (qsmall)
+      SCUDA(launch_pdl(k_solve_backward_q<T, kSmallThreads>, dim3(h.sv_qgrid), dim3(qth),
+                       (size_t)qsm, s, d, (const int*)h.sv_bq, (const int*)h.sv_dep,
+                       h.sv_qcount, d_x, nrhs, ldx, h.ubuf, (const long long*)h.uoff,
+                       qsm / 8, h.sv_ctr + 1, h.sv_done + d.nn, ep, h.sv_err));
     else
-      SCUDA(launch_pdl(k_solve_backward_q<T>, dim3(h.sv_qgrid), dim3(NT), (size_t)h.sv_qsmem,
-                       s, d, (const int*)h.sv_bq, (const int*)h.sv_dep, h.sv_qcount, d_x,
-                       nrhs, ldx, h.ubuf, (const long long*)h.uoff, h.sv_qsmem / 8,
-                       h.sv_ctr + 1, h.sv_done + d.nn, ep, h.sv_err));
+      SCUDA(launch_pdl(k_solve_backward_q<T>, dim3(h.sv_qgrid), dim3(qth), (size_t)qsm, s, d,
+                       (const int*)h.sv_bq, (const int*)h.sv_dep, h.sv_qcount, d_x, nrhs,
+                       ldx, h.ubuf, (const long long*)h.uoff, qsm / 8, h.sv_ctr + 1,
+                       h.sv_done + d.nn, ep, h.sv_err));
     ab::count_launch();
   }
   if (trace && queue) {

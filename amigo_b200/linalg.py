@@ -259,9 +259,9 @@ class SparseLDL:
 
     def set_solve_queue(self, mode):
         """Narrow-front solve schedule (ab_ldl_set_solve_queue): bit 0 one
-        work-queue launch per sweep over the all-narrow levels, bit 1 one
-        warp per front of at most 128 rows; default 1; every mode gives the
-        same result bit for bit."""
+        work-queue launch per sweep over the all-narrow levels, bit 1
+        fronts of at most 128 rows on 128-thread CTAs; default 1; every
+        mode gives the same result bit for bit."""
         _lib.call("ab_ldl_set_solve_queue", self._h, int(mode))
 
     def solve_status(self):

@@ -156,10 +156,9 @@ int ab_ldl_set_panel_mode(ab_ldl_t h, int mode, int min_rows);
  *          in dependency order from an atomic counter and each waits
  *          (bounded) for the fronts it depends on; without it, one launch
  *          per level;
- *   bit 1: fronts of at most 128 rows are solved by one warp each (four
- *          per CTA) instead of one CTA each (measured slower on the
- *          batched cart-pole KKT: the per-front steps are latency chains
- *          that a whole CTA shortens).
+ *   bit 1: fronts of at most 128 rows run on 128-thread CTAs instead of
+ *          256-thread ones (twice as many fronts in flight per SM;
+ *          measured slower on the batched cart-pole and 2D SIMP KKTs).
  * All modes give the same result bit for bit.  ab_ldl_solve_status
  * reports (AB_ERR_CUDA) and clears a wait that ran out since the last
  * check; ab_ldl_factor also reports it.  No reference counterpart (the

@@ -1,7 +1,7 @@
 """Narrow-front solve schedules against one another: one launch per level
 or one work-queue launch per sweep (over the levels whose fronts are all
-narrow), each with one CTA per front or one warp per front of at most 128
-rows.  The per-front arithmetic and the order of the children's update
+narrow), each with 256-thread CTAs for every front or 128-thread CTAs for
+the fronts of at most 128 rows.  The per-front arithmetic and the order of the children's update
 vectors are the same in all four, so the solutions agree bit for bit -- on
 seeded KKT systems (one and several right-hand sides) and on a batch of
 cart-pole KKT systems (every level narrow, every front small)."""
