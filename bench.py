@@ -700,7 +700,12 @@ def run_e2e(core, args, device):
     return {"value": round(flops / (ms * 1e-3) / 1e12, 6), "unit": "TFLOP/s",
             "ms_per_step": round(ms, 4),
             "h2d_bytes_per_step": int(8 * (m.nnz + m.n)),
-            "d2h_bytes_per_step": int(8 * m.n)}
+            "d2h_bytes_per_step": int(8 * m.n),
+            "work": "per step: KKT values and right-hand side copied in from pinned "
+                    "host memory, SparseLDL factor (inertia read back) and one solve, "
+                    "solution copied out; `value` times the whole IPM-iteration core "
+                    "(element kernels, factor, two solves, refinement, IPM vectors) "
+                    "on device-resident data"}
 
 
 # ---------------------------------------------------------- reference arm
