@@ -1,33 +1,35 @@
 // extern "C" entry points for the IPM vector kernels and CSR utilities
 // (include/amigo_b200.h).  The deterministic reductions need a small
-// per-device scratch array for block partials; it is allocated once per
-// device on first use and kept until process exit.
+// scratch array for block partials.  There is one per (device, stream):
+// calls on different streams may overlap, calls on one stream are ordered
+// by it.  Each is allocated on first use and kept until process exit.
 #include <cuda_runtime.h>
 
+#include <map>
 #include <mutex>
+#include <utility>
 
 #include "../../include/amigo_b200.h"
 #include "ipm_internal.h"
 
 namespace {
 
-constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
-double* g_scratch[kMaxDevices] = {nullptr};
+std::map<std::pair<int, void*>, double*> g_scratch;
 
-double* device_scratch() {
+double* device_scratch(void* stream) {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-    return nullptr;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return nullptr;
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch[dev]) {
+  double*& slot = g_scratch[std::make_pair(dev, stream)];
+  if (!slot) {
     void* p = nullptr;
     if (cudaMalloc(&p, (size_t)ab::ipm_scratch_doubles() * sizeof(double)) !=
         cudaSuccess)
       return nullptr;
-    g_scratch[dev] = static_cast<double*>(p);
+    slot = static_cast<double*>(p);
   }
-  return g_scratch[dev];
+  return slot;
 }
 
 bool bad(const ab_ipm_problem* p, const ab_ipm_state* s) {
@@ -43,7 +45,7 @@ int ab_ipm_residual(const ab_ipm_problem* p, const ab_ipm_state* s, double mu,
                     void* stream) {
   if (bad(p, s) || (p->n > 0 && (!grad || !res))) return AB_ERR_ARG;
   double* scratch = nullptr;
-  if (out2 && !(scratch = device_scratch())) return AB_ERR_CUDA;
+  if (out2 && !(scratch = device_scratch(stream))) return AB_ERR_CUDA;
   return ab::ipm_residual(p, s, mu, grad, res, out2, (cudaStream_t)stream,
                           scratch);
 }
@@ -66,7 +68,7 @@ int ab_ipm_max_step(const ab_ipm_problem* p, const ab_ipm_state* s,
                     const double* dzu, double* out, int* iout, void* stream) {
   if (bad(p, s) || !out || !iout || (p->np > 0 && (!px || !dzl || !dzu)))
     return AB_ERR_ARG;
-  double* scratch = device_scratch();
+  double* scratch = device_scratch(stream);
   if (!scratch) return AB_ERR_CUDA;
   return ab::ipm_max_step(p, s, tau, px, dzl, dzu, out, iout,
                           (cudaStream_t)stream, scratch);
@@ -88,7 +90,7 @@ int ab_ipm_reductions(const ab_ipm_problem* p, const ab_ipm_state* s,
                       double mu, const double* grad, double* out,
                       void* stream) {
   if (bad(p, s) || !out) return AB_ERR_ARG;
-  double* scratch = device_scratch();
+  double* scratch = device_scratch(stream);
   if (!scratch) return AB_ERR_CUDA;
   return ab::ipm_reductions(p, s, mu, grad, out, (cudaStream_t)stream,
                             scratch);
@@ -98,7 +100,7 @@ int ab_ipm_barrier_dphi(const ab_ipm_problem* p, const ab_ipm_state* s,
                         double mu, const double* grad, const double* px,
                         double* out, void* stream) {
   if (bad(p, s) || !out || (p->np > 0 && (!grad || !px))) return AB_ERR_ARG;
-  double* scratch = device_scratch();
+  double* scratch = device_scratch(stream);
   if (!scratch) return AB_ERR_CUDA;
   return ab::ipm_barrier_dphi(p, s, mu, grad, px, out, (cudaStream_t)stream,
                               scratch);
@@ -129,7 +131,7 @@ int ab_ipm_barrier_dphi_kkt(const ab_ipm_problem* p, const ab_ipm_state* s,
   if (bad(p, s) || !res || !px || !diag || !out ||
       (p->nc > 0 && !s->xlam))
     return AB_ERR_ARG;
-  double* scratch = device_scratch();
+  double* scratch = device_scratch(stream);
   if (!scratch) return AB_ERR_CUDA;
   return ab::ipm_barrier_dphi_kkt(p, s, res, px, diag, out,
                                   (cudaStream_t)stream, scratch);
@@ -188,7 +190,7 @@ int ab_ipm_refine_init(const ab_ipm_problem* p, const ab_ipm_state* s,
   if (bad(p, s) || !out || (p->n > 0 && (!grad || !rhs_saved || !px)) ||
       (p->np > 0 && (!dzl || !dzu)))
     return AB_ERR_ARG;
-  double* scratch = device_scratch();
+  double* scratch = device_scratch(stream);
   if (!scratch) return AB_ERR_CUDA;
   return ab::ipm_refine_init(p, s, mu, grad, rhs_saved, px, dzl, dzu, out,
                              (cudaStream_t)stream, scratch);
@@ -204,7 +206,7 @@ int ab_ipm_refine_residual(const ab_ipm_problem* p, const ab_ipm_state* s,
       (p->n > 0 && (!grad || !rhs_saved || !kpx || !px || !e_cond)) ||
       (p->np > 0 && (!dzl || !dzu || !e_zl || !e_zu)))
     return AB_ERR_ARG;
-  double* scratch = device_scratch();
+  double* scratch = device_scratch(stream);
   if (!scratch) return AB_ERR_CUDA;
   return ab::ipm_refine_residual(p, s, mu, grad, rhs_saved, kpx, px, dzl, dzu,
                                  e_cond, e_zl, e_zu, out, (cudaStream_t)stream,
@@ -234,7 +236,7 @@ int ab_ipm_refine_init_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
       (p->n > 0 && (!grad || !rhs_saved || !px)) ||
       (p->np > 0 && (!dzl || !dzu)))
     return AB_ERR_ARG;
-  double* scratch = device_scratch();
+  double* scratch = device_scratch(stream);
   if (!scratch) return AB_ERR_CUDA;
   return ab::ipm_refine_init(p, s, 0.0, grad, rhs_saved, px, dzl, dzu,
                              scratch + ab::ipm_scratch_doubles() - 8,
@@ -251,7 +253,7 @@ int ab_ipm_refine_residual_seg(const ab_ipm_problem* p, const ab_ipm_state* s,
       (p->n > 0 && (!grad || !rhs_saved || !kpx || !px || !e_cond)) ||
       (p->np > 0 && (!dzl || !dzu || !e_zl || !e_zu)))
     return AB_ERR_ARG;
-  double* scratch = device_scratch();
+  double* scratch = device_scratch(stream);
   if (!scratch) return AB_ERR_CUDA;
   return ab::ipm_refine_residual(p, s, 0.0, grad, rhs_saved, kpx, px, dzl,
                                  dzu, e_cond, e_zl, e_zu,
