@@ -166,3 +166,39 @@ def test_initialize_and_relax(oracle_ref):
     sl = v.sl.cpu().numpy()
     assert np.array_equal(sl[np.isfinite(lbx)], (x - lbx)[np.isfinite(lbx)])
     assert np.all(v.zl.cpu().numpy()[np.isfinite(lbx)] == 1.0)
+
+
+def test_reductions_on_two_streams_at_once():
+    """The reductions' block partials live in a scratch array per stream:
+    two problems reduced on two streams whose kernels overlap give the same
+    values as each alone on the default stream."""
+    from amigo_b200.ipm import InteriorPointOptimizer
+    probs = []
+    for seed in (11, 12):
+        mult, lower, upper = make_problem(300000, seed)
+        opt = InteriorPointOptimizer(mult, lower, upper, device="cuda:0")
+        v = make_state(opt, seed + 100)
+        g = dev(np.random.RandomState(seed).randn(opt.n))
+        probs.append((opt, v, g))
+    alone = [opt.compute_kkt_error_mu(0.05, v, g) + opt.compute_complementarity(v)
+             for opt, v, g in probs]
+    import threading
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    torch.cuda.synchronize()
+    outs = [[], []]
+
+    def work(i):
+        opt, v, g = probs[i]
+        with torch.cuda.stream(streams[i]):
+            for rep in range(20):
+                outs[i].append(opt.compute_kkt_error_mu(0.05, v, g) +
+                               opt.compute_complementarity(v))
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    torch.cuda.synchronize()
+    for i in range(2):
+        assert len(outs[i]) == 20 and all(o == alone[i] for o in outs[i])
