@@ -148,7 +148,7 @@ def solve(backend, options=None, verbose=False):
 
 
 def solve_batch(model, device="cuda", options=None, verbose=False,
-                precision="fp64", rescue=True):
+                precision="fp64", rescue=True, rescue_workers=4):
     """`solve` for every instance of a batch (problems.cartpole.CartPoleBatch)
     at once, on batch_engine.BatchEngine: each phase is one launch over all
     instances (the KKT matrices are factored together by the block-diagonal
@@ -162,10 +162,14 @@ def solve_batch(model, device="cuda", options=None, verbose=False,
     mixed-precision form after a stalled refinement), inertia_fallbacks
     (FP64 refactorizations on an FP32 inertia mismatch) and x (host,
     concatenated).  precision "fp32" factors with FP32 fronts and refines
-    every direction against the FP64 KKT.  With `rescue`, an instance the batched driver leaves unconverged is
-    solved again, alone, by optimizer.Optimizer (amigo's default algorithm:
-    heuristic barrier, filter line search, restoration) on the same GPU
-    core; `rescued` marks them (their time is part of time_s)."""
+    every direction against the FP64 KKT.  With `rescue`, an instance the
+    batched driver leaves unconverged is solved again, alone, by
+    optimizer.Optimizer (amigo's default algorithm: heuristic barrier,
+    filter line search, restoration) on the same GPU core; `rescued` marks
+    them (their time is part of time_s).  The re-solves run on
+    `rescue_workers` host threads, each with its own CUDA stream (every
+    re-solve is independent, so the results are those of the re-solves one
+    after another)."""
     from .batch_engine import BatchEngine
     dev = torch.device(device)
     t0 = time.perf_counter()
@@ -185,10 +189,11 @@ def solve_batch(model, device="cuda", options=None, verbose=False,
     R = [results[k] for k in range(model.k)]
     rescued = np.zeros(model.k, bool)
     if rescue:
-        for k, r in enumerate(R):
-            if not r["converged"]:
-                R[k] = _solve_reference_algorithm(model.inst[k], dev)
-                rescued[k] = True
+        todo = [k for k, r in enumerate(R) if not r["converged"]]
+        for k, r in zip(todo, _solve_reference_algorithm_many(
+                [model.inst[k] for k in todo], dev, rescue_workers)):
+            R[k] = r
+            rescued[k] = True
     col = lambda key, dt: np.array([r[key] for r in R], dtype=dt)
     return dict(converged=col("converged", bool), iterations=col("iterations", np.int64),
                 objective=col("objective", float), kkt_error=col("kkt_error", float),
@@ -196,6 +201,32 @@ def solve_batch(model, device="cuda", options=None, verbose=False,
                 time_s=time.perf_counter() - t0, setup_s=t_setup, rescued=rescued,
                 fallbacks=eng.fallbacks, inertia_fallbacks=eng.inertia_fallbacks,
                 x=np.concatenate([r["x"] for r in R]))
+
+
+def _solve_reference_algorithm_many(models, dev, workers):
+    """_solve_reference_algorithm for each model, on up to `workers` host
+    threads with one CUDA stream per thread (the library's calls take the
+    thread's current stream; its reductions keep scratch per stream)."""
+    if not models:
+        return []
+    if workers <= 1 or len(models) == 1:
+        return [_solve_reference_algorithm(m, dev) for m in models]
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+    local = threading.local()
+
+    def run(m):
+        s = getattr(local, "stream", None)
+        if s is None:
+            s = local.stream = torch.cuda.Stream(device=dev)
+        with torch.cuda.stream(s):
+            r = _solve_reference_algorithm(m, dev)
+            s.synchronize()
+        return r
+
+    torch.cuda.synchronize(dev)
+    with ThreadPoolExecutor(max_workers=min(workers, len(models))) as ex:
+        return list(ex.map(run, models))
 
 
 def _solve_reference_algorithm(m, dev):

@@ -53,3 +53,17 @@ def test_batch_mixed_precision_matches_fp64():
     rel = np.abs(r32["objective"] - r64["objective"]) / np.abs(r64["objective"])
     assert rel.max() <= 1e-9, rel
     assert r32["inertia_fallbacks"] >= 0 and r32["fallbacks"] >= 0
+
+
+def test_threaded_reference_resolves_equal_sequential():
+    """Re-solves by optimizer.Optimizer on several host threads (one CUDA
+    stream each) give the results of the same re-solves one after
+    another, bit for bit."""
+    B = batch_config(k=3, seed=9, nmin=50, nmax=120)
+    seq = ipm_driver._solve_reference_algorithm_many(B.inst, "cuda:0", 1)
+    par = ipm_driver._solve_reference_algorithm_many(B.inst, "cuda:0", 3)
+    for a, b in zip(seq, par):
+        assert a["converged"] and b["converged"]
+        assert a["iterations"] == b["iterations"]
+        assert a["objective"] == b["objective"]
+        assert np.array_equal(a["x"], b["x"])
