@@ -30,3 +30,18 @@ def test_results_same_alone_and_in_the_mix():
         assert abs(r["objective"] - ref) <= 1e-12 * max(1.0, abs(ref))
         assert np.abs(r["x"] - alone["x"]).max() <= 1e-12 * max(1.0, np.abs(alone["x"]).max())
         assert r["latency_s"] > 0.0
+
+
+def test_unconverged_requests_resolved_when_asked():
+    """rescue=True: a request the batched driver leaves unconverged (here
+    forced by a 5-iteration limit) is solved again by optimizer.Optimizer on
+    a worker thread while the batch keeps stepping, and converges."""
+    reqs = serve.make_stream(4, rate=100.0, seed=3, nmin=50, nmax=80)
+    srv = serve.Server("cuda:0", max_batch=4, admit_min=1, max_wait_s=0.01,
+                       options={"max_iter": 5}, rescue=True, rescue_workers=2)
+    res, summ = srv.run(reqs, time_limit=600)
+    assert summ["completed"] == len(reqs) and summ["rescued"] == len(reqs)
+    assert summ["converged"] == len(reqs)
+    for q in reqs:
+        r = res[q.id]
+        assert r["rescued"] and r["converged"] and r["latency_s"] > 0.0
