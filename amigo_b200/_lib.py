@@ -119,6 +119,8 @@ _SIGS = {
     "ab_ldl_inertia_device": (_i, [_vp, ctypes.POINTER(_vp)]),
     "ab_ldl_set_solve_queue": (_i, [_vp, _i]),
     "ab_ldl_solve_status": (_i, [_vp, _vp]),
+    "ab_ldl_autotune": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "ab_ldl_apply_tuning": (_i, [_vp, _vp]),
     "ab_ldl_create": (_i, [_i, _ip, _ip, _i, _i, _d, _d, _d, ctypes.POINTER(_vp)]),
     "ab_ldl_analyze": (_i, [_i, _ip, _ip, _i, ctypes.POINTER(_vp)]),
     "ab_ldl_destroy": (_i, [_vp]),

@@ -487,6 +487,254 @@ int ab_ldl_set_panel_mode(ab_ldl_t h, int mode, int min_rows) {
   return AB_OK;
 }
 
+// ---- autotuner ----------------------------------------------------------
+extern "C++" {
+namespace {
+
+struct Tuning {
+  int panel_mode, cl_min_rows, panel_cache;
+  long long cluster_entries, wide_entries;
+  int solve_queue;
+};
+
+Tuning get_tuning(const ab::LdlHandle& h) {
+  return {h.panel_mode, h.cl_min_rows, h.panel_cache_bytes, h.cluster_entries,
+          h.wide_entries, h.solve_queue};
+}
+
+void set_tuning(ab::LdlHandle& h, const Tuning& t) {
+  h.panel_mode = t.panel_mode;
+  h.cl_min_rows = t.cl_min_rows;
+  h.panel_cache_bytes = t.panel_cache;
+  if (h.cluster_entries != t.cluster_entries || h.wide_entries != t.wide_entries ||
+      h.solve_queue != t.solve_queue)
+    h.solve_epoch = -1;   // the solve schedule is rebuilt on the next solve
+  h.cluster_entries = t.cluster_entries;
+  h.wide_entries = t.wide_entries;
+  h.solve_queue = t.solve_queue;
+}
+
+// Best of `reps` event-timed runs of f() on stream s (after one untimed
+// run), in ms; the first non-zero status of f is returned in *rc.
+template <class F>
+double best_ms(cudaStream_t s, int reps, cudaEvent_t e0, cudaEvent_t e1, int* rc, F f) {
+  *rc = f();
+  if (*rc) return 0.0;
+  double best = 1e300;
+  for (int r = 0; r < reps; r++) {
+    if (cudaEventRecord(e0, s) != cudaSuccess) { *rc = AB_ERR_CUDA; return 0.0; }
+    *rc = f();
+    if (*rc) return 0.0;
+    float ms = 0.f;
+    if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      *rc = AB_ERR_CUDA;
+      return 0.0;
+    }
+    best = std::min(best, (double)ms);
+  }
+  return best;
+}
+
+}  // namespace
+}  // extern "C++"
+
+int ab_ldl_autotune(ab_ldl_t H, const double* d_vals, int reps, void* stream,
+                    ab_ldl_tuning* out) {
+  if (!H || reps < 1 || (!d_vals && H->h.d.nnz > 0)) return AB_ERR_ARG;
+  if (!H->h.has_plan) return AB_ERR_UNSUPPORTED;
+  ab::LdlHandle& h = H->h;
+  cudaStream_t s = (cudaStream_t)stream;
+  const Tuning start = get_tuning(h);
+  ab_ldl_tuning rep{};
+  if (h.sym.n == 0) {
+    h.factored = true;
+    if (out) *out = rep;
+    return AB_OK;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double* x = nullptr;
+  int rc = AB_OK;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess ||
+      cudaMalloc((void**)&x, (size_t)h.sym.n * sizeof(double)) != cudaSuccess) {
+    rc = AB_ERR_CUDA;
+  }
+  // the timed solves run on a zero right-hand side (their arithmetic does
+  // not depend on the values)
+  if (!rc && cudaMemsetAsync(x, 0, (size_t)h.sym.n * sizeof(double), s) != cudaSuccess)
+    rc = AB_ERR_CUDA;
+  auto factor = [&]() {
+    h.factored = false;
+    return ab::factor_numeric(h, d_vals, s);
+  };
+  auto solve = [&]() { return ab::solve_numeric(h, x, 1, h.sym.n, s); };
+  int timed = 0;
+  Tuning best = start;
+  double fbest = 0.0, f0 = 0.0;
+  bool factored_best = false;   // the handle's factor is of `best`
+  if (!rc) {
+    fbest = f0 = best_ms(s, reps, e0, e1, &rc, factor);
+    factored_best = true;
+    timed++;
+  }
+  // factor candidates: only patterns with a level of large fronts (the
+  // small-front kernel has no setting here)
+  int big_max = 0;
+  for (const auto& L : h.sched)
+    if (L.nbig > 0) big_max = std::max(big_max, L.big_max_f);
+  if (!rc && big_max > 0) {
+    std::vector<Tuning> cand;
+    // the one-CTA panel, then the cluster panels' row threshold
+    Tuning t = start;
+    t.panel_mode = 1;
+    cand.push_back(t);
+    const int rows[] = {512, 768, 1024, 1536, 2048};
+    for (int r : rows) {
+      t = start;
+      t.panel_mode = 0;
+      t.cl_min_rows = r;
+      cand.push_back(t);
+    }
+    // a threshold matters only through the levels it moves: keep one
+    // candidate per distinct set of large-front levels on cluster panels
+    auto signature = [&](const Tuning& c) {
+      std::vector<char> sig;
+      for (const auto& L : h.sched)
+        sig.push_back(L.nbig > 0 && c.panel_mode == 0 && L.big_max_f >= c.cl_min_rows);
+      return sig;
+    };
+    std::vector<std::vector<char>> seen{signature(start)};
+    for (const Tuning& c : cand) {
+      if (rc) break;
+      const auto sg = signature(c);
+      if (c.panel_mode == start.panel_mode &&
+          std::find(seen.begin(), seen.end(), sg) != seen.end())
+        continue;
+      if (c.panel_mode == 0) seen.push_back(sg);
+      set_tuning(h, c);
+      const double ms = best_ms(s, reps, e0, e1, &rc, factor);
+      timed++;
+      if (!rc && ms < 0.98 * fbest) {
+        fbest = ms;
+        best = c;
+        factored_best = true;
+      } else {
+        factored_best = false;
+      }
+    }
+    // the shared-memory copy of the panel's columns, on the chosen form
+    if (!rc) {
+      Tuning c = best;
+      c.panel_cache = best.panel_cache ? 0 : 96 * 1024;
+      set_tuning(h, c);
+      const double ms = best_ms(s, reps, e0, e1, &rc, factor);
+      timed++;
+      if (!rc && ms < 0.98 * fbest) {
+        fbest = ms;
+        best = c;
+        factored_best = true;
+      } else {
+        factored_best = false;
+      }
+    }
+    if (!rc) {
+      set_tuning(h, best);
+      if (!factored_best) rc = factor();
+    }
+  }
+  // solve candidates, one knob at a time on the chosen factorization
+  double sbest = 0.0, s0 = 0.0;
+  if (!rc) {
+    set_tuning(h, best);
+    sbest = s0 = best_ms(s, reps, e0, e1, &rc, solve);
+    timed++;
+  }
+  auto try_solve = [&](const Tuning& c) {
+    if (rc) return;
+    set_tuning(h, c);
+    const double ms = best_ms(s, reps, e0, e1, &rc, solve);
+    timed++;
+    if (!rc && ms < 0.98 * sbest) {
+      sbest = ms;
+      best = c;
+    }
+  };
+  {
+    const long long wide[] = {1LL << 20, 1LL << 21, 1LL << 22, 1LL << 23, 1LL << 24, 1LL << 26};
+    const Tuning base = best;
+    for (long long w : wide)
+      if (w != base.wide_entries) {
+        Tuning c = base;
+        c.wide_entries = w;
+        try_solve(c);
+      }
+  }
+  {
+    const long long clu[] = {1LL << 12, 1LL << 13, 1LL << 14, 1LL << 15, 1LL << 16};
+    const Tuning base = best;
+    for (long long v : clu)
+      if (v != base.cluster_entries) {
+        Tuning c = base;
+        c.cluster_entries = v;
+        try_solve(c);
+      }
+  }
+  {
+    const int modes[] = {0, 1, 3};
+    const Tuning base = best;
+    for (int m : modes)
+      if (m != base.solve_queue) {
+        Tuning c = base;
+        c.solve_queue = m;
+        try_solve(c);
+      }
+  }
+  if (!rc && h.sv_err) {
+    // a work-queue sweep whose dependency wait ran out: report it
+    int e = 0;
+    if (cudaMemcpyAsync(&e, h.sv_err, sizeof(int), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess || e) {
+      if (e) cudaMemsetAsync(h.sv_err, 0, sizeof(int), s);
+      rc = AB_ERR_CUDA;
+    }
+  }
+  if (!rc) {
+    set_tuning(h, best);
+    if (out) {
+      rep.panel_mode = best.panel_mode;
+      rep.cl_min_rows = best.cl_min_rows;
+      rep.panel_cache_bytes = best.panel_cache;
+      rep.cluster_entries = best.cluster_entries;
+      rep.wide_entries = best.wide_entries;
+      rep.solve_queue = best.solve_queue;
+      rep.factor_ms = fbest;
+      rep.solve_ms = sbest;
+      rep.factor_ms_initial = f0;
+      rep.solve_ms_initial = s0;
+      rep.configurations = timed;
+      *out = rep;
+    }
+  } else {
+    set_tuning(h, start);
+  }
+  if (x) cudaFree(x);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  return rc;
+}
+
+int ab_ldl_apply_tuning(ab_ldl_t H, const ab_ldl_tuning* t) {
+  if (!H || !t || t->panel_mode < 0 || t->panel_mode > 3 || t->cl_min_rows < 1 ||
+      t->panel_cache_bytes < 0 || t->panel_cache_bytes > 200 * 1024 ||
+      t->cluster_entries < 1 || t->wide_entries < 1 || t->solve_queue < 0 ||
+      t->solve_queue > 3)
+    return AB_ERR_ARG;
+  set_tuning(H->h, {t->panel_mode, t->cl_min_rows, t->panel_cache_bytes,
+                    t->cluster_entries, t->wide_entries, t->solve_queue});
+  return AB_OK;
+}
+
 int ab_ldl_stats(ab_ldl_t H, void* stream, double* flops,
                  double* factor_entries, int* max_front, int* num_delayed,
                  int* levels) {

@@ -176,6 +176,53 @@ class CSRMat:
                   yd.data_ptr(), _stream_ptr(self.device))
 
 
+class LdlTuning(ctypes.Structure):
+    """ab_ldl_tuning (include/amigo_b200.h)."""
+    _fields_ = [("panel_mode", ctypes.c_int), ("cl_min_rows", ctypes.c_int),
+                ("panel_cache_bytes", ctypes.c_int),
+                ("cluster_entries", ctypes.c_longlong),
+                ("wide_entries", ctypes.c_longlong), ("solve_queue", ctypes.c_int),
+                ("factor_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
+                ("factor_ms_initial", ctypes.c_double),
+                ("solve_ms_initial", ctypes.c_double),
+                ("configurations", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# Settings found by the autotuner, per pattern and precision: a later
+# handle of the same pattern takes them without timing again.
+_TUNED = {}
+
+
+def _pattern_key(rowps, colss, precision):
+    import hashlib
+    hsh = hashlib.blake2b(digest_size=16)
+    for rp, cl in zip(rowps, colss):
+        hsh.update(np.ascontiguousarray(rp, dtype=np.int32).tobytes())
+        hsh.update(np.ascontiguousarray(cl, dtype=np.int32).tobytes())
+    return (len(rowps), hsh.hexdigest(), precision)
+
+
+def _autotune(h, vals, device, key, reps, cache):
+    """ab_ldl_autotune on the handle (or the cached settings of its
+    pattern, then one factorization); returns the settings as a dict with
+    'cached' set accordingly."""
+    t = LdlTuning()
+    with torch.cuda.device(device):
+        if cache and key in _TUNED:
+            t = _TUNED[key]
+            _lib.call("ab_ldl_apply_tuning", h, ctypes.byref(t))
+            _lib.call("ab_ldl_factor", h, vals.data_ptr(), _stream_ptr(device))
+            return dict(t.as_dict(), cached=True)
+        _lib.call("ab_ldl_autotune", h, vals.data_ptr(), int(reps),
+                  _stream_ptr(device), ctypes.byref(t))
+    if cache:
+        _TUNED[key] = t
+    return dict(t.as_dict(), cached=False)
+
+
 class SparseLDL:
     """amigo.SparseLDL on the GPU (include/sparse_ldl.h:20).
 
@@ -225,6 +272,7 @@ class SparseLDL:
             _lib.call("ab_ldl_factor", self._h, self.mat.vals.data_ptr(),
                       _stream_ptr(self.device))
         self._factored = True
+        self.factor_count = getattr(self, "factor_count", 0) + 1
         return 0
 
     def get_inertia(self):
@@ -300,6 +348,21 @@ class SparseLDL:
                   _iptr(a), _iptr(b))
         return a, b
 
+    def autotune(self, reps=3, cache=True):
+        """Pick the large-front panel form and the solve schedule for this
+        pattern by timing them on mat's current values
+        (ab_ldl_autotune); the handle is left factored with the chosen
+        settings.  Panel forms change the factorization only to rounding,
+        the solve thresholds the solution only to rounding.  With
+        `cache`, a later SparseLDL of the same pattern and precision takes
+        the stored settings without timing.  Returns the settings and the
+        best factor / solve times before and after (ms)."""
+        key = _pattern_key([self.mat.rowp], [self.mat.cols], self.precision)
+        out = _autotune(self._h, self.mat.vals, self.device, key, reps, cache)
+        self._factored = True
+        self.factor_count = getattr(self, "factor_count", 0) + 1
+        return out
+
     def solve_device(self, xd):
         """Solve in place on a device tensor of shape (n,) or (nrhs, n)
         (rows contiguous: each right-hand side is one contiguous column of
@@ -335,6 +398,52 @@ class SparseLDL:
                 x[:, :] = out.T
             return
         raise RuntimeError("Expected either a NumPy array or amigo_b200.Vector")
+
+
+class SolveGraph:
+    """A solve on one device buffer captured as a CUDA graph.
+
+    ``g = SolveGraph(ldl, xd)``; ``g()`` solves in place on ``xd`` (as
+    ``ldl.solve_device(xd)``, same bits) by replaying the graph on the
+    current stream.  The solve's launch schedule depends on the front sizes
+    of the factorization (delayed pivots), so the graph is captured again
+    on the first call after each ``ldl.factor()``; replays between
+    factorizations cost one graph launch instead of one launch per level
+    and sweep.  The work-queue sweeps take their epoch from device memory,
+    so every replay is a fresh sweep.  ``ab_launch_count`` counts the
+    captured kernels once, at capture."""
+
+    def __init__(self, ldl, xd):
+        if xd.dtype != torch.float64 or not xd.is_cuda or not xd.is_contiguous():
+            raise TypeError("expected a contiguous float64 CUDA tensor")
+        self.ldl = ldl
+        self.xd = xd
+        self.graph = None
+        self._count = None
+        self.captures = 0
+        self.replays = 0
+
+    def _capture(self):
+        ldl, xd = self.ldl, self.xd
+        # the host-side schedule of this factorization is built by one solve
+        # outside the capture (on a copy)
+        warm = xd.clone()
+        ldl.solve_device(warm)
+        torch.cuda.current_stream(ldl.device).synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.device(ldl.device):
+            with torch.cuda.graph(g):
+                ldl.solve_device(xd)
+        self.graph = g
+        self._count = getattr(ldl, "factor_count", 0)
+        self.captures += 1
+
+    def __call__(self):
+        if self.graph is None or self._count != getattr(self.ldl, "factor_count", 0):
+            self.graph = None
+            self._capture()
+        self.graph.replay()
+        self.replays += 1
 
 
 def symbolic_arrays(h):
@@ -444,6 +553,7 @@ class BatchedSparseLDL:
         """Front precision ("fp64" default, or "fp32" mixed)."""
         bits = {"fp64": 64, "fp32": 32, 64: 64, 32: 32}[precision]
         _lib.call("ab_ldl_set_precision", self._h, bits)
+        self.precision = "fp64" if bits == 64 else "fp32"
 
     def set_tensor_cores(self, on):
         _lib.call("ab_ldl_set_tensor_cores", self._h, int(bool(on)))
@@ -454,7 +564,17 @@ class BatchedSparseLDL:
         with torch.cuda.device(self.device):
             _lib.call("ab_ldl_factor", self._h, vals.data_ptr(),
                       _stream_ptr(self.device))
+        self.factor_count = getattr(self, "factor_count", 0) + 1
         return 0
+
+    def autotune(self, vals, reps=3, cache=True):
+        """See SparseLDL.autotune; `vals` are the concatenated values."""
+        if vals.numel() != self.nnz or vals.dtype != torch.float64:
+            raise ValueError("expected the concatenated float64 values")
+        key = _pattern_key(self._rowp, self._cols, getattr(self, "precision", "fp64"))
+        out = _autotune(self._h, vals, self.device, key, reps, cache)
+        self.factor_count = getattr(self, "factor_count", 0) + 1
+        return out
 
     def get_inertia(self):
         a = np.zeros(self.k, np.int32)

@@ -166,6 +166,38 @@ int ab_ldl_set_panel_mode(ab_ldl_t h, int mode, int min_rows);
 int ab_ldl_set_solve_queue(ab_ldl_t h, int mode);
 int ab_ldl_solve_status(ab_ldl_t h, void* stream);
 
+/* Launch forms and thresholds picked by ab_ldl_autotune for one pattern. */
+typedef struct {
+  int panel_mode, cl_min_rows, panel_cache_bytes; /* factor: large-front panels */
+  long long cluster_entries, wide_entries;        /* solve: front classes */
+  int solve_queue;                                /* solve: narrow-front schedule */
+  double factor_ms, solve_ms;                 /* chosen settings, best of reps */
+  double factor_ms_initial, solve_ms_initial; /* settings on entry */
+  int configurations;                         /* settings timed */
+} ab_ldl_tuning;
+
+/* Autotuner: times the factorization of the KKT values d_vals (device, as
+ * for ab_ldl_factor) under the large-front panel forms (one-CTA panels,
+ * or cluster panels from 512 / 768 / 1,024 / 1,536 / 2,048 rows, with and
+ * without the shared-memory column copy), then one solve under the solve
+ * knobs (cooperative-grid threshold, cluster threshold, work-queue and
+ * 128-thread schedules), one knob at a time, best of `reps` (>= 1) each on
+ * `stream`, and keeps the fastest (a setting replaces the current one only
+ * when it is at least 2% faster).  Patterns without large fronts skip the
+ * factor candidates.  The chosen settings stay on the handle, which is
+ * left factored with them; *out (may be NULL) reports them.  Panel forms
+ * change the factorization to rounding (different panel widths; the same
+ * pivot tests); the solve thresholds change the solution to rounding (a
+ * front's class sets its reduction order) and the narrow-front schedules
+ * not at all.  On an error the settings on entry are restored.
+ * Allocates one n-vector of device memory for the timed solves.  No
+ * reference counterpart (the reference has one fixed host schedule). */
+int ab_ldl_autotune(ab_ldl_t h, const double* d_vals, int reps, void* stream,
+                    ab_ldl_tuning* out);
+/* Applies settings from ab_ldl_autotune (e.g. of another handle with the
+ * same pattern). */
+int ab_ldl_apply_tuning(ab_ldl_t h, const ab_ldl_tuning* t);
+
 /* The tensor-core Schur update on plain device arrays (column-major, FP32):
  * lower(C) -= A B^T for n x kw panels A, B (kw <= 31), as 3xTF32 tcgen05
  * products accumulated in FP32 in tensor memory -- the update the
