@@ -158,9 +158,8 @@ struct LdlHandle {
   int* sv_bq = nullptr;
   int* sv_dep = nullptr;
   unsigned* sv_done = nullptr;   // 2 x nn: forward, backward
-  unsigned* sv_ctr = nullptr;    // 2
+  unsigned* sv_ctr = nullptr;    // 4: forward and backward counters, epoch, pad
   int* sv_err = nullptr;
-  unsigned sv_epoch = 0;
 };
 
 int build_plan(LdlHandle& h, const int* rowp, const int* cols);

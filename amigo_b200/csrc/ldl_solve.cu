@@ -437,16 +437,28 @@ __device__ __forceinline__ void mark_done(unsigned* flag, unsigned epoch) {
   if (threadIdx.x == 0) st_release(flag, epoch);
 }
 
+// Start of a solve's two queued sweeps: zero both queue counters and move
+// to the next epoch (ctr[2]).  The epoch lives in device memory, so a
+// captured CUDA graph of a solve takes a new epoch on every replay.
+__global__ void k_sweep_begin(unsigned* ctr) {
+  if (threadIdx.x == 0) {
+    ctr[0] = 0u;
+    ctr[1] = 0u;
+    ctr[2] = ctr[2] + 1u;
+  }
+}
+
 template <class T, int NTH = NT>
 __global__ void __launch_bounds__(NTH)
 k_solve_forward_q(DevicePlan d, const int* __restrict__ nodes, int count, double* x,
                   int nrhs, int ldx, double* ubuf, const long long* uoff,
-                  int smem_doubles, unsigned* ctr, unsigned* done, unsigned epoch,
+                  int smem_doubles, unsigned* ctr, unsigned* done, const unsigned* ep,
                   int* err) {
   pdl_enter();
   extern __shared__ double sV[];
   __shared__ NarrowSmem sm;
   __shared__ int s_idx;
+  const unsigned epoch = *ep;
   for (;;) {
     const int idx = queue_next(ctr, count, &s_idx);
     if (idx < 0) break;
@@ -464,11 +476,12 @@ __global__ void __launch_bounds__(NTH)
 k_solve_backward_q(DevicePlan d, const int* __restrict__ nodes,
                    const int* __restrict__ dep, int count, double* x, int nrhs,
                    int ldx, double* ubuf, const long long* uoff, int smem_doubles,
-                   unsigned* ctr, unsigned* done, unsigned epoch, int* err) {
+                   unsigned* ctr, unsigned* done, const unsigned* ep, int* err) {
   pdl_enter();
   extern __shared__ double sV[];
   __shared__ NarrowSmem sm;
   __shared__ int s_idx;
+  const unsigned epoch = *ep;
   for (;;) {
     const int idx = queue_next(ctr, count, &s_idx);
     if (idx < 0) break;
@@ -1102,11 +1115,11 @@ static int build_solve_schedule(LdlHandle& h, cudaStream_t s) {
       SCUDA(cudaMalloc((void**)&h.sv_bq, std::max(nn, 1) * sizeof(int)));
       SCUDA(cudaMalloc((void**)&h.sv_dep, std::max(nn, 1) * sizeof(int)));
       SCUDA(cudaMalloc((void**)&h.sv_done, 2 * (size_t)std::max(nn, 1) * sizeof(unsigned)));
-      SCUDA(cudaMalloc((void**)&h.sv_ctr, 2 * sizeof(unsigned)));
+      SCUDA(cudaMalloc((void**)&h.sv_ctr, 4 * sizeof(unsigned)));
       SCUDA(cudaMalloc((void**)&h.sv_err, sizeof(int)));
       SCUDA(cudaMemsetAsync(h.sv_done, 0, 2 * (size_t)std::max(nn, 1) * sizeof(unsigned), s));
+      SCUDA(cudaMemsetAsync(h.sv_ctr, 0, 4 * sizeof(unsigned), s));
       SCUDA(cudaMemsetAsync(h.sv_err, 0, sizeof(int), s));
-      h.sv_epoch = 0;
     }
     SCUDA(cudaMemcpyAsync(h.sv_bq, bq.data(), qc * sizeof(int), cudaMemcpyHostToDevice, s));
     SCUDA(cudaMemcpyAsync(h.sv_dep, dep.data(), qc * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -1197,7 +1210,7 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
   const bool qsmall = queue && small && h.sv_qsmall;
   const int qth = qsmall ? kSmallThreads : NT;
   const int qsm = qsmall ? h.sv_qsmall_smem : h.sv_qsmem;
-  const unsigned ep = h.sv_epoch + 1;
+  const unsigned* ep = h.sv_ctr + 2;   // this solve's epoch, set on the device
   if (queue) {
     if (h.sv_qgrid == 0 || h.sv_qgrid_small != qsmall) {
       // CTAs resident at once, at most one per queued front
@@ -1213,8 +1226,8 @@ static int launch_solve(LdlHandle& h, double* d_x, int nrhs, int ldx,
       h.sv_qgrid = std::max(1, std::min(h.sv_qcount, sms * std::max(per, 1)));
       h.sv_qgrid_small = qsmall;
     }
-    h.sv_epoch = ep;
-    SCUDA(cudaMemsetAsync(h.sv_ctr, 0, 2 * sizeof(unsigned), s));
+    { k_sweep_begin<<<1, 32, 0, s>>>(h.sv_ctr); ab::count_launch(); }
+    SCUDA(cudaGetLastError());
     if (qsmall)
       SCUDA(launch_pdl(k_solve_forward_q<T, kSmallThreads>, dim3(h.sv_qgrid), dim3(qth),
                        (size_t)qsm, s, d, (const int*)h.sv_nodes, h.sv_qcount, d_x, nrhs,
