@@ -64,6 +64,9 @@ def parse():
                     help="requests in the serving run (0: skip)")
     ap.add_argument("--clock-dir", default=tempfile.gettempdir(),
                     help="folder for the nvidia-smi clock samples of the timed region")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default panel forms and solve schedule of the "
+                         "2D KKT instead of the autotuner's")
     ap.add_argument("--no-3d", action="store_true",
                     help="skip the 3D SIMP 48x24x24 factorization")
     ap.add_argument("--simp3d", default="48,24,24",
@@ -253,8 +256,13 @@ def run_ours(args, rank, world, local):
     device = torch.device("cuda", local)
     core = Core(device, args.nx, args.ny)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)
-    for _ in range(args.warmup):
+    tuning = None
+    for w in range(args.warmup):
         inertia = core.step()
+        if w == 0 and not args.no_autotune:
+            # panel forms and solve schedule picked by timing them on this
+            # KKT (ab_ldl_autotune); the remaining warm-up steps use them
+            tuning = core.ldl.autotune(reps=3)
     torch.cuda.synchronize()
     npiv_ours, _ = core.ldl.node_pivots()
     st = core.ldl.stats()
@@ -314,6 +322,7 @@ def run_ours(args, rank, world, local):
 
     # e2e through the public API with host buffers
     e2e = run_e2e(core, args, device)
+    graph = solve_graph_bench(core)
 
     out = {
         "metric": METRIC,
@@ -340,6 +349,8 @@ def run_ours(args, rank, world, local):
         "ldl_stats": st,
         "inertia": [int(inertia[0]), int(inertia[1])],
         "threads": threads_env(),
+        "autotune": tuning,
+        "solve_graph": graph,
     }
     core_npiv = npiv_ours
     out["roofline"] = roofline(core, fac_tot / args.steps)
@@ -706,6 +717,45 @@ def run_e2e(core, args, device):
                     "solution copied out; `value` times the whole IPM-iteration core "
                     "(element kernels, factor, two solves, refinement, IPM vectors) "
                     "on device-resident data"}
+
+
+def solve_graph_bench(core, reps=20):
+    """Repeated solves on the resident factorization (as refinement steps
+    and multi-right-hand-side sensitivities make them): one launch per level
+    and sweep against one replay of the captured graph (linalg.SolveGraph),
+    CUDA-event time per solve, and whether the replay gave the eager bits."""
+    import torch
+    from amigo_b200 import linalg
+    stream = torch.cuda.current_stream()
+    b = core.res.clone()
+    x = torch.empty_like(b)
+    g = linalg.SolveGraph(core.ldl, x)
+    x.copy_(b)
+    g()                      # capture
+    ref = b.clone()
+    core.ldl.solve_device(ref)
+    same = bool(torch.equal(x, ref))
+    t = {}
+    for name, fn in (("eager", lambda: core.ldl.solve_device(x)), ("graph", g)):
+        for _ in range(3):
+            x.copy_(b)
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        tot = 0.0
+        for _ in range(reps):
+            x.copy_(b)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        t[name] = round(tot / reps, 4)
+    return {"eager_ms_per_solve": t["eager"], "graph_ms_per_solve": t["graph"],
+            "replay_bits_equal_eager": same, "captures": g.captures,
+            "note": "one solve of the 2D KKT on its resident factorization, "
+                    "host-synchronised per solve"}
 
 
 # ---------------------------------------------------------- reference arm
