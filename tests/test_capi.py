@@ -31,3 +31,37 @@ def test_library_exports_all_declared_symbols():
 def test_binding_covers_header():
     assert set(declared()) <= set(_lib.exported_symbols()) | {"ab_ldl_analyze"}
     _lib.lib()
+
+
+def test_autotune_arguments_without_a_gpu():
+    """ab_ldl_autotune refuses an analysis-only handle (no device plan) and
+    bad arguments before any CUDA call; ab_ldl_apply_tuning checks every
+    field's range."""
+    import numpy as np
+    from amigo_b200 import linalg
+    L = _lib.lib()
+    n = 4
+    rowp = np.array([0, 2, 4, 6, 8], np.int32)
+    cols = np.array([0, 1, 0, 1, 2, 3, 2, 3], np.int32)
+    h = ctypes.c_void_p()
+    ip = ctypes.POINTER(ctypes.c_int)
+    assert L.ab_ldl_analyze(n, rowp.ctypes.data_as(ip), cols.ctypes.data_as(ip), 1,
+                            ctypes.byref(h)) == 0
+    try:
+        t = linalg.LdlTuning()
+        assert L.ab_ldl_autotune(None, None, 1, None, ctypes.byref(t)) == -1
+        assert L.ab_ldl_autotune(h, None, 0, None, ctypes.byref(t)) == -1
+        assert L.ab_ldl_autotune(h, None, 1, None, ctypes.byref(t)) == -4
+        good = linalg.LdlTuning(panel_mode=0, cl_min_rows=768, panel_cache_bytes=0,
+                                cluster_entries=1 << 14, wide_entries=1 << 22,
+                                solve_queue=1)
+        assert L.ab_ldl_apply_tuning(h, ctypes.byref(good)) == 0
+        assert L.ab_ldl_apply_tuning(h, None) == -1
+        for field, bad in (("panel_mode", 4), ("cl_min_rows", 0),
+                           ("panel_cache_bytes", 300 * 1024), ("cluster_entries", 0),
+                           ("wide_entries", 0), ("solve_queue", 4)):
+            b = linalg.LdlTuning.from_buffer_copy(good)
+            setattr(b, field, bad)
+            assert L.ab_ldl_apply_tuning(h, ctypes.byref(b)) == -1, field
+    finally:
+        L.ab_ldl_destroy(h)
