@@ -1,4 +1,4 @@
-"""Cart-pole collocation model (configs[0], N = 100) on the GPU: the
+"""Cart-pole swing-up collocation model (N = 100 intervals) on the GPU: the
 hyper-dual component kernels against finite differences of the numpy
 Lagrangian (oracle/cartpole_oracle.py), and the KKT factorization at the
 seeded initial point against the reference's own SparseLDL (identical
