@@ -116,7 +116,7 @@ class Server:
         steps = 0
         pool = (ThreadPoolExecutor(max_workers=self.rescue_workers)
                 if self.rescue else None)
-        if pool is not None:
+        if pool is not None and self.device.type == "cuda":
             torch.cuda.synchronize(self.device)
         t0 = time.perf_counter()
 
