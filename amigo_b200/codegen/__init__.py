@@ -6,11 +6,12 @@ groups of component instances into a KKT problem and compiles straight-line
 CUDA evaluators of each component's Lagrangian gradient and Hessian, with
 the gradient and the CSR Hessian scatter on the device.
 """
+from .amigo_format import AmigoComponent, from_amigo
 from .component import Component
 from .expr import (acos, asin, atan, cos, cosh, exp, fabs, log, log10, sin,
                    sinh, sqrt, tan, tanh)
-from .model import GeneratedModel, Group, host_evaluator
+from .model import GeneratedModel, Group, host_evaluator, host_evaluators
 
-__all__ = ["Component", "GeneratedModel", "Group", "host_evaluator", "sin", "cos",
+__all__ = ["Component", "AmigoComponent", "from_amigo", "GeneratedModel", "Group", "host_evaluator", "host_evaluators", "sin", "cos",
            "tan", "exp", "log", "log10", "sqrt", "tanh", "sinh", "cosh", "asin",
            "acos", "atan", "fabs"]

@@ -371,8 +371,17 @@ class GeneratedDevice:
 def host_evaluator(component, sym="comp"):
     """The generated evaluator compiled for the host: returns a function
     (q, d, alpha) -> (gradient, Hessian (NQ x NQ), objective)."""
-    src = emit.module_source([(sym, component)])
-    lib = ctypes.CDLL(compile_module(src, host=True))
+    return host_evaluators([(sym, component)])[0]
+
+
+def host_evaluators(pairs):
+    """host_evaluator for several (symbol, component) pairs compiled as one
+    host module; returns the evaluators in order."""
+    lib = ctypes.CDLL(compile_module(emit.module_source(list(pairs)), host=True))
+    return [_host_ev(lib, sym, comp) for sym, comp in pairs]
+
+
+def _host_ev(lib, sym, component):
     fn = getattr(lib, sym + "_eval_host")
     fn.restype = ctypes.c_int
     nq, nd = component.num_vars, component.num_data

@@ -1,0 +1,100 @@
+"""Components serialized by the reference's own front end, run through this
+package's code generator (codegen.from_amigo).  The fixture
+(tests/golden/ref_components.json, made by make_ref_components.py) holds
+the component classes of the reference's examples -- the cart-pole
+trajectory, Sellar, Rosenbrock and the Hock-Schittkowski test problems --
+as the reference serialized them, with the value of each serialized
+Lagrangian at two sample points (oracle/expr_oracle.py on the reference's
+tree).  The generated evaluators (host build of the device source) must
+give that Lagrangian, its gradient by central differences of the
+reference's tree, and a symmetric Hessian equal to the differences of the
+gradient."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from amigo_b200 import codegen as cg
+from oracle import expr_oracle as X
+
+FIX = os.path.join(os.path.dirname(__file__), "golden", "ref_components.json")
+
+
+@pytest.fixture(scope="module")
+def generated():
+    comps = json.load(open(FIX))["components"]
+    built = [cg.from_amigo(c["data"]) for c in comps]
+    evs = cg.host_evaluators([("ref%d" % i, b) for i, b in enumerate(built)])
+    return comps, built, evs
+
+
+def test_fixture_covers_the_examples(generated):
+    comps, _, _ = generated
+    names = {(c["source"].split("/")[-1], c["cls"]) for c in comps}
+    assert ("cart_pole.py", "CartComponent") in names
+    assert ("sellar.py", "Objective") in names
+    assert sum(1 for s, _ in names if s.startswith("hs")) >= 20
+    assert len(comps) >= 30
+
+
+def test_layout_matches_the_reference(generated):
+    comps, built, _ = generated
+    for c, b in zip(comps, built):
+        assert b.num_vars == X.num_vars(c["data"]), c["cls"]
+        assert b.num_data == X.num_data(c["data"]), c["cls"]
+
+
+def test_lagrangian_gradient_hessian(generated):
+    comps, built, evs = generated
+    for c, b, ev in zip(comps, built, evs):
+        data, ni = c["data"], b.num_inputs
+        for p in c["points"]:
+            x, d, alpha = np.array(p["x"]), np.array(p["d"]), p["alpha"]
+            g, H, obj = ev(x, d, alpha)
+            L = alpha * obj + x[ni:] @ g[ni:]
+            Lref = p["lagrangian"]
+            assert X.lagrangian(data, x, d, alpha) == Lref
+            scale = max(1.0, abs(Lref))
+            assert abs(L - Lref) <= 1e-12 * scale, (c["cls"], L, Lref)
+            h = 1e-6
+            gsc = max(scale, np.abs(g).max())
+            for i in range(len(x)):
+                e = np.zeros(len(x))
+                e[i] = h
+                fd = (X.lagrangian(data, x + e, d, alpha) -
+                      X.lagrangian(data, x - e, d, alpha)) / (2 * h)
+                assert abs(fd - g[i]) <= 1e-6 * gsc, (c["cls"], i, fd, g[i])
+                gp, _, _ = ev(x + e, d, alpha)
+                gm, _, _ = ev(x - e, d, alpha)
+                col = (gp - gm) / (2 * h)
+                hsc = max(gsc, np.abs(H).max())
+                assert np.abs(col - H[:, i]).max() <= 1e-6 * hsc, (c["cls"], i)
+            assert np.array_equal(H, H.T), c["cls"]
+
+
+def test_json_text_and_bounds(generated):
+    comps, built, _ = generated
+    c = next(c for c in comps if c["cls"] == "CartComponent")
+    b = cg.from_amigo(json.dumps(c["data"]))
+    lo, hi = b.input_bounds()
+    # the control x in [-50, 50]; q and qdot unbounded (amigo's defaults)
+    assert lo[0] == -50.0 and hi[0] == 50.0
+    assert np.all(np.isinf(lo[1:])) and np.all(np.isinf(hi[1:]))
+    assert b.num_constraints == 4
+
+
+def test_rejected_nodes():
+    base = {"name": "T", "args": [{}], "constants": {}, "data": {}, "outputs": {},
+            "objective": {}, "lagrangian": {},
+            "inputs": {"a": {"meta": {"shape": None}, "expr": ["var", "a", None, "float", True]}}}
+    for tree, what in ((["binary", "atan2", ["var", "a", None, "float", True],
+                         ["const", None, 1.0, "float"]], "atan2"),
+                       (["unary", "asinh", ["var", "a", None, "float", True]], "asinh"),
+                       (["passive", ["var", "a", None, "float", True]], "passive")):
+        d = dict(base, constraints={"c": {"meta": {"shape": None},
+                                          "expr": {"expr": {"0": {"expr": tree}}}}})
+        with pytest.raises(ValueError, match=what):
+            cg.from_amigo(d).build()
+    with pytest.raises(ValueError, match="argument sets"):
+        cg.from_amigo(dict(base, args=[{}, {}], constraints={}))
