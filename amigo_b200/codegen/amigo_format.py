@@ -13,13 +13,15 @@ The variable vector keeps amigo's layout: the inputs in declaration order,
 then one multiplier per constraint entry; bounds and starting values come
 from the metadata with amigo's defaults (inputs unbounded from 0.0,
 constraints equalities at 0, amigo/meta.py:7-17 and
-amigo/model.py:1362-1366).  Supported nodes: constants (named ones take
-the component's constant value), variables, indexing, unary minus and the
-A2D functions sin cos tan asin acos atan sinh cosh tanh exp log log10 sqrt
-fabs, and the binary + - * / ** operators.  A tree that uses another node
-(atan2, min2, max2, asinh, acosh, atanh, passive subexpressions), more than
-one compute() argument set, or a continuation component is rejected with a
-ValueError naming it.
+amigo/model.py:1362-1366).  Every node kind and function of amigo's
+expression layer is taken (amigo/unary_operations.py): constants (named
+ones take the component's constant value), variables, indexing, unary
+minus, sin cos tan asin acos atan sinh cosh tanh asinh acosh atanh exp log
+log10 sqrt fabs, the binary + - * / ** operators, atan2, min2 / max2 (the
+derivative follows the chosen argument; on a tie, the second) and passive
+subexpressions (value without derivative).  More than one compute()
+argument set, a continuation component or an unknown node is rejected with
+a ValueError naming it.
 """
 import json
 import math
@@ -32,7 +34,9 @@ from .component import Component
 
 _UNARY = {"sin": E.sin, "cos": E.cos, "tan": E.tan, "asin": E.asin, "acos": E.acos,
           "atan": E.atan, "sinh": E.sinh, "cosh": E.cosh, "tanh": E.tanh, "exp": E.exp,
-          "log": E.log, "log10": E.log10, "sqrt": E.sqrt, "fabs": E.fabs}
+          "log": E.log, "log10": E.log10, "sqrt": E.sqrt, "fabs": E.fabs,
+          "asinh": E.asinh, "acosh": E.acosh, "atanh": E.atanh}
+_BINARY = {"atan2": E.atan2, "min2": E.min2, "max2": E.max2}
 
 
 def _shape(s):
@@ -139,7 +143,11 @@ class AmigoComponent(Component):
                         raise ValueError("a constant base of ** must be positive")
                     return E.exp(b * math.log(a))
                 return a ** b
+            if op in _BINARY:
+                return _BINARY[op](a, b)
             raise ValueError("unsupported operation %r" % (op,))
+        if kind == "passive":
+            return E.passive(self._ev(t[1]))
         raise ValueError("unsupported node %r" % (kind,))
 
     def _entries(self, c, key=0):

@@ -321,6 +321,10 @@ class _Deserialized(Component):
                 n = g.neg(*a)
             elif op == "pow":
                 n = g.pow(a[0], val)
+            elif op in ("atan2", "min2", "max2", "lt", "gt"):
+                n = g.bfunc(op, a[0], a[1])
+            elif op == "passive":
+                n = g.passive(a[0])
             else:
                 n = g.func(op, a[0])
             made.append(n)

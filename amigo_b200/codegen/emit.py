@@ -28,7 +28,7 @@ from . import expr as E
 _FUNCS = {"sin": "sin", "cos": "cos", "tan": "tan", "exp": "exp", "log": "log",
           "sqrt": "sqrt", "tanh": "tanh", "sinh": "sinh", "cosh": "cosh",
           "asin": "asin", "acos": "acos", "atan": "atan", "log10": "log10",
-          "fabs": "fabs"}
+          "fabs": "fabs", "asinh": "asinh", "acosh": "acosh", "atanh": "atanh"}
 
 
 def _lit(v):
@@ -83,6 +83,18 @@ def _expr(n):
         return "pow(%s, %s)" % (a[0], _lit(p))
     if op == "sign":
         return "(%s > 0.0 ? 1.0 : (%s < 0.0 ? -1.0 : 0.0))" % (a[0], a[0])
+    if op == "atan2":
+        return "atan2(%s, %s)" % (a[0], a[1])
+    if op == "min2":
+        return "(%s < %s ? %s : %s)" % (a[0], a[1], a[0], a[1])
+    if op == "max2":
+        return "(%s > %s ? %s : %s)" % (a[0], a[1], a[0], a[1])
+    if op == "lt":
+        return "(%s < %s ? 1.0 : 0.0)" % (a[0], a[1])
+    if op == "gt":
+        return "(%s > %s ? 1.0 : 0.0)" % (a[0], a[1])
+    if op == "passive":
+        return a[0]
     if op in _FUNCS:
         return "%s(%s)" % (_FUNCS[op], a[0])
     raise ValueError("cannot emit %s" % op)

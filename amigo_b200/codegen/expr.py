@@ -144,14 +144,37 @@ class Graph:
             return self.const(_PY_FUNCS[name](ca))
         return self._make(name, (a,))
 
+    def bfunc(self, name, a, b):
+        """Binary functions: atan2(a, b); min2 / max2 (a if a < b, resp.
+        a > b, else b, the derivative following the chosen argument); lt /
+        gt (1.0 where a < b, resp. a > b, else 0.0; derivative 0)."""
+        ca, cb = self._c(a), self._c(b)
+        if ca is not None and cb is not None:
+            return self.const(_PY_BFUNCS[name](ca, cb))
+        return self._make(name, (a, b))
+
+    def passive(self, a):
+        """The value of a with zero derivative (amigo's passive)."""
+        if a.op == "const" or a.op == "passive":
+            return a
+        return self._make("passive", (a,))
+
 
 _PY_FUNCS = {
     "sin": math.sin, "cos": math.cos, "tan": math.tan, "exp": math.exp,
     "log": math.log, "sqrt": math.sqrt, "tanh": math.tanh, "sinh": math.sinh,
     "cosh": math.cosh, "asin": math.asin, "acos": math.acos, "atan": math.atan,
-    "log10": math.log10, "fabs": math.fabs,
+    "log10": math.log10, "fabs": math.fabs, "asinh": math.asinh, "acosh": math.acosh,
+    "atanh": math.atanh,
 }
 UNARY = tuple(_PY_FUNCS)
+_PY_BFUNCS = {
+    "atan2": math.atan2,
+    "min2": lambda a, b: a if a < b else b,
+    "max2": lambda a, b: a if a > b else b,
+    "lt": lambda a, b: 1.0 if a < b else 0.0,
+    "gt": lambda a, b: 1.0 if a > b else 0.0,
+}
 
 
 class Expr:
@@ -223,7 +246,29 @@ sin, cos, tan, exp, log, sqrt, tanh = (_unary(k) for k in
 sinh, cosh, asin, acos, atan, log10, fabs = (_unary(k) for k in
                                              ("sinh", "cosh", "asin", "acos", "atan",
                                               "log10", "fabs"))
+asinh, acosh, atanh = (_unary(k) for k in ("asinh", "acosh", "atanh"))
 abs_ = fabs
+
+
+def _binary(name):
+    def f(a, b):
+        if not isinstance(a, Expr) and not isinstance(b, Expr):
+            return _PY_BFUNCS[name](float(a), float(b))
+        e = a if isinstance(a, Expr) else b
+        return Expr(e.g, e.g.bfunc(name, e._lift(a), e._lift(b)))
+    f.__name__ = name
+    f.__doc__ = "%s of two expressions (or numbers)." % name
+    return f
+
+
+atan2, min2, max2 = (_binary(k) for k in ("atan2", "min2", "max2"))
+
+
+def passive(x):
+    """x without derivative (amigo's passive)."""
+    if isinstance(x, Expr):
+        return Expr(x.g, x.g.passive(x.n))
+    return float(x)
 
 
 # ---------------------------------------------------------------- derivatives
@@ -271,6 +316,24 @@ def _partials(g, n):
         return (g.neg(g.div(g.const(1.0), g.func("sqrt", g.sub(g.const(1.0), g.mul(x, x))))),)
     if op == "atan":
         return (g.div(g.const(1.0), g.add(g.const(1.0), g.mul(x, x))),)
+    if op == "asinh":
+        return (g.div(g.const(1.0), g.func("sqrt", g.add(g.mul(x, x), g.const(1.0)))),)
+    if op == "acosh":
+        return (g.div(g.const(1.0), g.func("sqrt", g.sub(g.mul(x, x), g.const(1.0)))),)
+    if op == "atanh":
+        return (g.div(g.const(1.0), g.sub(g.const(1.0), g.mul(x, x))),)
+    if op == "atan2":
+        # d atan2(y, x) = (x dy - y dx) / (x^2 + y^2)
+        y, xx = a
+        r2 = g.add(g.mul(y, y), g.mul(xx, xx))
+        return (g.div(xx, r2), g.neg(g.div(y, r2)))
+    if op in ("min2", "max2"):
+        s = g.bfunc("lt" if op == "min2" else "gt", a[0], a[1])
+        return (s, g.sub(g.const(1.0), s))
+    if op in ("lt", "gt"):
+        return (g.const(0.0), g.const(0.0))
+    if op == "passive":
+        return (g.const(0.0),)
     if op == "fabs":
         return (g._make("sign", (x,)),)
     if op == "sign":

@@ -54,10 +54,13 @@ def _binary(op, a, b):
     raise ValueError("unknown binary operation %r" % op)
 
 
-def evaluate(tree, env):
+def evaluate(tree, env, frozen=None):
     """Value of one serialized expression; env maps variable names to
     floats or numpy arrays (inputs, data, multipliers, alpha__) and
-    constant names to their values."""
+    constant names to their values.  Passive subexpressions (values that
+    amigo's derivatives treat as constants) are evaluated in `frozen` when
+    it is given, so differences taken around a point hold them at that
+    point."""
     kind = tree[0]
     if kind == "const":
         name, value = tree[1], tree[2]
@@ -67,15 +70,16 @@ def evaluate(tree, env):
     if kind == "var":
         return env[tree[1]]
     if kind == "index":
-        a = evaluate(tree[1], env)
+        a = evaluate(tree[1], env, frozen)
         idx = tree[2]
         return float(a[tuple(idx)] if isinstance(idx, (list, tuple)) else a[idx])
     if kind == "passive":
-        return evaluate(tree[1], env)
+        return evaluate(tree[1], env if frozen is None else frozen)
     if kind == "unary":
-        return _UNARY[tree[1]](evaluate(tree[2], env))
+        return _UNARY[tree[1]](evaluate(tree[2], env, frozen))
     if kind == "binary":
-        return _binary(tree[1], evaluate(tree[2], env), evaluate(tree[3], env))
+        return _binary(tree[1], evaluate(tree[2], env, frozen),
+                       evaluate(tree[3], env, frozen))
     raise ValueError("unknown node %r" % (kind,))
 
 
@@ -119,9 +123,13 @@ def environment(data, x, dvals, alpha):
     return env
 
 
-def lagrangian(data, x, dvals, alpha, key=0):
-    """The serialized Lagrangian (amigo's own tree) at (x, dvals, alpha)."""
-    return evaluate(_by_key(data["lagrangian"], key), environment(data, x, dvals, alpha))
+def lagrangian(data, x, dvals, alpha, key=0, x_frozen=None):
+    """The serialized Lagrangian (amigo's own tree) at (x, dvals, alpha);
+    with x_frozen, its passive subexpressions are taken at x_frozen."""
+    frozen = (None if x_frozen is None else
+              environment(data, x_frozen, dvals, alpha))
+    return evaluate(_by_key(data["lagrangian"], key), environment(data, x, dvals, alpha),
+                    frozen)
 
 
 def num_vars(data):

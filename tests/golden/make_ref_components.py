@@ -10,7 +10,9 @@ executed with `am` bound to the reference package (its compiled module
 replaced by oracle/ref_optimizer.py's stand-in, which component code does
 not touch).  Components that cannot be instantiated without arguments,
 define no constraint or objective, or use a node the importer rejects are
-listed under "skipped" with the reason.
+listed under "skipped" with the reason.  One more component, defined in this
+script with the reference's API, covers the functions the examples do not
+use (atan2, min2, max2, asinh, acosh, atanh, passive).
 
     python tests/golden/make_ref_components.py      # needs the reference sources
 """
@@ -70,6 +72,30 @@ def component_classes(path, am):
             if isinstance(v, type) and issubclass(v, am.Component) and v is not am.Component]
 
 
+def functions_component(am):
+    """A component of this script (not from the examples) that uses every
+    function of the reference's expression layer the examples leave out."""
+
+    class AllFunctions(am.Component):
+        def __init__(self):
+            super().__init__()
+            self.add_constant("k", value=0.3)
+            self.add_input("a")
+            self.add_input("b", shape=(2,))
+            self.add_data("w")
+            self.add_objective("f")
+            self.add_constraint("c", shape=(3,))
+
+        def compute(self):
+            a, b, w, k = self.inputs["a"], self.inputs["b"], self.data["w"], self.constants["k"]
+            self.objective["f"] = (am.atan2(a, b[0]) + am.min2(a * a, b[1]) + am.max2(a, w * b[0])
+                                   + am.asinh(a * w) + am.passive(a) * b[1] * a)
+            self.constraints["c"] = [am.acosh(1.5 + b[0] * b[0]), am.atanh(k * a),
+                                     am.passive(a) * b[0] + am.fabs(a - b[1])]
+
+    return AllFunctions
+
+
 def main():
     ref_root = RO.REF_ROOT
     am = reference_namespace()
@@ -81,8 +107,10 @@ def main():
             scripts.append(f)
     r = np.random.RandomState(0)
     out, skipped = [], {}
-    for rel in scripts:
-        for cls in component_classes(os.path.join(ref_root, rel), am):
+    for rel in scripts + ["make_ref_components.py"]:
+        classes = ([functions_component(am)] if rel == "make_ref_components.py" else
+                   component_classes(os.path.join(ref_root, rel), am))
+        for cls in classes:
             key = "%s:%s" % (rel, cls.__name__)
             try:
                 data = cls().serialize()

@@ -3,12 +3,14 @@ package's code generator (codegen.from_amigo).  The fixture
 (tests/golden/ref_components.json, made by make_ref_components.py) holds
 the component classes of the reference's examples -- the cart-pole
 trajectory, Sellar, Rosenbrock and the Hock-Schittkowski test problems --
-as the reference serialized them, with the value of each serialized
-Lagrangian at two sample points (oracle/expr_oracle.py on the reference's
-tree).  The generated evaluators (host build of the device source) must
-give that Lagrangian, its gradient by central differences of the
-reference's tree, and a symmetric Hessian equal to the differences of the
-gradient."""
+and one component of the fixture script that uses the expression functions
+the examples leave out, as the reference serialized them, with the value of
+each serialized Lagrangian at two sample points (oracle/expr_oracle.py on
+the reference's tree).  The generated evaluators (host build of the device
+source) must give that Lagrangian, its gradient by central differences of
+the reference's tree (passive subexpressions held), and a symmetric Hessian
+equal to the differences of the gradient (with passive subexpressions:
+second differences of the tree)."""
 import json
 import os
 
@@ -45,10 +47,28 @@ def test_layout_matches_the_reference(generated):
         assert b.num_data == X.num_data(c["data"]), c["cls"]
 
 
+def second_differences(data, x, d, alpha, h=1e-4):
+    """Lower triangle of the Hessian of the reference tree's Lagrangian by
+    second differences, passive subexpressions held at x."""
+    n = len(x)
+    H = np.zeros((n, n))
+    L = lambda y: X.lagrangian(data, y, d, alpha, x_frozen=x)
+    for i in range(n):
+        for j in range(i + 1):
+            ei = np.zeros(n)
+            ej = np.zeros(n)
+            ei[i] = h
+            ej[j] = h
+            H[i, j] = H[j, i] = (L(x + ei + ej) - L(x + ei - ej) - L(x - ei + ej)
+                                 + L(x - ei - ej)) / (4 * h * h)
+    return H
+
+
 def test_lagrangian_gradient_hessian(generated):
     comps, built, evs = generated
     for c, b, ev in zip(comps, built, evs):
         data, ni = c["data"], b.num_inputs
+        passive = "passive" in json.dumps(data)
         for p in c["points"]:
             x, d, alpha = np.array(p["x"]), np.array(p["d"]), p["alpha"]
             g, H, obj = ev(x, d, alpha)
@@ -62,14 +82,20 @@ def test_lagrangian_gradient_hessian(generated):
             for i in range(len(x)):
                 e = np.zeros(len(x))
                 e[i] = h
-                fd = (X.lagrangian(data, x + e, d, alpha) -
-                      X.lagrangian(data, x - e, d, alpha)) / (2 * h)
+                fd = (X.lagrangian(data, x + e, d, alpha, x_frozen=x) -
+                      X.lagrangian(data, x - e, d, alpha, x_frozen=x)) / (2 * h)
                 assert abs(fd - g[i]) <= 1e-6 * gsc, (c["cls"], i, fd, g[i])
-                gp, _, _ = ev(x + e, d, alpha)
-                gm, _, _ = ev(x - e, d, alpha)
-                col = (gp - gm) / (2 * h)
-                hsc = max(gsc, np.abs(H).max())
-                assert np.abs(col - H[:, i]).max() <= 1e-6 * hsc, (c["cls"], i)
+                if not passive:
+                    gp, _, _ = ev(x + e, d, alpha)
+                    gm, _, _ = ev(x - e, d, alpha)
+                    col = (gp - gm) / (2 * h)
+                    hsc = max(gsc, np.abs(H).max())
+                    assert np.abs(col - H[:, i]).max() <= 1e-6 * hsc, (c["cls"], i)
+            if passive:
+                # the generated gradient moves with the passive values, so
+                # the Hessian is checked against the tree directly
+                Hd = second_differences(data, x, d, alpha)
+                assert np.abs(Hd - H).max() <= 1e-5 * max(1.0, np.abs(H).max()), c["cls"]
             assert np.array_equal(H, H.T), c["cls"]
 
 
@@ -84,17 +110,40 @@ def test_json_text_and_bounds(generated):
     assert b.num_constraints == 4
 
 
+def test_every_expression_function(generated):
+    """The component the fixture script defines with the reference's API
+    covers atan2, min2, max2, asinh, acosh, atanh and passive."""
+    comps, _, _ = generated
+    c = next(c for c in comps if c["cls"] == "AllFunctions")
+    text = json.dumps(c["data"])
+    for op in ("atan2", "min2", "max2", "asinh", "acosh", "atanh", "passive", "fabs"):
+        assert '"%s"' % op in text, op
+
+
 def test_rejected_nodes():
     base = {"name": "T", "args": [{}], "constants": {}, "data": {}, "outputs": {},
             "objective": {}, "lagrangian": {},
             "inputs": {"a": {"meta": {"shape": None}, "expr": ["var", "a", None, "float", True]}}}
-    for tree, what in ((["binary", "atan2", ["var", "a", None, "float", True],
-                         ["const", None, 1.0, "float"]], "atan2"),
-                       (["unary", "asinh", ["var", "a", None, "float", True]], "asinh"),
-                       (["passive", ["var", "a", None, "float", True]], "passive")):
+    for tree, what in ((["binary", "hypot", ["var", "a", None, "float", True],
+                         ["const", None, 1.0, "float"]], "hypot"),
+                       (["unary", "erf", ["var", "a", None, "float", True]], "erf"),
+                       (["lambda", ["var", "a", None, "float", True]], "lambda")):
         d = dict(base, constraints={"c": {"meta": {"shape": None},
                                           "expr": {"expr": {"0": {"expr": tree}}}}})
         with pytest.raises(ValueError, match=what):
             cg.from_amigo(d).build()
     with pytest.raises(ValueError, match="argument sets"):
         cg.from_amigo(dict(base, args=[{}, {}], constraints={}))
+
+
+def test_device_module_compiles(generated):
+    """The same generated source, built for sm_100a (nvcc cross-compiles
+    without a GPU)."""
+    import shutil
+    from amigo_b200.codegen import emit
+    from amigo_b200.codegen.model import compile_module
+    if not (shutil.which("nvcc") or os.path.exists("/usr/local/cuda/bin/nvcc")):
+        pytest.skip("nvcc not available")
+    _, built, _ = generated
+    src = emit.module_source([("ref%d" % i, b) for i, b in enumerate(built)])
+    assert os.path.exists(compile_module(src, host=False))
