@@ -143,7 +143,9 @@ class InertiaCorrection:
     def _grow(self):
         prev = self.dx
         if self.dx == 0.0:
-            self.dx = 1e-4 if self.dx_last == 0.0 else max(1e-20, self.dx_last / 3.0)
+            # the reference's decrease factor is the double 1/3 (a product,
+            # not a division: the two differ in the last bit)
+            self.dx = 1e-4 if self.dx_last == 0.0 else max(1e-20, self.dx_last * (1.0 / 3))
         elif self.dx_last == 0.0 or 1e5 * self.dx_last < self.dx:
             self.dx *= 100.0
         else:

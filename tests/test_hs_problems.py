@@ -5,9 +5,11 @@ only: each problem is one component instance, its derivatives the
 generated evaluators of codegen.from_amigo (host build).  The reference's
 own Optimizer (oracle/ref_optimizer.py: its driver, AmigoSolver and
 SparseLDL over its C++ backend) and this package's optimizer.Optimizer run
-on the same host numeric core; they must converge alike, in the same
-number of iterations (within one) and to the same objective (1e-8
-relative).  CPU only; needs the reference sources."""
+on the same host numeric core; every iteration record (residual, barrier
+parameter, step lengths, line-search trials, inertia perturbation, the KKT
+error terms, objective) and the final iterate must be the same bits.
+Inequality rows get a bounded slack each (c(x) - s = 0), the same problem
+for both drivers.  CPU only; needs the reference sources."""
 import json
 import os
 import types
@@ -19,49 +21,89 @@ from amigo_b200 import codegen as cg
 
 FIX = os.path.join(os.path.dirname(__file__), "golden", "ref_components.json")
 REF = os.environ.get("AMIGO_REF_ROOT", "/root/reference")
+FIELDS = ("residual", "barrier_param", "alpha_x", "alpha_z", "line_iters",
+          "inertia_delta", "inf_pr", "inf_du", "compl", "nlp_error", "objective")
 needs_ref = pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "amigo", "algorithm")),
                                reason="reference sources absent")
 
 EQ_ONLY = ("HS6", "HS26", "HS39", "HS40", "HS53", "HS60", "HS77", "HS79", "HS99",
            "HS111", "HS119", "HS87")
+WITH_INEQ = ("HS14", "HS29", "HS35", "HS44", "HS71", "HS76", "HS93", "HS100", "HS104",
+             "HS106", "HS108", "HS109", "HS113", "HS114", "HS116", "HS117", "HS118",
+             "Rosenbrock")
 
 
 def problem(name):
-    """The single-instance model of one test problem: inputs then one
-    multiplier per constraint entry, a dense KKT block, bounds and start
-    from the component's metadata (constraint targets as the multipliers'
-    lower bounds)."""
+    """The single-instance model of one test problem: inputs, one slack per
+    inequality constraint entry (c(x) - s = 0 with s within the
+    constraint's bounds), then one multiplier per constraint entry; a dense
+    KKT block; bounds and start from the component's metadata (equality
+    targets as the multipliers' lower bounds)."""
     comps = json.load(open(FIX))["components"]
     c = next(c for c in comps if c["cls"] == name)
     comp = cg.from_amigo(c["data"])
     ev = cg.host_evaluator(comp, "hs_" + name.lower())
     ni, nq, nd = comp.num_inputs, comp.num_vars, comp.num_data
+    nc = nq - ni
     lo, hi = comp.input_bounds()
-    x0 = np.zeros(nq)
+    x0 = np.zeros(ni)
     k = 0
     for nm in comp._inputs:
         v = np.asarray(comp._inputs.meta[nm]["value"], float)
         n = int(np.prod(comp._inputs.shapes[nm])) if comp._inputs.shapes[nm] else 1
         x0[k:k + n] = np.broadcast_to(v, (n,))
         k += n
-    tgt = []
+    clo, chi = [], []
     for nm in comp._cons:
         n = int(np.prod(comp._cons.shapes[nm])) if comp._cons.shapes[nm] else 1
-        tgt += list(np.broadcast_to(np.asarray(comp._cons.meta[nm]["lower"], float), (n,)))
+        m_ = comp._cons.meta[nm]
+        clo += list(np.broadcast_to(np.asarray(m_["lower"], float), (n,)))
+        chi += list(np.broadcast_to(np.asarray(m_["upper"], float), (n,)))
+    clo, chi = np.array(clo), np.array(chi)
+    ineq = np.nonzero(clo < chi)[0]            # constraint rows with a slack
+    ns = len(ineq)
+    n = ni + ns + nc
+    S, M = slice(ni, ni + ns), slice(ni + ns, n)
+    tgt = np.where(clo < chi, 0.0, clo)
     m = types.SimpleNamespace(
-        n=nq, mult=np.arange(nq) >= ni,
-        lower=np.concatenate([lo, tgt]), upper=np.concatenate([hi, np.full(nq - ni, np.inf)]),
-        x0=x0, rowp=np.arange(0, nq * nq + 1, nq, dtype=np.int32),
-        cols=np.tile(np.arange(nq, dtype=np.int32), nq),
-        diag_pos=np.arange(nq) * (nq + 1))
+        n=n, mult=np.arange(n) >= ni + ns,
+        lower=np.concatenate([lo, clo[ineq], tgt]),
+        upper=np.concatenate([hi, chi[ineq], np.full(nc, np.inf)]),
+        x0=np.concatenate([x0, np.zeros(ns + nc)]),
+        rowp=np.arange(0, n * n + 1, n, dtype=np.int32),
+        cols=np.tile(np.arange(n, dtype=np.int32), n),
+        diag_pos=np.arange(n) * (n + 1))
     d = np.zeros(max(nd, 1))
-    grad = lambda x, a: ev(x, d, a)[0]
-    hess = lambda x, a: ev(x, d, a)[1].ravel()
+    sel = np.r_[0:ni, ni + ns:n]               # the component's own variables
+
+    def evx(x, a):
+        return ev(x[sel], d, a)
+
+    def grad(x, a):
+        gq, _, _ = evx(x, a)
+        g = np.zeros(n)
+        g[:ni] = gq[:ni]
+        g[M] = gq[ni:]
+        g[M][ineq] -= x[S]                     # c - s on the slack rows
+        g[S] = -x[M][ineq]                     # d/ds of -lam s
+        return g
+
+    def hess(x, a):
+        _, Hq, _ = evx(x, a)
+        H = np.zeros((n, n))
+        H[np.ix_(sel, sel)] = Hq
+        rows = ni + ns + ineq
+        H[np.arange(ni, ni + ns), rows] = -1.0
+        H[rows, np.arange(ni, ni + ns)] = -1.0
+        return H.ravel()
 
     def lag(x, a):
-        g, _, f = ev(x, d, a)
-        return a * f + x[ni:] @ g[ni:]
-    obj = lambda x: ev(x, d, 1.0)[2]
+        gq, _, f = evx(x, a)
+        cval = gq[ni:].copy()
+        cval[ineq] -= x[S]
+        return a * f + x[M] @ cval
+
+    obj = lambda x: evx(x, 1.0)[2]
     return m, grad, hess, lag, obj
 
 
@@ -81,14 +123,17 @@ def ours(m, grad, hess, lag):
 
 
 @needs_ref
-@pytest.mark.parametrize("name", EQ_ONLY)
+@pytest.mark.parametrize("name", EQ_ONLY + WITH_INEQ)
 def test_hs_problem_matches_reference_optimizer(oracle_ref, name):
     from oracle import ref_optimizer as RO
     m, grad, hess, lag, obj = problem(name)
     want = RO.optimize(m, grad, hess, lag, obj)
     got = ours(m, grad, hess, lag)
     assert got["converged"] == want["converged"]
-    assert abs((len(got["iterations"]) - 1) - want["iterations"]) <= 1
-    if want["converged"]:
-        f = obj(got["x"])
-        assert abs(f - want["objective"]) <= 1e-8 * max(1.0, abs(want["objective"]))
+    assert len(got["iterations"]) == len(want["records"])
+    for a, b in zip(got["iterations"], want["records"]):
+        for k in FIELDS:
+            if b.get(k) is None or isinstance(b.get(k), str):
+                continue
+            assert float(a[k]) == float(b[k]), (name, a["iteration"], k)
+    assert np.array_equal(got["x"], want["x"])
