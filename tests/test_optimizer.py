@@ -6,7 +6,7 @@ interior_point_backend.h functions and SparseLDL (oracle/_ref) behind the
 reference's backend interface, with the reference's own AmigoSolver and its
 iterative refinement -- so every decision (barrier updates, inertia
 corrections, line-search trials, step lengths) and every iterate must
-agree.  The golden records come from tests/golden/make_ref_optimizer_golden.py
+agree, and every record equals the golden one bit for bit.  The golden records come from tests/golden/make_ref_optimizer_golden.py
 (the reference Optimizer on the cart-pole configuration and six batched
 instances)."""
 import json
@@ -59,4 +59,4 @@ def test_driver_reproduces_reference_iterations(oracle_ref, name, m):
         for k in FIELDS:
             if b[k] is None:
                 continue
-            assert a[k] == pytest.approx(b[k], rel=1e-9, abs=1e-12), (a["iteration"], k)
+            assert a[k] == b[k], (a["iteration"], k)
