@@ -46,9 +46,10 @@ def _shape(s):
     return t or None
 
 
-def _bound(v, default):
+def _bound(v):
+    """A metadata value as a float or an array (None: unset)."""
     if v is None:
-        return default
+        return None
     a = np.asarray(v, dtype=np.float64)
     return float(a) if a.ndim == 0 else a
 
@@ -80,18 +81,15 @@ class AmigoComponent(Component):
             self.add_constant(k, c["meta"]["value"])
         for k, c in data["inputs"].items():
             m = c["meta"]
-            self.add_input(k, _shape(m.get("shape")),
-                           value=_bound(m.get("value"), 0.0),
-                           lower=_bound(m.get("lower"), -np.inf),
-                           upper=_bound(m.get("upper"), np.inf))
+            self.add_input(k, _shape(m.get("shape")), value=_bound(m.get("value")),
+                           lower=_bound(m.get("lower")), upper=_bound(m.get("upper")))
         for k, c in data["data"].items():
             m = c["meta"]
-            self.add_data(k, _shape(m.get("shape")), value=_bound(m.get("value"), 0.0))
+            self.add_data(k, _shape(m.get("shape")), value=_bound(m.get("value")))
         for k, c in data["constraints"].items():
             m = c["meta"]
-            self.add_constraint(k, _shape(m.get("shape")),
-                                lower=_bound(m.get("lower"), 0.0),
-                                upper=_bound(m.get("upper"), 0.0))
+            self.add_constraint(k, _shape(m.get("shape")), lower=_bound(m.get("lower")),
+                                upper=_bound(m.get("upper")))
         for k in data["objective"]:
             self.add_objective(k)
         for k, c in data.get("outputs", {}).items():

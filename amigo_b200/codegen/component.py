@@ -37,6 +37,38 @@ def _size(shape):
     return int(np.prod(shape)) if shape else 1
 
 
+_META_OPTIONS = ("type", "units", "scale", "label")
+
+
+def _check_meta(kind, name, shape, kw, value=None, lower=None, upper=None):
+    """amigo's declaration checks (amigo/meta.py:24-133): names with a
+    double underscore are reserved, unknown options are refused, value and
+    bounds are scalars or of the declared shape, lower <= upper, and an
+    input's value lies within its bounds."""
+    if "__" in name:
+        raise ValueError("Name %s cannot contain a double underscore" % name)
+    unknown = sorted(set(kw) - set(_META_OPTIONS))
+    if unknown:
+        raise ValueError("Unknown options: %s" % unknown)
+    n = _size(_shape(shape))
+
+    def flat(v, what):
+        if v is None:
+            return None
+        a = np.asarray(v, dtype=np.float64)
+        if a.ndim == 0:
+            return np.full(n, float(a))
+        if a.size != n:
+            raise ValueError("%s must be scalar or have shape %s" % (what, _shape(shape)))
+        return a.ravel()
+    val, lo, hi = flat(value, "value"), flat(lower, "lower"), flat(upper, "upper")
+    if lo is not None and hi is not None and np.any(lo > hi):
+        raise ValueError("lower bound cannot be greater than upper bound")
+    if (kind == "input" and val is not None and lo is not None and hi is not None
+            and np.any((val < lo) | (val > hi))):
+        raise ValueError("value must be within [lower, upper]")
+
+
 class _Decl:
     """Ordered declarations of one kind with their shapes and metadata."""
 
@@ -88,25 +120,36 @@ class Component:
         self._built = None
 
     # -- declarations (amigo/component.py:639-706) --------------------------
+    # Unset value / bounds are None (amigo's defaults apply: value 0.0,
+    # inputs unbounded, constraints equalities at 0); the declarations are
+    # checked as amigo's Meta checks them (_check_meta).
     def add_constant(self, name, value, **kw):
+        _check_meta("constant", name, None, kw)
         self._const.add(name, None, value=float(value), **kw)
 
-    def add_input(self, name, shape=None, value=0.0, lower=-np.inf,
-                  upper=np.inf, **kw):
-        self._inputs.add(name, shape, value=value, lower=lower, upper=upper, **kw)
+    def add_input(self, name, shape=None, value=None, lower=None, upper=None, **kw):
+        _check_meta("input", name, shape, kw, value, lower, upper)
+        self._inputs.add(name, shape, value=0.0 if value is None else value,
+                         lower=-np.inf if lower is None else lower,
+                         upper=np.inf if upper is None else upper, **kw)
 
-    def add_data(self, name, shape=None, value=0.0, **kw):
-        self._data.add(name, shape, value=value, **kw)
+    def add_data(self, name, shape=None, value=None, **kw):
+        _check_meta("data", name, shape, kw, value)
+        self._data.add(name, shape, value=0.0 if value is None else value, **kw)
 
-    def add_constraint(self, name, shape=None, lower=0.0, upper=0.0, **kw):
-        self._cons.add(name, shape, lower=lower, upper=upper, **kw)
+    def add_constraint(self, name, shape=None, lower=None, upper=None, **kw):
+        _check_meta("constraint", name, shape, kw, None, lower, upper)
+        self._cons.add(name, shape, lower=0.0 if lower is None else lower,
+                       upper=0.0 if upper is None else upper, **kw)
 
     def add_objective(self, name, **kw):
+        _check_meta("objective", name, None, kw)
         self._obj.add(name, None, **kw)
 
     def add_output(self, name, shape=None, **kw):
         """A model output computed from the inputs and data (amigo's
         add_output); outputs do not enter the Lagrangian."""
+        _check_meta("output", name, shape, kw)
         self._outs.add(name, shape, **kw)
 
     def compute(self):

@@ -147,3 +147,29 @@ def test_device_module_compiles(generated):
     _, built, _ = generated
     src = emit.module_source([("ref%d" % i, b) for i, b in enumerate(built)])
     assert os.path.exists(compile_module(src, host=False))
+
+
+def test_declarations_checked_like_amigo():
+    """The declaration checks of amigo's Meta (amigo/meta.py): reserved
+    double-underscore names, lower > upper, an input value outside its
+    bounds, unknown options and misshaped values are ValueErrors; unset
+    values take amigo's defaults."""
+    bad = [lambda c: c.add_input("bad__name"),
+           lambda c: c.add_input("x", lower=10.0, upper=1.0),
+           lambda c: c.add_input("x", value=5.0, lower=0.0, upper=4.0),
+           lambda c: c.add_input("x", unknown_kwarg=42),
+           lambda c: c.add_input("x", shape=(3,), value=[1.0, 2.0]),
+           lambda c: c.add_constraint("c", shape=(2,), lower=[0.0, 2.0], upper=[1.0, 1.0]),
+           lambda c: c.add_data("d__x"),
+           lambda c: c.add_objective("f", scale=1.0, bogus=True)]
+    for k, f in enumerate(bad):
+        with pytest.raises(ValueError):
+            f(cg.Component())
+    c = cg.Component()
+    c.add_input("x", shape=(2,), lower=[1.0, 2.0], upper=[3.0, 4.0], label="state")
+    c.add_input("u", value=0.5, lower=0.0, upper=1.0, units="N", scale=2.0)
+    c.add_constraint("c", lower=-1.0, upper=np.inf)
+    lo, hi = c.input_bounds()
+    assert list(lo) == [1.0, 2.0, 0.0] and list(hi) == [3.0, 4.0, 1.0]
+    assert c._inputs.meta["x"]["value"] == 0.0     # unset: amigo's default
+    assert c._cons.meta["c"]["lower"] == -1.0 and c._cons.meta["c"]["upper"] == np.inf
