@@ -27,6 +27,7 @@ import scipy.sparse as sp
 import torch
 
 from . import emit
+from .component import Component
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
@@ -47,6 +48,54 @@ class Group:
         self.data = np.ascontiguousarray(np.asarray(data, dtype=np.float64).reshape(E, nd))
         self.name = name or type(component).__name__
         self.E = E
+
+
+class Slack(Component):
+    """amigo's slack coupling (include/slack_coupling.h:22-80; the Model
+    adds one per inequality constraint row, amigo/model.py:975-1010): an
+    input s and the constraint res = -s, so that with the row's own
+    constraint c the multiplier row reads c(x) - s = 0 and s carries the
+    row's bounds."""
+
+    def __init__(self):
+        super().__init__()
+        self.add_input("s")
+        self.add_constraint("res")
+
+    def compute(self):
+        self.constraints["res"] = -self.inputs["s"]
+
+
+def with_slacks(n, groups, mult, lower, upper, rows, row_lower, row_upper, x0=None,
+                fixed=(), f=None):
+    """GeneratedModel whose multiplier rows `rows` are inequalities
+    row_lower <= c(x) <= row_upper: one slack variable per row appended
+    after the n variables (bounds [row_lower, row_upper], start 0), coupled
+    into its row by a Slack group, and the row's target set to 0.  The
+    model's slack_indices / slack_rows give the pairs for
+    InteriorPointOptimizer.set_slack_mapping."""
+    rows = np.asarray(rows, np.int64)
+    ns = len(rows)
+    mult = np.asarray(mult, bool)
+    if ns and not np.all(mult[rows]):
+        raise ValueError("slack rows must be multiplier rows")
+    lo = np.asarray(row_lower, float)
+    hi = np.asarray(row_upper, float)
+    if np.any(lo > hi):
+        raise ValueError("lower bound cannot be greater than upper bound")
+    sidx = np.arange(n, n + ns)
+    lower = np.concatenate([np.asarray(lower, float), lo])
+    upper = np.concatenate([np.asarray(upper, float), hi])
+    lower[rows] = 0.0
+    x0 = None if x0 is None else np.concatenate([np.asarray(x0, float), np.zeros(ns)])
+    groups = list(groups)
+    if ns:
+        groups.append(Group(Slack(), np.stack([sidx, rows], axis=1), name="Slack"))
+    m = GeneratedModel(n + ns, groups, np.concatenate([mult, np.zeros(ns, bool)]),
+                       lower, upper, fixed=fixed, x0=x0, f=f)
+    m.slack_indices = sidx.astype(np.int32)
+    m.slack_rows = rows.astype(np.int32)
+    return m
 
 
 def _symbol(name, k):
