@@ -46,6 +46,34 @@ try:
 except ImportError:  # a host core needs no torch
     torch = None
 
+# amigo's options whose default values are the default algorithm that
+# this driver restates (amigo/algorithm/default_options.py): they are
+# accepted at these values; other values select strategies (adaptive or
+# quality-function barrier updates, Armijo-only line search, adaptive
+# regularisation settings, ...) that are not restated.
+DEFAULT_ALGORITHM_OPTIONS = {
+    "adaptive_mu_globalization": "obj-constr-filter", "adaptive_mu_kkterror_red_fact": 0.9999,
+    "adaptive_mu_kkterror_red_iters": 4, "adaptive_mu_monotone_init_factor": 0.8,
+    "adaptive_mu_safeguard_factor": 0.0, "adaptive_regularization": True,
+    "armijo_constant": 1e-4, "barrier_progress_tol": 10.0, "barrier_strategy": "heuristic",
+    "check_update_step": False, "continuation_control": None, "debug_cycling": False,
+    "equal_primal_dual_step": False, "filter_line_search": True,
+    "init_affine_step_multipliers": False, "max_regularization": 0.01,
+    "monotone_barrier_fraction": 0.1, "mu_linear_decrease_factor": 0.2,
+    "mu_max_fact": 1000.0, "mu_min": 1e-11, "mu_superlinear_decrease_power": 1.5,
+    "progress_based_barrier": True, "quality_function_balancing_term": "none",
+    "quality_function_centrality": "none", "quality_function_golden_iters": 8,
+    "quality_function_norm_scaling": True, "quality_function_predictor_corrector": False,
+    "quality_function_section_qf_tol": 0.0, "quality_function_section_sigma_tol": 0.01,
+    "quality_function_sigma_max": 100.0, "quality_function_sigma_min": 1e-6,
+    "record_components": [], "regularization_eps_x": 1e-8,
+    "regularization_eps_x_zero_hessian": 1.0, "regularization_eps_z": 1e-8,
+    "regularization_increase_factor": 10.0, "use_armijo_line_search": True,
+    "verbose_barrier": False, "zero_hessian_variables": [],
+}
+# of these, the ones that only change what is printed or recorded
+DIAGNOSTIC_OPTIONS = ("debug_cycling", "verbose_barrier", "record_components")
+
 DEFAULT_OPTIONS = dict(
     max_iterations=100, convergence_tolerance=1e-8, dual_inf_tol=1.0,
     constr_viol_tol=1e-4, compl_inf_tol=1e-4, diverging_iterates_tol=1e20,
@@ -796,12 +824,22 @@ class Optimizer:
         converged, iterations (a record per iteration: residual,
         barrier_param, step lengths, line-search trials, inertia
         perturbation, KKT error components, barrier objective), plus
-        the final objective-free summary fields and the wall time."""
+        the final objective-free summary fields and the wall time.
+        Options are amigo's (amigo/algorithm/default_options.py): an
+        unknown name is a ValueError as there; a name of amigo's whose
+        value selects a strategy other than its default algorithm raises
+        NotImplementedError."""
         o = dict(DEFAULT_OPTIONS)
         for k, v in (options or {}).items():
-            if k not in o:
-                raise ValueError("unrecognized option %s" % k)
-            o[k] = v
+            if k in o:
+                o[k] = v
+            elif k in DEFAULT_ALGORITHM_OPTIONS:
+                if k not in DIAGNOSTIC_OPTIONS and v != DEFAULT_ALGORITHM_OPTIONS[k]:
+                    raise NotImplementedError(
+                        "option %s=%r selects a part of amigo's optimizer other than "
+                        "its default algorithm, which is the one restated here" % (k, v))
+            else:
+                raise ValueError("Unrecognized option %s" % k)
         t0 = time.perf_counter()
         ipo = self.ipo
         self.mu = o["initial_barrier_param"]

@@ -211,3 +211,91 @@ def test_generated_model_solves_match(oracle_ref, name):
     dense = problem(name)
     ref_dense = RO.optimize(*dense)
     assert abs(obj(got["x"]) - ref_dense["objective"]) <= 1e-7 * max(1.0, abs(ref_dense["objective"]))
+
+
+@needs_ref
+def test_sellar_multi_component_model(oracle_ref):
+    """The reference's Sellar example: its five components (imported from
+    their reference serialization) share the inputs of the same name, as
+    its Model.link_by_name links them; its bounds, start and optimizer
+    options.  Both drivers run the generated model on the same host core
+    and agree bit for bit."""
+    from oracle import ref_optimizer as RO
+    comps = {c["cls"]: c for c in json.load(open(FIX))["components"]
+             if c["source"].endswith("sellar.py")}
+    names = ["x", "z1", "z2", "y1", "y2"]
+    groups, ncon = [], 0
+    for cls in ("Disp1", "Disp2", "Objective", "Con1", "Con2"):
+        comp = cg.from_amigo(comps[cls]["data"])
+        idx = [names.index(k) for k in comp._inputs]
+        idx += list(range(len(names) + ncon, len(names) + ncon + comp.num_constraints))
+        ncon += comp.num_constraints
+        groups.append(cg.Group(comp, np.array([idx]), name=cls))
+    n = len(names) + ncon
+    mult = np.arange(n) >= len(names)
+    # the example's vectors: lower from a zero vector with x, y1, z1 set to
+    # -inf; upper +inf on the inputs; constraint targets 0
+    lower = np.zeros(n)
+    lower[[0, 1, 3]] = -np.inf
+    upper = np.zeros(n)
+    upper[:len(names)] = np.inf
+    x0 = np.zeros(n)
+    x0[[1, 2, 3, 4]] = 1.0
+    G = cg.GeneratedModel(n, groups, mult, lower, upper, x0=x0)
+    grad = lambda x, a: G.host_derivatives(x, a)[0]
+    hess = lambda x, a: G.host_derivatives(x, a)[1]
+    lag = lambda x, a: G.host_lagrangian(x, a)
+    obj = lambda x: G.host_lagrangian(x * ~G.mult, 1.0)
+    m = types.SimpleNamespace(n=n, mult=mult, lower=lower, upper=upper, x0=x0,
+                              rowp=G.rowp, cols=G.cols, diag_pos=G.diag_pos)
+    opts = {"initial_barrier_param": 0.1, "max_line_search_iterations": 1,
+            "max_iterations": 500, "init_affine_step_multipliers": False}
+    want = RO.optimize(m, grad, hess, lag, obj, options=opts)
+
+    from amigo_b200.optimizer import Optimizer
+    alg = RO.install()
+    P = RO.HostProblem(m, grad, hess, lag)
+    opt = Optimizer(P, RO.HostVector(arr=x0.copy()), RO.HostVector(arr=lower.copy()),
+                    RO.HostVector(arr=upper.copy()), alg.solvers.AmigoSolver(P),
+                    backend_class=RO.InteriorPointOptimizer)
+    got = opt.optimize(dict(opts))
+    assert got["converged"] == want["converged"]
+    assert len(got["iterations"]) == len(want["records"])
+    for a, b in zip(got["iterations"], want["records"]):
+        for k in FIELDS:
+            if b.get(k) is None or isinstance(b.get(k), str):
+                continue
+            assert float(a[k]) == float(b[k]), (a["iteration"], k)
+    assert np.array_equal(np.array(opt.vars.get_solution().arr), want["x"])
+
+
+@needs_ref
+def test_every_amigo_option_name_is_accepted():
+    """Every option of amigo's get_default_options is known here: the
+    restated ones take any value, the others their default (the default
+    algorithm) and raise NotImplementedError otherwise; unknown names are a
+    ValueError, as in amigo."""
+    import importlib
+    from amigo_b200 import optimizer as O
+    from oracle import ref_optimizer as RO
+    RO.install()
+    ref = importlib.import_module("amigo.algorithm.default_options").get_default_options()
+    assert set(ref) == set(O.DEFAULT_OPTIONS) | set(O.DEFAULT_ALGORITHM_OPTIONS)
+    for k, v in O.DEFAULT_ALGORITHM_OPTIONS.items():
+        assert ref[k] == v, k
+    for k, v in O.DEFAULT_OPTIONS.items():
+        assert ref[k] == v, k
+    m, grad, hess, lag, _ = problem("HS6")
+    alg = RO.install()
+    P = RO.HostProblem(m, grad, hess, lag)
+
+    def run(opts):
+        opt = O.Optimizer(P, RO.HostVector(arr=m.x0.copy()), RO.HostVector(arr=m.lower.copy()),
+                          RO.HostVector(arr=m.upper.copy()), alg.solvers.AmigoSolver(P),
+                          backend_class=RO.InteriorPointOptimizer)
+        return opt.optimize(opts)
+    assert run(dict(O.DEFAULT_ALGORITHM_OPTIONS, verbose_barrier=True))["converged"]
+    with pytest.raises(NotImplementedError, match="barrier_strategy"):
+        run({"barrier_strategy": "quality_function"})
+    with pytest.raises(ValueError, match="Unrecognized option"):
+        run({"no_such_option": 1})
