@@ -299,3 +299,84 @@ def test_every_amigo_option_name_is_accepted():
         run({"barrier_strategy": "quality_function"})
     with pytest.raises(ValueError, match="Unrecognized option"):
         run({"no_such_option": 1})
+
+
+@needs_ref
+def test_reference_cart_pole_model(oracle_ref):
+    """The reference's cart-pole trajectory example (its create_cart_model,
+    100 steps): its components imported from their reference serialization
+    and laid out as its links lay them out -- cart instances k = 0..100,
+    trapezoid instance i*100 + k joining state i of carts k and k+1, the
+    objective joining the controls of carts k and k+1, initial and final
+    conditions on carts 0 and 100 -- with its start values and data.  Both
+    drivers agree bit for bit on the generated model."""
+    from oracle import ref_optimizer as RO
+    comps = {c["cls"]: c for c in json.load(open(FIX))["components"]
+             if c["source"].endswith("cart_pole.py")}
+    N = 100
+    cart = cg.from_amigo(comps["CartComponent"]["data"])
+    trap = cg.from_amigo(comps["TrapezoidRule"]["data"])
+    objc = cg.from_amigo(comps["Objective"]["data"])
+    ic = cg.from_amigo(comps["InitialConditions"]["data"])
+    fc = cg.from_amigo(comps["FinalConditions"]["data"])
+    nv = 9                                   # x, q[4], qdot[4] per cart
+    X = lambda k: k * nv
+    Q = lambda k, i: k * nv + 1 + i
+    QD = lambda k, i: k * nv + 5 + i
+    nxt = [nv * (N + 1)]
+
+    def mults(count):
+        a = np.arange(nxt[0], nxt[0] + count)
+        nxt[0] += count
+        return a
+    cart_idx = np.array([[X(k)] + [Q(k, i) for i in range(4)] + [QD(k, i) for i in range(4)]
+                         + list(mults(4)) for k in range(N + 1)])
+    trap_idx = np.array([[Q(k, i), Q(k + 1, i), QD(k, i), QD(k + 1, i)] + list(mults(1))
+                         for i in range(4) for k in range(N)])
+    obj_idx = np.array([[X(k), X(k + 1)] for k in range(N)])
+    ic_idx = np.array([[Q(0, i) for i in range(4)] + list(mults(4))])
+    fc_idx = np.array([[Q(N, i) for i in range(4)] + list(mults(4))])
+    n = nxt[0]
+    data = np.tile([0.5, 1.0, 0.3], (N + 1, 1))       # L, m1, m2
+    groups = [cg.Group(cart, cart_idx, data, name="cart"), cg.Group(trap, trap_idx, name="trap"),
+              cg.Group(objc, obj_idx, name="obj"), cg.Group(ic, ic_idx, name="ic"),
+              cg.Group(fc, fc_idx, name="fc")]
+    mult = np.arange(n) >= nv * (N + 1)
+    lower = np.where(mult, 0.0, -np.inf)
+    upper = np.where(mult, 0.0, np.inf)
+    lower[[X(k) for k in range(N + 1)]] = -50.0
+    upper[[X(k) for k in range(N + 1)]] = 50.0
+    upper[mult] = np.inf
+    x0 = np.zeros(n)
+    x0[[Q(k, 0) for k in range(N + 1)]] = np.linspace(0.0, 2.0, N + 1)
+    x0[[Q(k, 1) for k in range(N + 1)]] = np.linspace(0.0, np.pi, N + 1)
+    x0[[Q(k, 2) for k in range(N + 1)]] = 1.0
+    x0[[Q(k, 3) for k in range(N + 1)]] = 1.0
+    G = cg.GeneratedModel(n, groups, mult, lower, upper, x0=x0)
+    cache = {}
+
+    def deriv(x, a):
+        key = (x.tobytes(), a)
+        if key not in cache:
+            cache.clear()
+            cache[key] = G.host_derivatives(x, a)
+        return cache[key]
+    grad = lambda x, a: deriv(x, a)[0]
+    hess = lambda x, a: deriv(x, a)[1]
+    lag = lambda x, a: G.host_lagrangian(x, a)
+    obj = lambda x: G.host_lagrangian(x * ~G.mult, 1.0)
+    m = types.SimpleNamespace(n=n, mult=mult, lower=lower, upper=upper, x0=x0,
+                              rowp=G.rowp, cols=G.cols, diag_pos=G.diag_pos)
+    want = RO.optimize(m, grad, hess, lag, obj)
+    got = ours(m, grad, hess, lag)
+    assert want["converged"] and got["converged"]
+    assert len(got["iterations"]) == len(want["records"])
+    for a, b in zip(got["iterations"], want["records"]):
+        for k in FIELDS:
+            if b.get(k) is None or isinstance(b.get(k), str):
+                continue
+            assert float(a[k]) == float(b[k]), (a["iteration"], k)
+    assert np.array_equal(got["x"], want["x"])
+    # the swing-up reaches its final conditions
+    xs = got["x"]
+    assert abs(xs[Q(N, 0)] - 2.0) < 1e-6 and abs(xs[Q(N, 1)] - np.pi) < 1e-6
